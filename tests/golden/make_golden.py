@@ -1,0 +1,249 @@
+"""Generate the golden fixtures under tests/golden from the reference implementation (saulpingerman/FastSAR 0.3.1).
+
+Run in a container where the reference's sources are present (default /root/reference, or --ref PATH):
+
+    python tests/golden/make_golden.py [--ref /root/reference]
+
+The reference's modules fastsar/ffbp.py and fastsar/ffbp2.py import JAX at module level but its planner and CPU paths
+use only NumPy, so a stub `jax` package is inserted before the import; its C++ kernels are compiled by its own
+fastsar/_build.py with the system g++ (CXX=/usr/bin/g++, which has libgomp). Nothing here is needed at test time:
+the tests read only the .npz files this writes.
+
+Fixtures:
+  plan_<case>.npz     make_plan / choose_T / collection_arrays of a geometry (integers exact, floats to 1e-12)
+  fir.npz             decimator_fir kernels for a spread of (n_in, D, pass) values
+  kernels.npz         the reference C++ kernels rot_fir_k_cplx, rot_fir_k, fir_p, final_tiles on seeded small inputs
+  image_<case>.npz    ImageFormer(backend='cpu') images (history, image), ExactFormer(cpu) and backproject(cpu, 64x)
+"""
+import argparse
+import os
+import sys
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+
+
+def import_reference(path):
+    os.environ['CXX'] = '/usr/bin/g++'
+    os.environ.setdefault('FASTSAR_CACHE_DIR', '/tmp/fastsar_golden_cache')
+    jax = types.ModuleType('jax')
+    jnp = types.ModuleType('jax.numpy')
+    lax = types.ModuleType('jax.lax')
+
+    class Precision:
+        HIGHEST, HIGH, DEFAULT = 'highest', 'high', None
+    lax.Precision = Precision
+    jax.numpy, jax.lax = jnp, lax
+    jax.jit = lambda f=None, **k: (f if f is not None else (lambda g: g))
+    jax.devices = lambda *a, **k: []
+    sys.modules.update({'jax': jax, 'jax.numpy': jnp, 'jax.lax': lax})
+    sys.path.insert(0, path)
+    import fastsar  # noqa: F401
+    return fastsar
+
+
+def stats(a):
+    """Summary of a large float array: count, sum, sum of squares, a strided sample (fixture size stays small)."""
+    a = np.asarray(a, np.float64).ravel()
+    step = max(1, len(a) // 4096)
+    return np.concatenate([[len(a), a.sum(), (a * a).sum()], a[::step]])
+
+
+def plan_record(ffbp2, col, nx, ny, spx, spy, e1, e2, T, nlev, pmax=0.4, full_limit=30000):
+    plan = ffbp2.make_plan(col, nx, ny, spx, spy, T=T, nlev=nlev, pmax=pmax, e1=e1, e2=e2)
+    rec = dict(ant=col.ant, scal=np.array([col.fmin, col.df, col.K, nx, ny, spx, spy, T, nlev, pmax], np.float64),
+               e1=np.asarray(e1, np.float64), e2=np.asarray(e2, np.float64),
+               top=np.array([plan['T'], plan['Nx'], plan['Ny'], plan['ox'], plan['oy']], np.int64),
+               nlevels=np.array(len(plan['levels'])))
+    for i, l in enumerate(plan['levels']):
+        fk, fp = l['fir_k'], l['fir_p']
+        rec[f'lv{i}_ints'] = np.array([l['sx'], l['sy'], l['C'], l['Dk'], l['Dp'], l['K'], l['P'], l['Ko'], l['Po'],
+                                       fk['L'] if fk else -1, fk['pl'] if fk else -1, fk['pr'] if fk else -1,
+                                       fk['n_out'] if fk else -1, fp['L'] if fp else -1, fp['pl'] if fp else -1,
+                                       fp['pr'] if fp else -1, fp['n_out'] if fp else -1], np.int64)
+        rec[f'lv{i}_f'] = np.array([l['f0'], l['df'], l['pass_k'], l['pass_p'], l['Fk'].args[2], l['Fp'].args[2]])
+        if fk:
+            rec[f'lv{i}_kk'] = np.asarray(fk['kern'])
+        if fp:
+            rec[f'lv{i}_kp'] = np.asarray(fp['kern'])
+        for key in ('cen', 'd', 'ref', 'pidx'):
+            a = np.asarray(l[key], np.float64)
+            rec[f'lv{i}_{key}'] = a if a.size <= full_limit else stats(a)
+    f = plan['final']
+    rec['final_f'] = np.array([f['P'], f['K'], f['f0'], f['df'], f['fc']], np.float64)
+    rec['final_cen'] = f['cen'] if f['cen'].size <= full_limit else stats(f['cen'])
+    fmax = col.fmin + col.K * col.df
+    Tc, err = ffbp2.choose_T(col.ant, fmax, nx, ny, spx, spy, np.asarray(e1, float), np.asarray(e2, float))
+    rec['choose_T'] = np.array([Tc, err])
+    rec['phase_err'] = np.array([ffbp2.final_phase_error(col.ant, fmax, nx, ny, spx, spy, np.asarray(e1, float),
+                                                         np.asarray(e2, float), t) for t in (16, 32)])
+    coll = ffbp2.collection_arrays(plan, col.ant)
+    for i, c in enumerate(coll['levels']):
+        for key in ('u', 'r0', 'c0', 'slope'):
+            if key in c:
+                a = np.asarray(c[key])
+                rec[f'ca{i}_{key}'] = a if a.size <= full_limit else stats(a)
+    rec['caf_u'] = coll['final']['u'] if coll['final']['u'].size <= full_limit else stats(coll['final']['u'])
+    rec['caf_r0'] = coll['final']['r0'] if coll['final']['r0'].size <= full_limit else stats(coll['final']['r0'])
+    return plan, coll, rec
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--ref', default='/root/reference')
+    args = ap.parse_args()
+    fs = import_reference(args.ref)
+    from fastsar import sim, ffbp2, ffbp_cpu, bp
+    from fastsar.api import ImageFormer, _window
+    from fastsar.exact import ExactFormer
+    from fastsar_b200 import sim as mysim
+
+    out = {}
+    # --- plans ------------------------------------------------------------------------------------------------
+    cases = {}
+    c_small = sim.make_collect(res=0.5, scene=60.0, r0=5e3)
+    cases['small2'] = (c_small, 128, 128, 0.5, 0.5, (1.0, 0.0, 0.0), (0.0, 1.0, 0.0), 16, 2)
+    cases['small3'] = (c_small, 128, 128, 0.5, 0.5, (1.0, 0.0, 0.0), (0.0, 1.0, 0.0), 16, 3)
+    c_600 = sim.make_collect(res=0.5, scene=60.0, r0=600e3)
+    cases['orbit3'] = (c_600, 100, 120, 0.5, 0.5, (0.0, 1.0, 0.0), (1.0, 0.0, 0.0), 32, 3)
+    w512 = mysim.workload('spotlight_512')
+    cases['spot512'] = (w512['col'], 512, 512, 0.25, 0.25, w512['e1'], w512['e2'], 32, 3)
+    w12 = mysim.workload('spotlight_12k')
+    cases['spot12k'] = (w12['col'], 12288, 8832, 0.2, 0.2, w12['e1'], w12['e2'], 32, 3)
+    w4 = mysim.workload('spotlight_4k')
+    cases['spot4k'] = (w4['col'], 2048, 2048, 0.25, 0.25, w4['e1'], w4['e2'], 32, 3)
+    # patches of uneven sides from one collection (batched workloads), and a 4-level plan
+    wp = mysim.spotlight(4096, 2048, 9.6e9, 600e6, 500e3, 50.0, 2.0)
+    cases['patch_256x1000'] = (wp, 256, 1000, 0.3, 0.3, (0.0, 1.0, 0.0), (1.0, 0.0, 0.0), 32, 3)
+    cases['patch_1500x700'] = (wp, 1500, 700, 0.3, 0.3, (0.0, 1.0, 0.0), (1.0, 0.0, 0.0), 32, 3)
+    cases['four_levels'] = (c_small, 256, 256, 0.25, 0.25, (1.0, 0.0, 0.0), (0.0, 1.0, 0.0), 16, 4)
+    for name, (col, nx, ny, spx, spy, e1, e2, T, nlev) in cases.items():
+        _, _, rec = plan_record(ffbp2, col, nx, ny, spx, spy, e1, e2, T, nlev)
+        np.savez_compressed(os.path.join(HERE, f'plan_{name}.npz'), **rec)
+        print('plan', name, rec['top'], [tuple(rec[f'lv{i}_ints'][:9]) for i in range(int(rec['nlevels']))])
+    # choose_splits beyond three levels of factors up to 8 (the fallback to larger factors)
+    def splits_or_none(n, T, nl):
+        try:
+            return ffbp2.choose_splits(n, T, nl)
+        except ValueError:
+            return ()                                               # the reference refuses: too few levels
+    sp = [(n, T, nl, splits_or_none(n, T, nl)) for n, T, nl in
+          [(128, 16, 2), (8832, 32, 3), (12288, 32, 3), (100000, 32, 3), (70000, 16, 3), (60000, 16, 3), (300, 32, 1),
+           (33, 32, 2), (5000, 16, 2), (12207, 32, 3), (8808, 32, 3), (1000, 32, 1), (4000, 16, 2)]]
+    np.savez_compressed(os.path.join(HERE, 'splits.npz'),
+                        rows=np.array([[n, T, nl, len(s)] + list(s) + [0] * (3 - len(s)) for n, T, nl, s in sp], np.int64))
+
+    # --- FIR kernels ------------------------------------------------------------------------------------------
+    fir = {}
+    k = 0
+    for n_in, D, pf in [(8192, 3, 0.5), (1647, 8, 0.3), (214, 2, 0.95), (4096, 7, 0.82), (16384, 10, 0.11),
+                        (400, 5, 0.67), (1024, 4, 0.25), (512, 2, 0.42)]:
+        fr, m = ffbp2.decimator_fir(n_in, D, pf)
+        fir[f'k{k}_args'] = np.array([n_in, D, pf])
+        fir[f'k{k}_ints'] = np.array([fr['L'], fr['pl'], fr['pr'], fr['n_out'], m])
+        fir[f'k{k}_kern'] = np.asarray(fr['kern'])
+        k += 1
+    np.savez_compressed(os.path.join(HERE, 'fir.npz'), n=np.array(k), **fir)
+
+    # --- the reference's C++ kernels on seeded inputs ----------------------------------------------------------
+    L = ffbp_cpu.lib()
+    rng = np.random.default_rng(11)
+    kr = {}
+    Np, P, K, Cn, Dk, Ko = 2, 9, 61, 5, 3, 0
+    fr, _ = ffbp2.decimator_fir(K, Dk, 0.6)
+    Ko = fr['n_out']
+    x = (rng.standard_normal((Np, P, K)) + 1j * rng.standard_normal((Np, P, K))).astype(np.complex64)
+    c0 = rng.uniform(-0.5, 0.5, (Np, Cn, P)).astype(np.float32)
+    sl = rng.uniform(-0.02, 0.02, (Np, Cn, P)).astype(np.float32)
+    taps = np.asarray(fr['kern'], np.float32)
+    yre = np.zeros((Np * Cn, P, Ko), np.float32)
+    yim = np.zeros((Np * Cn, P, Ko), np.float32)
+    L.rot_fir_k_cplx(x.view(np.float32), Np, P, K, c0, sl, Cn, taps, fr['L'], fr['pl'], Dk, Ko, (K - 1) / 2.0, yre, yim)
+    kr.update(rk_x=x, rk_c0=c0, rk_sl=sl, rk_taps=taps, rk_ints=np.array([Np, P, K, Cn, fr['L'], fr['pl'], Dk, Ko]),
+              rk_yre=yre.copy(), rk_yim=yim.copy())
+    xre, xim = np.ascontiguousarray(x.real), np.ascontiguousarray(x.imag)
+    L.rot_fir_k(xre, xim, Np, P, K, c0, sl, Cn, taps, fr['L'], fr['pl'], Dk, Ko, (K - 1) / 2.0, yre, yim)
+    kr.update(rk2_yre=yre.copy(), rk2_yim=yim.copy())
+    B, P2, K2, Dp = 3, 77, 13, 4
+    fp, _ = ffbp2.decimator_fir(P2, Dp, 0.5)
+    Po = fp['n_out']
+    a = rng.standard_normal((B, P2, K2)).astype(np.float32)
+    b = rng.standard_normal((B, P2, K2)).astype(np.float32)
+    zre = np.zeros((B, Po, K2), np.float32)
+    zim = np.zeros((B, Po, K2), np.float32)
+    tp = np.asarray(fp['kern'], np.float32)
+    L.fir_p(a, b, B, P2, K2, tp, fp['L'], fp['pl'], Dp, Po, zre, zim)
+    kr.update(fp_a=a, fp_b=b, fp_taps=tp, fp_ints=np.array([B, P2, K2, fp['L'], fp['pl'], Dp, Po]), fp_zre=zre, fp_zim=zim)
+    for T in (16, 32):
+        B, Pf, Qf = 3, 7, 11
+        d = (rng.standard_normal((B, Pf, Qf)) + 1j * rng.standard_normal((B, Pf, Qf))).astype(np.complex64)
+        ux = rng.uniform(-0.9, 0.9, (B, Pf))
+        uy = rng.uniform(-0.9, 0.9, (B, Pf))
+        dlx = (np.arange(T) - (T - 1) / 2.0) * 0.3
+        dly = (np.arange(T) - (T - 1) / 2.0) * 0.45
+        a0, a1, fc2 = 64.1, 0.013, 64.4
+        ucx, ucy = rng.uniform(-0.5, 0.5, B), rng.uniform(-0.5, 0.5, B)
+        rc = rng.uniform(4e3, 6e3, B)
+        ore = np.zeros((B, T, T), np.float32)
+        oim = np.zeros((B, T, T), np.float32)
+        dre, dim = np.ascontiguousarray(d.real), np.ascontiguousarray(d.imag)
+        L.final_tiles(dre, dim, B, Pf, Qf, T, ux, uy, dlx, dly, a0, a1, ucx, ucy, rc, fc2, ore, oim, None, None, None)
+        w0 = rng.uniform(0.5, 1.5, (B, Pf)).astype(np.float32)
+        gx = rng.uniform(-0.01, 0.01, (B, Pf)).astype(np.float32)
+        gyr = rng.uniform(-0.01, 0.01, (B, Pf)).astype(np.float32)
+        ore_w = np.zeros((B, T, T), np.float32)
+        oim_w = np.zeros((B, T, T), np.float32)
+        L.final_tiles(dre, dim, B, Pf, Qf, T, ux, uy, dlx, dly, a0, a1, ucx, ucy, rc, fc2, ore_w, oim_w,
+                      w0.ctypes.data, gx.ctypes.data, gyr.ctypes.data)
+        kr.update({f'ft{T}_d': d, f'ft{T}_ux': ux, f'ft{T}_uy': uy, f'ft{T}_dlx': dlx, f'ft{T}_dly': dly,
+                   f'ft{T}_s': np.array([a0, a1, fc2]), f'ft{T}_ucx': ucx, f'ft{T}_ucy': ucy, f'ft{T}_rc': rc,
+                   f'ft{T}_out': (ore + 1j * oim).astype(np.complex64), f'ft{T}_w': np.stack([w0, gx, gyr]),
+                   f'ft{T}_outw': (ore_w + 1j * oim_w).astype(np.complex64)})
+    np.savez_compressed(os.path.join(HERE, 'kernels.npz'), **kr)
+
+    # --- images -----------------------------------------------------------------------------------------------
+    rng = np.random.default_rng(1)                                 # the scene of fastsar tests/test_ffbp_cpu.py
+    pos = np.stack([rng.uniform(-25, 25, 40), rng.uniform(-25, 25, 40), np.zeros(40)], 1)
+    amp = rng.standard_normal(40) + 1j * rng.standard_normal(40)
+    S = sim.simulate_brute(c_small, pos, amp).astype(np.complex64)
+    rec = dict(S=S, ant=c_small.ant, scal=np.array([c_small.fmin, c_small.df, c_small.K]))
+    for nlev in (2, 3):
+        f = ImageFormer(c_small.ant, c_small.fmin, c_small.df, c_small.K, 128, 128, 0.5, 0.5, backend='cpu', T=16,
+                        levels=nlev)
+        rec[f'ffbp_l{nlev}'] = f(S)
+    f = ImageFormer(c_small.ant, c_small.fmin, c_small.df, c_small.K, 128, 128, 0.5, 0.5, backend='cpu', T=16,
+                    levels=3, window=False)
+    rec['ffbp_l3_nowin'] = f(S)
+    rec['wp'], rec['wk'] = _window(*S.shape)
+    grid = dict(nx=128, ny=128, spx=0.5, spy=0.5, e1=(1.0, 0.0, 0.0), e2=(0.0, 1.0, 0.0))
+    rec['exact_cubic'] = ExactFormer(c_small.ant, c_small.fmin, c_small.df, c_small.K, **grid, backend='cpu')(S)
+    rec['exact_linear'] = ExactFormer(c_small.ant, c_small.fmin, c_small.df, c_small.K, **grid, backend='cpu',
+                                      interp='linear')(S)
+    pts = bp.plane_points(**grid)
+    rec['bp64'] = bp.backproject(S, c_small.ant, c_small.fmin, c_small.df, pts, backend='cpu', upsample=64)
+    np.savez_compressed(os.path.join(HERE, 'image_small.npz'), **rec)
+    print('image_small done')
+
+    # the 512-pulse spotlight at 600 km: 32 unit targets plus clutter and noise (seeded; reference simulate_brute)
+    rng = np.random.default_rng(2024)
+    col = w512['col']
+    pos, amp = mysim.scene(rng, 400, 400, 0.25, 0.25, w512['e1'], w512['e2'], n_points=32, clutter_db=-30.0,
+                           res=(0.6, 0.5), max_clutter=400)
+    S = sim.simulate_brute(col, pos, amp)
+    S = mysim.add_noise(S, 10 ** (-40 / 20.0), rng).astype(np.complex64)
+    f = ImageFormer(col.ant, col.fmin, col.df, col.K, 512, 512, 0.25, 0.25, w512['e1'], w512['e2'], backend='cpu')
+    img = f(S)
+    sub = np.random.default_rng(5).choice(512 * 512, 4096, replace=False)
+    pts = bp.plane_points(512, 512, 0.25, 0.25, w512['e1'], w512['e2']).reshape(-1, 3)[sub]
+    ref64 = bp.backproject(S, col.ant, col.fmin, col.df, pts, backend='cpu', upsample=64)
+    np.savez_compressed(os.path.join(HERE, 'image_spot512.npz'), S=S, ffbp=img, bp64_idx=sub, bp64=ref64,
+                        T=np.array(f.T), err=np.array(f.predicted_error_db))
+    print('image_spot512 done', f.T, f.predicted_error_db)
+
+
+if __name__ == '__main__':
+    main()

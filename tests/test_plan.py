@@ -1,0 +1,143 @@
+"""The planner (fastsar_b200.plan) against the reference planner's own output (tests/golden/plan_*.npz, written by
+tests/golden/make_golden.py from fastsar/ffbp2.py): every integer field bit-exact (tile grid, splits, decimations,
+filter lengths and offsets, sizes), every float field to 1e-12 relative, the filter kernels and the float64
+collection geometry (fastsar tests/test_units.py:90-110 pins decimator_fir the same way)."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from fastsar_b200 import plan as P_
+from fastsar_b200.sim import Collect
+
+from conftest import GOLDEN
+
+CASES = sorted(os.path.basename(p)[5:-4] for p in glob.glob(os.path.join(GOLDEN, 'plan_*.npz')))
+
+
+def _close(a, b, rtol=1e-12, atol=1e-9):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    assert a.shape == b.shape, (a.shape, b.shape)
+    scale = np.abs(b).max() if b.size else 0.0
+    np.testing.assert_allclose(a, b, rtol=rtol, atol=max(atol, rtol * scale))
+
+
+def _stats(a):
+    a = np.asarray(a, np.float64).ravel()
+    step = max(1, len(a) // 4096)
+    return np.concatenate([[len(a), a.sum(), (a * a).sum()], a[::step]])
+
+
+def _check_array(mine, gold):
+    mine = np.asarray(mine, np.float64)
+    if mine.shape == gold.shape:
+        _close(mine, gold)
+    else:                                                    # a large array: its summary
+        s = _stats(mine)
+        assert s[0] == gold[0]
+        _close(s[3:], gold[3:])
+        _close(s[1:3], gold[1:3], rtol=1e-9)
+
+
+def _plan_of(rec):
+    fmin, df, K, nx, ny, spx, spy, T, nlev, pmax = rec['scal']
+    col = Collect(fmin=fmin, df=df, K=int(K), ant=rec['ant'], res=0.5)
+    return col, P_.make_plan(col, int(nx), int(ny), spx, spy, T=int(T), nlev=int(nlev), pmax=pmax, e1=rec['e1'], e2=rec['e2'])
+
+
+@pytest.mark.parametrize('case', CASES)
+def test_plan_matches_reference(golden, case):
+    rec = golden('plan_' + case)
+    col, plan = _plan_of(rec)
+    assert [plan['T'], plan['Nx'], plan['Ny'], plan['ox'], plan['oy']] == rec['top'].tolist()
+    assert len(plan['levels']) == int(rec['nlevels'])
+    for i, l in enumerate(plan['levels']):
+        fk, fp = l['fir_k'], l['fir_p']
+        ints = [l['sx'], l['sy'], l['C'], l['Dk'], l['Dp'], l['K'], l['P'], l['Ko'], l['Po'],
+                fk['L'] if fk else -1, fk['pl'] if fk else -1, fk['pr'] if fk else -1, fk['n_out'] if fk else -1,
+                fp['L'] if fp else -1, fp['pl'] if fp else -1, fp['pr'] if fp else -1, fp['n_out'] if fp else -1]
+        assert ints == rec[f'lv{i}_ints'].tolist(), (case, i)
+        _close([l['f0'], l['df'], l['pass_k'], l['pass_p'], l['dec_k'][2], l['dec_p'][2]], rec[f'lv{i}_f'])
+        if fk:
+            _close(fk['kern'], rec[f'lv{i}_kk'], rtol=1e-13)
+        if fp:
+            _close(fp['kern'], rec[f'lv{i}_kp'], rtol=1e-13)
+        for key in ('cen', 'd', 'ref', 'pidx'):
+            _check_array(l[key], rec[f'lv{i}_{key}'])
+    f = plan['final']
+    _close([f['P'], f['K'], f['f0'], f['df'], f['fc']], rec['final_f'])
+    _check_array(f['cen'], rec['final_cen'])
+
+
+@pytest.mark.parametrize('case', CASES)
+def test_collection_arrays_match_reference(golden, case):
+    rec = golden('plan_' + case)
+    col, plan = _plan_of(rec)
+    coll = P_.collection_arrays(plan, col.ant)
+    for i, c in enumerate(coll['levels']):
+        for key in ('u', 'r0', 'c0', 'slope'):
+            if f'ca{i}_{key}' in rec:
+                g = rec[f'ca{i}_{key}']
+                if key in ('c0', 'slope'):
+                    a = np.asarray(c[key])
+                    assert a.dtype == np.float32
+                    if a.shape == g.shape:
+                        # float32 of float64 phases: equal, or one float32 ulp apart where the wrap or the rounding of
+                        # an ulp-level float64 difference flips
+                        d = np.abs(a.astype(np.float64) - g.astype(np.float64))
+                        assert (d <= 2 * np.spacing(np.abs(g).astype(np.float32)).astype(np.float64) + 1e-12).mean() > 0.999
+                        assert d.max() < 1e-5
+                    else:
+                        s = _stats(a)
+                        assert s[0] == g[0]
+                        np.testing.assert_allclose(s[3:], g[3:], atol=1e-5)
+                else:
+                    _check_array(c[key], g)
+    _check_array(coll['final']['u'], rec['caf_u'])
+    _check_array(coll['final']['r0'], rec['caf_r0'])
+
+
+@pytest.mark.parametrize('case', CASES)
+def test_choose_T_matches_reference(golden, case):
+    rec = golden('plan_' + case)
+    fmin, df, K, nx, ny, spx, spy = rec['scal'][:7]
+    fmax = fmin + K * df
+    T, err = P_.choose_T(rec['ant'], fmax, int(nx), int(ny), spx, spy, rec['e1'], rec['e2'])
+    assert T == int(rec['choose_T'][0])
+    _close(err, rec['choose_T'][1], rtol=1e-9)
+    for t, e in zip((16, 32), rec['phase_err']):
+        _close(P_.final_phase_error(rec['ant'], fmax, int(nx), int(ny), spx, spy, rec['e1'], rec['e2'], t), e, rtol=1e-9)
+
+
+def test_choose_splits_matches_reference(golden):
+    for row in golden('splits')['rows']:
+        n, T, nl, ns = (int(v) for v in row[:4])
+        if ns == 0:
+            with pytest.raises(ValueError, match='cannot split'):
+                P_.choose_splits(n, T, nl)
+        else:
+            assert list(P_.choose_splits(n, T, nl)) == row[4:4 + ns].tolist(), (n, T, nl)
+
+
+def test_decimator_fir_matches_reference(golden):
+    g = golden('fir')
+    for k in range(int(g['n'])):
+        n_in, D, pf = g[f'k{k}_args']
+        fr, m = P_.decimator_fir(int(n_in), int(D), pf)
+        assert [fr['L'], fr['pl'], fr['pr'], fr['n_out'], m] == g[f'k{k}_ints'].tolist()
+        _close(fr['kern'], g[f'k{k}_kern'], rtol=1e-13)
+        assert P_.decimator_shape(int(n_in), int(D), pf) == (fr['n_out'], m)
+
+
+def test_decimator_rows_sum_to_one():
+    """Every input sample's weights over the outputs sum to one (the normalisation the kernel carries)."""
+    fr, m = P_.decimator_fir(300, 4, 0.5)
+    F = np.zeros((300, fr['n_out']))
+    for j in range(fr['n_out']):
+        for r in range(fr['L']):
+            i = 4 * j + r - fr['pl']
+            if 0 <= i < 300:
+                F[i, j] = fr['kern'][r]
+    interior = slice(fr['L'], 300 - fr['L'])
+    np.testing.assert_allclose(F.sum(1)[interior], 1.0, atol=1e-12)
