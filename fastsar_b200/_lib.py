@@ -1,0 +1,111 @@
+"""ctypes binding of the C ABI in include/ffbp_b200.h (the library fastsar_b200/libffbp_b200.so).
+
+There is no fallback: a missing library, or a machine without a CUDA device, raises when a former is built."""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, 'libffbp_b200.so')
+
+FFBP_OK, FFBP_E_ARG, FFBP_E_CUDA, FFBP_E_NOMEM, FFBP_E_WORKSPACE, FFBP_E_UNSUPPORTED = 0, -1, -2, -3, -4, -5
+FFBP_FINAL_FP32, FFBP_FINAL_TC_F16, FFBP_FINAL_TC_BF16X3 = 0, 1, 2
+
+# every symbol include/ffbp_b200.h declares
+EXPORTS = ('ffbp_last_error', 'ffbp_abi_version', 'ffbp_plan_create', 'ffbp_plan_destroy', 'ffbp_plan_workspace_bytes',
+           'ffbp_form', 'ffbp_form_timed', 'ffbp_plan_info', 'ffbp_level', 'ffbp_phases', 'ffbp_final')
+
+_c_int, _c_double, _vp = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+
+
+class LevelDesc(ctypes.Structure):
+    _fields_ = [('sx', _c_int), ('sy', _c_int), ('C', _c_int), ('Dk', _c_int), ('Dp', _c_int), ('K', _c_int),
+                ('P', _c_int), ('Ko', _c_int), ('Po', _c_int),
+                ('h_taps_k', _vp), ('Lk', _c_int), ('plk', _c_int),
+                ('h_taps_p', _vp), ('Lp', _c_int), ('plp', _c_int),
+                ('f0', _c_double), ('df', _c_double),
+                ('h_ant', _vp), ('h_ref', _vp), ('h_cen', _vp), ('h_range', _vp)]
+
+
+class PlanDesc(ctypes.Structure):
+    _fields_ = [('nlev', _c_int), ('levels', ctypes.POINTER(LevelDesc)), ('T', _c_int), ('nx', _c_int), ('ny', _c_int),
+                ('Nx', _c_int), ('Ny', _c_int), ('ox', _c_int), ('oy', _c_int), ('spx', _c_double), ('spy', _c_double),
+                ('e1', _c_double * 3), ('e2', _c_double * 3), ('Pf', _c_int), ('Qf', _c_int),
+                ('f0f', _c_double), ('dff', _c_double), ('fcf', _c_double),
+                ('h_ant_f', _vp), ('h_cen_f', _vp), ('h_first_f', _vp), ('h_wp', _vp), ('h_wk', _vp),
+                ('h_wf', _vp), ('wf_ndim', _c_int), ('final_mode', _c_int)]
+
+
+_LIB = None
+
+
+def load():
+    """The library, loaded once (built first when it is missing or older than its sources and nvcc is present)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    from . import build as _build
+    if _build.stale():
+        try:
+            _build.build()
+        except (OSError, RuntimeError) as e:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(f'fastsar_b200: the CUDA library {LIB_PATH} is not built and could not be built '
+                                   f'({e}); run python -m fastsar_b200.build on a machine with nvcc') from None
+    L = ctypes.CDLL(LIB_PATH)
+    L.ffbp_last_error.argtypes = [ctypes.c_char_p, _c_int]
+    L.ffbp_abi_version.restype = _c_int
+    L.ffbp_plan_create.argtypes = [ctypes.POINTER(PlanDesc), _vp, ctypes.POINTER(_vp)]
+    L.ffbp_plan_destroy.argtypes = [_vp]
+    L.ffbp_plan_workspace_bytes.argtypes = [_vp, ctypes.POINTER(ctypes.c_size_t)]
+    L.ffbp_form.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_size_t, _vp, ctypes.POINTER(_c_int)]
+    L.ffbp_form_timed.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_size_t, _vp, ctypes.POINTER(ctypes.c_float), _c_int]
+    L.ffbp_plan_info.argtypes = [_vp, ctypes.POINTER(_c_int), ctypes.POINTER(_c_int)]
+    L.ffbp_level.argtypes = [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_int, _c_double,
+                             _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp]
+    L.ffbp_phases.argtypes = [_vp, _c_int, _vp, _c_int, _vp, _c_int, _vp, _c_double, _c_double, _c_int, _vp, _vp]
+    L.ffbp_final.argtypes = [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _c_double, _c_double, _c_double,
+                             _c_double, _vp, _vp, _vp, _c_double, _vp, _c_int, _vp, _vp]
+    for name in EXPORTS:
+        getattr(L, name).restype = _c_int
+    _LIB = L
+    return L
+
+
+def last_error():
+    L = load()
+    buf = ctypes.create_string_buffer(2048)
+    L.ffbp_last_error(buf, len(buf))
+    return buf.value.decode(errors='replace')
+
+
+def check(rc, what):
+    """Raise the Python exception for a status code: ValueError for arguments and unsupported shapes, MemoryError
+    for allocations, RuntimeError for CUDA failures."""
+    if rc == FFBP_OK:
+        return
+    msg = f'{what}: {last_error()}'
+    if rc in (FFBP_E_ARG, FFBP_E_UNSUPPORTED, FFBP_E_WORKSPACE):
+        raise ValueError(msg)
+    if rc == FFBP_E_NOMEM or 'out of memory' in msg:
+        raise MemoryError(msg)
+    raise RuntimeError(msg)
+
+
+def ptr(a):
+    """Address of a numpy array's data (None for None)."""
+    return None if a is None else a.ctypes.data
+
+
+def tptr(t):
+    """Address of a torch tensor's data (None for None)."""
+    return None if t is None else t.data_ptr()
+
+
+def c64(a):
+    return np.ascontiguousarray(a, np.float64)
+
+
+def c32(a):
+    return np.ascontiguousarray(a, np.float32)

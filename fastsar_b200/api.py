@@ -1,0 +1,386 @@
+"""The former surface of the reference (fastsar/api.py): ImageFormer and form_image, on the B200.
+
+    former = ImageFormer(ant, fmin, df, K, nx, ny, spx, spy, e1, e2)     # plan + device geometry, once per geometry
+    img = former(S)                                                      # S [P, K] complex -> complex64 [nx, ny]
+    img = form_image(S, ant, fmin, df, nx, ny, spx, spy, e1, e2)         # one call (plans every time)
+
+Same arguments, defaults, conventions and errors as the reference's (fastsar/api.py:312-716): pixel (i, j) sits at
+(i - nx/2) spx e1 + (j - ny/2) spy e2 about the scene reference point; the history follows the CPHD convention
+exp(-j 4 pi f dR / c); a Taylor window (-35 dB, nbar 4) is applied unless window=False; T='auto' picks the largest
+final tile (32 or 16) whose predicted error meets target_db. The planner is fastsar_b200.plan (the reference's,
+restated); the formation runs in the CUDA library (fastsar_b200/libffbp_b200.so) through its C ABI
+(include/ffbp_b200.h), with device memory and streams from PyTorch.
+
+Backends: 'auto' and 'cuda' run on the GPU. There is no CPU, JAX or TPU path in this package; asking for one raises
+ValueError, as the reference does for a backend its machine lacks.
+
+Precision: 'float32' (default): float32 arithmetic everywhere, the final stage on the CUDA cores or, where built,
+as three bfloat16 products on the tensor cores (the reference's float32 CUDA default, fastsar/ffbp_cuda.py:949-953);
+FASTSAR_FINAL=fp32 keeps the CUDA cores. 'float16': the final stage's operands in float16 on the tensor cores with
+float32 accumulation (T = 32).
+"""
+import ctypes
+import os
+import warnings
+
+import numpy as np
+
+from . import _lib
+from . import plan as _plan
+from .sim import Collect
+
+C = 299792458.0
+BACKENDS = ('auto', 'tpu', 'cuda', 'cpu', 'jax', 'metal')
+
+
+def _window(P, K, sll=35.0, nbar=4):
+    """The Taylor windows over pulses and samples, float32 (fastsar/api.py:54-56)."""
+    from scipy.signal.windows import taylor
+    return (taylor(P, nbar=nbar, sll=sll, norm=False).astype(np.float32),
+            taylor(K, nbar=nbar, sll=sll, norm=False).astype(np.float32))
+
+
+def _backend(backend):
+    if backend not in BACKENDS:
+        raise ValueError(f'unknown backend {backend!r}: one of {", ".join(map(repr, BACKENDS))}')
+    if backend not in ('auto', 'cuda'):
+        raise ValueError(f"backend {backend!r} is not part of fastsar_b200, which forms images on the GPU only "
+                         "(backend='auto' or 'cuda')")
+    import torch
+    if not torch.cuda.is_available():
+        raise ValueError("backend 'cuda' needs an NVIDIA GPU; this machine has none")
+    return 'cuda'
+
+
+def _check_history(S, P=None, name='phase history'):
+    """S [P, K] complex with at least 2 pulses and 2 samples (fastsar/api.py:132-152; the scan for NaN and inf runs
+    on the device, in the first level)."""
+    if not hasattr(S, 'ndim'):
+        S = np.asarray(S)
+    if S.ndim != 2:
+        raise ValueError(f'{name} must be 2-D [pulses, samples], got shape {tuple(S.shape)}')
+    kind = S.dtype.kind if isinstance(S, np.ndarray) else ('c' if S.is_complex() else 'f')
+    if kind != 'c':
+        raise TypeError(f'{name} must be complex (complex64 or complex128), got {S.dtype}')
+    if P is not None and S.shape[0] != P:
+        raise ValueError(f'{name} has {S.shape[0]} pulses but there are {P} antenna positions')
+    if S.shape[0] < 2 or S.shape[1] < 2:
+        raise ValueError(f'{name} needs at least 2 pulses and 2 samples, got shape {tuple(S.shape)}')
+    return S
+
+
+def _check_positions(a, name='antenna positions', P=None):
+    """a [P, 3] finite float64 with at least 2 rows (fastsar/api.py:155-166)."""
+    a = np.asarray(a, np.float64)
+    if a.ndim != 2 or a.shape[1] != 3:
+        raise ValueError(f'{name} must be [pulses, 3], got shape {a.shape}')
+    if P is not None and len(a) != P:
+        raise ValueError(f'{name}: {len(a)} rows for {P} pulses')
+    if len(a) < 2:
+        raise ValueError(f'{name}: at least 2 pulses are needed, got {len(a)}')
+    if not np.isfinite(a).all():
+        raise ValueError(f'{name}: non-finite values (NaN or inf)')
+    return a
+
+
+def _check_grid(nx, ny, spx, spy, e1, e2):
+    """Positive integer pixel counts, positive spacings and orthonormal axes (fastsar/api.py:169-183)."""
+    for n, v in (('nx', nx), ('ny', ny)):
+        if np.ndim(v) != 0 or not np.isfinite(v) or v < 1 or int(v) != v:
+            raise ValueError(f'{n} must be a positive integer, got {v!r}')
+    for n, v in (('spx', spx), ('spy', spy)):
+        if not np.isfinite(v) or v <= 0:
+            raise ValueError(f'{n} must be a positive spacing in meters, got {v!r}')
+    e1, e2 = np.asarray(e1, np.float64), np.asarray(e2, np.float64)
+    if e1.shape != (3,) or e2.shape != (3,):
+        raise ValueError(f'e1 and e2 must be 3-vectors, got shapes {e1.shape} and {e2.shape}')
+    if abs(e1 @ e1 - 1) > 1e-6 or abs(e2 @ e2 - 1) > 1e-6 or abs(e1 @ e2) > 1e-6:
+        raise ValueError(f'e1 and e2 must be orthonormal (unit length, perpendicular), got {e1.tolist()} and {e2.tolist()}')
+    return int(nx), int(ny), e1, e2
+
+
+def _final_mode(precision):
+    if precision == 'float16':
+        return _lib.FFBP_FINAL_TC_F16
+    choice = os.environ.get('FASTSAR_FINAL', 'fp32').strip().lower() or 'fp32'
+    if choice not in ('fp32', 'tc3'):
+        raise ValueError(f"FASTSAR_FINAL must be 'fp32' or 'tc3', got {choice!r}")
+    return _lib.FFBP_FINAL_TC_BF16X3 if choice == 'tc3' else _lib.FFBP_FINAL_FP32
+
+
+class DevicePlan:
+    """A plan of fastsar_b200.plan uploaded through ffbp_plan_create: the device-resident filters, windows, child
+    phases and final-stage geometry, and the workspace of a form call. Owns the library's plan handle."""
+
+    def __init__(self, plan, wp=None, wk=None, wf=None, ref=None, final_mode=_lib.FFBP_FINAL_FP32, device=None):
+        import torch
+        L = _lib.load()
+        self.plan = plan
+        self.device = torch.device('cuda', torch.cuda.current_device() if device is None else device)
+        keep = []                                   # host arrays the descriptors point to, alive until the call returns
+
+        def k64(a):
+            a = _lib.c64(a)
+            keep.append(a)
+            return a.ctypes.data
+
+        def k32(a):
+            a = _lib.c32(a)
+            keep.append(a)
+            return a.ctypes.data
+
+        lvs = (_lib.LevelDesc * len(plan['levels']))()
+        for i, lv in enumerate(plan['levels']):
+            d = lvs[i]
+            d.sx, d.sy, d.C, d.Dk, d.Dp = lv['sx'], lv['sy'], lv['C'], lv['Dk'], lv['Dp']
+            d.K, d.P, d.Ko, d.Po = lv['K'], lv['P'], lv['Ko'], lv['Po']
+            if lv['fir_k'] is not None:
+                d.h_taps_k, d.Lk, d.plk = k32(lv['fir_k']['kern']), lv['fir_k']['L'], lv['fir_k']['pl']
+            if lv['fir_p'] is not None:
+                d.h_taps_p, d.Lp, d.plp = k32(lv['fir_p']['kern']), lv['fir_p']['L'], lv['fir_p']['pl']
+            d.f0, d.df = lv['f0'], lv['df']
+            d.h_ant, d.h_ref, d.h_cen = k64(lv['ant']), k64(lv['ref']), k64(lv['cen'])
+            if i == 0 and ref is not None:
+                d.h_range = k64(ref)
+        fin = plan['final']
+        pd = _lib.PlanDesc()
+        pd.nlev, pd.levels = len(plan['levels']), ctypes.cast(lvs, ctypes.POINTER(_lib.LevelDesc))
+        pd.T, pd.nx, pd.ny, pd.Nx, pd.Ny, pd.ox, pd.oy = plan['T'], plan['nx'], plan['ny'], plan['Nx'], plan['Ny'], plan['ox'], plan['oy']
+        pd.spx, pd.spy = plan['spx'], plan['spy']
+        pd.e1[:] = list(map(float, plan['e1']))
+        pd.e2[:] = list(map(float, plan['e2']))
+        pd.Pf, pd.Qf, pd.f0f, pd.dff, pd.fcf = fin['P'], fin['K'], fin['f0'], fin['df'], fin['fc']
+        pd.h_ant_f, pd.h_cen_f = k64(fin['ant']), k64(fin['cen'])
+        first = np.ascontiguousarray(fin['first'], np.int32)
+        keep.append(first)
+        pd.h_first_f = first.ctypes.data
+        if wp is not None:
+            pd.h_wp, pd.h_wk = k32(wp), k32(wk)
+        if wf is not None:
+            pd.h_wf, pd.wf_ndim = k32(wf), int(wf.ndim)
+        pd.final_mode = final_mode
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            stream = torch.cuda.current_stream(self.device)
+            _lib.check(L.ffbp_plan_create(ctypes.byref(pd), ctypes.c_void_p(stream.cuda_stream), ctypes.byref(h)),
+                       'ffbp_plan_create')
+        del keep
+        self.handle = h
+        n = ctypes.c_size_t()
+        _lib.check(L.ffbp_plan_workspace_bytes(h, ctypes.byref(n)), 'ffbp_plan_workspace_bytes')
+        self.ws_bytes = int(n.value)
+        self._ws = None
+
+    def workspace(self):
+        import torch
+        if self._ws is None:
+            self._ws = torch.empty(self.ws_bytes + 256, dtype=torch.uint8, device=self.device)
+        off = (-self._ws.data_ptr()) % 256
+        return self._ws.data_ptr() + off
+
+    def release_workspace(self):
+        self._ws = None
+
+    def form(self, S_dev, img_dev, stream=None, check=True):
+        """S_dev [P, K] complex64 torch tensor on the device -> img_dev [nx, ny] complex64 (written). check: read back
+        the first non-finite pulse (a wait for the stream) and raise ValueError naming it."""
+        import torch
+        L = _lib.load()
+        stream = torch.cuda.current_stream(self.device) if stream is None else stream
+        bad = ctypes.c_int(-1)
+        _lib.check(L.ffbp_form(self.handle, ctypes.c_void_p(S_dev.data_ptr()), ctypes.c_void_p(img_dev.data_ptr()),
+                               ctypes.c_void_p(self.workspace()), ctypes.c_size_t(self.ws_bytes),
+                               ctypes.c_void_p(stream.cuda_stream), ctypes.byref(bad) if check else None), 'ffbp_form')
+        if check and bad.value >= 0:
+            raise ValueError(f'phase history has non-finite samples (NaN or inf), the first in pulse {bad.value}; '
+                             'zero them (S[~np.isfinite(S)] = 0) or drop the pulses')
+        return img_dev
+
+    def form_timed(self, S_dev, img_dev, stream=None):
+        """form with the device time (ms) of each launch: [level 0, ..., level nlev-1, final] (waits for the stream)."""
+        import torch
+        L = _lib.load()
+        stream = torch.cuda.current_stream(self.device) if stream is None else stream
+        n = len(self.plan['levels']) + 1
+        ms = (ctypes.c_float * n)()
+        _lib.check(L.ffbp_form_timed(self.handle, ctypes.c_void_p(S_dev.data_ptr()), ctypes.c_void_p(img_dev.data_ptr()),
+                                     ctypes.c_void_p(self.workspace()), ctypes.c_size_t(self.ws_bytes),
+                                     ctypes.c_void_p(stream.cuda_stream), ms, n), 'ffbp_form_timed')
+        return list(ms)
+
+    def launches(self):
+        """Kernels one form call launches."""
+        L = _lib.load()
+        nl, nk = ctypes.c_int(), ctypes.c_int()
+        _lib.check(L.ffbp_plan_info(self.handle, ctypes.byref(nl), ctypes.byref(nk)), 'ffbp_plan_info')
+        return int(nk.value)
+
+    def __del__(self):
+        h = getattr(self, 'handle', None)
+        if h is not None and h.value:
+            try:
+                _lib.load().ffbp_plan_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
+
+
+class ImageFormer:
+    """Factorized backprojection set up once for a collection geometry and output grid, then called on phase
+    histories (fastsar/api.py:312-677): former = ImageFormer(ant, fmin, df, K, nx, ny, spx, spy, e1, e2);
+    img = former(S). Building plans the tiles and filters and computes the float64 geometry on the device; each call
+    performs only the image formation. aperture_weight(points [m, 3], pulses [n]) -> W [n, m] applies a per-pixel
+    weight of pulses in the final stage (final_weights); ref [P] is the one-way range each pulse is referenced to
+    when it is not |ant|. One former must not be called from two threads at once."""
+
+    def __init__(self, ant, fmin, df, K, nx, ny, spx, spy, e1=(1.0, 0.0, 0.0), e2=(0.0, 1.0, 0.0), *, backend='auto',
+                 precision='float32', window=True, T='auto', levels=None, pmax=0.4, target_db=-40.0, aperture_weight=None,
+                 ref=None, range_gate='auto', padded=None):
+        self.ant = _check_positions(ant)
+        self.P, self.K = self.ant.shape[0], int(K)
+        if self.K < 2:
+            raise ValueError(f'K must be at least 2 frequency samples, got {K}')
+        if not (np.isfinite(fmin) and np.isfinite(df) and fmin > 0 and df > 0):
+            raise ValueError(f'fmin and df must be positive frequencies in Hz, got {fmin!r} and {df!r}')
+        nx, ny, e1, e2 = _check_grid(nx, ny, spx, spy, e1, e2)
+        self.backend = _backend(backend)
+        if precision not in ('float32', 'float16'):
+            raise ValueError("cuda precision: 'float32' or 'float16'")
+        self.precision = precision
+        self.window = window
+        self.nx, self.ny = nx, ny
+        self.predicted_error_db = None
+        fmax = float(fmin) + self.K * float(df)
+        if T == 'auto':
+            if precision == 'float16':
+                T, err = 32, _plan.final_phase_error(self.ant, fmax, nx, ny, spx, spy, e1, e2, 32)
+                if err > target_db:
+                    warnings.warn(f'cuda float16 needs T=32, predicted error {err:.1f} dB misses target {target_db:.1f} dB; '
+                                  "use precision='float32' for this geometry")
+            else:
+                T, err = _plan.choose_T(self.ant, fmax, nx, ny, spx, spy, e1, e2, target_db)
+                if err > target_db:
+                    warnings.warn(f'predicted error {err:.1f} dB at T={T} misses target {target_db:.1f} dB '
+                                  '(short range for this pixel size)')
+            self.predicted_error_db = float(err)
+        if T not in (16, 32):
+            raise ValueError(f'the final stage supports T=16 or T=32, not {T}')
+        if precision == 'float16' and T != 32:
+            raise ValueError('cuda float16 uses the tensor-core final stage, which is built for T=32')
+        self.T = T
+        if ref is not None and np.shape(ref) != (self.P,):
+            raise ValueError(f'ref must hold one range per pulse ({self.P}), got shape {np.shape(ref)}')
+        if ref is not None and not np.all(np.isfinite(ref)):
+            raise ValueError('ref has non-finite values')
+        if range_gate not in ('auto', True, False):
+            raise ValueError(f"range_gate must be 'auto', True or False, got {range_gate!r}")
+        if padded is not None and (aperture_weight is None or levels is None or len(padded[2]) != levels
+                                   or not 0 <= padded[0] <= self.P - padded[1]):
+            raise ValueError('padded=(first, count, pulse) goes with an aperture_weight, the levels of the plan that '
+                             f'pulse is from and an aperture within the {self.P} pulses, got {padded!r}')
+        col = Collect(fmin=float(fmin), df=float(df), K=self.K, ant=self.ant, res=0.5)
+        nlev = 3 if levels is None else levels
+        while True:
+            try:
+                plan = _plan.make_plan(col, nx, ny, spx, spy, T=T, nlev=nlev, pmax=pmax, e1=e1, e2=e2,
+                                       pulse=padded and padded[2])
+                break
+            except ValueError as e:
+                if levels is not None or 'cannot split' not in str(e) or nlev >= 8:
+                    raise
+                nlev += 1
+        self.levels = nlev
+        self._plan = plan
+        self.range_gate = None
+        if range_gate is True:
+            raise ValueError('range_gate=True: the range gate is not part of this version; form with range_gate=False')
+        lk = plan['levels'][0]['fir_k']['L'] if plan['levels'][0]['fir_k'] else 1
+        if lk > 256:
+            raise ValueError(f'the first level\'s frequency filter has {lk} taps (range decimation '
+                             f"{plan['levels'][0]['Dk']}: an image narrow in range from a wide-band collection), more "
+                             'than the level kernel holds (256); the range gate that shortens it is not part of this '
+                             'version: form a wider image or several')
+        wf = None
+        if aperture_weight is not None:
+            wspan = dict(P=self.P) if padded is None else dict(P=int(padded[1]), first=int(padded[0]))
+            wf = _plan.final_weights(plan, aperture_weight, grad=True, **wspan)
+            G = plan['levels'][0]['C']
+            w0 = wf[0].reshape(G, -1)
+            big = np.abs(w0) > 1e-6 * np.maximum(np.abs(w0).max(1, keepdims=True), 1e-30)
+            gyr = np.where(big, wf[2].reshape(G, -1) / np.where(w0 == 0, 1, w0), 0.0).astype(np.float32)
+            wf = np.stack([wf[0], wf[1], gyr.reshape(wf[0].shape)]).astype(np.float32)
+        wp = wk = None
+        if window:
+            self.wp, self.wk = wp, wk = _window(self.P, self.K)
+        self._dev = DevicePlan(plan, wp, wk, wf, None if ref is None else np.asarray(ref, np.float64),
+                               _final_mode(precision))
+        self._S = None
+        self._img = None
+
+    # ------------------------------------------------------------------------------------------------ calls
+    def memory(self):
+        """What a call needs on the device and what is free: dict(backend, needed, available, full_speed, parts)."""
+        import torch
+        free, _ = torch.cuda.mem_get_info(self._dev.device)
+        parts = dict(history=self.P * self.K * 8, workspace=self._dev.ws_bytes, image=self.nx * self.ny * 8)
+        need = float(sum(parts.values()))
+        return dict(backend=self.backend, needed=need, available=float(free), full_speed=need <= free, parts=parts)
+
+    def stage(self, S):
+        """The work of a call that precedes formation, done ahead of it; former(former.stage(S)) equals former(S).
+        Here: S checked and uploaded to the device (a torch tensor)."""
+        return self._upload(S)
+
+    def _upload(self, S):
+        import torch
+        if isinstance(S, torch.Tensor):
+            if tuple(S.shape) != (self.P, self.K):
+                raise ValueError(f'phase history must be {(self.P, self.K)}, got {tuple(S.shape)}')
+            if not S.is_complex():
+                raise TypeError(f'phase history must be complex (complex64 or complex128), got {S.dtype}')
+            return S.to(device=self._dev.device, dtype=torch.complex64).contiguous()
+        S = _check_history(np.asarray(S), self.P)
+        if S.shape != (self.P, self.K):
+            raise ValueError(f'phase history must be {(self.P, self.K)}, got {S.shape}')
+        S = np.ascontiguousarray(S, np.complex64)
+        if self._S is None:
+            self._S = torch.empty((self.P, self.K), dtype=torch.complex64, device=self._dev.device)
+        self._S.copy_(torch.from_numpy(S), non_blocking=False)
+        return self._S
+
+    def form_device(self, S_dev, out=None, check=True):
+        """S_dev [P, K] complex64 on the device -> the image [nx, ny] complex64 on the device (torch)."""
+        import torch
+        if out is None:
+            out = torch.empty((self.nx, self.ny), dtype=torch.complex64, device=self._dev.device)
+        return self._dev.form(S_dev, out, check=check)
+
+    def __call__(self, S):
+        """S [P, K] complex phase history (numpy, or a torch tensor) -> complex64 image [nx, ny] (numpy)."""
+        Sd = self._upload(S)
+        img = self.form_device(Sd)
+        return img.cpu().numpy()
+
+
+def form_image(S, ant, fmin, df, nx, ny, spx, spy, e1=(1.0, 0.0, 0.0), e2=(0.0, 1.0, 0.0), *, algorithm='ffbp',
+               backend='auto', precision='float32', window=True, T='auto', levels=None, pmax=0.4, pfa_guard=300.0,
+               pfa_support='union', target_db=-40.0, ref=None, interp=None, upsample=None, center=None,
+               range_gate='auto'):
+    """The complex image [nx, ny] (complex64) in one call (fastsar/api.py:680-716): algorithm='ffbp' builds an
+    ImageFormer, 'bp' an ExactFormer; 'pfa' (polar format) is not part of this package."""
+    if algorithm not in ('ffbp', 'pfa', 'bp'):
+        raise ValueError("algorithm must be 'ffbp', 'pfa' or 'bp'")
+    if algorithm != 'bp':
+        for n, v in (('interp', interp), ('upsample', upsample), ('center', center)):
+            if v is not None:
+                raise ValueError(f"{n} applies to exact backprojection (algorithm='bp'), not to algorithm={algorithm!r}")
+    if algorithm == 'pfa':
+        raise ValueError("algorithm='pfa' (polar format) is not part of fastsar_b200; use 'ffbp' or 'bp'")
+    S = _check_history(np.asarray(S), len(_check_positions(ant)))
+    if algorithm == 'bp':
+        from .exact import ExactFormer
+        return ExactFormer(ant, fmin, df, S.shape[1], nx, ny, spx, spy, e1, e2, backend=backend, window=window,
+                           interp='cubic' if interp is None else interp, upsample=upsample, ref=ref, center=center)(S)
+    return ImageFormer(ant, fmin, df, S.shape[1], nx, ny, spx, spy, e1, e2, backend=backend, precision=precision,
+                       window=window, T=T, levels=levels, pmax=pmax, target_db=target_db, ref=ref,
+                       range_gate=range_gate)(S)

@@ -1,0 +1,368 @@
+// The C ABI of include/ffbp_b200.h: plan objects, the form call and the stage entry points.
+//
+// A plan keeps, in device memory, everything of the reference's make_ffbp_cuda set-up (fastsar/ffbp_cuda.py:889-962)
+// that depends on the geometry alone: the filters, the windows, every level's child phases (computed here in
+// float64, where the reference computes the first two levels on its host, fastsar/ffbp2.py:313-342, and the rest
+// per call, fastsar/ffbp_cuda.py:1016) and the final-stage geometry (computed per call in the reference,
+// fastsar/ffbp_cuda.py:964-975). A form call is then one launch per level and one for the final stage, all on the
+// caller's stream, over the caller's workspace: the B200 holds a whole 16,384 x 8,192 history and every level's
+// intermediate at once, so the reference's first-level groups and batches (fastsar/ffbp_cuda.py:1154-1198) are not
+// needed for the workloads of record and the launches cover all children of a level.
+#include <climits>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ffbp_b200.h"
+#include "common.cuh"
+#include "kernels.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what)
+{
+    return fail(FFBP_E_CUDA, "%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+struct DevLevel {
+    int C, Dk, Dp, K, P, Ko, Po, Lk, plk, Lp, plp, Np;
+    float *tk = nullptr, *tp = nullptr;
+    float2 *phase = nullptr;
+    double kc;
+};
+
+size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
+
+}  // namespace
+
+struct ffbp_plan {
+    int nlev, T, nx, ny, Nx, Ny, ox, oy, Pf, Qf, ntiles, final_mode;
+    double spx, spy, a0, a1, fc2;
+    std::vector<DevLevel> lv;
+    float *wp = nullptr, *wk = nullptr, *wf = nullptr;
+    double *ux = nullptr, *uy = nullptr, *ucx = nullptr, *ucy = nullptr, *rc = nullptr;
+    int2 *first = nullptr;
+    size_t bufA = 0, bufB = 0;
+    std::vector<void *> owned;
+
+    template <class T_>
+    cudaError_t alloc(T_ **p, size_t count)
+    {
+        void *q = nullptr;
+        cudaError_t e = cudaMalloc(&q, count * sizeof(T_) + 16);
+        if (e == cudaSuccess) {
+            owned.push_back(q);
+            *p = static_cast<T_ *>(q);
+        }
+        return e;
+    }
+    ~ffbp_plan()
+    {
+        for (void *q : owned) cudaFree(q);
+    }
+};
+
+extern "C" {
+
+int ffbp_last_error(char *buf, int n)
+{
+    if (buf && n > 0) {
+        strncpy(buf, g_err.c_str(), (size_t)n - 1);
+        buf[n - 1] = 0;
+    }
+    return (int)g_err.size();
+}
+
+int ffbp_abi_version(void) { return FFBP_B200_ABI_VERSION; }
+
+int ffbp_plan_destroy(ffbp_plan *plan)
+{
+    delete plan;
+    return FFBP_OK;
+}
+
+int ffbp_plan_create(const ffbp_plan_desc *d, void *stream_, ffbp_plan **out)
+{
+    if (!d || !out) return fail(FFBP_E_ARG, "ffbp_plan_create: null argument");
+    *out = nullptr;
+    cudaStream_t s = static_cast<cudaStream_t>(stream_);
+    if (d->nlev < 1 || !d->levels) return fail(FFBP_E_ARG, "plan needs at least one level, got %d", d->nlev);
+    if (d->T != 16 && d->T != 32) return fail(FFBP_E_ARG, "final tile size T must be 16 or 32, got %d", d->T);
+    if (d->final_mode != FFBP_FINAL_FP32 && d->final_mode != FFBP_FINAL_TC_F16 && d->final_mode != FFBP_FINAL_TC_BF16X3)
+        return fail(FFBP_E_ARG, "unknown final_mode %d", d->final_mode);
+    if (d->nx < 1 || d->ny < 1 || d->Nx < d->nx || d->Ny < d->ny || d->ox < 0 || d->oy < 0)
+        return fail(FFBP_E_ARG, "bad grid: nx %d ny %d Nx %d Ny %d ox %d oy %d", d->nx, d->ny, d->Nx, d->Ny, d->ox, d->oy);
+    if (!d->h_ant_f || !d->h_cen_f || !d->h_first_f) return fail(FFBP_E_ARG, "final-stage geometry missing");
+    ffbp_plan *p = new ffbp_plan();
+    p->nlev = d->nlev; p->T = d->T; p->nx = d->nx; p->ny = d->ny; p->Nx = d->Nx; p->Ny = d->Ny;
+    p->ox = d->ox; p->oy = d->oy; p->Pf = d->Pf; p->Qf = d->Qf; p->final_mode = d->final_mode;
+    p->spx = d->spx; p->spy = d->spy;
+    p->a0 = 2.0 * d->f0f / ffbp::C_LIGHT;
+    p->a1 = 2.0 * d->dff / ffbp::C_LIGHT;
+    p->fc2 = 2.0 * d->fcf / ffbp::C_LIGHT;
+    cudaError_t e = cudaSuccess;
+    std::vector<void *> temp;
+    auto cleanup = [&](int rc) {
+        for (void *q : temp) cudaFree(q);
+        if (rc != FFBP_OK) delete p;
+        return rc;
+    };
+    auto upload = [&](const void *h, size_t bytes, void **dst, bool keep) -> cudaError_t {
+        void *q = nullptr;
+        cudaError_t r = cudaMalloc(&q, bytes + 16);
+        if (r != cudaSuccess) return r;
+        (keep ? p->owned : temp).push_back(q);
+        *dst = q;
+        return cudaMemcpyAsync(q, h, bytes, cudaMemcpyHostToDevice, s);
+    };
+    int B = 1;                                            // parents of the current level
+    for (int l = 0; l < d->nlev; ++l) {
+        const ffbp_level_desc &L = d->levels[l];
+        if (L.C != L.sx * L.sy || L.C < 1) return cleanup(fail(FFBP_E_ARG, "level %d: C %d != sx %d * sy %d", l, L.C, L.sx, L.sy));
+        if (L.Dk < 1 || L.Dp < 1 || L.K < 1 || L.P < 1 || L.Ko < 1 || L.Po < 1)
+            return cleanup(fail(FFBP_E_ARG, "level %d: non-positive size", l));
+        if ((L.Dk > 1 && (!L.h_taps_k || L.Lk < 1)) || (L.Dp > 1 && (!L.h_taps_p || L.Lp < 1)))
+            return cleanup(fail(FFBP_E_ARG, "level %d: decimating axis without taps", l));
+        if (L.Dk == 1 && L.Ko != L.K) return cleanup(fail(FFBP_E_ARG, "level %d: Dk 1 needs Ko == K", l));
+        if (L.Dp == 1 && L.Po != L.P) return cleanup(fail(FFBP_E_ARG, "level %d: Dp 1 needs Po == P", l));
+        if (l > 0) {
+            const ffbp_level_desc &Q = d->levels[l - 1];
+            if (L.K != Q.Ko || L.P != Q.Po) return cleanup(fail(FFBP_E_ARG, "level %d: input %dx%d != previous output %dx%d", l, L.P, L.K, Q.Po, Q.Ko));
+        }
+        if (!L.h_ant || !L.h_ref || !L.h_cen) return cleanup(fail(FFBP_E_ARG, "level %d: geometry missing", l));
+        DevLevel v;
+        v.C = L.C; v.Dk = L.Dk; v.Dp = L.Dp; v.K = L.K; v.P = L.P; v.Ko = L.Ko; v.Po = L.Po;
+        v.Lk = L.Dk > 1 ? L.Lk : 1; v.plk = L.Dk > 1 ? L.plk : 0;
+        v.Lp = L.Dp > 1 ? L.Lp : 1; v.plp = L.Dp > 1 ? L.plp : 0;
+        v.Np = B;
+        v.kc = (L.K - 1) / 2.0;
+        void *q;
+        if (L.Dk > 1) {
+            if ((e = upload(L.h_taps_k, sizeof(float) * L.Lk, &q, true)) != cudaSuccess) return cleanup(cuda_fail(e, "upload taps"));
+            v.tk = (float *)q;
+        }
+        if (L.Dp > 1) {
+            if ((e = upload(L.h_taps_p, sizeof(float) * L.Lp, &q, true)) != cudaSuccess) return cleanup(cuda_fail(e, "upload taps"));
+            v.tp = (float *)q;
+        }
+        if ((e = p->alloc(&v.phase, (size_t)B * L.C * L.P)) != cudaSuccess) return cleanup(cuda_fail(e, "allocate phases"));
+        // geometry to the device (temporary), then the phases in float64
+        void *dant, *dref, *dcen, *drange = nullptr;
+        const bool cancel_free = l >= 2;                  // the reference's host levels take the plain difference
+        if ((e = upload(L.h_ant, sizeof(double) * 3 * L.P, &dant, false)) != cudaSuccess) return cleanup(cuda_fail(e, "upload antenna"));
+        if ((e = upload(L.h_ref, sizeof(double) * 3 * B, &dref, false)) != cudaSuccess) return cleanup(cuda_fail(e, "upload refs"));
+        if (cancel_free) {
+            // the children's offsets from their parent's reference, those of the first parent (fastsar/ffbp2.py:239 d)
+            std::vector<double> off(3 * (size_t)L.C);
+            for (int c = 0; c < L.C; ++c)
+                for (int k = 0; k < 3; ++k) off[3 * c + k] = L.h_cen[3 * c + k] - L.h_ref[k];
+            if ((e = upload(off.data(), sizeof(double) * off.size(), &dcen, false)) != cudaSuccess) return cleanup(cuda_fail(e, "upload offsets"));
+            if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cleanup(cuda_fail(e, "upload"));
+        } else {
+            if ((e = upload(L.h_cen, sizeof(double) * 3 * (size_t)B * L.C, &dcen, false)) != cudaSuccess) return cleanup(cuda_fail(e, "upload centres"));
+        }
+        if (l == 0 && L.h_range) {
+            if ((e = upload(L.h_range, sizeof(double) * L.P, &drange, false)) != cudaSuccess) return cleanup(cuda_fail(e, "upload ranges"));
+        }
+        const double k0c = 2.0 * (L.f0 + v.kc * L.df) / ffbp::C_LIGHT;
+        const double k1 = 2.0 * L.df / ffbp::C_LIGHT;
+        e = ffbp::launch_phases((const double *)dant, L.P, (const double *)dref, B, (const double *)dcen, L.C,
+                                (const double *)drange, k0c, k1, cancel_free ? 1 : 0, v.phase, s);
+        if (e != cudaSuccess) return cleanup(cuda_fail(e, "phases kernel"));
+        const size_t outn = (size_t)B * L.C * L.Po * L.Ko;
+        if (l % 2 == 0) p->bufA = std::max(p->bufA, outn); else p->bufB = std::max(p->bufB, outn);
+        p->lv.push_back(v);
+        B *= L.C;
+    }
+    p->ntiles = B;
+    const ffbp_level_desc &last = d->levels[d->nlev - 1];
+    if (p->Pf != last.Po || p->Qf != last.Ko) return cleanup(fail(FFBP_E_ARG, "final stage %dx%d != last level output %dx%d", p->Pf, p->Qf, last.Po, last.Ko));
+    if ((long)B * d->T * d->T != (long)d->Nx * d->Ny) return cleanup(fail(FFBP_E_ARG, "tiles %d of %d^2 do not cover %dx%d", B, d->T, d->Nx, d->Ny));
+    void *q;
+    if (d->h_wp) {
+        if ((e = upload(d->h_wp, sizeof(float) * d->levels[0].P, &q, true)) != cudaSuccess) return cleanup(cuda_fail(e, "upload window"));
+        p->wp = (float *)q;
+    }
+    if (d->h_wk) {
+        if ((e = upload(d->h_wk, sizeof(float) * d->levels[0].K, &q, true)) != cudaSuccess) return cleanup(cuda_fail(e, "upload window"));
+        p->wk = (float *)q;
+    }
+    if (d->h_wf) {
+        if (d->wf_ndim != 3) return cleanup(fail(FFBP_E_UNSUPPORTED, "aperture weights: pass the [3, ntiles, Pf] form (weight and gradients)"));
+        if ((e = upload(d->h_wf, sizeof(float) * 3 * (size_t)B * d->Pf, &q, true)) != cudaSuccess) return cleanup(cuda_fail(e, "upload weights"));
+        p->wf = (float *)q;
+    }
+    if ((e = upload(d->h_first_f, sizeof(int) * 2 * (size_t)B, &q, true)) != cudaSuccess) return cleanup(cuda_fail(e, "upload tile origins"));
+    p->first = (int2 *)q;
+    void *dantf, *dcenf;
+    if ((e = upload(d->h_ant_f, sizeof(double) * 3 * d->Pf, &dantf, false)) != cudaSuccess) return cleanup(cuda_fail(e, "upload final antenna"));
+    if ((e = upload(d->h_cen_f, sizeof(double) * 3 * (size_t)B, &dcenf, false)) != cudaSuccess) return cleanup(cuda_fail(e, "upload tile centres"));
+    if ((e = p->alloc(&p->ux, (size_t)B * d->Pf)) != cudaSuccess || (e = p->alloc(&p->uy, (size_t)B * d->Pf)) != cudaSuccess ||
+        (e = p->alloc(&p->ucx, (size_t)B)) != cudaSuccess || (e = p->alloc(&p->ucy, (size_t)B)) != cudaSuccess ||
+        (e = p->alloc(&p->rc, (size_t)B)) != cudaSuccess)
+        return cleanup(cuda_fail(e, "allocate final geometry"));
+    e = ffbp::launch_final_geom((const double *)dantf, d->Pf, (const double *)dcenf, B, d->e1, d->e2, p->ux, p->uy,
+                                p->ucx, p->ucy, p->rc, s);
+    if (e != cudaSuccess) return cleanup(cuda_fail(e, "final geometry kernel"));
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cleanup(cuda_fail(e, "plan set-up"));
+    *out = p;
+    return cleanup(FFBP_OK);
+}
+
+int ffbp_plan_workspace_bytes(const ffbp_plan *p, size_t *bytes)
+{
+    if (!p || !bytes) return fail(FFBP_E_ARG, "null argument");
+    *bytes = 256 + align256(p->bufA * sizeof(float2)) + align256(p->bufB * sizeof(float2));
+    return FFBP_OK;
+}
+
+static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, size_t ws_bytes, void *stream_, int *h_bad,
+                     float *stage_ms, int n_stage)
+{
+    if (!p || !d_S || !d_img || !d_ws) return fail(FFBP_E_ARG, "ffbp_form: null argument");
+    size_t need;
+    ffbp_plan_workspace_bytes(p, &need);
+    if (ws_bytes < need) return fail(FFBP_E_WORKSPACE, "workspace of %zu bytes, %zu needed", ws_bytes, need);
+    if (((uintptr_t)d_ws & 255) != 0) return fail(FFBP_E_ARG, "workspace must be 256-byte aligned");
+    cudaStream_t s = static_cast<cudaStream_t>(stream_);
+    char *ws = static_cast<char *>(d_ws);
+    int *bad = reinterpret_cast<int *>(ws);
+    float2 *bufA = reinterpret_cast<float2 *>(ws + 256);
+    float2 *bufB = reinterpret_cast<float2 *>(ws + 256 + align256(p->bufA * sizeof(float2)));
+    cudaError_t e = cudaMemsetAsync(bad, 0x7f, sizeof(int), s);
+    if (e != cudaSuccess) return cuda_fail(e, "status reset");
+    const bool timed = stage_ms != nullptr;
+    if (timed && n_stage < p->nlev + 1) return fail(FFBP_E_ARG, "stage_ms holds %d entries, %d needed", n_stage, p->nlev + 1);
+    std::vector<cudaEvent_t> ev;
+    if (timed) {
+        ev.resize(p->nlev + 2);
+        for (auto &x : ev) cudaEventCreate(&x);
+        cudaEventRecord(ev[0], s);
+    }
+    auto destroy_events = [&]() { for (auto &x : ev) cudaEventDestroy(x); };
+    const float2 *in = static_cast<const float2 *>(d_S);
+    for (int l = 0; l < p->nlev; ++l) {
+        const DevLevel &v = p->lv[l];
+        float2 *outp = (l % 2 == 0) ? bufA : bufB;
+        ffbp::LevelLaunch L;
+        L.x = in; L.phase = v.phase; L.tk = v.tk; L.tp = v.tp;
+        L.wp = l == 0 ? p->wp : nullptr; L.wk = l == 0 ? p->wk : nullptr;
+        L.out = outp; L.bad = l == 0 ? bad : nullptr;
+        L.Np = v.Np; L.C = v.C; L.P = v.P; L.K = v.K; L.Ko = v.Ko; L.Po = v.Po; L.Dk = v.Dk; L.Lk = v.Lk; L.plk = v.plk;
+        L.Dp = v.Dp; L.Lp = v.Lp; L.plp = v.plp; L.kc = v.kc;
+        const char *why = nullptr;
+        e = ffbp::launch_level(L, s, &why);
+        if (why) { destroy_events(); return fail(FFBP_E_UNSUPPORTED, "level %d: %s", l, why); }
+        if (e != cudaSuccess) { destroy_events(); return cuda_fail(e, "level kernel"); }
+        if (timed) cudaEventRecord(ev[l + 1], s);
+        in = outp;
+    }
+    ffbp::FinalLaunch F;
+    F.d = in; F.B = p->ntiles; F.Pf = p->Pf; F.Qf = p->Qf; F.T = p->T; F.ux = p->ux; F.uy = p->uy;
+    F.spx = p->spx; F.spy = p->spy; F.a0 = p->a0; F.a1 = p->a1; F.fc2 = p->fc2; F.ucx = p->ucx; F.ucy = p->ucy;
+    F.rc = p->rc; F.w = p->wf; F.tiles = nullptr; F.img = static_cast<float2 *>(d_img); F.first = p->first;
+    F.nx = p->nx; F.ny = p->ny; F.ox = p->ox; F.oy = p->oy; F.scale = 1.f;
+    const char *why = nullptr;
+    e = p->final_mode == FFBP_FINAL_FP32 ? ffbp::launch_final_fp32(F, s, &why) : ffbp::launch_final_tc(F, p->final_mode, s, &why);
+    if (why) { destroy_events(); return fail(FFBP_E_UNSUPPORTED, "final stage: %s", why); }
+    if (e != cudaSuccess) { destroy_events(); return cuda_fail(e, "final kernel"); }
+    if (timed) {
+        cudaEventRecord(ev[p->nlev + 1], s);
+        if ((e = cudaEventSynchronize(ev[p->nlev + 1])) != cudaSuccess) { destroy_events(); return cuda_fail(e, "form"); }
+        for (int l = 0; l <= p->nlev; ++l) cudaEventElapsedTime(&stage_ms[l], ev[l], ev[l + 1]);
+        destroy_events();
+    }
+    if (h_bad) {
+        int v = 0;
+        if ((e = cudaMemcpyAsync(&v, bad, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return cuda_fail(e, "status read");
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "form");
+        *h_bad = (v == 0x7f7f7f7f) ? -1 : v;
+    }
+    return FFBP_OK;
+}
+
+int ffbp_form(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, size_t ws_bytes, void *stream, int *h_bad)
+{
+    return form_impl(p, d_S, d_img, d_ws, ws_bytes, stream, h_bad, nullptr, 0);
+}
+
+int ffbp_form_timed(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, size_t ws_bytes, void *stream,
+                    float *h_stage_ms, int n_stage)
+{
+    if (!h_stage_ms) return fail(FFBP_E_ARG, "ffbp_form_timed: null stage_ms");
+    return form_impl(p, d_S, d_img, d_ws, ws_bytes, stream, nullptr, h_stage_ms, n_stage);
+}
+
+int ffbp_plan_info(const ffbp_plan *p, int *nlev, int *launches)
+{
+    if (!p) return fail(FFBP_E_ARG, "ffbp_plan_info: null plan");
+    if (nlev) *nlev = p->nlev;
+    if (launches) *launches = p->nlev + 1;
+    return FFBP_OK;
+}
+
+int ffbp_level(const void *d_x, int Np, int P, int K, const void *d_phase, int C, const float *d_tk, int Lk, int plk,
+               int Dk, int Ko, double kc, const float *d_tp, int Lp, int plp, int Dp, int Po, const float *d_wp,
+               const float *d_wk, void *d_out, int *d_bad, void *stream)
+{
+    if (!d_x || !d_phase || !d_out) return fail(FFBP_E_ARG, "ffbp_level: null buffer");
+    if (Np < 1 || P < 1 || K < 1 || C < 1 || Dk < 1 || Dp < 1 || Ko < 1 || Po < 1) return fail(FFBP_E_ARG, "ffbp_level: non-positive size");
+    if ((Dk > 1 && (!d_tk || Lk < 1)) || (Dp > 1 && (!d_tp || Lp < 1))) return fail(FFBP_E_ARG, "ffbp_level: taps missing");
+    ffbp::LevelLaunch L;
+    L.x = static_cast<const float2 *>(d_x); L.phase = static_cast<const float2 *>(d_phase); L.tk = d_tk; L.tp = d_tp;
+    L.wp = d_wp; L.wk = d_wk; L.out = static_cast<float2 *>(d_out); L.bad = d_bad;
+    L.Np = Np; L.C = C; L.P = P; L.K = K; L.Ko = Ko; L.Po = Po; L.Dk = Dk; L.Lk = Lk; L.plk = plk; L.Dp = Dp;
+    L.Lp = Lp; L.plp = plp; L.kc = kc;
+    const char *why = nullptr;
+    cudaError_t e = ffbp::launch_level(L, static_cast<cudaStream_t>(stream), &why);
+    if (why) return fail(FFBP_E_UNSUPPORTED, "ffbp_level: %s", why);
+    if (e != cudaSuccess) return cuda_fail(e, "ffbp_level");
+    return FFBP_OK;
+}
+
+int ffbp_phases(const double *d_ant, int P, const double *d_ref, int Np, const double *d_cen, int C,
+                const double *d_range, double k0c, double k1, int cancel_free, void *d_phase, void *stream)
+{
+    if (!d_ant || !d_ref || !d_cen || !d_phase) return fail(FFBP_E_ARG, "ffbp_phases: null buffer");
+    if (P < 1 || Np < 1 || C < 1) return fail(FFBP_E_ARG, "ffbp_phases: non-positive size");
+    cudaError_t e = ffbp::launch_phases(d_ant, P, d_ref, Np, d_cen, C, d_range, k0c, k1, cancel_free,
+                                        static_cast<float2 *>(d_phase), static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "ffbp_phases");
+    return FFBP_OK;
+}
+
+int ffbp_final(const void *d_d, int B, int Pf, int Qf, int T, const double *d_ux, const double *d_uy, double spx,
+               double spy, double a0, double a1, const double *d_ucx, const double *d_ucy, const double *d_rc,
+               double fc2, const float *d_w, int mode, void *d_out, void *stream)
+{
+    if (!d_d || !d_ux || !d_uy || !d_ucx || !d_ucy || !d_rc || !d_out) return fail(FFBP_E_ARG, "ffbp_final: null buffer");
+    if (B < 1 || Pf < 1 || Qf < 1) return fail(FFBP_E_ARG, "ffbp_final: non-positive size");
+    ffbp::FinalLaunch F;
+    F.d = static_cast<const float2 *>(d_d); F.B = B; F.Pf = Pf; F.Qf = Qf; F.T = T; F.ux = d_ux; F.uy = d_uy;
+    F.spx = spx; F.spy = spy; F.a0 = a0; F.a1 = a1; F.fc2 = fc2; F.ucx = d_ucx; F.ucy = d_ucy; F.rc = d_rc; F.w = d_w;
+    F.tiles = static_cast<float2 *>(d_out); F.img = nullptr; F.first = nullptr; F.nx = F.ny = F.ox = F.oy = 0;
+    F.scale = 1.f;
+    const char *why = nullptr;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e = mode == FFBP_FINAL_FP32 ? ffbp::launch_final_fp32(F, s, &why) : ffbp::launch_final_tc(F, mode, s, &why);
+    if (why) return fail(FFBP_E_UNSUPPORTED, "ffbp_final: %s", why);
+    if (e != cudaSuccess) return cuda_fail(e, "ffbp_final");
+    return FFBP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,38 @@
+// Shared helpers of the ffbp_b200 kernels (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ffbp {
+
+constexpr float TWO_PI_F = 6.28318530717958647692f;
+constexpr double TWO_PI = 6.28318530717958647692;
+constexpr double C_LIGHT = 299792458.0;
+
+// exp(2 pi i c) for a phase c in cycles already reduced to [-0.5, 0.5]: the hardware sine and cosine are accurate to
+// about 4e-7 absolute on [-pi, pi], which is the whole range they are given here.
+__device__ __forceinline__ float2 cis_reduced(float c)
+{
+    float s, co;
+    __sincosf(TWO_PI_F * c, &s, &co);
+    return make_float2(co, s);
+}
+
+// exp(2 pi i c) for any float32 phase in cycles (reduced first).
+__device__ __forceinline__ float2 cis_cycles(float c)
+{
+    return cis_reduced(c - rintf(c));
+}
+
+// exp(2 pi i c) for a float64 phase in cycles: the reduction in float64, the sine and cosine in float32.
+__device__ __forceinline__ float2 cis_cycles_d(double c)
+{
+    return cis_reduced((float)(c - rint(c)));
+}
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b)
+{
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+
+}  // namespace ffbp

@@ -1,0 +1,53 @@
+// Internal launch interface between the C ABI (capi.cu) and the kernels. Not part of the public header.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+namespace ffbp {
+
+// One level (level.cu). Device pointers; see ffbp_level in include/ffbp_b200.h for the arithmetic.
+struct LevelLaunch {
+    const float2 *x;      // [Np, P, K]
+    const float2 *phase;  // [Np, C, P] (c0, sl)
+    const float *tk;      // [Lk] or null (Dk == 1)
+    const float *tp;      // [Lp] or null (Dp == 1)
+    const float *wp;      // [P] or null
+    const float *wk;      // [K] or null
+    float2 *out;          // [Np C, Po, Ko]
+    int *bad;             // or null
+    int Np, C, P, K, Ko, Po, Dk, Lk, plk, Dp, Lp, plp;
+    double kc;
+};
+
+// Returns cudaSuccess, or an error with *why set to a static message for shapes the kernels do not cover.
+cudaError_t launch_level(const LevelLaunch &L, cudaStream_t s, const char **why);
+
+// Child phases (geometry.cu).
+cudaError_t launch_phases(const double *ant, int P, const double *ref, int Np, const double *cen, int C,
+                          const double *range, double k0c, double k1, int cancel_free, float2 *phase, cudaStream_t s);
+
+// Final-stage geometry (geometry.cu): per tile b and final subaperture p the direction cosines of the antenna seen
+// from the tile centre along e1, e2 (ux, uy), and per tile the aperture-mean line of sight (ucx, ucy) and range (rc).
+cudaError_t launch_final_geom(const double *ant_f, int Pf, const double *cen, int B, const double *e1,
+                              const double *e2, double *ux, double *uy, double *ucx, double *ucy, double *rc,
+                              cudaStream_t s);
+
+// Final stage (final_fp32.cu, final_tc.cu).
+struct FinalLaunch {
+    const float2 *d;      // [B, Pf, Qf]
+    int B, Pf, Qf, T;
+    const double *ux, *uy;            // [B, Pf]
+    double spx, spy, a0, a1, fc2;
+    const double *ucx, *ucy, *rc;     // [B]
+    const float *w;       // [3, B, Pf] (w0, gx, gyr) or null
+    // output: either tiles [B, T, T] (img == null) or straight into an image with the tile origins
+    float2 *tiles;
+    float2 *img;          // [nx, ny]
+    const int2 *first;    // [B] first pixel of each tile on the padded grid
+    int nx, ny, ox, oy;
+    float scale;
+};
+cudaError_t launch_final_fp32(const FinalLaunch &F, cudaStream_t s, const char **why);
+cudaError_t launch_final_tc(const FinalLaunch &F, int mode, cudaStream_t s, const char **why);
+
+}  // namespace ffbp

@@ -135,8 +135,10 @@ def make_plan(col, nx, ny, spx, spy, T=32, nlev=3, pmax=0.4, atten=70.0, splits=
     """The plan of an nx x ny image of spacings spx, spy along the orthonormal e1, e2 about the origin, for the
     collection col (fmin, df, K, ant). Returns a dict with the padded grid (Nx, Ny, ox, oy), the per-level records
     (splits sx, sy and children C; decimations Dk, Dp; sizes K, P in and Ko, Po out; filters fir_k, fir_p; the band
-    f0, df of the level's input; the parents' reference points ref [B, 3], the child offsets d [C, 3], the child
-    centres cen [B, C, 3], the output pulse positions pidx) and the final-stage record (fastsar/ffbp2.py:192-250).
+    f0, df of the level's input; the antenna path ant [P, 3] on the level's input pulse grid; the parents' reference
+    points ref [B, 3], the child offsets d [C, 3], the child centres cen [B, C, 3], the output pulse positions pidx)
+    and the final-stage record (fastsar/ffbp2.py:192-250), which adds the tiles' first pixels and the antenna path
+    of the final subapertures to the reference's.
     pulse: per-level (Dp, pass_p) that replace the ones this aperture would get."""
     e1, e2 = np.asarray(e1, np.float64), np.asarray(e2, np.float64)
     if splits is None:
@@ -152,7 +154,6 @@ def make_plan(col, nx, ny, spx, spy, T=32, nlev=3, pmax=0.4, atten=70.0, splits=
     cx, cy = Nx, Ny
     plan = dict(levels=[], T=T, nx=nx, ny=ny, Nx=Nx, Ny=Ny, ox=ox, oy=oy, spx=spx, spy=spy,
                 split=list(zip(sxs, sys_)), e1=e1, e2=e2)
-    fmaxk = None
     for lev, (sx, sy) in enumerate(zip(sxs, sys_)):
         cx, cy = cx // sx, cy // sy
         gx, gy = np.meshgrid(np.arange(sx) * cx, np.arange(sy) * cy, indexing='ij')
@@ -188,13 +189,15 @@ def make_plan(col, nx, ny, spx, spy, T=32, nlev=3, pmax=0.4, atten=70.0, splits=
             fir_k=decimator_fir(K, Dk, ak, atten)[0] if Dk > 1 else None,
             fir_p=decimator_fir(P, Dp, ap, atten)[0] if Dp > 1 else None,
             dec_k=(K, Dk, ak, atten), dec_p=(P, Dp, ap, atten),
-            f0=f0, df=df, ref=ref, d=cen[0] - ref[0], cen=cen, pidx=pidx,
+            f0=f0, df=df, ant=ant, ref=ref, d=cen[0] - ref[0], cen=cen, pidx=pidx,
             pass_k=float(pass_k), pass_p=float(pass_p)))
         ant = positions(ant, pidx)
         f0, df, K, P = f0 + ((Dk - 1) / 2.0 - mk * Dk) * df, df * Dk, Ko, Po
         ref, first = cen.reshape(-1, 3), cfirst.reshape(-1, 2)
     assert (cx, cy) == (T, T)
-    plan['final'] = dict(cen=ref, f0=f0, df=df, K=K, P=P, fc=f0 + (K - 1) / 2.0 * df)
+    # first: the first pixel (x, y) of each final tile on the padded grid, in the tile order of cen
+    plan['final'] = dict(cen=ref, first=first.astype(np.int64), f0=f0, df=df, K=K, P=P, fc=f0 + (K - 1) / 2.0 * df,
+                         ant=ant)
     return plan
 
 

@@ -1,0 +1,156 @@
+/*
+ * ffbp_b200 -- factorized backprojection (FFBP) spotlight image formation on the NVIDIA B200 (sm_100a).
+ *
+ * The drop-in boundary for the reference's factorized-backprojection former (saulpingerman/FastSAR 0.3.1): the
+ * reference's Python former (fastsar/api.py:312-677, ImageFormer) plans on the host and hands the plan to a backend
+ * (fastsar/ffbp_cuda.py:889 make_ffbp_cuda, fastsar/ffbp_cpu.py:158 make_ffbp_cpu) whose form(S) returns the image.
+ * This C ABI is that backend: a plan object built from the host plan, and a form call on device buffers. The stage
+ * entry points mirror the three kernels of the reference's CPU backend (fastsar/ffbp_cpu.cpp:244-260 rot_fir_k and
+ * fir_p, fastsar/ffbp_cpu.cpp:458-461 final_tiles), on device pointers and a stream.
+ *
+ * Conventions
+ *   - Every function returns 0 on success and a negative FFBP_E* code on failure; ffbp_last_error() gives the
+ *     message of the last failure on the calling thread. No C++ exception crosses this boundary.
+ *   - Pointers named d_* are device pointers; h_* are host pointers. Complex samples are interleaved float pairs
+ *     (re, im): the layout of numpy's complex64 and of torch.complex64.
+ *   - Streams are passed as void* (a cudaStream_t; NULL is the legacy default stream).
+ *   - The caller owns every buffer it passes. A plan owns the device copies of its own constants (filters, float64
+ *     geometry, child phases), allocated in ffbp_plan_create and freed in ffbp_plan_destroy.
+ *   - A plan may be used by one thread at a time (fastsar/exact.py:412-413 states the same for a former).
+ */
+#ifndef FFBP_B200_H
+#define FFBP_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FFBP_B200_ABI_VERSION 1
+
+enum {
+    FFBP_OK = 0,
+    FFBP_E_ARG = -1,        /* an argument is out of range (the message names it)                         */
+    FFBP_E_CUDA = -2,       /* a CUDA call failed                                                           */
+    FFBP_E_NOMEM = -3,      /* a device allocation of the plan failed                                       */
+    FFBP_E_WORKSPACE = -4,  /* the workspace passed to ffbp_form is smaller than ffbp_plan_workspace_bytes   */
+    FFBP_E_UNSUPPORTED = -5 /* a shape the kernels do not cover (the message says which limit)              */
+};
+
+/* Final-stage arithmetic (ImageFormer's precision=, fastsar/api.py:27-31).                                     */
+enum {
+    FFBP_FINAL_FP32 = 0,    /* float32 on the CUDA cores: the plain path                                        */
+    FFBP_FINAL_TC_F16 = 1,  /* tcgen05 tensor cores, float16 operands, float32 accumulation                    */
+    FFBP_FINAL_TC_BF16X3 = 2 /* tcgen05 tensor cores, three bfloat16 products (hi*hi + hi*lo + lo*hi), float32  */
+};
+
+/* One level of the plan (fastsar/ffbp2.py:192-250, make_plan's per-level record). All pointers are host memory. */
+typedef struct {
+    int sx, sy;             /* children per parent along e1 and e2; C = sx * sy                                   */
+    int C;
+    int Dk, Dp;             /* decimation along frequency samples and along pulses (1: none)                     */
+    int K, P;               /* samples and pulses of this level's input                                          */
+    int Ko, Po;             /* samples and pulses of its output                                                  */
+    const float *h_taps_k;  /* [Lk] frequency FIR (decimator_fir kernel), NULL when Dk == 1                      */
+    int Lk, plk;
+    const float *h_taps_p;  /* [Lp] pulse FIR, NULL when Dp == 1                                                 */
+    int Lp, plp;
+    double f0, df;          /* frequency of input sample 0 and the sample spacing (Hz)                           */
+    const double *h_ant;    /* [P, 3] antenna phase centres on this level's input pulse grid (m)                 */
+    const double *h_ref;    /* [B, 3] the parents' reference points (B = product of the earlier levels' C)        */
+    const double *h_cen;    /* [B, C, 3] the children's centres                                                  */
+    const double *h_range;  /* level 0 only, optional: [P] per-pulse one-way reference range (ImageFormer's ref=) */
+} ffbp_level_desc;
+
+/* The plan of one image (make_plan's record plus the final stage and the call options). Host memory.          */
+typedef struct {
+    int nlev;
+    const ffbp_level_desc *levels;  /* [nlev] */
+    int T;                  /* final tile side, 16 or 32                                                          */
+    int nx, ny;             /* the image                                                                          */
+    int Nx, Ny, ox, oy;     /* the padded grid and the crop offsets                                               */
+    double spx, spy;        /* pixel spacings (m) along e1, e2                                                    */
+    double e1[3], e2[3];
+    int Pf, Qf;             /* final stage: subapertures and frequency samples per final tile                    */
+    double f0f, dff, fcf;   /* final-stage band: sample 0, spacing and centre frequency (Hz)                      */
+    const double *h_ant_f;  /* [Pf, 3] antenna positions of the final subapertures                                */
+    const double *h_cen_f;  /* [ntiles, 3] final tile centres, in the plan's tile order                           */
+    const int *h_first_f;   /* [ntiles, 2] first pixel (x, y) of each final tile on the padded grid              */
+    const float *h_wp;      /* [P0] Taylor window over pulses, or NULL (no window)                                */
+    const float *h_wk;      /* [K0] Taylor window over samples, or NULL                                           */
+    const float *h_wf;      /* aperture weights per (tile, final subaperture): [ntiles, Pf] (wf_ndim 2) or       */
+    int wf_ndim;            /* [3, ntiles, Pf] weight and its gradients along e1, e2 (wf_ndim 3); NULL / 0 none  */
+    int final_mode;         /* FFBP_FINAL_*                                                                       */
+} ffbp_plan_desc;
+
+typedef struct ffbp_plan ffbp_plan;
+
+/* Last error message of the calling thread (NUL-terminated, truncated to n bytes). Returns its full length.    */
+int ffbp_last_error(char *buf, int n);
+
+/* ABI version (FFBP_B200_ABI_VERSION) and the build's target, for a loader's check.                            */
+int ffbp_abi_version(void);
+
+/* Build a plan: checks the description, uploads the filters and windows, and computes on the device, in float64,
+ * every level's child phases (fastsar/ffbp2.py:313-342 for the first two levels, fastsar/ffbp_cuda.py:598-632
+ * below them) and the final-stage geometry (fastsar/ffbp_cuda.py:870-886, 964-975). Runs on `stream` and returns
+ * once the plan is ready. Replaces make_ffbp_cuda / make_ffbp_cpu (fastsar/ffbp_cuda.py:889, fastsar/ffbp_cpu.py:158)
+ * together with collection_arrays (fastsar/ffbp2.py:313).                                                        */
+int ffbp_plan_create(const ffbp_plan_desc *desc, void *stream, ffbp_plan **out);
+int ffbp_plan_destroy(ffbp_plan *plan);
+
+/* Bytes of device workspace a form call needs (the level intermediates and a status word).                     */
+int ffbp_plan_workspace_bytes(const ffbp_plan *plan, size_t *bytes);
+
+/* Form the image: d_S [P0, K0] complex64 phase history (unwindowed; the plan's window is applied here) ->
+ * d_img [nx, ny] complex64. d_ws: the workspace (ffbp_plan_workspace_bytes, 256-byte aligned). Asynchronous on
+ * `stream`. The first non-finite sample's pulse index (or -1) is written to h_bad_pulse when it is not NULL,
+ * which makes the call wait for the stream. Replaces form(S) of fastsar/ffbp_cuda.py:1084-1211.                */
+int ffbp_form(ffbp_plan *plan, const void *d_S, void *d_img, void *d_ws, size_t ws_bytes, void *stream,
+              int *h_bad_pulse);
+
+/* ffbp_form with the device time of each launch (the reference's CUDA-event stage timers, fastsar/ffbp_cuda.py:
+ * 635-652 PROFILE): stage_ms[l] for level l < nlev and stage_ms[nlev] for the final stage, measured by CUDA events
+ * recorded on `stream` around each launch. Waits for the stream. n_stage: the length of stage_ms (>= nlev + 1).    */
+int ffbp_form_timed(ffbp_plan *plan, const void *d_S, void *d_img, void *d_ws, size_t ws_bytes, void *stream,
+                    float *h_stage_ms, int n_stage);
+
+/* Levels and launches of a plan: *nlev, and the kernels one ffbp_form launches (*launches).                  */
+int ffbp_plan_info(const ffbp_plan *plan, int *nlev, int *launches);
+
+/* ---- stage entry points (device buffers, asynchronous on `stream`) -------------------------------------- */
+
+/* One level for Np parents: the rotation of each parent's pulses to each child's centre, the pulse FIR and the
+ * frequency FIR (fastsar/ffbp_cpu.cpp:146-255 rot_fir_k then fastsar/ffbp_cpu.cpp:258-293 fir_p, fused):
+ *   out[n C + c, i, j] = sum_{rp<Lp} tp[rp] sum_{rk<Lk} tk[rk] z_{n,c}[Dp i + rp - plp, Dk j + rk - plk]
+ *   z_{n,c}[p, k] = w(p, k) x[n, p, k] exp(2 pi i (c0[n,c,p] + sl[n,c,p] (k - kc))),  zero outside [0,P) x [0,K)
+ * d_x [Np, P, K] complex64; d_phase [Np, C, P] float pairs (c0, sl); d_tk [Lk] / d_tp [Lp] float32 (NULL with
+ * Dk == 1 / Dp == 1); d_wp [P], d_wk [K] the window w(p, k) = wp[p] wk[k], or NULL; d_out [Np C, Po, Ko] complex64.
+ * d_bad (optional) receives the smallest pulse index of a non-finite sample (atomic min; initialise to INT_MAX). */
+int ffbp_level(const void *d_x, int Np, int P, int K, const void *d_phase, int C, const float *d_tk, int Lk, int plk,
+               int Dk, int Ko, double kc, const float *d_tp, int Lp, int plp, int Dp, int Po, const float *d_wp,
+               const float *d_wk, void *d_out, int *d_bad, void *stream);
+
+/* Child phases in float64 for one level (fastsar/ffbp2.py:329-339 / fastsar/ffbp_cuda.py:598-632): for parent n,
+ * child c and pulse p, ddr = |cen[n,c] - ant[p]| - |ref[n] - ant[p]| (or - range[p] when d_range is given),
+ * c0 = ddr k0c - rint(ddr k0c), sl = ddr k1, stored as float pairs into d_phase [Np, C, P]. cancel_free selects
+ * the cancellation-free form of the difference used below the first two levels. All inputs are float64.        */
+int ffbp_phases(const double *d_ant, int P, const double *d_ref, int Np, const double *d_cen, int C,
+                const double *d_range, double k0c, double k1, int cancel_free, void *d_phase, void *stream);
+
+/* The final stage for B tiles (fastsar/ffbp_cpu.cpp:302-469 final_tiles):
+ *   out[b, i, j] = exp(2 pi i qc_bij) sum_{p<Pf, q<Qf} d[b,p,q] wx(b,p,i) wy(b,p,j)
+ *                                      exp(-2 pi i (ux[b,p] dlx_i + uy[b,p] dly_j)(a0 + a1 q))
+ *   qc_bij = (dlx_i^2 + dly_j^2 - (ucx[b] dlx_i + ucy[b] dly_j)^2) fc2 / (2 rc[b]),  dl_i = (i - (T-1)/2) sp
+ * d_d [B, Pf, Qf] complex64; d_ux, d_uy [B, Pf] float64; d_ucx, d_ucy, d_rc [B] float64; d_w (NULL, or [3, B, Pf]
+ * float32: w0, gx, gyr with wx = w0 + gx dlx_i, wy = 1 + gyr dly_j); d_out [B, T, T] complex64. mode: FFBP_FINAL_*.*/
+int ffbp_final(const void *d_d, int B, int Pf, int Qf, int T, const double *d_ux, const double *d_uy, double spx,
+               double spy, double a0, double a1, const double *d_ucx, const double *d_ucy, const double *d_rc,
+               double fc2, const float *d_w, int mode, void *d_out, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FFBP_B200_H */

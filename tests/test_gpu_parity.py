@@ -1,0 +1,252 @@
+"""Parity of the CUDA path with the reference and the oracle, through the C ABI, on a B200.
+
+* Stage kernels (ffbp_level, ffbp_final, ffbp_phases) against the oracle's float64 restatement of the reference's
+  kernels on seeded inputs, including the edges the reference's tests exercise (levels that do not decimate along
+  one axis, child counts that are not a multiple of a block's group, odd sizes, aperture weights).
+* Whole images against the reference CPU former's images (tests/golden, no gain fitted; the bar of
+  fastsar tests/test_ffbp_cpu.py:34-38: -70 dB and the peak within 1e-3) and against the oracle run here.
+* The non-finite scan, bitwise repeatability, and the float64 phases against the planner's host float64 geometry.
+Tolerances: the plain float32 path must be within -70 dB of the reference (the parity bar); kernels within 2e-5
+relative of the float64 oracle."""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip('torch')
+if not torch.cuda.is_available():
+    pytest.skip('no CUDA device', allow_module_level=True)
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, np.complex128).ravel(), np.asarray(b, np.complex128).ravel()
+    return float(np.sqrt(np.sum(np.abs(a - b) ** 2) / np.sum(np.abs(b) ** 2)))
+
+
+def _dev(a, dtype=None):
+    t = torch.from_numpy(np.ascontiguousarray(a))
+    return t.cuda() if dtype is None else t.to(dtype).cuda()
+
+
+@pytest.fixture(scope='module')
+def lib():
+    from fastsar_b200 import _lib
+    return _lib
+
+
+def _level_case(rng, Np, P, K, C, Dk, Dp, pk=0.6, pp=0.5):
+    from fastsar_b200 import plan as P_
+    fk = P_.decimator_fir(K, Dk, pk)[0] if Dk > 1 else None
+    fp = P_.decimator_fir(P, Dp, pp)[0] if Dp > 1 else None
+    Ko = fk['n_out'] if fk else K
+    Po = fp['n_out'] if fp else P
+    x = (rng.standard_normal((Np, P, K)) + 1j * rng.standard_normal((Np, P, K))).astype(np.complex64)
+    c0 = rng.uniform(-0.5, 0.5, (Np, C, P)).astype(np.float32)
+    sl = rng.uniform(-0.01, 0.01, (Np, C, P)).astype(np.float32)
+    return x, c0, sl, fk, fp, Ko, Po
+
+
+def _run_level_gpu(lib, x, c0, sl, fk, fp, Ko, Po, Dk, Dp, window=None, bad=None):
+    L = lib.load()
+    Np, P, K = x.shape
+    C = c0.shape[1]
+    ph = np.stack([c0, sl], axis=-1).astype(np.float32)
+    dx, dph = _dev(x), _dev(ph)
+    tk = _dev(np.asarray(fk['kern'], np.float32)) if fk else None
+    tp = _dev(np.asarray(fp['kern'], np.float32)) if fp else None
+    wp = _dev(window[0]) if window is not None else None
+    wk = _dev(window[1]) if window is not None else None
+    out = torch.zeros((Np * C, Po, Ko), dtype=torch.complex64, device='cuda')
+    s = torch.cuda.current_stream().cuda_stream
+    lib.check(L.ffbp_level(dx.data_ptr(), Np, P, K, dph.data_ptr(), C, lib.tptr(tk), fk['L'] if fk else 1,
+                           fk['pl'] if fk else 0, Dk, Ko, (K - 1) / 2.0, lib.tptr(tp), fp['L'] if fp else 1,
+                           fp['pl'] if fp else 0, Dp, Po, lib.tptr(wp), lib.tptr(wk), out.data_ptr(),
+                           lib.tptr(bad), s), 'ffbp_level')
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+def _oracle_level_full(oracle_lib, x, c0, sl, fk, fp, Ko, Po, Dk, Dp, window=None):
+    L = oracle_lib.lib('port')
+    Np, P, K = x.shape
+    C = c0.shape[1]
+    if window is not None:
+        x = (x * (window[0][:, None] * window[1][None, :]).astype(np.float32)[None]).astype(np.complex64)
+    taps = np.asarray(fk['kern'], np.float32) if fk else np.ones(1, np.float32)
+    yre = np.zeros((Np * C, P, Ko), np.float32)
+    yim = np.zeros_like(yre)
+    L.rot_fir_k_cplx(np.ascontiguousarray(x).view(np.float32), Np, P, K, c0, sl, C, taps, fk['L'] if fk else 1,
+                     fk['pl'] if fk else 0, Dk, Ko, (K - 1) / 2.0, yre, yim)
+    if fp is None:
+        return yre + 1j * yim
+    zre = np.zeros((Np * C, Po, Ko), np.float32)
+    zim = np.zeros_like(zre)
+    L.fir_p(yre, yim, Np * C, P, Ko, np.asarray(fp['kern'], np.float32), fp['L'], fp['pl'], Dp, Po, zre, zim)
+    return zre + 1j * zim
+
+
+LEVEL_CASES = [
+    # Np, P, K, C, Dk, Dp
+    (1, 300, 520, 8, 3, 4),      # a first level: one parent, both axes decimated
+    (3, 97, 131, 5, 2, 3),       # C not a multiple of the block's 4 children, odd sizes
+    (2, 64, 90, 4, 1, 2),        # no frequency decimation (Dk = 1)
+    (2, 80, 200, 6, 4, 1),       # no pulse decimation (Dp = 1)
+    (1, 50, 700, 2, 7, 2),       # a long frequency FIR (Lk > 100)
+    (4, 40, 60, 3, 1, 1),        # rotation only
+]
+
+
+@pytest.mark.parametrize('case', LEVEL_CASES, ids=[f'Np{c[0]}-P{c[1]}-K{c[2]}-C{c[3]}-Dk{c[4]}-Dp{c[5]}' for c in LEVEL_CASES])
+def test_level_kernel_matches_oracle(lib, oracle_lib, case):
+    Np, P, K, C, Dk, Dp = case
+    rng = np.random.default_rng(sum(case))
+    x, c0, sl, fk, fp, Ko, Po = _level_case(rng, Np, P, K, C, Dk, Dp)
+    got = _run_level_gpu(lib, x, c0, sl, fk, fp, Ko, Po, Dk, Dp)
+    ref = _oracle_level_full(oracle_lib, x, c0, sl, fk, fp, Ko, Po, Dk, Dp)
+    e = _rel(got, ref)
+    print(f'level {case}: rel {e:.2e}')
+    assert e < 2e-5, e
+
+
+def test_level_kernel_window_and_nonfinite(lib, oracle_lib):
+    rng = np.random.default_rng(3)
+    x, c0, sl, fk, fp, Ko, Po = _level_case(rng, 1, 120, 256, 4, 3, 2)
+    from fastsar_b200.api import _window
+    w = _window(120, 256)
+    got = _run_level_gpu(lib, x, c0, sl, fk, fp, Ko, Po, 3, 2, window=w)
+    ref = _oracle_level_full(oracle_lib, x, c0, sl, fk, fp, Ko, Po, 3, 2, window=w)
+    assert _rel(got, ref) < 2e-5
+    x[0, 77, 5] = np.nan
+    x[0, 90, 100] = np.inf
+    bad = torch.full((1,), 2 ** 31 - 1, dtype=torch.int32, device='cuda')
+    _run_level_gpu(lib, x, c0, sl, fk, fp, Ko, Po, 3, 2, window=w, bad=bad)
+    assert int(bad.item()) == 77
+
+
+@pytest.mark.parametrize('T', [16, 32])
+@pytest.mark.parametrize('weighted', [False, True])
+def test_final_kernel_matches_oracle(lib, oracle_lib, T, weighted):
+    rng = np.random.default_rng(T + weighted)
+    B, Pf, Qf = 5, 13, 57
+    d = (rng.standard_normal((B, Pf, Qf)) + 1j * rng.standard_normal((B, Pf, Qf))).astype(np.complex64)
+    ux, uy = rng.uniform(-0.9, 0.9, (B, Pf)), rng.uniform(-0.9, 0.9, (B, Pf))
+    spx, spy = 0.3, 0.45
+    a0, a1, fc2 = 64.1, 0.013, 64.4
+    ucx, ucy, rc = rng.uniform(-0.5, 0.5, B), rng.uniform(-0.5, 0.5, B), rng.uniform(4e3, 6e3, B)
+    w = np.stack([rng.uniform(0.5, 1.5, (B, Pf)), rng.uniform(-0.01, 0.01, (B, Pf)),
+                  rng.uniform(-0.01, 0.01, (B, Pf))]).astype(np.float32) if weighted else None
+    L = lib.load()
+    out = torch.zeros((B, T, T), dtype=torch.complex64, device='cuda')
+    dd = [_dev(a) for a in (d, ux, uy, ucx, ucy, rc)]
+    dw = _dev(w) if weighted else None
+    lib.check(L.ffbp_final(dd[0].data_ptr(), B, Pf, Qf, T, dd[1].data_ptr(), dd[2].data_ptr(), spx, spy, a0, a1,
+                           dd[3].data_ptr(), dd[4].data_ptr(), dd[5].data_ptr(), fc2, lib.tptr(dw), 0, out.data_ptr(),
+                           torch.cuda.current_stream().cuda_stream), 'ffbp_final')
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    O = oracle_lib.lib('port')
+    dlx = (np.arange(T) - (T - 1) / 2.0) * spx
+    dly = (np.arange(T) - (T - 1) / 2.0) * spy
+    ore = np.zeros((B, T, T), np.float32)
+    oim = np.zeros_like(ore)
+    wp = [None] * 3 if w is None else [np.ascontiguousarray(x) for x in w]
+    O.final_tiles(np.ascontiguousarray(d.real), np.ascontiguousarray(d.imag), B, Pf, Qf, T, ux, uy, dlx, dly, a0, a1,
+                  ucx, ucy, rc, fc2, ore, oim, *[None if x is None else x.ctypes.data for x in wp])
+    e = _rel(got, ore + 1j * oim)
+    print(f'final T={T} weighted={weighted}: rel {e:.2e}')
+    assert e < 2e-5, e
+
+
+def test_phases_match_host_float64(lib, golden):
+    """The device float64 phases of the first two levels against the planner's host float64 (collection_arrays)."""
+    from fastsar_b200 import plan as P_
+    from fastsar_b200.sim import Collect
+    rec = golden('plan_spot512')
+    fmin, df, K, nx, ny, spx, spy, T, nlev, pmax = rec['scal']
+    col = Collect(fmin=fmin, df=df, K=int(K), ant=rec['ant'], res=0.5)
+    plan = P_.make_plan(col, int(nx), int(ny), spx, spy, T=int(T), nlev=int(nlev), pmax=pmax, e1=rec['e1'], e2=rec['e2'])
+    coll = P_.collection_arrays(plan, col.ant)
+    L = lib.load()
+    for i in range(2):
+        lv = plan['levels'][i]
+        B = lv['ref'].shape[0]
+        out = torch.zeros((B, lv['C'], lv['P'], 2), dtype=torch.float32, device='cuda')
+        ant, ref, cen = _dev(lv['ant']), _dev(lv['ref']), _dev(lv['cen'])
+        kc = (lv['K'] - 1) / 2.0
+        k0c, k1 = 2.0 * (lv['f0'] + kc * lv['df']) / 299792458.0, 2.0 * lv['df'] / 299792458.0
+        lib.check(L.ffbp_phases(ant.data_ptr(), lv['P'], ref.data_ptr(), B, cen.data_ptr(), lv['C'], None, k0c, k1, 0,
+                                out.data_ptr(), torch.cuda.current_stream().cuda_stream), 'ffbp_phases')
+        torch.cuda.synchronize()
+        g = out.cpu().numpy()
+        dc0 = np.abs(g[..., 0] - coll['levels'][i]['c0'])
+        dc0 = np.minimum(dc0, 1 - dc0)                   # a wrap at +-0.5 cycles
+        assert dc0.max() < 1e-6
+        np.testing.assert_allclose(g[..., 1], coll['levels'][i]['slope'], rtol=1e-6, atol=1e-9)
+
+
+# ------------------------------------------------------------------------------------------------ whole images
+
+def _former(golden, nlev, **kw):
+    from fastsar_b200 import ImageFormer
+    g = golden('image_small')
+    fmin, df, K = g['scal']
+    return ImageFormer(g['ant'], fmin, df, int(K), 128, 128, 0.5, 0.5, T=16, levels=nlev, **kw), g
+
+
+@pytest.mark.parametrize('nlev', [2, 3])
+def test_image_matches_reference_former(golden, oracle_lib, nlev):
+    """The reference's CPU test scene (fastsar tests/test_ffbp_cpu.py:10-38): -70 dB and the peak within 1e-3 of the
+    reference former's image, no gain fitted."""
+    f, g = _former(golden, nlev)
+    img = f(g['S'])
+    ref = g[f'ffbp_l{nlev}']
+    e = oracle_lib.err_db(img, ref)
+    peak = np.abs(img).max() / np.abs(ref).max()
+    print(f'{nlev} levels: {e:.1f} dB vs reference former, peak ratio {peak:.6f}')
+    assert e < -70.0 and abs(peak - 1) < 1e-3
+
+
+def test_image_without_window(golden, oracle_lib):
+    f, g = _former(golden, 3, window=False)
+    assert oracle_lib.err_db(f(g['S']), g['ffbp_l3_nowin']) < -70.0
+
+
+def test_spotlight512_matches_reference_and_fp64(golden, oracle_lib):
+    """The 512-pulse, 600 km spotlight (32 targets, clutter -30 dB, noise -40 dB): against the reference former's
+    image, and against the reference's float64 64x backprojection on 4,096 pixels."""
+    from fastsar_b200 import ImageFormer, sim
+    g = golden('image_spot512')
+    w = sim.workload('spotlight_512')
+    col = w['col']
+    f = ImageFormer(col.ant, col.fmin, col.df, col.K, 512, 512, 0.25, 0.25, w['e1'], w['e2'])
+    assert f.T == int(g['T'])
+    img = f(g['S'])
+    e = oracle_lib.err_db(img, g['ffbp'])
+    e64 = oracle_lib.rel_db(img.ravel()[g['bp64_idx']], g['bp64'])
+    print(f'spotlight 512: {e:.1f} dB vs reference former; {e64:.1f} dB vs float64 BP 64x')
+    assert e < -70.0
+    assert e64 < -55.0
+
+
+def test_repeatable_bitwise(golden):
+    f, g = _former(golden, 3)
+    a = f(g['S'])
+    b = f(g['S'])
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_nonfinite_history_raises(golden):
+    f, g = _former(golden, 2)
+    S = g['S'].copy()
+    S[123, 7] = np.nan
+    with pytest.raises(ValueError, match='pulse 123'):
+        f(S)
+
+
+def test_torch_input_matches_numpy(golden):
+    f, g = _former(golden, 2)
+    a = f(g['S'])
+    b = f.form_device(torch.from_numpy(g['S']).cuda()).cpu().numpy()
+    assert np.array_equal(a, b)
