@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""Benchmark of the FFBP image former on the B200: giga-backprojections per second (pixels x pulses / s / 1e9) of
+the chosen form against the plain float32 FFBP, with the image's error against a float64 exact backprojection.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload spotlight_12k]
+
+Workload (default): the 16,384-pulse x 8,192-sample X-band spotlight (9.6 GHz, 1.2 GHz, 500 km, 55 deg grazing,
+3 deg aperture) formed to 12,288 x 8,832 pixels at 0.2 m; a seeded synthetic scene (2,000 log-normal targets, 10
+corner reflectors at +40 dB, clutter at -25 dB per resolution cell, noise at -40 dB) simulated on the GPU in
+float64 (fastsar_b200.sim). A step is one image formation. The timed region holds exactly K steps on the device,
+bracketed by a barrier and a synchronize; the 1.07 GB history is larger than the L2 cache, so no flush is needed.
+`e2e` repeats the timing through the public call with host buffers: each step copies the history from pinned host
+memory to the device and the image back.
+
+--gpus N (torchrun, one process per GPU): every rank forms its own collection (independent replicas; weak
+scaling); the step time is the maximum over ranks and the value counts every rank's backprojections.
+
+--impl reference: the reference's own CPU implementation (its fastsar/ffbp_cpu.cpp kernels, compiled from its
+sources by oracle/Makefile, driven by the oracle's restatement of its host orchestration) on this host's cores, on
+a bounded sample of the same workload: a fixed subset of the first level's children, whose work is a fixed
+fraction of the image's; rank 0 alone runs and prints.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = 'giga-backprojections/s at ≤-60 dB vs FP64: chosen form vs plain FFBP on B200'
+FP32_PEAK_NOMINAL = 148 * 128 * 2 * 1.965e9 / 1e12      # TFLOP/s, FP32 FMA on the CUDA cores at the maximum clock
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as fh:
+            m = json.load(fh)
+        return float(m['hbm_gbs']), float(m['bf16_tflops']), 'measured'
+    except (OSError, KeyError, ValueError):
+        return 6650.0, 1590.0, 'fallback'
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile('w+', suffix='.csv', delete=False)
+        q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,'
+             'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
+             'clocks_event_reasons.sw_power_cap')
+        try:
+            self.p = subprocess.Popen(['nvidia-smi', '-i', str(index), f'--query-gpu={q}', '--format=csv,noheader,nounits',
+                                       '-lms', '200'], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(',') for r in self.f.read().strip().splitlines() if r.count(',') >= 8]
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace('.', '').isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace('.', '').isdigit()]
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if 'Active' in v and 'Not' not in v})
+        return dict(sm_mhz=float(np.median(sm)) if sm else None, sm_max_mhz=max(mx) if mx else None, reasons=reasons,
+                    samples=len(rows))
+
+
+def plan_work(plan):
+    """Algorithmic bytes and flops of each launch of a form call (the level kernels, then the final stage):
+    bytes = the launch's compulsory reads and writes (its input samples, its child phases, its output samples);
+    flops = the rotation (8 per input sample and child) and the two FIRs (4 per tap and output sample, complex
+    data by real taps) of a level, and 8 T^2 Pf Qf per final tile (the separable tile sum as a real product)."""
+    out = []
+    B = 1
+    for lv in plan['levels']:
+        N = B * lv['C']
+        Lk = lv['fir_k']['L'] if lv['fir_k'] else 1
+        Lp = lv['fir_p']['L'] if lv['fir_p'] else 1
+        byt = 8 * (B * lv['P'] * lv['K'] + N * lv['P'] + N * lv['Po'] * lv['Ko'])
+        fl = N * lv['P'] * (8.0 * lv['K'] + 4.0 * Lk * lv['Ko']) + N * lv['Po'] * lv['Ko'] * 4.0 * Lp
+        out.append(dict(bytes=float(byt), flops=float(fl), kind='level'))
+        B = N
+    fin = plan['final']
+    T = plan['T']
+    out.append(dict(bytes=float(8 * (B * fin['P'] * fin['K'] + plan['nx'] * plan['ny'])),
+                    flops=float(8.0 * T * T * fin['P'] * fin['K'] * B), kind='final'))
+    return out
+
+
+def cpu_sample(w, S_host, steps, warmup, kind):
+    """The reference CPU former on a bounded sample of the workload: the first-level children of `children`.
+    -> (GBP/s of the sample, threads, description)."""
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import oracle as O
+    col = w['col']
+    form, plan = O.image_former(col.ant, col.fmin, col.df, col.K, w['nx'], w['ny'], w['spx'], w['spy'], w['e1'],
+                                w['e2'], kind=kind)
+    G = plan['levels'][0]['C']
+    nch = max(1, G // 16)
+    children = list(range(0, G, G // nch))[:nch]
+    pix = O.children_pixels(plan, children)
+    times = []
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        form(S_host, ng=8, children=children)
+        dt = time.perf_counter() - t0
+        if i >= warmup:
+            times.append(dt)
+    t = float(np.median(times))
+    gbps = pix * col.Np / t / 1e9
+    threads = O.lib(kind).ffbp_cpu_threads()
+    desc = (f'{len(children)} of the {G} first-level children ({pix} of {w["nx"] * w["ny"]} pixels, all '
+            f'{col.Np} pulses), median of {len(times)} warm calls of {t:.2f} s')
+    return gbps, threads, desc, t
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=10)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', choices=('ours', 'reference'), default='ours')
+    ap.add_argument('--workload', default='spotlight_12k')
+    ap.add_argument('--err-pixels', type=int, default=10000)
+    ap.add_argument('--no-cpu', action='store_true', help='skip the cpu_baseline leg')
+    ap.add_argument('--seed', type=int, default=0)
+    args = ap.parse_args()
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+
+    if args.impl == 'reference':
+        return run_reference(args, world, rank)
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=300), device_id=torch.device('cuda', local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device='cuda')
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    from fastsar_b200 import sim, ImageFormer, _lib
+    from fastsar_b200.exact import backproject_device, plane_points
+    t0 = time.time()
+    w, S = sim.synthetic_history(args.workload, seed=args.seed + rank)
+    torch.cuda.synchronize()
+    col = w['col']
+    log(f'[bench] history {tuple(S.shape)} from {w["n_scatterers"]} scatterers in {time.time() - t0:.1f} s')
+
+    # the chosen form and the plain float32 FFBP
+    modes = {'plain': 'fp32'}
+    try:
+        os.environ['FASTSAR_FINAL'] = 'tc3'
+        chosen = ImageFormer(col.ant, col.fmin, col.df, col.K, w['nx'], w['ny'], w['spx'], w['spy'], w['e1'], w['e2'])
+        probe = chosen.form_device(S)
+        torch.cuda.synchronize()
+        modes['chosen'] = 'tc3'
+    except ValueError as e:
+        log(f'[bench] tensor-core final stage unavailable ({e}); the chosen form is the plain float32 FFBP')
+        chosen = None
+    os.environ['FASTSAR_FINAL'] = 'fp32'
+    plain = ImageFormer(col.ant, col.fmin, col.df, col.K, w['nx'], w['ny'], w['spx'], w['spy'], w['e1'], w['e2'])
+    if chosen is None:
+        chosen, modes['chosen'] = plain, 'fp32'
+    plan = plain._plan
+    npix, P = w['nx'] * w['ny'], col.Np
+    out = torch.empty((w['nx'], w['ny']), dtype=torch.complex64, device='cuda')
+    out_plain = torch.empty_like(out)
+
+    def timed(former, img, steps, warmup, clocks=False):
+        for _ in range(warmup):
+            former.form_device(S, img, check=False)
+        torch.cuda.synchronize()
+        barrier()
+        clk = Clocks(local) if clocks else None
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(steps):
+            former.form_device(S, img, check=False)
+        e1.record()
+        torch.cuda.synchronize()
+        c = clk.stop() if clk else None
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1) / steps), c
+
+    ms, clocks = timed(chosen, out, args.steps, args.warmup, clocks=True)
+    ms_plain = ms if chosen is plain else timed(plain, out_plain, args.steps, args.warmup)[0]
+    if chosen is plain:
+        out_plain = out
+    stages = chosen._dev.form_timed(S, out)
+    stages_plain = stages if chosen is plain else plain._dev.form_timed(S, out_plain)
+    torch.cuda.synchronize()
+
+    # end to end through the public call: pinned host history -> device -> image -> pinned host
+    S_host = torch.empty(S.shape, dtype=torch.complex64, pin_memory=True)
+    S_host.copy_(S)
+    img_host = torch.empty((w['nx'], w['ny']), dtype=torch.complex64, pin_memory=True)
+    S_dev = torch.empty_like(S)
+    stream = torch.cuda.current_stream()
+    for _ in range(max(1, args.warmup)):
+        S_dev.copy_(S_host, non_blocking=True)
+        chosen.form_device(S_dev, out, check=False)
+        img_host.copy_(out, non_blocking=True)
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        S_dev.copy_(S_host, non_blocking=True)
+        chosen.form_device(S_dev, out, check=False)
+        img_host.copy_(out, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    barrier()
+
+    # error against the float64 exact backprojection at 64x on random pixels
+    chosen.form_device(S, out)
+    plain.form_device(S, out_plain)
+    rng = np.random.default_rng(1234)
+    idx = rng.choice(npix, size=min(args.err_pixels, npix), replace=False)
+    pts = plane_points(w['nx'], w['ny'], w['spx'], w['spy'], w['e1'], w['e2']).reshape(-1, 3)[idx]
+    t1 = time.time()
+    ref64 = backproject_device(S, col.ant, col.fmin, col.df, pts, upsample=64).cpu().numpy()
+    it = torch.from_numpy(idx).cuda()
+
+    def rel_db(a):
+        a = a.reshape(-1)[it].cpu().numpy().astype(np.complex128)
+        g = np.vdot(a, ref64) / np.vdot(a, a)
+        return float(10 * np.log10(np.sum(np.abs(g * a - ref64) ** 2) / np.sum(np.abs(ref64) ** 2)))
+    err_chosen, err_plain = rel_db(out), rel_db(out_plain)
+    log(f'[bench] float64 BP 64x on {len(idx)} pixels in {time.time() - t1:.1f} s: chosen {err_chosen:.1f} dB, '
+        f'plain {err_plain:.1f} dB')
+
+    # roofline of the dominant launch of the chosen form
+    hbm, bf16, src = peaks()
+    work = plan_work(chosen._plan)
+    k = int(np.argmax(stages))
+    names = [f'level{i}' for i in range(len(stages) - 1)] + ['final']
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, 'profiles', 'traffic.json')) as fh:
+            traffic = json.load(fh).get(args.workload, {}).get(names[k])
+    except (OSError, ValueError):
+        pass
+    is_tc = names[k] == 'final' and modes['chosen'] != 'fp32'
+    if is_tc:
+        ach = work[k]['flops'] / (stages[k] * 1e-3) / 1e12
+        roof = dict(bound='tensor', achieved=ach, peak=bf16, unit='TFLOP/s', frac=ach / bf16, traffic=traffic)
+    else:
+        ach = work[k]['bytes'] / (stages[k] * 1e-3) / 1e9
+        tf = work[k]['flops'] / (stages[k] * 1e-3) / 1e12
+        roof = dict(bound='hbm', achieved=ach, peak=hbm, unit='GB/s', frac=ach / hbm, traffic=traffic,
+                    fp32_cores=dict(achieved_tflops=tf, peak_tflops_nominal=FP32_PEAK_NOMINAL,
+                                    frac=tf / FP32_PEAK_NOMINAL))
+    roof.update(kernel=names[k], peak_source=src, ms=stages[k], algorithmic_bytes=work[k]['bytes'],
+                algorithmic_flops=work[k]['flops'])
+
+    # the reference CPU former on this host, bounded sample
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+            import oracle as O
+            kind = 'reference' if O.available('reference') else 'port'
+            Sh = S_host.numpy()
+            gbps_c, thr, desc, _ = cpu_sample(w, Sh, 1, 1, kind)
+            cpu = dict(value=gbps_c, unit='GBP/s', cores=thr, kind=kind, sample=desc)
+        except Exception as e:  # the baseline is reported, never required
+            log(f'[bench] cpu baseline failed: {type(e).__name__}: {e}')
+
+    value = world * npix * P / (ms * 1e-3) / 1e9
+    launches = chosen._dev.launches()
+    line = dict(
+        metric=METRIC, value=value, unit='GBP/s', n_gpus=world, steps=args.steps, warmup=args.warmup,
+        ms_per_step=ms, higher_is_better=True, scaling='weak', vs_baseline=None,
+        dtype='f32' if modes['chosen'] == 'fp32' else 'f32+bf16x3',
+        data=f'synthetic: {w["n_scatterers"]} seeded scatterers simulated on the GPU in float64, noise -40 dB',
+        config=dict(workload=f'{args.workload}: {P} pulses x {col.K} samples -> {w["nx"]} x {w["ny"]} px at '
+                             f'{w["spx"]} m', final=modes['chosen'], T=plain.T,
+                    levels=[(l['C'], l['Dk'], l['Dp']) for l in plan['levels']],
+                    l2='inputs larger than L2 (1.07 GB history per step), no flush',
+                    parallelism=f'replicas x{world}' if world > 1 else 'single GPU'),
+        err_db=dict(chosen=err_chosen, plain=err_plain, reference='float64 exact backprojection, 64x, linear, '
+                    f'{len(idx)} random pixels, one complex gain fitted'),
+        plain_fp32=dict(value=world * npix * P / (ms_plain * 1e-3) / 1e9, ms_per_step=ms_plain, stages_ms=stages_plain),
+        speedup_vs_plain=ms_plain / ms,
+        stages_ms=dict(zip(names, stages)),
+        roofline=roof,
+        cpu_baseline=cpu,
+        e2e=dict(value=world * npix * P / (ms_e2e * 1e-3) / 1e9, unit='GBP/s', ms_per_step=ms_e2e,
+                 h2d_bytes_per_step=int(S.numel() * 8), d2h_bytes_per_step=int(npix * 8)),
+        gpu_launches=launches * args.steps,
+        clocks=clocks)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_reference(args, world, rank):
+    """The reference arm: its CPU former on this host's cores, rank 0 only."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    ncpu = len(os.sched_getaffinity(0)) if hasattr(os, 'sched_getaffinity') else os.cpu_count()
+    os.environ.setdefault('OMP_NUM_THREADS', str(ncpu))
+    os.environ.setdefault('OMP_PROC_BIND', 'close')
+    os.environ.setdefault('OMP_PLACES', 'cores')
+    import oracle as O
+    kind = 'reference' if O.available('reference') else 'port'
+    import torch
+    from fastsar_b200 import sim
+    torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', '0')))
+    w, S = sim.synthetic_history(args.workload, seed=args.seed)
+    Sh = S.cpu().numpy()
+    del S
+    gbps, thr, desc, t = cpu_sample(w, Sh, args.steps, args.warmup, kind)
+    line = dict(metric=METRIC, value=gbps, unit='GBP/s', n_gpus=world, steps=args.steps, warmup=args.warmup,
+                ms_per_step=t * 1e3, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32',
+                data='synthetic (the same seeded history as the GPU arm)', impl='reference',
+                config=dict(workload=f'{args.workload}: {w["col"].Np} pulses x {w["col"].K} samples -> '
+                                     f'{w["nx"]} x {w["ny"]} px at {w["spx"]} m'),
+                cpu_baseline=dict(value=gbps, unit='GBP/s', cores=thr, kind=kind, sample=desc),
+                e2e=dict(value=gbps, unit='GBP/s', h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == '__main__':
+    main()

@@ -14,7 +14,8 @@ FFBP_FINAL_FP32, FFBP_FINAL_TC_F16, FFBP_FINAL_TC_BF16X3 = 0, 1, 2
 
 # every symbol include/ffbp_b200.h declares
 EXPORTS = ('ffbp_last_error', 'ffbp_abi_version', 'ffbp_plan_create', 'ffbp_plan_destroy', 'ffbp_plan_workspace_bytes',
-           'ffbp_form', 'ffbp_form_timed', 'ffbp_plan_info', 'ffbp_level', 'ffbp_phases', 'ffbp_final')
+           'ffbp_form', 'ffbp_form_timed', 'ffbp_plan_info', 'ffbp_level', 'ffbp_phases', 'ffbp_final',
+           'ffbp_bp_points_f64', 'ffbp_simulate')
 
 _c_int, _c_double, _vp = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
 
@@ -67,6 +68,9 @@ def load():
     L.ffbp_phases.argtypes = [_vp, _c_int, _vp, _c_int, _vp, _c_int, _vp, _c_double, _c_double, _c_int, _vp, _vp]
     L.ffbp_final.argtypes = [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _c_double, _c_double, _c_double,
                              _c_double, _vp, _vp, _vp, _c_double, _vp, _c_int, _vp, _vp]
+    L.ffbp_bp_points_f64.argtypes = [_vp, _c_int, _c_int, _vp, _vp, _vp, _vp, ctypes.c_long, _c_double, _c_double, _vp,
+                                     _vp]
+    L.ffbp_simulate.argtypes = [_vp, _c_int, _c_int, _c_double, _c_double, _vp, _vp, _c_int, _vp, _vp]
     for name in EXPORTS:
         getattr(L, name).restype = _c_int
     _LIB = L

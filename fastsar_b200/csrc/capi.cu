@@ -365,4 +365,28 @@ int ffbp_final(const void *d_d, int B, int Pf, int Qf, int T, const double *d_ux
     return FFBP_OK;
 }
 
+int ffbp_bp_points_f64(const void *d_prof, int P, int nfft, const double *d_tx, const double *d_rcv,
+                       const double *d_ref, const double *d_pts, long N, double inv_dr, double kcyc, void *d_out,
+                       void *stream)
+{
+    if (!d_prof || !d_tx || !d_ref || !d_pts || !d_out) return fail(FFBP_E_ARG, "ffbp_bp_points_f64: null buffer");
+    if (P < 0 || nfft < 2 || N < 0) return fail(FFBP_E_ARG, "ffbp_bp_points_f64: bad size");
+    cudaError_t e = ffbp::launch_bp_points_f64(static_cast<const double2 *>(d_prof), P, nfft, d_tx, d_rcv, d_ref, d_pts,
+                                               N, inv_dr, kcyc, static_cast<double2 *>(d_out),
+                                               static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "ffbp_bp_points_f64");
+    return FFBP_OK;
+}
+
+int ffbp_simulate(const double *d_ant, int P, int K, double fmin, double df, const double *d_pos, const void *d_amp,
+                  int N, void *d_S, void *stream)
+{
+    if (!d_ant || !d_pos || !d_amp || !d_S) return fail(FFBP_E_ARG, "ffbp_simulate: null buffer");
+    if (P < 1 || K < 1 || N < 0) return fail(FFBP_E_ARG, "ffbp_simulate: bad size");
+    cudaError_t e = ffbp::launch_simulate(d_ant, P, K, fmin, df, d_pos, static_cast<const double2 *>(d_amp), N,
+                                          static_cast<float2 *>(d_S), static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "ffbp_simulate");
+    return FFBP_OK;
+}
+
 }  // extern "C"

@@ -50,4 +50,11 @@ struct FinalLaunch {
 cudaError_t launch_final_fp32(const FinalLaunch &F, cudaStream_t s, const char **why);
 cudaError_t launch_final_tc(const FinalLaunch &F, int mode, cudaStream_t s, const char **why);
 
+// Exact backprojection at points in float64 and the phase-history synthesis (exact.cu).
+cudaError_t launch_bp_points_f64(const double2 *prof, int P, int nfft, const double *tx, const double *rcv,
+                                 const double *ref, const double *pts, long N, double inv_dr, double kcyc, double2 *out,
+                                 cudaStream_t s);
+cudaError_t launch_simulate(const double *ant, int P, int K, double fmin, double df, const double *pos,
+                            const double2 *amp, int N, float2 *S, cudaStream_t s);
+
 }  // namespace ffbp

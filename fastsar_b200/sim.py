@@ -195,4 +195,59 @@ def workload(name):
         col = spotlight(4096, 4096, 9.6e9, 300e6, 600e3, 45.0, 1.5)
         return dict(col=col, nx=2048, ny=2048, spx=0.25, spy=0.25, e1=e1, e2=e2,
                     scene=dict(n_points=32, clutter_db=-30.0, noise_db=-40.0, extent=(400.0, 400.0)))
+    if name == 'spotlight_12k_strip':
+        # the spotlight_12k collection formed to a quarter of its azimuth extent: the same level shapes per parent
+        # on about a quarter of the device memory (the profiling case of the level and final kernels)
+        w = workload('spotlight_12k')
+        w.update(nx=3072, scene=dict(w['scene'], n_points=500, extent=(600.0, 1800.0)))
+        return w
     raise ValueError(f'unknown workload {name!r}')
+
+
+def simulate(col, pos, amp, out=None, device=None, chunk=65536):
+    """Phase history [P, K] complex64 on the GPU (a torch tensor) by the direct sum over scatterers, float64 ranges
+    and phases, through ffbp_simulate (fastsar/sim.py:69-90 computes the same sum with a NUFFT). out: a tensor to add
+    into (default zeros)."""
+    import torch
+    from . import _lib
+    L = _lib.load()
+    dev = torch.device('cuda', torch.cuda.current_device() if device is None else device)
+    P, K = col.Np, col.K
+    if out is None:
+        out = torch.zeros((P, K), dtype=torch.complex64, device=dev)
+    ant = torch.from_numpy(np.ascontiguousarray(col.ant, np.float64)).to(dev)
+    pos = np.ascontiguousarray(pos, np.float64)
+    amp = np.ascontiguousarray(amp, np.complex128)
+    s = torch.cuda.current_stream(dev).cuda_stream
+    for n0 in range(0, len(amp), chunk):
+        p_ = torch.from_numpy(pos[n0:n0 + chunk]).to(dev)
+        a_ = torch.from_numpy(amp[n0:n0 + chunk]).to(dev)
+        _lib.check(L.ffbp_simulate(ant.data_ptr(), P, K, float(col.fmin), float(col.df), p_.data_ptr(), a_.data_ptr(),
+                                   len(a_), out.data_ptr(), s), 'ffbp_simulate')
+    return out
+
+
+def synthetic_history(name, seed=0, device=None, n_clutter=None):
+    """The seeded synthetic history of a named workload (workload()) on the GPU: its scene simulated by `simulate`,
+    plus complex Gaussian noise at the stated level per sample relative to a unit target. -> (workload dict, S)."""
+    import torch
+    w = workload(name)
+    col, sc = w['col'], w['scene']
+    rng = np.random.default_rng(seed)
+    ex, ey = sc['extent']
+    res = (C / (2.0 * (col.K * col.df)), C / (2.0 * (col.fmin + col.K / 2 * col.df)) /
+           (2.0 * np.arctan(0.5 * np.ptp(col.ant[:, 1]) / np.abs(col.ant[0, 0]))))
+    kw = dict(n_points=sc['n_points'], rcs_sigma_db=sc.get('rcs_sigma_db', 0.0), n_corners=sc.get('n_corners', 0),
+              clutter_db=sc.get('clutter_db'), res=res, col=col, fill=1.0)
+    if n_clutter is not None:
+        kw['max_clutter'] = n_clutter
+    pos, amp = scene(rng, ex / w['spx'], ey / w['spy'], w['spx'], w['spy'], w['e1'], w['e2'], **kw)
+    dev = torch.device('cuda', torch.cuda.current_device() if device is None else device)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    sigma = 10.0 ** (sc['noise_db'] / 20.0)
+    S = (torch.randn((col.Np, col.K, 2), device=dev, generator=g, dtype=torch.float32) * (sigma / np.sqrt(2.0)))
+    S = torch.view_as_complex(S).contiguous()
+    simulate(col, pos, amp, out=S, device=dev)
+    w = dict(w, n_scatterers=len(amp))
+    return w, S

@@ -149,6 +149,23 @@ int ffbp_final(const void *d_d, int B, int Pf, int Qf, int T, const double *d_ux
                double spy, double a0, double a1, const double *d_ucx, const double *d_ucy, const double *d_rc,
                double fc2, const float *d_w, int mode, void *d_out, void *stream);
 
+/* ---- exact backprojection and synthesis (the oracle family, on the device) ----------------------------------- */
+
+/* Exact backprojection at N points in float64 (fastsar/bp.py:99-137 bp_points, with float64 profiles): for each point
+ * and pulse p, dR = |x - tx[p]| (+ |x - rcv[p]| halved, when d_rcv is not NULL) - ref[p], the profile read at bin
+ * dR inv_dr + nfft/2 by linear interpolation, circularly, times exp(2 pi i kcyc dR), accumulated into d_out.
+ * d_prof [P, nfft] complex128 range profiles (fastsar/bp.py:55-63 range_compress); d_tx, d_rcv [P, 3], d_ref [P],
+ * d_pts [N, 3] float64; d_out [N] complex128 (added to).                                                          */
+int ffbp_bp_points_f64(const void *d_prof, int P, int nfft, const double *d_tx, const double *d_rcv,
+                       const double *d_ref, const double *d_pts, long N, double inv_dr, double kcyc, void *d_out,
+                       void *stream);
+
+/* Phase history of point scatterers (fastsar/sim.py:69-90 simulate, as a direct sum): d_S [P, K] complex64 +=
+ * sum_n amp[n] exp(-4 pi i (fmin + k df) dR_pn / c), dR_pn = |pos[n] - ant[p]| - |ant[p]|. Ranges and phases in
+ * float64, the sum in float64 per sample. d_ant [P, 3], d_pos [N, 3] float64; d_amp [N] complex128.               */
+int ffbp_simulate(const double *d_ant, int P, int K, double fmin, double df, const double *d_pos, const void *d_amp,
+                  int N, void *d_S, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -225,7 +225,9 @@ def make_ffbp(plan, coll, kind='port', wf=None):
 
     ox, oy, nx, ny = plan['ox'], plan['oy'], plan['nx'], plan['ny']
 
-    def form(S, ng=8):
+    def form(S, ng=8, children=None):
+        """children: the level-0 children to form (default all); the others' pixels are left zero (a bounded
+        sample of the image's work, which scales with the number of children)."""
         S = np.asarray(S)
         lv0, la0 = levels[0], coll['levels'][0]
         if S.dtype == np.complex64 and S.flags.c_contiguous and lv0['Dk'] > 1:
@@ -233,9 +235,10 @@ def make_ffbp(plan, coll, kind='port', wf=None):
         else:
             pre = np.ascontiguousarray(S.real, np.float32)[None]
             pim = np.ascontiguousarray(S.imag, np.float32)[None]
-        full = np.empty((plan['Nx'], plan['Ny']), np.complex64)
-        for g0 in range(0, G, ng):
-            gs = list(range(g0, min(G, g0 + ng)))
+        full = np.zeros((plan['Nx'], plan['Ny']), np.complex64)
+        todo = list(range(G)) if children is None else sorted(children)
+        for g0 in range(0, len(todo), ng):
+            gs = todo[g0:g0 + ng]
             A, Bm = _children(L, pre, pim, la0['c0'][0, gs][None], la0['slope'][0, gs][None], lv0)
             for k, g in enumerate(gs):
                 re, im = one_tile(A[k], Bm[k], g)
@@ -271,14 +274,27 @@ def image_former(ant, fmin, df, K, nx, ny, spx, spy, e1=(1.0, 0.0, 0.0), e2=(0.0
     P = ant.shape[0]
     wp, wk = window(P, K) if window_on else (None, None)
 
-    def form(S, ng=8):
+    def form(S, ng=8, children=None):
         S = np.asarray(S)
         if window_on:
             S = (S * (wp[:, None] * wk[None, :]).astype(np.float32)).astype(np.complex64)
         else:
             S = S.astype(np.complex64)
-        return inner(np.ascontiguousarray(S), ng)
+        return inner(np.ascontiguousarray(S), ng, children)
     return form, plan
+
+
+def children_pixels(plan, children):
+    """Pixels of the cropped image that the given level-0 children form."""
+    sx0, sy0 = plan['levels'][0]['sx'], plan['levels'][0]['sy']
+    mx, my = plan['Nx'] // sx0, plan['Ny'] // sy0
+    n = 0
+    for g in children:
+        x, y = g // sy0, g % sy0
+        x0, x1 = max(x * mx, plan['ox']), min((x + 1) * mx, plan['ox'] + plan['nx'])
+        y0, y1 = max(y * my, plan['oy']), min((y + 1) * my, plan['oy'] + plan['ny'])
+        n += max(0, x1 - x0) * max(0, y1 - y0)
+    return n
 
 
 # ------------------------------------------------------------------------------------------------ FP64 exact BP
