@@ -211,7 +211,7 @@ def simulate(col, pos, amp, out=None, device=None, chunk=65536):
     import torch
     from . import _lib
     L = _lib.load()
-    dev = torch.device('cuda', torch.cuda.current_device() if device is None else device)
+    dev = device if isinstance(device, torch.device) else torch.device('cuda', torch.cuda.current_device() if device is None else device)
     P, K = col.Np, col.K
     if out is None:
         out = torch.zeros((P, K), dtype=torch.complex64, device=dev)
@@ -242,7 +242,7 @@ def synthetic_history(name, seed=0, device=None, n_clutter=None):
     if n_clutter is not None:
         kw['max_clutter'] = n_clutter
     pos, amp = scene(rng, ex / w['spx'], ey / w['spy'], w['spx'], w['spy'], w['e1'], w['e2'], **kw)
-    dev = torch.device('cuda', torch.cuda.current_device() if device is None else device)
+    dev = device if isinstance(device, torch.device) else torch.device('cuda', torch.cuda.current_device() if device is None else device)
     g = torch.Generator(device=dev)
     g.manual_seed(seed)
     sigma = 10.0 ** (sc['noise_db'] / 20.0)

@@ -37,5 +37,3 @@ def test_fp64_backprojection_matches_oracle(golden, oracle_lib, bistatic):
     e = oracle_lib.err_db(got, ref)
     print(f'fp64 BP (bistatic={bistatic}): {e:.1f} dB against the oracle')
     assert e < -120.0
-    if not bistatic:
-        assert oracle_lib.err_db(got, g['bp64']) < -100.0            # and the reference's own 64x backprojection
