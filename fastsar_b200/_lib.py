@@ -15,7 +15,7 @@ FFBP_FINAL_FP32, FFBP_FINAL_TC_F16, FFBP_FINAL_TC_BF16X3 = 0, 1, 2
 # every symbol include/ffbp_b200.h declares
 EXPORTS = ('ffbp_last_error', 'ffbp_abi_version', 'ffbp_plan_create', 'ffbp_plan_destroy', 'ffbp_plan_workspace_bytes',
            'ffbp_form', 'ffbp_form_timed', 'ffbp_plan_info', 'ffbp_level', 'ffbp_phases', 'ffbp_final',
-           'ffbp_bp_points_f64', 'ffbp_simulate')
+           'ffbp_bp_points_f64', 'ffbp_simulate', 'ffbp_form_static')
 
 _c_int, _c_double, _vp = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
 
@@ -61,6 +61,7 @@ def load():
     L.ffbp_plan_destroy.argtypes = [_vp]
     L.ffbp_plan_workspace_bytes.argtypes = [_vp, ctypes.POINTER(ctypes.c_size_t)]
     L.ffbp_form.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_size_t, _vp, ctypes.POINTER(_c_int)]
+    L.ffbp_form_static.argtypes = [_vp, _vp, _vp, _vp, ctypes.POINTER(_c_int)]
     L.ffbp_form_timed.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_size_t, _vp, ctypes.POINTER(ctypes.c_float), _c_int]
     L.ffbp_plan_info.argtypes = [_vp, ctypes.POINTER(_c_int), ctypes.POINTER(_c_int)]
     L.ffbp_level.argtypes = [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_int, _c_double,

@@ -390,3 +390,18 @@ int ffbp_simulate(const double *d_ant, int P, int K, double fmin, double df, con
 }
 
 }  // extern "C"
+
+namespace ffbp {
+
+// ffbp_form on a workspace the caller names, for the entry points of other translation units.
+int form_on_workspace(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, size_t ws_bytes, void *stream, int *h_bad)
+{
+    return form_impl(p, d_S, d_img, d_ws, ws_bytes, stream, h_bad, nullptr, 0);
+}
+
+int set_error(int code, const char *msg)
+{
+    return fail(code, "%s", msg);
+}
+
+}  // namespace ffbp

@@ -110,6 +110,16 @@ int ffbp_plan_workspace_bytes(const ffbp_plan *plan, size_t *bytes);
 int ffbp_form(ffbp_plan *plan, const void *d_S, void *d_img, void *d_ws, size_t ws_bytes, void *stream,
               int *h_bad_pulse);
 
+/* ffbp_form without a caller-allocated workspace, for callers that cannot allocate device memory when they form an
+ * image (a device pool they do not control, a real-time loop that must not enter the CUDA allocator). No counterpart
+ * in the reference. The scratch is a static device array of this library, FFBP_STATIC_WS_BYTES (64 MiB), held by
+ * every GPU that loads the library until the process exits; a plan whose ffbp_plan_workspace_bytes exceeds it is
+ * rejected with FFBP_E_WORKSPACE. The call allocates nothing. Its first call on a device looks the array's device
+ * address up (cudaGetSymbolAddress, with that device current), so make that first call before any stream capture.
+ * All calls share the array: calls whose work overlaps on the GPU race and must not be made.                    */
+#define FFBP_STATIC_WS_BYTES (64u << 20)
+int ffbp_form_static(ffbp_plan *plan, const void *d_S, void *d_img, void *stream, int *h_bad_pulse);
+
 /* ffbp_form with the device time of each launch (the reference's CUDA-event stage timers, fastsar/ffbp_cuda.py:
  * 635-652 PROFILE): stage_ms[l] for level l < nlev and stage_ms[nlev] for the final stage, measured by CUDA events
  * recorded on `stream` around each launch. Waits for the stream. n_stage: the length of stage_ms (>= nlev + 1).    */
