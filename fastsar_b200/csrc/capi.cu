@@ -245,6 +245,7 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
     float2 *bufA = reinterpret_cast<float2 *>(ws + 256);
     float2 *bufB = reinterpret_cast<float2 *>(ws + 256 + align256(p->bufA * sizeof(float2)));
     cudaError_t e = cudaMemsetAsync(bad, 0x7f, sizeof(int), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(bad + 1, 0, sizeof(int), s);
     if (e != cudaSuccess) return cuda_fail(e, "status reset");
     const bool timed = stage_ms != nullptr;
     if (timed && n_stage < p->nlev + 1) return fail(FFBP_E_ARG, "stage_ms holds %d entries, %d needed", n_stage, p->nlev + 1);
@@ -276,7 +277,7 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
     F.d = in; F.B = p->ntiles; F.Pf = p->Pf; F.Qf = p->Qf; F.T = p->T; F.ux = p->ux; F.uy = p->uy;
     F.spx = p->spx; F.spy = p->spy; F.a0 = p->a0; F.a1 = p->a1; F.fc2 = p->fc2; F.ucx = p->ucx; F.ucy = p->ucy;
     F.rc = p->rc; F.w = p->wf; F.tiles = nullptr; F.img = static_cast<float2 *>(d_img); F.first = p->first;
-    F.nx = p->nx; F.ny = p->ny; F.ox = p->ox; F.oy = p->oy; F.scale = 1.f;
+    F.nx = p->nx; F.ny = p->ny; F.ox = p->ox; F.oy = p->oy; F.scale = 1.f; F.err = bad + 1;
     const char *why = nullptr;
     e = p->final_mode == FFBP_FINAL_FP32 ? ffbp::launch_final_fp32(F, s, &why) : ffbp::launch_final_tc(F, p->final_mode, s, &why);
     if (why) { destroy_events(); return fail(FFBP_E_UNSUPPORTED, "final stage: %s", why); }
@@ -288,10 +289,11 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
         destroy_events();
     }
     if (h_bad) {
-        int v = 0;
-        if ((e = cudaMemcpyAsync(&v, bad, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return cuda_fail(e, "status read");
+        int v[2] = {0, 0};
+        if ((e = cudaMemcpyAsync(v, bad, 2 * sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return cuda_fail(e, "status read");
         if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "form");
-        *h_bad = (v == 0x7f7f7f7f) ? -1 : v;
+        *h_bad = (v[0] == 0x7f7f7f7f) ? -1 : v[0];
+        if (v[1]) return fail(FFBP_E_CUDA, "the tensor-core final stage stopped waiting on its pipeline (a bounded wait ran out)");
     }
     return FFBP_OK;
 }

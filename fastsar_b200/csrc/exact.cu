@@ -7,8 +7,8 @@
 //                The profiles are the caller's (a zero-padded inverse FFT per pulse: cuFFT through torch).
 // simulate       the phase history of point scatterers, S[p, k] += sum_n a_n exp(-2 pi i (2 f_k / c) dR_pn),
 //                dR_pn = |x_n - ant_p| - |ant_p| (the CPHD convention, fastsar/sim.py:1-8): ranges and phases in
-//                float64, the sine and cosine in float32 of the float64-reduced phase, the sum over each chunk of
-//                256 scatterers in float32 and over the chunks in float64.
+//                float64 per thread's run of 8 samples, a float32 complex recurrence along the run, the sum over
+//                each chunk of 256 scatterers in float32 and over the chunks in float64.
 #include "common.cuh"
 
 namespace ffbp {
@@ -51,54 +51,80 @@ __global__ void bp_points_f64_kernel(const double2 *__restrict__ prof, int P, in
 }
 
 constexpr int SIM_NT = 256;
+constexpr int SIM_RUN = 8;                               // consecutive samples per thread
 
+// One block: pulse p, SIM_NT * SIM_RUN consecutive samples. Per scatterer the block stages in shared memory the
+// phase at its first sample (float64, reduced) and the per-sample step (float64 phase, its phasor in float32); each
+// thread seeds its run's phasor from the float64 phase of its first sample and advances it by the step's phasor
+// across its SIM_RUN samples (a complex recurrence of SIM_RUN - 1 steps: about 1e-6 relative).
 __global__ void __launch_bounds__(SIM_NT) simulate_kernel(const double *__restrict__ ant, int P, int K, double fmin,
                                                           double df, const double *__restrict__ pos,
                                                           const double2 *__restrict__ amp, int N,
                                                           float2 *__restrict__ S)
 {
     __shared__ double s_ph[SIM_NT], s_st[SIM_NT];
+    __shared__ float2 s_w[SIM_NT];
     __shared__ double2 s_a[SIM_NT];
-    const int nkb = (K + SIM_NT - 1) / SIM_NT;
+    const int span = SIM_NT * SIM_RUN;
+    const int nkb = (K + span - 1) / span;
     const int p = blockIdx.x / nkb;
-    const int k0 = (blockIdx.x % nkb) * SIM_NT;
+    const int k0 = (blockIdx.x % nkb) * span;
     const int t = threadIdx.x;
     const double ax = ant[3 * p], ay = ant[3 * p + 1], az = ant[3 * p + 2];
     const double r0 = sqrt(ax * ax + ay * ay + az * az);
     const double two_c = 2.0 / C_LIGHT;
-    double sr = 0.0, si = 0.0;
+    double sr[SIM_RUN], si[SIM_RUN];
+#pragma unroll
+    for (int j = 0; j < SIM_RUN; ++j) sr[j] = si[j] = 0.0;
     for (int n0 = 0; n0 < N; n0 += SIM_NT) {
         const int n = n0 + t;
         if (n < N) {
             const double dx = pos[3 * n] - ax, dy = pos[3 * n + 1] - ay, dz = pos[3 * n + 2] - az;
             const double dR = sqrt(dx * dx + dy * dy + dz * dz) - r0;
-            double ph = -two_c * (fmin + k0 * df) * dR;     // cycles at this block's first sample
-            double st = -two_c * df * dR;                   // cycles per sample
+            const double ph = -two_c * (fmin + k0 * df) * dR;     // cycles at this block's first sample
+            double st = -two_c * df * dR;                         // cycles per sample
+            st -= rint(st);
             s_ph[t] = ph - rint(ph);
-            s_st[t] = st - rint(st);
+            s_st[t] = st;
+            float sn, cs;
+            sincospif(2.f * (float)st, &sn, &cs);
+            s_w[t] = make_float2(cs, sn);
             s_a[t] = amp[n];
         } else {
-            s_ph[t] = 0.0; s_st[t] = 0.0; s_a[t] = make_double2(0.0, 0.0);
+            s_ph[t] = 0.0; s_st[t] = 0.0; s_w[t] = make_float2(1.f, 0.f); s_a[t] = make_double2(0.0, 0.0);
         }
         __syncthreads();
         const int nn = min(SIM_NT, N - n0);
-        float cr = 0.f, ci = 0.f;                          // this chunk's sum in float32, then added in float64
+        float cr[SIM_RUN], ci[SIM_RUN];
+#pragma unroll
+        for (int j = 0; j < SIM_RUN; ++j) cr[j] = ci[j] = 0.f;
         for (int m = 0; m < nn; ++m) {
-            double ph = fma((double)t, s_st[m], s_ph[m]);
-            const float2 e = cis_reduced((float)(ph - rint(ph)));
+            const double ph = fma((double)(SIM_RUN * t), s_st[m], s_ph[m]);
+            float sn, cs;
+            sincospif(2.f * (float)(ph - rint(ph)), &sn, &cs);
+            const float2 st = s_w[m];
             const double2 a = s_a[m];
-            const float axf = (float)a.x, ayf = (float)a.y;
-            cr = fmaf(axf, e.x, fmaf(-ayf, e.y, cr));
-            ci = fmaf(axf, e.y, fmaf(ayf, e.x, ci));
+            float wr = (float)a.x * cs - (float)a.y * sn, wi = (float)a.x * sn + (float)a.y * cs;
+#pragma unroll
+            for (int j = 0; j < SIM_RUN; ++j) {
+                cr[j] += wr;
+                ci[j] += wi;
+                const float nr = wr * st.x - wi * st.y;
+                wi = wr * st.y + wi * st.x;
+                wr = nr;
+            }
         }
-        sr += cr;
-        si += ci;
+#pragma unroll
+        for (int j = 0; j < SIM_RUN; ++j) { sr[j] += cr[j]; si[j] += ci[j]; }
         __syncthreads();
     }
-    const int k = k0 + t;
-    if (k < K) {
-        const float2 o = S[(size_t)p * K + k];
-        S[(size_t)p * K + k] = make_float2(o.x + (float)sr, o.y + (float)si);
+#pragma unroll
+    for (int j = 0; j < SIM_RUN; ++j) {
+        const int k = k0 + SIM_RUN * t + j;
+        if (k < K) {
+            const float2 o = S[(size_t)p * K + k];
+            S[(size_t)p * K + k] = make_float2(o.x + (float)sr[j], o.y + (float)si[j]);
+        }
     }
 }
 
@@ -118,7 +144,7 @@ cudaError_t launch_simulate(const double *ant, int P, int K, double fmin, double
                             const double2 *amp, int N, float2 *S, cudaStream_t s)
 {
     if (P <= 0 || K <= 0 || N <= 0) return cudaSuccess;
-    const long nb = (long)((K + SIM_NT - 1) / SIM_NT) * P;
+    const long nb = (long)((K + SIM_NT * SIM_RUN - 1) / (SIM_NT * SIM_RUN)) * P;
     if (nb > 0x7fffffffL) return cudaErrorInvalidValue;
     simulate_kernel<<<(unsigned)nb, SIM_NT, 0, s>>>(ant, P, K, fmin, df, pos, amp, N, S);
     return cudaGetLastError();

@@ -46,6 +46,7 @@ struct FinalLaunch {
     const int2 *first;    // [B] first pixel of each tile on the padded grid
     int nx, ny, ox, oy;
     float scale;
+    int *err = nullptr;   // set to 1 by a kernel whose bounded wait ran out (tensor-core stage), or null
 };
 cudaError_t launch_final_fp32(const FinalLaunch &F, cudaStream_t s, const char **why);
 cudaError_t launch_final_tc(const FinalLaunch &F, int mode, cudaStream_t s, const char **why);

@@ -250,3 +250,61 @@ def test_torch_input_matches_numpy(golden):
     a = f(g['S'])
     b = f.form_device(torch.from_numpy(g['S']).cuda()).cpu().numpy()
     assert np.array_equal(a, b)
+
+
+# ------------------------------------------------------------------------------------------------ tensor-core final
+
+@pytest.mark.parametrize('mode,tol', [(2, 2e-4), (1, 3e-3)], ids=['bf16x3', 'f16'])
+@pytest.mark.parametrize('weighted', [False, True])
+@pytest.mark.parametrize('shape', [(5, 13, 57), (300, 7, 96), (3, 40, 130)], ids=['small', 'many-tiles', 'long-q'])
+def test_final_tensor_cores_match_oracle(lib, oracle_lib, mode, tol, weighted, shape):
+    """The tcgen05 final stage (T = 32) against the float64 oracle: three bfloat16 products within 2e-4, one
+    float16 product within 3e-3 (its operands carry 11 bits); tiles beyond one per multiprocessor, padding of Qf to
+    a multiple of 16, aperture weights."""
+    T = 32
+    rng = np.random.default_rng(7 * mode + weighted + shape[0])
+    B, Pf, Qf = shape
+    d = (rng.standard_normal((B, Pf, Qf)) + 1j * rng.standard_normal((B, Pf, Qf))).astype(np.complex64)
+    ux, uy = rng.uniform(-0.9, 0.9, (B, Pf)), rng.uniform(-0.9, 0.9, (B, Pf))
+    spx, spy = 0.3, 0.45
+    a0, a1, fc2 = 64.1, 0.013, 64.4
+    ucx, ucy, rc = rng.uniform(-0.5, 0.5, B), rng.uniform(-0.5, 0.5, B), rng.uniform(4e3, 6e3, B)
+    w = np.stack([rng.uniform(0.5, 1.5, (B, Pf)), rng.uniform(-0.01, 0.01, (B, Pf)),
+                  rng.uniform(-0.01, 0.01, (B, Pf))]).astype(np.float32) if weighted else None
+    L = lib.load()
+    out = torch.zeros((B, T, T), dtype=torch.complex64, device='cuda')
+    dd = [_dev(a) for a in (d, ux, uy, ucx, ucy, rc)]
+    dw = _dev(w) if weighted else None
+    lib.check(L.ffbp_final(dd[0].data_ptr(), B, Pf, Qf, T, dd[1].data_ptr(), dd[2].data_ptr(), spx, spy, a0, a1,
+                           dd[3].data_ptr(), dd[4].data_ptr(), dd[5].data_ptr(), fc2, lib.tptr(dw), mode,
+                           out.data_ptr(), torch.cuda.current_stream().cuda_stream), 'ffbp_final')
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    O = oracle_lib.lib('port')
+    dlx = (np.arange(T) - (T - 1) / 2.0) * spx
+    dly = (np.arange(T) - (T - 1) / 2.0) * spy
+    ore = np.zeros((B, T, T), np.float32)
+    oim = np.zeros_like(ore)
+    wp = [None] * 3 if w is None else [np.ascontiguousarray(x) for x in w]
+    O.final_tiles(np.ascontiguousarray(d.real), np.ascontiguousarray(d.imag), B, Pf, Qf, T, ux, uy, dlx, dly, a0, a1,
+                  ucx, ucy, rc, fc2, ore, oim, *[None if x is None else x.ctypes.data for x in wp])
+    e = _rel(got, ore + 1j * oim)
+    print(f'tensor-core final mode {mode} {shape} weighted={weighted}: rel {e:.2e}')
+    assert e < tol, e
+
+
+@pytest.mark.parametrize('precision,final,bar', [('float32', 'tc3', -70.0), ('float16', 'fp32', -60.0)])
+def test_image_tensor_cores_match_reference(golden, oracle_lib, monkeypatch, precision, final, bar):
+    """The 512-pulse spotlight (T = 32) with the tensor-core final stage against the reference former's image: three
+    bfloat16 products within the -70 dB parity bar; one float16 product within -60 dB."""
+    from fastsar_b200 import ImageFormer, sim
+    monkeypatch.setenv('FASTSAR_FINAL', final)
+    g = golden('image_spot512')
+    w = sim.workload('spotlight_512')
+    col = w['col']
+    f = ImageFormer(col.ant, col.fmin, col.df, col.K, 512, 512, 0.25, 0.25, w['e1'], w['e2'], precision=precision)
+    img = f(g['S'])
+    e = oracle_lib.err_db(img, g['ffbp'])
+    e64 = oracle_lib.rel_db(img.ravel()[g['bp64_idx']], g['bp64'])
+    print(f'{precision}/{final}: {e:.1f} dB vs reference former; {e64:.1f} dB vs float64 BP 64x')
+    assert e < bar
