@@ -6,21 +6,27 @@
 // As one real product, D = [Ar; Ai] [Br; Bi]^T (64 x 64, K = Pf Qfp with Qf padded to a multiple of 16 by zeros):
 // re = D[i][j] - D[i+32][j+32], im = D[i][j+32] + D[i+32][j].
 //
-// Block roles (persistent over tiles; one block per SM):
-//   warps 5..12  producers: per final subaperture they build A' and B' (64 rows x Qfp) in shared memory, a row's
-//                ramp by a complex recurrence along q seeded in float64, converted to the MMA operand type, into a
-//                ring of S stages (K-major, no swizzle: core matrices of 8 rows x 16 bytes);
-//   warp 4       one thread issues tcgen05.mma (M = 64, N = 64, K = 16) from each stage into a TMEM accumulator
-//                and commits to the stage's "empty" barrier; after a tile's last stage it commits to the
-//                accumulator's "full" barrier. The warp allocates two 64-column accumulators (128 TMEM columns);
-//   warps 0..3   epilogue: reads the accumulator (rows 16w..16w+15 sit in TMEM lanes 32w..32w+15), releases it,
-//                combines re/im through shared memory, applies the quadratic phase and writes the tile into the
-//                image (cropped).
-// Operand types: FFBP_FINAL_TC_F16 one float16 product; FFBP_FINAL_TC_BF16X3 three bfloat16 products
-// (hi hi + hi lo + lo hi, with x = hi + lo), float32 accumulation in both.
+// One MMA is M = 128, N = 128, K = 16, and a "unit" is what one accumulator holds:
+//   FFBP_FINAL_TC_BF16X3  one tile, operands split x = hi + lo in bfloat16: A' = [A_hi; A_lo], B' = [B_hi; B_lo], so
+//                         one product gives hi hi, hi lo, lo hi and lo lo of the tile, summed in the epilogue;
+//   FFBP_FINAL_TC_F16     two tiles in float16, A' = [A_1; A_2], B' = [B_1; B_2]: the two diagonal 64 x 64 blocks
+//                         of the product are the tiles.
+// The per-instruction issue cost of tcgen05.mma is the same for a 64 x 64 and a 128 x 128 product, so the larger
+// shape does two or four times the work per instruction; two issuing warps double the rate again.
+//
+// Block roles (persistent over units; one block per SM):
+//   warps 6..17  producers: per final subaperture they build A' and B' (128 rows x Qfp each) in shared memory, a
+//                row's ramp by a complex recurrence along q seeded in float64, converted to the operand type, into a
+//                ring of S stages (K-major, no swizzle: core matrices of 8 rows x 16 bytes). Each warp stages the
+//                samples and geometry it needs RS - 1 stages ahead with cp.async into its own ring;
+//   warps 4, 5   one thread each issues tcgen05.mma: warp 4 + k takes the final subapertures p = k mod 2 of every
+//                unit into its own accumulator (two 128-column accumulators per issuer, 512 TMEM columns), commits
+//                each stage to the stage's "empty" barrier and the unit to the accumulator's "full" barrier;
+//   warps 0..3   epilogue: sum the issuers' accumulators (and, for bfloat16, the four split products), combine
+//                re/im through shared memory, apply the quadratic phase and write the tile into the image (cropped).
 //
 // Every wait on a barrier is bounded: a wait that runs out sets *err (when given) and the block winds down without
-// touching the barrier again; the MMA thread drains its MMAs (bounded) before the accumulator columns are freed.
+// touching the barrier again; each issuing thread drains its MMAs (bounded) before the accumulator columns are freed.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -32,10 +38,18 @@ namespace ffbp {
 namespace {
 
 constexpr int TT = 32;                     // tile side
-constexpr int NTHREADS = 13 * 32;          // 4 epilogue warps, 1 MMA warp, 8 producer warps
-constexpr int PRODUCER0 = 5 * 32;
-constexpr int NPROD = 8 * 32;
-constexpr long WAIT_LIMIT = 1L << 24;      // polls of a barrier before it counts as stuck
+constexpr int NEPI = 4;                    // epilogue warps 0..3 (TMEM lane quarters 0..3)
+constexpr int NISS = 2;                    // MMA issuing warps 4, 5
+constexpr int NPW = 12;                    // producer warps 6..17
+constexpr int PW0 = NEPI + NISS;
+constexpr int NTHREADS = (NEPI + NISS + NPW) * 32;
+constexpr int RS = 8;                      // depth of each producer warp's staging ring (a power of 2)
+constexpr int SLOT_BYTES = 160;            // staging of one warp item: 16 float2 samples, u (double), 3 weights
+constexpr int TMEM_COLS = 512;             // NISS issuers x 2 accumulators x 128 columns
+constexpr uint64_t WAIT_NS = 2000000000ull;   // a barrier that has not completed after 2 s counts as stuck
+constexpr uint32_t PRODUCER_HINT_NS = 1000;   // suspend-time hints of the waits: producers on a free stage,
+constexpr uint32_t ISSUER_HINT_NS = 0;        // the issuers poll without one,
+constexpr uint32_t EPILOGUE_HINT_NS = 4000;   // the epilogue on a finished accumulator
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -57,13 +71,36 @@ __device__ __forceinline__ uint32_t mbar_test(uint64_t *bar, uint32_t parity)
     return done;
 }
 
-// Bounded wait for the phase of parity `parity` of *bar; false (and the block's abort flag and *err set) when it
-// does not complete, or when another thread of the block has aborted.
+__device__ __forceinline__ uint32_t mbar_test_sleep(uint64_t *bar, uint32_t parity, uint32_t hint_ns)
+{
+    // the thread may be suspended until the phase completes or about hint_ns have passed
+    uint32_t done;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+                 : "=r"(done) : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns) : "memory");
+    return done;
+}
+
+__device__ __forceinline__ uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait for the phase of parity `parity` of *bar: false (and the block's abort flag and *err set) when it
+// has not completed after WAIT_NS of wall time, or when another thread of the block has aborted. HINT_NS is the
+// suspend-time hint of each poll (0: poll without one).
+template <uint32_t HINT_NS>
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort, int *err)
 {
-    for (long it = 0; it < WAIT_LIMIT; ++it) {
-        if (mbar_test(bar, parity)) return true;
-        if (*abort) return false;
+    if (mbar_test(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (uint32_t it = 1;; ++it) {
+        if (HINT_NS ? mbar_test_sleep(bar, parity, HINT_NS) : mbar_test(bar, parity)) return true;
+        if ((it & 255u) == 0) {
+            if (*abort) return false;
+            if (global_ns() - t0 > WAIT_NS) break;
+        }
     }
     *abort = 1;
     if (err) atomicExch(err, 1);
@@ -91,21 +128,29 @@ __device__ __forceinline__ void mma_commit(uint64_t *bar)
                  :: "r"(smem_u32(bar)) : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t addr, float *v)
+// 16 consecutive accumulator columns of this thread's TMEM lane, without waiting
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t *r)
 {
-    uint32_t r[16];
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
                  : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
                    "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
                  : "r"(addr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// bytes = 4 or 8; the copy of an invalid element reads nothing and zero-fills the destination
+__device__ __forceinline__ void cp_async(uint32_t dst, const void *src, int bytes, bool valid)
+{
+    if (bytes == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" :: "r"(dst), "l"(src), "r"(valid ? 8 : 0) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" :: "r"(dst), "l"(src), "r"(valid ? 4 : 0) : "memory");
 }
 
 struct TcArgs {
     const float2 *__restrict__ d;
-    int B, Pf, Qf, Qfp, S, parts;
+    int B, Pf, Qf, Qfp, S, nunits, nis;
     const double *__restrict__ ux;
     const double *__restrict__ uy;
     double spx, spy, a0, a1, fc2;
@@ -121,15 +166,7 @@ struct TcArgs {
     int *err;
 };
 
-__device__ __forceinline__ float2 cis_acc(double cyc)
-{
-    const float f = (float)(cyc - rint(cyc));
-    float s, c;
-    sincospif(2.f * f, &s, &c);
-    return make_float2(c, s);
-}
-
-// 8 values -> 16 bytes of operand: float16, or bfloat16 high parts (lo = nullptr) and low parts
+// 8 values -> 16 bytes of operand: float16, or bfloat16 high parts (and the low parts in lo)
 template <bool BF>
 __device__ __forceinline__ void pack8(const float *v, uint4 &hi, uint4 &lo)
 {
@@ -152,35 +189,91 @@ __device__ __forceinline__ void pack8(const float *v, uint4 &hi, uint4 &lo)
     lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
-template <bool BF, bool WEIGHTED, int MAXIT>
+__device__ __forceinline__ uint4 flip_sign(uint4 v)
+{
+    const uint32_t sg = 0x80008000u;
+    return make_uint4(v.x ^ sg, v.y ^ sg, v.z ^ sg, v.w ^ sg);
+}
+
+// The tile of slot ts (0, or 1 for the second float16 tile) of this block's local unit ul (>= B when none).
+template <bool BF>
+__device__ __forceinline__ int unit_tile(int ul, int ts)
+{
+    const int u = (int)blockIdx.x + ul * (int)gridDim.x;
+    return BF ? u : 2 * u + ts;
+}
+
+// The pixels of one tile from P0 = D'[0:32, :] and P1 = D'[32:64, :] (rows of 64 + 1 floats in shared memory):
+// thread t of the 128 epilogue threads takes row i = t / 4 and eight consecutive columns.
+__device__ __forceinline__ void tile_pixels(const TcArgs &a, int tile, const float *P0, const float *P1, int t)
+{
+    const int i = t >> 2, jb = (t & 3) * 8;
+    const double cx = a.ucx[tile], cy = a.ucy[tile];
+    const float f = (float)(a.fc2 / (2.0 * a.rc[tile]));
+    const float dx = ((float)i - 0.5f * (TT - 1)) * (float)a.spx;
+    const int2 f0 = a.img ? a.first[tile] : make_int2(0, 0);
+    const int x = f0.x + i - a.ox;
+    float2 outv[8];
+#pragma unroll
+    for (int jj = 0; jj < 8; ++jj) {
+        const int j = jb + jj;
+        const float re = P0[i * 65 + j] - P1[i * 65 + j + 32];
+        const float im = P0[i * 65 + j + 32] + P1[i * 65 + j];
+        const float dy = ((float)j - 0.5f * (TT - 1)) * (float)a.spy;
+        const float los = (float)cx * dx + (float)cy * dy;
+        const float qc = (dx * dx + dy * dy - los * los) * f;
+        const float2 e = cis_cycles(qc);
+        const float2 o = cmul(make_float2(re, im), e);
+        outv[jj] = make_float2(o.x * a.scale, o.y * a.scale);
+    }
+    if (a.img) {
+        if (x >= 0 && x < a.nx) {
+#pragma unroll
+            for (int jj = 0; jj < 8; ++jj) {
+                const int y = f0.y + jb + jj - a.oy;
+                if (y >= 0 && y < a.ny) a.img[(size_t)x * a.ny + y] = outv[jj];
+            }
+        }
+    } else {
+#pragma unroll
+        for (int jj = 0; jj < 8; ++jj) a.tiles[((size_t)tile * TT + i) * TT + jb + jj] = outv[jj];
+    }
+}
+
+template <bool BF, bool WEIGHTED, int MAXWI>
 __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
-    // layout: [S stages][parts][A', B'] operand buffers (64 x Qfp elements of 2 bytes each), then sD, then barriers
     const int ng = a.Qfp / 8;                                   // core matrices along K per operand
-    const uint32_t opbytes = 64u * a.Qfp * 2u;                  // one operand buffer
-    const uint32_t stagebytes = opbytes * 2u * a.parts;
-    float *sD = reinterpret_cast<float *>(smem + (size_t)a.S * stagebytes);           // [64][65]
-    uint64_t *bars = reinterpret_cast<uint64_t *>(sD + 64 * 65);
-    uint64_t *full = bars, *empty = bars + a.S, *accf = bars + 2 * a.S, *acce = accf + 2;
+    const uint32_t H = 64u * a.Qfp * 2u;                        // 64 operand rows
+    const uint32_t stagebytes = 4u * H;                         // A' (128 rows), B' (128 rows)
+    float *sP = reinterpret_cast<float *>(smem + (size_t)a.S * stagebytes);             // [2][32][65]
+    unsigned char *stg0 = reinterpret_cast<unsigned char *>(sP + 2 * 32 * 65);          // producer staging
+    uint64_t *bars = reinterpret_cast<uint64_t *>(stg0 + (size_t)NPW * RS * MAXWI * SLOT_BYTES);
+    uint64_t *full = bars, *empty = bars + a.S, *accf = bars + 2 * a.S, *acce = accf + 2, *drain = acce + 2;
     __shared__ uint32_t s_tmem;
     __shared__ volatile int s_abort;
 
     const int t = threadIdx.x, warp = t / 32, lane = t % 32;
+    const int nis = a.nis;
+    // this block's units: blockIdx.x + ul gridDim.x
+    const int nul = a.nunits > (int)blockIdx.x ? (a.nunits - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     if (t == 0) {
         s_abort = 0;
         for (int s = 0; s < a.S; ++s) {
-            mbar_init(&full[s], 8);
+            mbar_init(&full[s], NPW);
             mbar_init(&empty[s], 1);
         }
         for (int k = 0; k < 2; ++k) {
-            mbar_init(&accf[k], 1);
-            mbar_init(&acce[k], 4);
+            mbar_init(&accf[k], (uint32_t)nis);
+            mbar_init(&acce[k], NEPI);
+            mbar_init(&drain[k], 1);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 4) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;" :: "r"(smem_u32(&s_tmem)));
+    if (warp == NEPI) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(&s_tmem)), "r"(TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -189,192 +282,217 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
     const uint32_t tmem = s_tmem;
     const uint32_t smem0 = smem_u32(smem);
 
-    if (t >= PRODUCER0) {
+    if (warp >= PW0) {
         // ------------------------------------------------------------------ producers
-        // Work items: (row pair, group of 8 frequency samples). Pixel rows r and 31 - r have offsets dl and -dl,
-        // so their ramps are complex conjugates: one recurrence serves both rows of a pair. An A item writes
-        // Ar, Ai of rows r and 31 - r (d times the ramp and d times its conjugate); a B item writes Br, Bi of row r
-        // and, for row 31 - r, the same real part and the negated imaginary part (a sign flip of the packed words).
-        // Each thread's next stage's data (its d samples and the geometry) are loaded a stage ahead.
-        const int pt = t - PRODUCER0;
-        const int nitems = 32 * ng;                             // 16 A pairs and 16 B pairs per group
-        const float sp32x = (float)a.spx, sp32y = (float)a.spy;
-        // the items of this thread
-        int it_kind[MAXIT], it_pair[MAXIT], it_g[MAXIT], nmine = 0;
-        uint32_t it_off[MAXIT][4];                              // byte offsets of rows r, r+32, 31-r, 63-r at group g
-        for (int item = pt; item < nitems && nmine < MAXIT; item += NPROD) {
-            const bool A = item < 16 * ng;
-            const int rel = A ? item : item - 16 * ng;
-            it_kind[nmine] = A ? 1 : 0;
-            const int r = rel & 15, g = rel >> 4;
-            it_pair[nmine] = r;
-            it_g[nmine] = g;
+        // Warp items: (tile slot ts, operand A or B, pair of 8-sample groups gp). Lane l of the warp takes pixel
+        // row pair r = l % 16 (rows r and 31 - r, whose offsets are dl and -dl, so that their ramps are complex
+        // conjugates and one recurrence serves both) and group g = 2 gp + l / 16. An A item writes Ar, Ai of rows
+        // r and 31 - r (d times the ramp and d times its conjugate); a B item writes Br, Bi of row r and, without
+        // weights, row 31 - r from row r's words (the same real part, the imaginary part's sign flipped).
+        const int pw = warp - PW0;
+        const int hg = (ng + 1) / 2;
+        const int nts = BF ? 1 : 2;
+        const int nwi = nts * 2 * hg;
+        const int ntot = nul * a.Pf;
+        const int r = lane & 15, sub = lane >> 4;
+        const size_t nbp = (size_t)a.B * a.Pf;
+        const uint32_t stg_me = smem_u32(stg0) + (uint32_t)(pw * RS * MAXWI * SLOT_BYTES);
+        const float *stg_me_p = reinterpret_cast<const float *>(stg0 + (size_t)pw * RS * MAXWI * SLOT_BYTES);
+        // byte offsets (without the group) of rows r, r + 32, 31 - r, 63 - r within a 64-row half operand
+        uint32_t roff[4];
+        {
             const int rows[4] = {r, r + 32, 31 - r, 63 - r};
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
-                it_off[nmine][q] = (uint32_t)(((rows[q] >> 3) * ng + g) * 128 + (rows[q] & 7) * 16) + (A ? 0u : opbytes);
-            ++nmine;
+            for (int k = 0; k < 4; ++k) roff[k] = (uint32_t)(((rows[k] >> 3) * ng) * 128 + (rows[k] & 7) * 16);
         }
-        // the next tile's samples and geometry into L2 while this tile is formed (128-byte lines, spread over the
-        // producer threads)
-        auto prefetch_tile = [&](int tile) {
-            if (tile >= a.B) return;
-            const char *dbeg = reinterpret_cast<const char *>(a.d + (size_t)tile * a.Pf * a.Qf);
-            const size_t dbytes = (size_t)a.Pf * a.Qf * sizeof(float2);
-            for (size_t o = (size_t)pt * 128; o < dbytes; o += (size_t)NPROD * 128)
-                asm volatile("prefetch.global.L2 [%0];" :: "l"(dbeg + o));
-            if (pt < 8) {
-                const double *src = (pt < 4 ? a.ux : a.uy) + (size_t)tile * a.Pf;
-                const size_t ub = (size_t)a.Pf * sizeof(double);
-                for (size_t o = (size_t)(pt & 3) * 128; o < ub; o += 4 * 128)
-                    asm volatile("prefetch.global.L2 [%0];" :: "l"(reinterpret_cast<const char *>(src) + o));
-            }
-        };
-        // prefetched data of the next stage: per item 8 d samples (A) and the direction cosine (A: ux, B: uy)
-        float2 dnext[MAXIT][8];
-        double unext[MAXIT];
-        float wnext[MAXIT][3];
-        auto fetch = [&](int tile, int p) {
-            const size_t bp = (size_t)tile * a.Pf + p;
-            const float2 *dp = a.d + bp * a.Qf;
+        // this warp's items (the same in every stage): tile slot, operand (0 = A), pair of groups; -1 = none
+        int it_ts[MAXWI], it_op[MAXWI], it_gp[MAXWI];
 #pragma unroll
-            for (int k = 0; k < MAXIT; ++k) {
-                if (k >= nmine) break;
-                unext[k] = it_kind[k] ? __ldg(&a.ux[bp]) : __ldg(&a.uy[bp]);
-                if (it_kind[k]) {
+        for (int k = 0; k < MAXWI; ++k) {
+            const int wi = pw + k * NPW;
+            it_ts[k] = wi < nwi ? wi / (2 * hg) : -1;
+            it_op[k] = (wi / hg) & 1;
+            it_gp[k] = wi % hg;
+        }
+        // copies of the stage (unit ul, subaperture p) into ring slot `slot`, one cp.async group per stage
+        // (empty past the last stage)
+        auto issue = [&](int ul, int p, int slot) {
+            if (ul < nul) {
 #pragma unroll
-                    for (int e = 0; e < 8; ++e) {
-                        const int q = 8 * it_g[k] + e;
-                        dnext[k][e] = q < a.Qf ? __ldg(&dp[q]) : make_float2(0.f, 0.f);
+                for (int k = 0; k < MAXWI; ++k) {
+                    if (it_ts[k] < 0) break;
+                    const int tile = unit_tile<BF>(ul, it_ts[k]);
+                    const bool tv = tile < a.B;
+                    const size_t bp = tv ? (size_t)tile * a.Pf + p : 0;
+                    const uint32_t sl = stg_me + (uint32_t)((slot * MAXWI + k) * SLOT_BYTES);
+                    if (lane < 16) {
+                        if (it_op[k] == 0) {
+                            const int q = 16 * it_gp[k] + lane;
+                            const bool v = tv && q < a.Qf;
+                            cp_async(sl + 8u * lane, v ? (const void *)(a.d + bp * a.Qf + q) : (const void *)a.d, 8, v);
+                        }
+                    } else if (lane == 16) {
+                        cp_async(sl + 128u, it_op[k] == 0 ? (const void *)(a.ux + bp) : (const void *)(a.uy + bp), 8, tv);
+                    } else if (WEIGHTED && lane < 20) {
+                        cp_async(sl + 136u + 4u * (lane - 17), (const void *)(a.w + (size_t)(lane - 17) * nbp + bp), 4,
+                                 tv);
                     }
                 }
-                if (WEIGHTED) {
-                    const size_t nbp = (size_t)a.B * a.Pf;
-                    wnext[k][0] = __ldg(&a.w[bp]);
-                    wnext[k][1] = __ldg(&a.w[nbp + bp]);
-                    wnext[k][2] = __ldg(&a.w[2 * nbp + bp]);
+            }
+            asm volatile("cp.async.commit_group;" ::: "memory");
+        };
+        // the next unit's samples and geometry into L2 while this one is formed
+        auto prefetch_unit = [&](int ul) {
+            if (ul >= nul) return;
+            const int pt = t - PW0 * 32;
+            for (int ts = 0; ts < nts; ++ts) {
+                const int tile = unit_tile<BF>(ul, ts);
+                if (tile >= a.B) break;
+                const char *dbeg = reinterpret_cast<const char *>(a.d + (size_t)tile * a.Pf * a.Qf);
+                const int dbytes = a.Pf * a.Qf * (int)sizeof(float2);
+                for (int o = pt * 128; o < dbytes; o += NPW * 32 * 128)
+                    asm volatile("prefetch.global.L2 [%0];" :: "l"(dbeg + o));
+                if (pt < 16) {
+                    const double *src = (pt < 8 ? a.ux : a.uy) + (size_t)tile * a.Pf;
+                    const int ub = a.Pf * (int)sizeof(double);
+                    for (int o = (pt & 7) * 128; o < ub; o += 8 * 128)
+                        asm volatile("prefetch.global.L2 [%0];" :: "l"(reinterpret_cast<const char *>(src) + o));
                 }
             }
         };
-        long it = 0;
-        int tile = blockIdx.x, p = 0;
-        if (tile < a.B) fetch(tile, 0);
-        prefetch_tile(tile + gridDim.x);
-        for (; tile < a.B && !s_abort; ++it) {
-            float2 dcur[MAXIT][8];
-            double ucur[MAXIT];
-            float wcur[MAXIT][3];
+        prefetch_unit(0);
+        // stage counters, advanced by one per stage: (ul2, p2, slot2) the next stage to stage RS - 1 ahead;
+        // (ul, p) the stage being built, stg its ring stage and par that stage's phase parity, slot its staging
+        int ul2 = 0, p2 = 0, slot2 = 0;
 #pragma unroll
-            for (int k = 0; k < MAXIT; ++k) {
-                ucur[k] = unext[k];
-#pragma unroll
-                for (int e = 0; e < 8; ++e) dcur[k][e] = dnext[k][e];
-                wcur[k][0] = wnext[k][0]; wcur[k][1] = wnext[k][1]; wcur[k][2] = wnext[k][2];
-            }
-            int ntile = tile, np_ = p + 1;
-            if (np_ == a.Pf) { np_ = 0; ntile += gridDim.x; prefetch_tile(ntile + gridDim.x); }
-            if (ntile < a.B) fetch(ntile, np_);
-            const int stg = (int)(it % a.S);
-            if (!mbar_wait(&empty[stg], (uint32_t)(((it / a.S) & 1) ^ 1), &s_abort, a.err)) break;
+        for (int i = 0; i < RS - 1; ++i) {
+            issue(ul2, p2, slot2);
+            if (++p2 == a.Pf) { p2 = 0; ++ul2; }
+            slot2 = (slot2 + 1) & (RS - 1);
+        }
+        const float sp32x = (float)a.spx, sp32y = (float)a.spy;
+        int ul = 0, p = 0, stg = 0, slot = 0;
+        uint32_t par = 0;
+        for (int it = 0; it < ntot; ++it) {
+            issue(ul2, p2, slot2);
+            if (++p2 == a.Pf) { p2 = 0; ++ul2; }
+            slot2 = (slot2 + 1) & (RS - 1);
+            asm volatile("cp.async.wait_group %0;" :: "n"(RS - 1) : "memory");
+            __syncwarp();
+            if (p == 0) prefetch_unit(ul + 1);
+            if (!mbar_wait<PRODUCER_HINT_NS>(&empty[stg], par ^ 1u, &s_abort, a.err)) break;
             unsigned char *sbase = smem + (size_t)stg * stagebytes;
 #pragma unroll
-            for (int k = 0; k < MAXIT; ++k) {
-                if (k >= nmine) break;
-                const bool isA = it_kind[k];
-                const int r = it_pair[k], g = it_g[k];
-                const float dlf = ((float)r - 0.5f * (TT - 1)) * (isA ? sp32x : sp32y);       // r < 16: dl < 0
+            for (int k = 0; k < MAXWI; ++k) {
+                if (it_ts[k] < 0) break;
+                const int ts = it_ts[k], op = it_op[k];
+                const int g = 2 * it_gp[k] + sub;
+                if (g >= ng) continue;
+                const float *slotp = stg_me_p + (slot * MAXWI + k) * (SLOT_BYTES / 4);
+                const bool isA = op == 0;
+                const double u = *reinterpret_cast<const double *>(slotp + 32);
+                const float dlf = ((float)r - 0.5f * (TT - 1)) * (isA ? sp32x : sp32y);      // r < 16: dl < 0
                 const double dl = ((double)r - 0.5 * (TT - 1)) * (isA ? a.spx : a.spy);
-                float2 wv = cis_cycles_d(-(ucur[k] * dl) * (a.a0 + a.a1 * (8.0 * g)));
-                const float2 st = cis_cycles_d(-(ucur[k] * dl) * a.a1);
+                const double ud = -(u * dl);
+                float2 wv = cis_cycles_d(ud * fma(a.a1, 8.0 * g, a.a0));
+                const float2 st = cis_cycles_d(ud * a.a1);
                 float w1 = 1.f, w2 = 1.f;                       // the weights of rows r and 31 - r
                 if (WEIGHTED) {
-                    if (isA) { w1 = wcur[k][0] + wcur[k][1] * dlf; w2 = wcur[k][0] - wcur[k][1] * dlf; }
-                    else { w1 = 1.f + wcur[k][2] * dlf; w2 = 1.f - wcur[k][2] * dlf; }
+                    if (isA) { w1 = slotp[34] + slotp[35] * dlf; w2 = slotp[34] - slotp[35] * dlf; }
+                    else { w1 = 1.f + slotp[36] * dlf; w2 = 1.f - slotp[36] * dlf; }
                 }
+                // operand base: A' or B'; half: bfloat16 hi (lo one half further), float16 the tile slot's; group g
+                unsigned char *ob = sbase + (isA ? 0u : 2u * H) + (BF ? 0u : (uint32_t)ts * H) + (uint32_t)g * 128u;
                 float r1[8], i1[8], r2[8], i2[8];
+                if (isA) {
+                    const float4 *dq = reinterpret_cast<const float4 *>(slotp + 16 * sub);
 #pragma unroll
-                for (int e = 0; e < 8; ++e) {
-                    if (isA) {
-                        const float2 dd = dcur[k][e];
-                        const float p1 = dd.x * wv.x, p2 = dd.y * wv.y, p3 = dd.x * wv.y, p4 = dd.y * wv.x;
-                        r1[e] = (p1 - p2) * w1; i1[e] = (p3 + p4) * w1;       // d x
-                        r2[e] = (p1 + p2) * w2; i2[e] = (p4 - p3) * w2;       // d conj(x)
-                    } else {
-                        r1[e] = wv.x * w1; i1[e] = wv.y * w1;
-                        // row 31 - r: the conjugate ramp; without weights it is written from row r's packed words
-                        r2[e] = WEIGHTED ? wv.x * w2 : 0.f;
-                        i2[e] = WEIGHTED ? -wv.y * w2 : 0.f;
-                    }
-                    wv = cmul(wv, st);
-                }
-                uint4 h, l;
-                pack8<BF>(r1, h, l);
-                *reinterpret_cast<uint4 *>(sbase + it_off[k][0]) = h;
-                if (BF) *reinterpret_cast<uint4 *>(sbase + 2 * opbytes + it_off[k][0]) = l;
-                const bool mirror = !isA && !WEIGHTED;          // B row 31 - r from row r's words
-                if (mirror) {                                   // row 31 - r: the same real part
-                    *reinterpret_cast<uint4 *>(sbase + it_off[k][2]) = h;
-                    if (BF) *reinterpret_cast<uint4 *>(sbase + 2 * opbytes + it_off[k][2]) = l;
-                }
-                pack8<BF>(i1, h, l);
-                *reinterpret_cast<uint4 *>(sbase + it_off[k][1]) = h;
-                if (BF) *reinterpret_cast<uint4 *>(sbase + 2 * opbytes + it_off[k][1]) = l;
-                if (mirror) {                                   // row 31 - r: the imaginary part negated
-                    const uint32_t sg = 0x80008000u;
-                    h.x ^= sg; h.y ^= sg; h.z ^= sg; h.w ^= sg;
-                    *reinterpret_cast<uint4 *>(sbase + it_off[k][3]) = h;
-                    if (BF) {
-                        l.x ^= sg; l.y ^= sg; l.z ^= sg; l.w ^= sg;
-                        *reinterpret_cast<uint4 *>(sbase + 2 * opbytes + it_off[k][3]) = l;
+                    for (int e2 = 0; e2 < 4; ++e2) {
+                        const float4 dd = dq[e2];
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int e = 2 * e2 + h;
+                            const float dr = h ? dd.z : dd.x, di = h ? dd.w : dd.y;
+                            const float p1 = dr * wv.x, p2 = di * wv.y, p3 = dr * wv.y, p4 = di * wv.x;
+                            r1[e] = (p1 - p2) * w1; i1[e] = (p3 + p4) * w1;       // d x
+                            r2[e] = (p1 + p2) * w2; i2[e] = (p4 - p3) * w2;       // d conj(x)
+                            wv = cmul(wv, st);
+                        }
                     }
                 } else {
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) {
+                        r1[e] = wv.x * w1; i1[e] = wv.y * w1;
+                        r2[e] = WEIGHTED ? wv.x * w2 : 0.f;
+                        i2[e] = WEIGHTED ? -wv.y * w2 : 0.f;
+                        wv = cmul(wv, st);
+                    }
+                }
+                uint4 h, l;
+                const bool mirror = !isA && !WEIGHTED;
+                pack8<BF>(r1, h, l);
+                *reinterpret_cast<uint4 *>(ob + roff[0]) = h;
+                if (BF) *reinterpret_cast<uint4 *>(ob + H + roff[0]) = l;
+                if (mirror) {
+                    *reinterpret_cast<uint4 *>(ob + roff[2]) = h;
+                    if (BF) *reinterpret_cast<uint4 *>(ob + H + roff[2]) = l;
+                }
+                pack8<BF>(i1, h, l);
+                *reinterpret_cast<uint4 *>(ob + roff[1]) = h;
+                if (BF) *reinterpret_cast<uint4 *>(ob + H + roff[1]) = l;
+                if (mirror) {
+                    *reinterpret_cast<uint4 *>(ob + roff[3]) = flip_sign(h);
+                    if (BF) *reinterpret_cast<uint4 *>(ob + H + roff[3]) = flip_sign(l);
+                } else {
                     pack8<BF>(r2, h, l);
-                    *reinterpret_cast<uint4 *>(sbase + it_off[k][2]) = h;
-                    if (BF) *reinterpret_cast<uint4 *>(sbase + 2 * opbytes + it_off[k][2]) = l;
+                    *reinterpret_cast<uint4 *>(ob + roff[2]) = h;
+                    if (BF) *reinterpret_cast<uint4 *>(ob + H + roff[2]) = l;
                     pack8<BF>(i2, h, l);
-                    *reinterpret_cast<uint4 *>(sbase + it_off[k][3]) = h;
-                    if (BF) *reinterpret_cast<uint4 *>(sbase + 2 * opbytes + it_off[k][3]) = l;
+                    *reinterpret_cast<uint4 *>(ob + roff[3]) = h;
+                    if (BF) *reinterpret_cast<uint4 *>(ob + H + roff[3]) = l;
                 }
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive(&full[stg]);
-            p = np_;
-            tile = ntile;
+            if (++p == a.Pf) { p = 0; ++ul; }
+            if (++stg == a.S) { stg = 0; par ^= 1u; }
+            slot = (slot + 1) & (RS - 1);
         }
-    } else if (warp == 4) {
+        asm volatile("cp.async.wait_all;" ::: "memory");
+    } else if (warp >= NEPI) {
         // ------------------------------------------------------------------ MMA issue
-        if (lane == 0) {
-            const uint32_t idesc = (1u << 4) | ((BF ? 1u : 0u) << 7) | ((BF ? 1u : 0u) << 10) | ((64u >> 3) << 17) |
-                                   ((64u >> 4) << 24);
+        const int k = warp - NEPI;
+        if (lane == 0 && k < nis) {
+            const uint32_t idesc = (1u << 4) | ((BF ? 1u : 0u) << 7) | ((BF ? 1u : 0u) << 10) | ((128u >> 3) << 17) |
+                                   ((128u >> 4) << 24);
             const uint32_t lbo = 128, sbo = (uint32_t)ng * 128;
-            long it = 0;
-            int lt = 0;
-            for (int tile = blockIdx.x; tile < a.B && !s_abort; tile += gridDim.x, ++lt) {
-                const int ab = lt & 1;
-                if (!mbar_wait(&acce[ab], (uint32_t)(((lt >> 1) & 1) ^ 1), &s_abort, a.err)) break;
+            const int nks = a.Qfp / 16;
+            // descriptors of stage 0's A' and B'; stage s adds s stagebytes, K step ks adds 256 bytes (16 units)
+            const uint64_t da0 = smem_desc(smem0, lbo, sbo), db0 = smem_desc(smem0 + 2u * H, lbo, sbo);
+            const uint64_t dstage = (uint64_t)(stagebytes >> 4);
+            for (int ul = 0; ul < nul; ++ul) {
+                const int ab = ul & 1;
+                if (!mbar_wait<ISSUER_HINT_NS>(&acce[ab], (uint32_t)(((ul >> 1) & 1) ^ 1), &s_abort, a.err)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t dt = tmem + (uint32_t)(ab * 64);
+                const uint32_t dt = tmem + (uint32_t)((k * 2 + ab) * 128);
+                // ring stage and phase parity of this issuer's first stage of the unit, ul Pf + k
+                const int it0 = ul * a.Pf + k;
+                int stg = it0 % a.S;
+                uint32_t par = (uint32_t)(it0 / a.S) & 1u;
                 bool ok = true;
-                for (int p = 0; p < a.Pf; ++p, ++it) {
-                    const int stg = (int)(it % a.S);
-                    if (!mbar_wait(&full[stg], (uint32_t)((it / a.S) & 1), &s_abort, a.err)) { ok = false; break; }
+                uint32_t accum = 0;
+                for (int p = k; p < a.Pf; p += nis) {
+                    if (!mbar_wait<ISSUER_HINT_NS>(&full[stg], par, &s_abort, a.err)) { ok = false; break; }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    const uint32_t sb = smem0 + (uint32_t)stg * stagebytes;
-                    for (int ks = 0; ks < a.Qfp / 16; ++ks) {
-                        const uint32_t koff = (uint32_t)ks * 256;
-                        const uint64_t ah = smem_desc(sb + koff, lbo, sbo);
-                        const uint64_t bh = smem_desc(sb + opbytes + koff, lbo, sbo);
-                        const uint32_t accum = (p > 0 || ks > 0) ? 1u : 0u;
-                        mma_f16kind(dt, ah, bh, idesc, accum);
-                        if (BF) {
-                            const uint64_t al = smem_desc(sb + 2 * opbytes + koff, lbo, sbo);
-                            const uint64_t bl = smem_desc(sb + 3 * opbytes + koff, lbo, sbo);
-                            mma_f16kind(dt, ah, bl, idesc, 1u);
-                            mma_f16kind(dt, al, bh, idesc, 1u);
-                        }
+                    const uint64_t da = da0 + dstage * (uint64_t)stg, db = db0 + dstage * (uint64_t)stg;
+                    for (int ks = 0; ks < nks; ++ks) {
+                        mma_f16kind(dt, da + 16u * ks, db + 16u * ks, idesc, accum);
+                        accum = 1u;
                     }
                     mma_commit(&empty[stg]);
+                    stg += nis;
+                    if (stg >= a.S) { stg -= a.S; par ^= 1u; }
                 }
                 if (!ok) break;
                 mma_commit(&accf[ab]);
@@ -383,78 +501,94 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
         __syncwarp();
     } else {
         // ------------------------------------------------------------------ epilogue (warps 0..3)
-        int lt = 0;
-        for (int tile = blockIdx.x; tile < a.B && !s_abort; tile += gridDim.x, ++lt) {
-            const int ab = lt & 1;
-            if (!mbar_wait(&accf[ab], (uint32_t)((lt >> 1) & 1), &s_abort, a.err)) break;
+        float *P0 = sP, *P1 = sP + 32 * 65;
+        for (int ul = 0; ul < nul; ++ul) {
+            const int ab = ul & 1;
+            if (!mbar_wait<EPILOGUE_HINT_NS>(&accf[ab], (uint32_t)((ul >> 1) & 1), &s_abort, a.err)) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t base = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(ab * 64);
-            float v[16];
-            const int m = 16 * warp + lane;                      // the accumulator row of this lane (lanes < 16)
+            const uint32_t lanes = (uint32_t)(32 * warp) << 16;
+            float *mine = (warp & 1) ? P1 : P0;                 // accumulator rows 32..63 (mod 64) are the Ai rows
+            // the sum over the issuers' accumulators of columns [c0, c0 + 16), plus [c0 + c1, c0 + c1 + 16) if c1
+            auto gather = [&](int c0, int c1, float *v) {
+                uint32_t q0[16], q1[16];
 #pragma unroll
-            for (int c0 = 0; c0 < 64; c0 += 16) {
-                tmem_ld16(base + (uint32_t)c0, v);
-                if (lane < 16) {
+                for (int j = 0; j < 16; ++j) v[j] = 0.f;
+                for (int k = 0; k < nis; ++k) {
+                    const uint32_t base = tmem + lanes + (uint32_t)((k * 2 + ab) * 128);
+                    tmem_ld16(base + (uint32_t)c0, q0);
+                    if (c1) tmem_ld16(base + (uint32_t)(c0 + c1), q1);
+                    tmem_wait_ld();
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) sD[m * 65 + c0 + j] = v[j];
+                    for (int j = 0; j < 16; ++j) v[j] += __uint_as_float(q0[j]) + (c1 ? __uint_as_float(q1[j]) : 0.f);
                 }
-            }
-            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&acce[ab]);
-            asm volatile("bar.sync 1, 128;" ::: "memory");
-            // pixels: thread -> row i, eight consecutive columns
-            const int i = t >> 2, jb = (t & 3) * 8;
-            const double cx = a.ucx[tile], cy = a.ucy[tile];
-            const float f = (float)(a.fc2 / (2.0 * a.rc[tile]));
-            const float dx = ((float)i - 0.5f * (TT - 1)) * (float)a.spx;
-            const int2 f0 = a.img ? a.first[tile] : make_int2(0, 0);
-            const int x = f0.x + i - a.ox;
-            float2 outv[8];
+            };
+            if (BF) {
+                // warps 0, 1: hi rows (hi hi + hi lo); then warps 2, 3 add the lo rows (lo hi + lo lo)
+                float v[16];
+                if (warp < 2) {
 #pragma unroll
-            for (int jj = 0; jj < 8; ++jj) {
-                const int j = jb + jj;
-                const float re = sD[i * 65 + j] - sD[(i + 32) * 65 + j + 32];
-                const float im = sD[i * 65 + j + 32] + sD[(i + 32) * 65 + j];
-                const float dy = ((float)j - 0.5f * (TT - 1)) * (float)a.spy;
-                const float los = (float)cx * dx + (float)cy * dy;
-                const float qc = (dx * dx + dy * dy - los * los) * f;
-                const float2 e = cis_cycles(qc);
-                const float2 o = cmul(make_float2(re, im), e);
-                outv[jj] = make_float2(o.x * a.scale, o.y * a.scale);
-            }
-            if (a.img) {
-                if (x >= 0 && x < a.nx) {
+                    for (int c0 = 0; c0 < 64; c0 += 16) {
+                        gather(c0, 64, v);
 #pragma unroll
-                    for (int jj = 0; jj < 8; ++jj) {
-                        const int y = f0.y + jb + jj - a.oy;
-                        if (y >= 0 && y < a.ny) a.img[(size_t)x * a.ny + y] = outv[jj];
+                        for (int j = 0; j < 16; ++j) mine[lane * 65 + c0 + j] = v[j];
                     }
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&acce[ab]);
                 }
-            } else {
+                asm volatile("bar.sync 1, 128;" ::: "memory");
+                if (warp >= 2) {
 #pragma unroll
-                for (int jj = 0; jj < 8; ++jj) a.tiles[((size_t)tile * TT + i) * TT + jb + jj] = outv[jj];
+                    for (int c0 = 0; c0 < 64; c0 += 16) {
+                        gather(c0, 64, v);
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) mine[lane * 65 + c0 + j] += v[j];
+                    }
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&acce[ab]);
+                }
+                asm volatile("bar.sync 1, 128;" ::: "memory");
+                tile_pixels(a, unit_tile<BF>(ul, 0), P0, P1, t);
+                asm volatile("bar.sync 1, 128;" ::: "memory");
+            } else {
+                // tile slot ts: accumulator rows and columns [64 ts, 64 ts + 64), read by warps 2 ts and 2 ts + 1
+                for (int ts = 0; ts < 2; ++ts) {
+                    if ((warp >> 1) == ts) {
+                        float v[16];
+#pragma unroll
+                        for (int c0 = 0; c0 < 64; c0 += 16) {
+                            gather(64 * ts + c0, 0, v);
+#pragma unroll
+                            for (int j = 0; j < 16; ++j) mine[lane * 65 + c0 + j] = v[j];
+                        }
+                        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(&acce[ab]);
+                    }
+                    asm volatile("bar.sync 1, 128;" ::: "memory");
+                    const int tile = unit_tile<BF>(ul, ts);
+                    if (tile < a.B) tile_pixels(a, tile, P0, P1, t);
+                    asm volatile("bar.sync 1, 128;" ::: "memory");
+                }
             }
-            asm volatile("bar.sync 1, 128;" ::: "memory");
         }
     }
 
-    // teardown: every role is done (or aborted); drain outstanding MMAs before freeing the accumulators
+    // teardown: every role is done (or aborted); each issuer drains its MMAs before the accumulators are freed
     __syncthreads();
-    if (warp == 4) {
-        if (lane == 0) {
-            // a final commit on a fresh barrier arrives once every earlier MMA of this thread has completed
-            uint64_t *drain = &acce[0];
-            mbar_init(drain, 1);
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-            mma_commit(drain);
-            for (long it = 0; it < WAIT_LIMIT && !mbar_test(drain, 0); ++it) {
-            }
+    if (warp >= NEPI && warp < NEPI + NISS && lane == 0) {
+        // a commit on a fresh barrier arrives once every earlier MMA of this thread has completed
+        uint64_t *dr = &drain[warp - NEPI];
+        mma_commit(dr);
+        const uint64_t t0 = global_ns();
+        while (!mbar_test(dr, 0) && global_ns() - t0 < WAIT_NS) {
         }
-        __syncwarp();
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" :: "r"(tmem));
     }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (warp == NEPI) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TMEM_COLS));
 }
 
 }  // namespace
@@ -464,9 +598,12 @@ cudaError_t launch_final_tc(const FinalLaunch &F, int mode, cudaStream_t s, cons
     *why = nullptr;
     if (F.T != 32) { *why = "the tensor-core final stage is built for T = 32"; return cudaErrorNotSupported; }
     if (F.B <= 0) return cudaSuccess;
+    if ((long long)F.B * F.Pf >= (1LL << 31)) { *why = "more than 2^31 final tile subapertures"; return cudaErrorNotSupported; }
+    const bool bf = mode == 2;
     TcArgs a;
     a.d = F.d; a.B = F.B; a.Pf = F.Pf; a.Qf = F.Qf; a.Qfp = (F.Qf + 15) & ~15;
-    a.parts = (mode == 2) ? 2 : 1;
+    a.nunits = bf ? F.B : (F.B + 1) / 2;
+    a.nis = F.Pf >= NISS ? NISS : 1;
     a.ux = F.ux; a.uy = F.uy; a.spx = F.spx; a.spy = F.spy; a.a0 = F.a0; a.a1 = F.a1; a.fc2 = F.fc2;
     a.ucx = F.ucx; a.ucy = F.ucy; a.rc = F.rc; a.w = F.w; a.tiles = F.tiles; a.img = F.img; a.first = F.first;
     a.nx = F.nx; a.ny = F.ny; a.ox = F.ox; a.oy = F.oy; a.scale = F.scale; a.err = F.err;
@@ -474,37 +611,38 @@ cudaError_t launch_final_tc(const FinalLaunch &F, int mode, cudaStream_t s, cons
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    const size_t stage = (size_t)64 * a.Qfp * 2 * 2 * a.parts;
-    const size_t fixed = (size_t)64 * 65 * 4 + 16 * 8 + 64;
+    // warp items per producer warp and stage: (tile slots) x (A, B) x (pairs of 8-sample groups) over NPW warps
+    const int ng = a.Qfp / 8, hg = (ng + 1) / 2;
+    const int nwi = (bf ? 1 : 2) * 2 * hg;
+    const int maxwi = (nwi + NPW - 1) / NPW;
+    if (maxwi > 4) { *why = "more than 256 frequency samples per final tile"; return cudaErrorNotSupported; }
+    const int mw = maxwi <= 1 ? 1 : (maxwi <= 2 ? 2 : 4);
+    const size_t stage = (size_t)4 * 64 * a.Qfp * 2;
+    const size_t fixed = (size_t)2 * 32 * 65 * 4 + (size_t)NPW * RS * mw * SLOT_BYTES + (size_t)(2 * 4 + 6) * 8;
+    const size_t avail = (size_t)maxsmem - 1024;                // static shared memory and slack
     int S = 4;
-    while (S > 2 && (size_t)S * stage + fixed > (size_t)maxsmem - 2048) --S;
-    if ((size_t)S * stage + fixed > (size_t)maxsmem - 2048) {
+    while (S > 2 && (size_t)S * stage + fixed > avail) --S;
+    if ((size_t)S * stage + fixed > avail) {
         *why = "a final subaperture's operands do not fit shared memory (Qf too large for the tensor-core stage)";
         return cudaErrorNotSupported;
     }
-    if (a.Qfp / 8 > 32) { *why = "more than 256 frequency samples per final tile"; return cudaErrorNotSupported; }
     a.S = S;
     const size_t smem = (size_t)S * stage + fixed;
-    const int grid = F.B < nsm ? F.B : nsm;
-    cudaError_t e;
+    const int grid = a.nunits < nsm ? a.nunits : nsm;
     auto run = [&](auto kern) -> cudaError_t {
         cudaError_t r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (r != cudaSuccess) return r;
         kern<<<grid, NTHREADS, smem, s>>>(a);
         return cudaGetLastError();
     };
-    // items (row pair, group of 8 samples) per producer thread: 32 ng items over 256 threads
-    const int maxit = (32 * (a.Qfp / 8) + NPROD - 1) / NPROD;
-    if (maxit <= 1) {
-        if (a.parts == 2) e = a.w ? run(final_tc_kernel<true, true, 1>) : run(final_tc_kernel<true, false, 1>);
-        else e = a.w ? run(final_tc_kernel<false, true, 1>) : run(final_tc_kernel<false, false, 1>);
-    } else if (maxit <= 2) {
-        if (a.parts == 2) e = a.w ? run(final_tc_kernel<true, true, 2>) : run(final_tc_kernel<true, false, 2>);
-        else e = a.w ? run(final_tc_kernel<false, true, 2>) : run(final_tc_kernel<false, false, 2>);
-    } else {
-        if (a.parts == 2) e = a.w ? run(final_tc_kernel<true, true, 4>) : run(final_tc_kernel<true, false, 4>);
-        else e = a.w ? run(final_tc_kernel<false, true, 4>) : run(final_tc_kernel<false, false, 4>);
-    }
+#define FFBP_TC_RUN(MW)                                                                                    \
+    (bf ? (a.w ? run(final_tc_kernel<true, true, MW>) : run(final_tc_kernel<true, false, MW>))             \
+        : (a.w ? run(final_tc_kernel<false, true, MW>) : run(final_tc_kernel<false, false, MW>)))
+    cudaError_t e;
+    if (mw == 1) e = FFBP_TC_RUN(1);
+    else if (mw == 2) e = FFBP_TC_RUN(2);
+    else e = FFBP_TC_RUN(4);
+#undef FFBP_TC_RUN
     return e;
 }
 

@@ -256,11 +256,13 @@ def test_torch_input_matches_numpy(golden):
 
 @pytest.mark.parametrize('mode,tol', [(2, 2e-4), (1, 3e-3)], ids=['bf16x3', 'f16'])
 @pytest.mark.parametrize('weighted', [False, True])
-@pytest.mark.parametrize('shape', [(5, 13, 57), (300, 7, 96), (3, 40, 130)], ids=['small', 'many-tiles', 'long-q'])
+@pytest.mark.parametrize('shape', [(5, 13, 57), (300, 7, 96), (3, 40, 130), (4, 1, 40), (301, 44, 88)],
+                         ids=['small', 'many-tiles', 'long-q', 'one-subaperture', 'spotlight-12k-final'])
 def test_final_tensor_cores_match_oracle(lib, oracle_lib, mode, tol, weighted, shape):
-    """The tcgen05 final stage (T = 32) against the float64 oracle: three bfloat16 products within 2e-4, one
-    float16 product within 3e-3 (its operands carry 11 bits); tiles beyond one per multiprocessor, padding of Qf to
-    a multiple of 16, aperture weights."""
+    """The tcgen05 final stage (T = 32) against the float64 oracle: split bfloat16 products within 2e-4, one
+    float16 product within 3e-3 (its operands carry 11 bits); units beyond one per multiprocessor, an odd tile count
+    (the float16 form pairs tiles), one final subaperture (one MMA issuer), padding of Qf to a multiple of 16,
+    aperture weights, and the final stage's shape at the 12,288 x 8,832 spotlight (Pf 44, Qf 88)."""
     T = 32
     rng = np.random.default_rng(7 * mode + weighted + shape[0])
     B, Pf, Qf = shape
@@ -308,3 +310,18 @@ def test_image_tensor_cores_match_reference(golden, oracle_lib, monkeypatch, pre
     e64 = oracle_lib.rel_db(img.ravel()[g['bp64_idx']], g['bp64'])
     print(f'{precision}/{final}: {e:.1f} dB vs reference former; {e64:.1f} dB vs float64 BP 64x')
     assert e < bar
+
+
+@pytest.mark.parametrize('precision,final', [('float32', 'tc3'), ('float16', 'fp32')], ids=['bf16x3', 'f16'])
+def test_image_tensor_cores_repeatable_bitwise(golden, monkeypatch, precision, final):
+    """Two MMA issuers accumulate fixed subsets of the final subapertures into their own accumulators, summed in a
+    fixed order: the tensor-core image is the same bits on every call."""
+    from fastsar_b200 import ImageFormer, sim
+    monkeypatch.setenv('FASTSAR_FINAL', final)
+    g = golden('image_spot512')
+    w = sim.workload('spotlight_512')
+    col = w['col']
+    f = ImageFormer(col.ant, col.fmin, col.df, col.K, 512, 512, 0.25, 0.25, w['e1'], w['e2'], precision=precision)
+    a = f(g['S'])
+    b = f(g['S'])
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
