@@ -244,8 +244,10 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
     int *bad = reinterpret_cast<int *>(ws);
     float2 *bufA = reinterpret_cast<float2 *>(ws + 256);
     float2 *bufB = reinterpret_cast<float2 *>(ws + 256 + align256(p->bufA * sizeof(float2)));
+    // status words: bad[0] the first non-finite pulse (0x7f7f7f7f: none), bad[1] the tensor-core stage's wait
+    // status, bad[2] the largest |component| of the last level's output (float bits)
     cudaError_t e = cudaMemsetAsync(bad, 0x7f, sizeof(int), s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(bad + 1, 0, sizeof(int), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(bad + 1, 0, 2 * sizeof(int), s);
     if (e != cudaSuccess) return cuda_fail(e, "status reset");
     const bool timed = stage_ms != nullptr;
     if (timed && n_stage < p->nlev + 1) return fail(FFBP_E_ARG, "stage_ms holds %d entries, %d needed", n_stage, p->nlev + 1);
@@ -266,6 +268,7 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
         L.out = outp; L.bad = l == 0 ? bad : nullptr;
         L.Np = v.Np; L.C = v.C; L.P = v.P; L.K = v.K; L.Ko = v.Ko; L.Po = v.Po; L.Dk = v.Dk; L.Lk = v.Lk; L.plk = v.plk;
         L.Dp = v.Dp; L.Lp = v.Lp; L.plp = v.plp; L.kc = v.kc;
+        L.amax = (l == p->nlev - 1 && p->final_mode == FFBP_FINAL_TC_F16) ? bad + 2 : nullptr;
         const char *why = nullptr;
         e = ffbp::launch_level(L, s, &why);
         if (why) { destroy_events(); return fail(FFBP_E_UNSUPPORTED, "level %d: %s", l, why); }
@@ -278,6 +281,7 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
     F.spx = p->spx; F.spy = p->spy; F.a0 = p->a0; F.a1 = p->a1; F.fc2 = p->fc2; F.ucx = p->ucx; F.ucy = p->ucy;
     F.rc = p->rc; F.w = p->wf; F.tiles = nullptr; F.img = static_cast<float2 *>(d_img); F.first = p->first;
     F.nx = p->nx; F.ny = p->ny; F.ox = p->ox; F.oy = p->oy; F.scale = 1.f; F.err = bad + 1;
+    F.amax = p->final_mode == FFBP_FINAL_TC_F16 ? bad + 2 : nullptr;
     const char *why = nullptr;
     e = p->final_mode == FFBP_FINAL_FP32 ? ffbp::launch_final_fp32(F, s, &why) : ffbp::launch_final_tc(F, p->final_mode, s, &why);
     if (why) { destroy_events(); return fail(FFBP_E_UNSUPPORTED, "final stage: %s", why); }
@@ -287,6 +291,9 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
         if ((e = cudaEventSynchronize(ev[p->nlev + 1])) != cudaSuccess) { destroy_events(); return cuda_fail(e, "form"); }
         for (int l = 0; l <= p->nlev; ++l) cudaEventElapsedTime(&stage_ms[l], ev[l], ev[l + 1]);
         destroy_events();
+        int st = 0;
+        if ((e = cudaMemcpy(&st, bad + 1, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess) return cuda_fail(e, "status read");
+        if (st) return fail(FFBP_E_CUDA, "the tensor-core final stage stopped waiting on its pipeline (a bounded wait ran out)");
     }
     if (h_bad) {
         int v[2] = {0, 0};

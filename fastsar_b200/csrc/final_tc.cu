@@ -10,7 +10,9 @@
 //   FFBP_FINAL_TC_BF16X3  one tile, operands split x = hi + lo in bfloat16: A' = [A_hi; A_lo], B' = [B_hi; B_lo], so
 //                         one product gives hi hi, hi lo, lo hi and lo lo of the tile, summed in the epilogue;
 //   FFBP_FINAL_TC_F16     two tiles in float16, A' = [A_1; A_2], B' = [B_1; B_2]: the two diagonal 64 x 64 blocks
-//                         of the product are the tiles.
+//                         of the product are the tiles. The samples are scaled by a power of two (from the largest
+//                         sample component, which the last level kernel records) into float16's range, and the
+//                         pixels by its inverse.
 // The per-instruction issue cost of tcgen05.mma is the same for a 64 x 64 and a 128 x 128 product, so the larger
 // shape does two or four times the work per instruction; two issuing warps double the rate again.
 //
@@ -20,8 +22,10 @@
 //                ring of S stages (K-major, no swizzle: core matrices of 8 rows x 16 bytes). Each warp stages the
 //                samples and geometry it needs RS - 1 stages ahead with cp.async into its own ring;
 //   warps 4, 5   one thread each issues tcgen05.mma: warp 4 + k takes the final subapertures p = k mod 2 of every
-//                unit into its own accumulator (two 128-column accumulators per issuer, 512 TMEM columns), commits
-//                each stage to the stage's "empty" barrier and the unit to the accumulator's "full" barrier;
+//                unit into its own accumulator (two 128-column accumulators per issuer, 512 TMEM columns), from its
+//                own stages k, k + 2, ... of the ring (a stage with one consumer, so that no parity wait can run two
+//                phases ahead of its barrier), commits each stage to the stage's "empty" barrier and the unit to the
+//                accumulator's "full" barrier;
 //   warps 0..3   epilogue: sum the issuers' accumulators (and, for bfloat16, the four split products), combine
 //                re/im through shared memory, apply the quadratic phase and write the tile into the image (cropped).
 //
@@ -164,7 +168,21 @@ struct TcArgs {
     int nx, ny, ox, oy;
     float scale;
     int *err;
+    const int *amax;
 };
+
+// The power of two s that brings samples whose components are at most *amax (a float's bits; null: unknown) to
+// below 2^13 in magnitude, so that d s times a ramp and a weight stays inside float16's range (65504).
+__device__ __forceinline__ float operand_scale(const int *amax)
+{
+    if (!amax) return 1.f;
+    const float m = __int_as_float(*amax);
+    if (!(m > 0.f) || !isfinite(m)) return 1.f;
+    int ex;
+    frexpf(m, &ex);                                             // m < 2^ex
+    ex = ex < -100 ? -100 : (ex > 100 ? 100 : ex);
+    return ldexpf(1.f, 13 - ex);
+}
 
 // 8 values -> 16 bytes of operand: float16, or bfloat16 high parts (and the low parts in lo)
 template <bool BF>
@@ -205,7 +223,8 @@ __device__ __forceinline__ int unit_tile(int ul, int ts)
 
 // The pixels of one tile from P0 = D'[0:32, :] and P1 = D'[32:64, :] (rows of 64 + 1 floats in shared memory):
 // thread t of the 128 epilogue threads takes row i = t / 4 and eight consecutive columns.
-__device__ __forceinline__ void tile_pixels(const TcArgs &a, int tile, const float *P0, const float *P1, int t)
+__device__ __forceinline__ void tile_pixels(const TcArgs &a, int tile, const float *P0, const float *P1, int t,
+                                            float scale)
 {
     const int i = t >> 2, jb = (t & 3) * 8;
     const double cx = a.ucx[tile], cy = a.ucy[tile];
@@ -224,7 +243,7 @@ __device__ __forceinline__ void tile_pixels(const TcArgs &a, int tile, const flo
         const float qc = (dx * dx + dy * dy - los * los) * f;
         const float2 e = cis_cycles(qc);
         const float2 o = cmul(make_float2(re, im), e);
-        outv[jj] = make_float2(o.x * a.scale, o.y * a.scale);
+        outv[jj] = make_float2(o.x * scale, o.y * scale);
     }
     if (a.img) {
         if (x >= 0 && x < a.nx) {
@@ -371,8 +390,14 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
             slot2 = (slot2 + 1) & (RS - 1);
         }
         const float sp32x = (float)a.spx, sp32y = (float)a.spy;
-        int ul = 0, p = 0, stg = 0, slot = 0;
-        uint32_t par = 0;
+        // the float16 operands carry d scaled by a power of two that keeps them inside the format's range
+        const float dscale = BF ? 1.f : operand_scale(a.amax);
+        // issuer k's stages are k + nis s for s < S / nis, filled and consumed in that issuer's order (one
+        // consumer per stage: no wait can run two phases ahead); (ps_k, pp_k) is issuer k's next slot and parity
+        const int rs = a.S / nis;
+        int ps0 = 0, ps1 = 0;
+        uint32_t pp0 = 0, pp1 = 0;
+        int ul = 0, p = 0, slot = 0;
         for (int it = 0; it < ntot; ++it) {
             issue(ul2, p2, slot2);
             if (++p2 == a.Pf) { p2 = 0; ++ul2; }
@@ -380,7 +405,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
             asm volatile("cp.async.wait_group %0;" :: "n"(RS - 1) : "memory");
             __syncwarp();
             if (p == 0) prefetch_unit(ul + 1);
-            if (!mbar_wait<PRODUCER_HINT_NS>(&empty[stg], par ^ 1u, &s_abort, a.err)) break;
+            const int kq = nis == 2 ? (p & 1) : 0;
+            const int stg = kq + nis * (kq ? ps1 : ps0);
+            if (!mbar_wait<PRODUCER_HINT_NS>(&empty[stg], (kq ? pp1 : pp0) ^ 1u, &s_abort, a.err)) break;
             unsigned char *sbase = smem + (size_t)stg * stagebytes;
 #pragma unroll
             for (int k = 0; k < MAXWI; ++k) {
@@ -395,6 +422,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
                 const double dl = ((double)r - 0.5 * (TT - 1)) * (isA ? a.spx : a.spy);
                 const double ud = -(u * dl);
                 float2 wv = cis_cycles_d(ud * fma(a.a1, 8.0 * g, a.a0));
+                if (isA) { wv.x *= dscale; wv.y *= dscale; }
                 const float2 st = cis_cycles_d(ud * a.a1);
                 float w1 = 1.f, w2 = 1.f;                       // the weights of rows r and 31 - r
                 if (WEIGHTED) {
@@ -455,8 +483,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive(&full[stg]);
+            if (kq) {
+                if (++ps1 == rs) { ps1 = 0; pp1 ^= 1u; }
+            } else if (++ps0 == rs) {
+                ps0 = 0;
+                pp0 ^= 1u;
+            }
             if (++p == a.Pf) { p = 0; ++ul; }
-            if (++stg == a.S) { stg = 0; par ^= 1u; }
             slot = (slot + 1) & (RS - 1);
         }
         asm volatile("cp.async.wait_all;" ::: "memory");
@@ -471,18 +504,18 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
             // descriptors of stage 0's A' and B'; stage s adds s stagebytes, K step ks adds 256 bytes (16 units)
             const uint64_t da0 = smem_desc(smem0, lbo, sbo), db0 = smem_desc(smem0 + 2u * H, lbo, sbo);
             const uint64_t dstage = (uint64_t)(stagebytes >> 4);
+            const int rs = a.S / nis;
+            int slot = 0;                                       // this issuer's stages: k + nis slot
+            uint32_t par = 0;
             for (int ul = 0; ul < nul; ++ul) {
                 const int ab = ul & 1;
                 if (!mbar_wait<ISSUER_HINT_NS>(&acce[ab], (uint32_t)(((ul >> 1) & 1) ^ 1), &s_abort, a.err)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t dt = tmem + (uint32_t)((k * 2 + ab) * 128);
-                // ring stage and phase parity of this issuer's first stage of the unit, ul Pf + k
-                const int it0 = ul * a.Pf + k;
-                int stg = it0 % a.S;
-                uint32_t par = (uint32_t)(it0 / a.S) & 1u;
                 bool ok = true;
                 uint32_t accum = 0;
                 for (int p = k; p < a.Pf; p += nis) {
+                    const int stg = k + nis * slot;
                     if (!mbar_wait<ISSUER_HINT_NS>(&full[stg], par, &s_abort, a.err)) { ok = false; break; }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                     const uint64_t da = da0 + dstage * (uint64_t)stg, db = db0 + dstage * (uint64_t)stg;
@@ -491,8 +524,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
                         accum = 1u;
                     }
                     mma_commit(&empty[stg]);
-                    stg += nis;
-                    if (stg >= a.S) { stg -= a.S; par ^= 1u; }
+                    if (++slot == rs) { slot = 0; par ^= 1u; }
                 }
                 if (!ok) break;
                 mma_commit(&accf[ab]);
@@ -502,6 +534,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
     } else {
         // ------------------------------------------------------------------ epilogue (warps 0..3)
         float *P0 = sP, *P1 = sP + 32 * 65;
+        const float oscale = a.scale / (BF ? 1.f : operand_scale(a.amax));
         for (int ul = 0; ul < nul; ++ul) {
             const int ab = ul & 1;
             if (!mbar_wait<EPILOGUE_HINT_NS>(&accf[ab], (uint32_t)((ul >> 1) & 1), &s_abort, a.err)) break;
@@ -549,7 +582,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
                     if (lane == 0) mbar_arrive(&acce[ab]);
                 }
                 asm volatile("bar.sync 1, 128;" ::: "memory");
-                tile_pixels(a, unit_tile<BF>(ul, 0), P0, P1, t);
+                tile_pixels(a, unit_tile<BF>(ul, 0), P0, P1, t, oscale);
                 asm volatile("bar.sync 1, 128;" ::: "memory");
             } else {
                 // tile slot ts: accumulator rows and columns [64 ts, 64 ts + 64), read by warps 2 ts and 2 ts + 1
@@ -568,7 +601,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
                     }
                     asm volatile("bar.sync 1, 128;" ::: "memory");
                     const int tile = unit_tile<BF>(ul, ts);
-                    if (tile < a.B) tile_pixels(a, tile, P0, P1, t);
+                    if (tile < a.B) tile_pixels(a, tile, P0, P1, t, oscale);
                     asm volatile("bar.sync 1, 128;" ::: "memory");
                 }
             }
@@ -606,7 +639,7 @@ cudaError_t launch_final_tc(const FinalLaunch &F, int mode, cudaStream_t s, cons
     a.nis = F.Pf >= NISS ? NISS : 1;
     a.ux = F.ux; a.uy = F.uy; a.spx = F.spx; a.spy = F.spy; a.a0 = F.a0; a.a1 = F.a1; a.fc2 = F.fc2;
     a.ucx = F.ucx; a.ucy = F.ucy; a.rc = F.rc; a.w = F.w; a.tiles = F.tiles; a.img = F.img; a.first = F.first;
-    a.nx = F.nx; a.ny = F.ny; a.ox = F.ox; a.oy = F.oy; a.scale = F.scale; a.err = F.err;
+    a.nx = F.nx; a.ny = F.ny; a.ox = F.ox; a.oy = F.oy; a.scale = F.scale; a.err = F.err; a.amax = F.amax;
     int dev = 0, nsm = 148, maxsmem = 227 * 1024;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -620,8 +653,9 @@ cudaError_t launch_final_tc(const FinalLaunch &F, int mode, cudaStream_t s, cons
     const size_t stage = (size_t)4 * 64 * a.Qfp * 2;
     const size_t fixed = (size_t)2 * 32 * 65 * 4 + (size_t)NPW * RS * mw * SLOT_BYTES + (size_t)(2 * 4 + 6) * 8;
     const size_t avail = (size_t)maxsmem - 1024;                // static shared memory and slack
+    // stages: a multiple of the issuers (each owns S / nis of them)
     int S = 4;
-    while (S > 2 && (size_t)S * stage + fixed > avail) --S;
+    while (S > 2 && ((size_t)S * stage + fixed > avail || S % a.nis)) --S;
     if ((size_t)S * stage + fixed > avail) {
         *why = "a final subaperture's operands do not fit shared memory (Qf too large for the tensor-core stage)";
         return cudaErrorNotSupported;

@@ -17,6 +17,7 @@ struct LevelLaunch {
     int *bad;             // or null
     int Np, C, P, K, Ko, Po, Dk, Lk, plk, Dp, Lp, plp;
     double kc;
+    int *amax = nullptr;  // or the largest |component| of the output, as float bits (atomicMax; start at 0)
 };
 
 // Returns cudaSuccess, or an error with *why set to a static message for shapes the kernels do not cover.
@@ -47,6 +48,7 @@ struct FinalLaunch {
     int nx, ny, ox, oy;
     float scale;
     int *err = nullptr;   // set to 1 by a kernel whose bounded wait ran out (tensor-core stage), or null
+    const int *amax = nullptr;   // the largest |component| of d (float bits), for the float16 operands' scale
 };
 cudaError_t launch_final_fp32(const FinalLaunch &F, cudaStream_t s, const char **why);
 cudaError_t launch_final_tc(const FinalLaunch &F, int mode, cudaStream_t s, const char **why);

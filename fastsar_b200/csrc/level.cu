@@ -46,6 +46,7 @@ struct LevelArgs {
     const float *__restrict__ wk;
     float2 *__restrict__ out;
     int *bad;
+    int *amax;
     int Np, C, P, K, Ko, Po, Dk, Lk, plk, Dp, Lp, plp;
     int JB, NK, ncb, ngrp, nseg, SEG;
     float kc;
@@ -103,6 +104,7 @@ __global__ void __launch_bounds__(NT) level_kernel(const LevelArgs a)
 #pragma unroll
         for (int s = 0; s < AP; ++s) acc[c][s] = make_float2(0.f, 0.f);
 
+    float vmax = 0.f;                                     // the largest |component| this thread writes
     const int g_end = i_e + AP - 1;
     const int p_start = a.Dp * i_s - a.plp;
     const int p_stop = a.Dp * g_end - a.plp;              // rows p_start .. p_stop - 1 are swept
@@ -194,7 +196,9 @@ __global__ void __launch_bounds__(NT) level_kernel(const LevelArgs a)
                         sr = fmaf(s_tk[r], z0.x, sr);
                         si = fmaf(s_tk[r], z0.y, si);
                     }
-                    a.out[(((size_t)n * a.C + c0 + c) * a.Po + i) * a.Ko + j0 + jj] = make_float2(sr + sr2, si + si2);
+                    const float2 o = make_float2(sr + sr2, si + si2);
+                    vmax = fmaxf(vmax, fmaxf(fabsf(o.x), fabsf(o.y)));
+                    a.out[(((size_t)n * a.C + c0 + c) * a.Po + i) * a.Ko + j0 + jj] = o;
                 }
             }
 #pragma unroll
@@ -207,6 +211,11 @@ __global__ void __launch_bounds__(NT) level_kernel(const LevelArgs a)
         }
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");
+    if (a.amax) {                                         // non-negative floats order as their bits
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+        if ((t & 31) == 0 && vmax > 0.f) atomicMax(a.amax, __float_as_int(vmax));
+    }
 }
 
 template <int AP, int G, int NT>
@@ -291,6 +300,7 @@ cudaError_t launch_level(const LevelLaunch &L, cudaStream_t s, const char **why)
     *why = nullptr;
     LevelArgs a;
     a.x = L.x; a.ph = L.phase; a.tk = L.tk; a.tp = L.tp; a.wp = L.wp; a.wk = L.wk; a.out = L.out; a.bad = L.bad;
+    a.amax = L.amax;
     a.Np = L.Np; a.C = L.C; a.P = L.P; a.K = L.K; a.Ko = L.Ko; a.Po = L.Po;
     a.Dk = L.Dk; a.Lk = L.Dk > 1 ? L.Lk : 1; a.plk = L.Dk > 1 ? L.plk : 0;
     a.Dp = L.Dp; a.Lp = L.Dp > 1 ? L.Lp : 1; a.plp = L.Dp > 1 ? L.plp : 0;

@@ -41,8 +41,11 @@ enum {
 /* Final-stage arithmetic (ImageFormer's precision=, fastsar/api.py:27-31).                                     */
 enum {
     FFBP_FINAL_FP32 = 0,    /* float32 on the CUDA cores: the plain path                                        */
-    FFBP_FINAL_TC_F16 = 1,  /* tcgen05 tensor cores, float16 operands, float32 accumulation                    */
-    FFBP_FINAL_TC_BF16X3 = 2 /* tcgen05 tensor cores, three bfloat16 products (hi*hi + hi*lo + lo*hi), float32  */
+    FFBP_FINAL_TC_F16 = 1,  /* tcgen05 tensor cores, float16 operands, float32 accumulation; ffbp_form scales  */
+                            /* the samples by a power of two into float16's range, ffbp_final takes them as    */
+                            /* given (each component below 2^14 in magnitude)                                   */
+    FFBP_FINAL_TC_BF16X3 = 2 /* tcgen05 tensor cores, operands split x = hi + lo in bfloat16, the hi*hi, hi*lo,  */
+                             /* lo*hi and lo*lo products accumulated in float32                                */
 };
 
 /* One level of the plan (fastsar/ffbp2.py:192-250, make_plan's per-level record). All pointers are host memory. */

@@ -256,13 +256,14 @@ def test_torch_input_matches_numpy(golden):
 
 @pytest.mark.parametrize('mode,tol', [(2, 2e-4), (1, 3e-3)], ids=['bf16x3', 'f16'])
 @pytest.mark.parametrize('weighted', [False, True])
-@pytest.mark.parametrize('shape', [(5, 13, 57), (300, 7, 96), (3, 40, 130), (4, 1, 40), (301, 44, 88)],
-                         ids=['small', 'many-tiles', 'long-q', 'one-subaperture', 'spotlight-12k-final'])
+@pytest.mark.parametrize('shape', [(5, 13, 57), (300, 7, 96), (3, 40, 130), (4, 1, 40), (301, 44, 88), (400, 59, 113)],
+                         ids=['small', 'many-tiles', 'long-q', 'one-subaperture', 'spotlight-12k-final', 'two-stages'])
 def test_final_tensor_cores_match_oracle(lib, oracle_lib, mode, tol, weighted, shape):
     """The tcgen05 final stage (T = 32) against the float64 oracle: split bfloat16 products within 2e-4, one
     float16 product within 3e-3 (its operands carry 11 bits); units beyond one per multiprocessor, an odd tile count
     (the float16 form pairs tiles), one final subaperture (one MMA issuer), padding of Qf to a multiple of 16,
-    aperture weights, and the final stage's shape at the 12,288 x 8,832 spotlight (Pf 44, Qf 88)."""
+    aperture weights, the final stage's shape at the 12,288 x 8,832 spotlight (Pf 44, Qf 88), and a shape whose
+    operands leave room for two pipeline stages only, with an odd subaperture count and several units per block."""
     T = 32
     rng = np.random.default_rng(7 * mode + weighted + shape[0])
     B, Pf, Qf = shape
@@ -325,3 +326,20 @@ def test_image_tensor_cores_repeatable_bitwise(golden, monkeypatch, precision, f
     a = f(g['S'])
     b = f(g['S'])
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_image_float16_large_amplitudes(golden, oracle_lib):
+    """The float16 tensor-core final stage scales the samples into float16's range: a history 2^24 times larger
+    (corner reflectors and the coherent gain of a large image reach far beyond 65504) gives a finite image that
+    matches the reference former's within -60 dB."""
+    from fastsar_b200 import ImageFormer, sim
+    g = golden('image_spot512')
+    w = sim.workload('spotlight_512')
+    col = w['col']
+    f = ImageFormer(col.ant, col.fmin, col.df, col.K, 512, 512, 0.25, 0.25, w['e1'], w['e2'], precision='float16')
+    big = float(2 ** 24)
+    img = f((g['S'] * big).astype(np.complex64))
+    assert np.all(np.isfinite(img.view(np.float32)))
+    e = oracle_lib.err_db(img / big, g['ffbp'])
+    print(f'float16 at 2^24 x amplitude: {e:.1f} dB vs reference former')
+    assert e < -60.0
