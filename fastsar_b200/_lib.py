@@ -11,11 +11,12 @@ LIB_PATH = os.path.join(HERE, 'libffbp_b200.so')
 
 FFBP_OK, FFBP_E_ARG, FFBP_E_CUDA, FFBP_E_NOMEM, FFBP_E_WORKSPACE, FFBP_E_UNSUPPORTED = 0, -1, -2, -3, -4, -5
 FFBP_FINAL_FP32, FFBP_FINAL_TC_F16, FFBP_FINAL_TC_BF16X3 = 0, 1, 2
+FFBP_LEVELS_TC = 0x100
 
 # every symbol include/ffbp_b200.h declares
 EXPORTS = ('ffbp_last_error', 'ffbp_abi_version', 'ffbp_plan_create', 'ffbp_plan_destroy', 'ffbp_plan_workspace_bytes',
            'ffbp_form', 'ffbp_form_timed', 'ffbp_plan_info', 'ffbp_level', 'ffbp_phases', 'ffbp_final',
-           'ffbp_bp_points_f64', 'ffbp_simulate', 'ffbp_form_static')
+           'ffbp_bp_points_f64', 'ffbp_simulate', 'ffbp_form_static', 'ffbp_level_tc', 'ffbp_level_tc_scratch_bytes')
 
 _c_int, _c_double, _vp = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
 
@@ -66,6 +67,10 @@ def load():
     L.ffbp_plan_info.argtypes = [_vp, ctypes.POINTER(_c_int), ctypes.POINTER(_c_int)]
     L.ffbp_level.argtypes = [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_int, _c_double,
                              _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp]
+    L.ffbp_level_tc.argtypes = [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_int,
+                                _c_double, _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t,
+                                _vp, _vp]
+    L.ffbp_level_tc_scratch_bytes.argtypes = [_c_int, _c_int, _c_int, _c_int]
     L.ffbp_phases.argtypes = [_vp, _c_int, _vp, _c_int, _vp, _c_int, _vp, _c_double, _c_double, _c_int, _vp, _vp]
     L.ffbp_final.argtypes = [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _c_double, _c_double, _c_double,
                              _c_double, _vp, _vp, _vp, _c_double, _vp, _c_int, _vp, _vp]
@@ -74,6 +79,7 @@ def load():
     L.ffbp_simulate.argtypes = [_vp, _c_int, _c_int, _c_double, _c_double, _vp, _vp, _c_int, _vp, _vp]
     for name in EXPORTS:
         getattr(L, name).restype = _c_int
+    L.ffbp_level_tc_scratch_bytes.restype = ctypes.c_size_t
     _LIB = L
     return L
 

@@ -100,8 +100,14 @@ def _check_grid(nx, ny, spx, spy, e1, e2):
 
 
 def _final_mode(precision):
+    """The formation mode of a precision: 'float32' the float32 kernels (FASTSAR_FINAL=tc3 puts the final stage on
+    the tensor cores in split bfloat16); 'float16' the levels and the final stage on the tensor cores (FASTSAR_LEVELS=
+    fp32 keeps the levels on the float32 kernel)."""
     if precision == 'float16':
-        return _lib.FFBP_FINAL_TC_F16
+        lv = os.environ.get('FASTSAR_LEVELS', 'tc').strip().lower() or 'tc'
+        if lv not in ('tc', 'fp32'):
+            raise ValueError(f"FASTSAR_LEVELS must be 'tc' or 'fp32', got {lv!r}")
+        return _lib.FFBP_FINAL_TC_F16 | (_lib.FFBP_LEVELS_TC if lv == 'tc' else 0)
     choice = os.environ.get('FASTSAR_FINAL', 'fp32').strip().lower() or 'fp32'
     if choice not in ('fp32', 'tc3'):
         raise ValueError(f"FASTSAR_FINAL must be 'fp32' or 'tc3', got {choice!r}")
@@ -231,11 +237,16 @@ class ImageFormer:
     img = former(S). Building plans the tiles and filters and computes the float64 geometry on the device; each call
     performs only the image formation. aperture_weight(points [m, 3], pulses [n]) -> W [n, m] applies a per-pixel
     weight of pulses in the final stage (final_weights); ref [P] is the one-way range each pulse is referenced to
-    when it is not |ant|. One former must not be called from two threads at once."""
+    when it is not |ant|. One former must not be called from two threads at once.
+
+    precision='float32' runs the float32 kernels with the reference's filters (70 dB stop band); 'float16' is the
+    mixed-precision form: the levels and the final stage on the tensor cores (split bfloat16 products, a float16
+    intermediate, float16 final operands, float32 accumulation) with 80 dB filters, whose smaller error leaves room
+    for the reduced-precision arithmetic. atten (an extension of this package) sets the filters' stop band in dB."""
 
     def __init__(self, ant, fmin, df, K, nx, ny, spx, spy, e1=(1.0, 0.0, 0.0), e2=(0.0, 1.0, 0.0), *, backend='auto',
                  precision='float32', window=True, T='auto', levels=None, pmax=0.4, target_db=-40.0, aperture_weight=None,
-                 ref=None, range_gate='auto', padded=None):
+                 ref=None, range_gate='auto', padded=None, atten=None):
         self.ant = _check_positions(ant)
         self.P, self.K = self.ant.shape[0], int(K)
         if self.K < 2:
@@ -247,6 +258,11 @@ class ImageFormer:
         if precision not in ('float32', 'float16'):
             raise ValueError("cuda precision: 'float32' or 'float16'")
         self.precision = precision
+        if atten is None:
+            atten = 80.0 if precision == 'float16' else 70.0
+        if not (np.isfinite(atten) and 20.0 <= float(atten) <= 200.0):
+            raise ValueError(f'atten must be a stop-band attenuation in dB between 20 and 200, got {atten!r}')
+        self.atten = float(atten)
         self.window = window
         self.nx, self.ny = nx, ny
         self.predicted_error_db = None
@@ -283,7 +299,7 @@ class ImageFormer:
         while True:
             try:
                 plan = _plan.make_plan(col, nx, ny, spx, spy, T=T, nlev=nlev, pmax=pmax, e1=e1, e2=e2,
-                                       pulse=padded and padded[2])
+                                       pulse=padded and padded[2], atten=self.atten)
                 break
             except ValueError as e:
                 if levels is not None or 'cannot split' not in str(e) or nlev >= 8:

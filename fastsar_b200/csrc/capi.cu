@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <algorithm>
 #include <vector>
 
 #include "../../include/ffbp_b200.h"
@@ -103,8 +104,12 @@ int ffbp_plan_create(const ffbp_plan_desc *d, void *stream_, ffbp_plan **out)
     cudaStream_t s = static_cast<cudaStream_t>(stream_);
     if (d->nlev < 1 || !d->levels) return fail(FFBP_E_ARG, "plan needs at least one level, got %d", d->nlev);
     if (d->T != 16 && d->T != 32) return fail(FFBP_E_ARG, "final tile size T must be 16 or 32, got %d", d->T);
-    if (d->final_mode != FFBP_FINAL_FP32 && d->final_mode != FFBP_FINAL_TC_F16 && d->final_mode != FFBP_FINAL_TC_BF16X3)
-        return fail(FFBP_E_ARG, "unknown final_mode %d", d->final_mode);
+    {
+        const int fm = d->final_mode & 0xff, flags = d->final_mode & ~0xff;
+        if ((fm != FFBP_FINAL_FP32 && fm != FFBP_FINAL_TC_F16 && fm != FFBP_FINAL_TC_BF16X3) || (flags & ~FFBP_LEVELS_TC))
+            return fail(FFBP_E_ARG, "unknown final_mode %d", d->final_mode);
+    }
+    if (d->nlev > 8) return fail(FFBP_E_ARG, "%d levels, at most 8", d->nlev);
     if (d->nx < 1 || d->ny < 1 || d->Nx < d->nx || d->Ny < d->ny || d->ox < 0 || d->oy < 0)
         return fail(FFBP_E_ARG, "bad grid: nx %d ny %d Nx %d Ny %d ox %d oy %d", d->nx, d->ny, d->Nx, d->Ny, d->ox, d->oy);
     if (!d->h_ant_f || !d->h_cen_f || !d->h_first_f) return fail(FFBP_E_ARG, "final-stage geometry missing");
@@ -224,10 +229,29 @@ int ffbp_plan_create(const ffbp_plan_desc *d, void *stream_, ffbp_plan **out)
     return cleanup(FFBP_OK);
 }
 
+// Whether level l runs on the tensor cores (FFBP_LEVELS_TC and a shape the kernel covers).
+static bool level_on_tc(const ffbp_plan *p, int l)
+{
+    const DevLevel &v = p->lv[l];
+    return (p->final_mode & FFBP_LEVELS_TC) && ffbp::level_tc_supported(v.C, v.Dk > 1 ? v.Lk : 1, v.Dk);
+}
+
+// The float16 intermediate of the tensor-core levels: the largest any of them needs.
+static size_t tc_scratch(const ffbp_plan *p)
+{
+    size_t m = 0;
+    for (int l = 0; l < p->nlev; ++l) {
+        if (!level_on_tc(p, l)) continue;
+        const DevLevel &v = p->lv[l];
+        m = std::max(m, ffbp::level_tc_scratch_bytes(v.Np, v.C, v.P, v.Ko));
+    }
+    return m;
+}
+
 int ffbp_plan_workspace_bytes(const ffbp_plan *p, size_t *bytes)
 {
     if (!p || !bytes) return fail(FFBP_E_ARG, "null argument");
-    *bytes = 256 + align256(p->bufA * sizeof(float2)) + align256(p->bufB * sizeof(float2));
+    *bytes = 256 + align256(p->bufA * sizeof(float2)) + align256(p->bufB * sizeof(float2)) + align256(tc_scratch(p));
     return FFBP_OK;
 }
 
@@ -244,10 +268,12 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
     int *bad = reinterpret_cast<int *>(ws);
     float2 *bufA = reinterpret_cast<float2 *>(ws + 256);
     float2 *bufB = reinterpret_cast<float2 *>(ws + 256 + align256(p->bufA * sizeof(float2)));
-    // status words: bad[0] the first non-finite pulse (0x7f7f7f7f: none), bad[1] the tensor-core stage's wait
-    // status, bad[2] the largest |component| of the last level's output (float bits)
+    void *scratch = ws + 256 + align256(p->bufA * sizeof(float2)) + align256(p->bufB * sizeof(float2));
+    // status words: bad[0] the first non-finite pulse (0x7f7f7f7f: none), bad[1] the tensor-core kernels' wait
+    // status, bad[2 + l] the largest |component| of level l's input (float bits; l = nlev: the final stage's)
+    int *amax = bad + 2;
     cudaError_t e = cudaMemsetAsync(bad, 0x7f, sizeof(int), s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(bad + 1, 0, 2 * sizeof(int), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(bad + 1, 0, (size_t)(p->nlev + 2) * sizeof(int), s);
     if (e != cudaSuccess) return cuda_fail(e, "status reset");
     const bool timed = stage_ms != nullptr;
     if (timed && n_stage < p->nlev + 1) return fail(FFBP_E_ARG, "stage_ms holds %d entries, %d needed", n_stage, p->nlev + 1);
@@ -259,6 +285,10 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
     }
     auto destroy_events = [&]() { for (auto &x : ev) cudaEventDestroy(x); };
     const float2 *in = static_cast<const float2 *>(d_S);
+    if (level_on_tc(p, 0) && (e = ffbp::launch_amax(in, (size_t)p->lv[0].P * p->lv[0].K, amax, s)) != cudaSuccess) {
+        destroy_events();
+        return cuda_fail(e, "history scan");
+    }
     for (int l = 0; l < p->nlev; ++l) {
         const DevLevel &v = p->lv[l];
         float2 *outp = (l % 2 == 0) ? bufA : bufB;
@@ -268,9 +298,9 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
         L.out = outp; L.bad = l == 0 ? bad : nullptr;
         L.Np = v.Np; L.C = v.C; L.P = v.P; L.K = v.K; L.Ko = v.Ko; L.Po = v.Po; L.Dk = v.Dk; L.Lk = v.Lk; L.plk = v.plk;
         L.Dp = v.Dp; L.Lp = v.Lp; L.plp = v.plp; L.kc = v.kc;
-        L.amax = (l == p->nlev - 1 && p->final_mode == FFBP_FINAL_TC_F16) ? bad + 2 : nullptr;
+        L.amax = amax + l + 1;
         const char *why = nullptr;
-        e = ffbp::launch_level(L, s, &why);
+        e = level_on_tc(p, l) ? ffbp::launch_level_tc(L, amax + l, scratch, bad + 1, s, &why) : ffbp::launch_level(L, s, &why);
         if (why) { destroy_events(); return fail(FFBP_E_UNSUPPORTED, "level %d: %s", l, why); }
         if (e != cudaSuccess) { destroy_events(); return cuda_fail(e, "level kernel"); }
         if (timed) cudaEventRecord(ev[l + 1], s);
@@ -281,9 +311,10 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
     F.spx = p->spx; F.spy = p->spy; F.a0 = p->a0; F.a1 = p->a1; F.fc2 = p->fc2; F.ucx = p->ucx; F.ucy = p->ucy;
     F.rc = p->rc; F.w = p->wf; F.tiles = nullptr; F.img = static_cast<float2 *>(d_img); F.first = p->first;
     F.nx = p->nx; F.ny = p->ny; F.ox = p->ox; F.oy = p->oy; F.scale = 1.f; F.err = bad + 1;
-    F.amax = p->final_mode == FFBP_FINAL_TC_F16 ? bad + 2 : nullptr;
+    F.amax = amax + p->nlev;
+    const int fm = p->final_mode & 0xff;
     const char *why = nullptr;
-    e = p->final_mode == FFBP_FINAL_FP32 ? ffbp::launch_final_fp32(F, s, &why) : ffbp::launch_final_tc(F, p->final_mode, s, &why);
+    e = fm == FFBP_FINAL_FP32 ? ffbp::launch_final_fp32(F, s, &why) : ffbp::launch_final_tc(F, fm, s, &why);
     if (why) { destroy_events(); return fail(FFBP_E_UNSUPPORTED, "final stage: %s", why); }
     if (e != cudaSuccess) { destroy_events(); return cuda_fail(e, "final kernel"); }
     if (timed) {
@@ -293,14 +324,14 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
         destroy_events();
         int st = 0;
         if ((e = cudaMemcpy(&st, bad + 1, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess) return cuda_fail(e, "status read");
-        if (st) return fail(FFBP_E_CUDA, "the tensor-core final stage stopped waiting on its pipeline (a bounded wait ran out)");
+        if (st) return fail(FFBP_E_CUDA, "a tensor-core kernel stopped waiting on its pipeline (a bounded wait ran out)");
     }
     if (h_bad) {
         int v[2] = {0, 0};
         if ((e = cudaMemcpyAsync(v, bad, 2 * sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return cuda_fail(e, "status read");
         if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "form");
         *h_bad = (v[0] == 0x7f7f7f7f) ? -1 : v[0];
-        if (v[1]) return fail(FFBP_E_CUDA, "the tensor-core final stage stopped waiting on its pipeline (a bounded wait ran out)");
+        if (v[1]) return fail(FFBP_E_CUDA, "a tensor-core kernel stopped waiting on its pipeline (a bounded wait ran out)");
     }
     return FFBP_OK;
 }
@@ -321,7 +352,11 @@ int ffbp_plan_info(const ffbp_plan *p, int *nlev, int *launches)
 {
     if (!p) return fail(FFBP_E_ARG, "ffbp_plan_info: null plan");
     if (nlev) *nlev = p->nlev;
-    if (launches) *launches = p->nlev + 1;
+    if (launches) {
+        int n = 1;
+        for (int l = 0; l < p->nlev; ++l) n += level_on_tc(p, l) ? 2 + (l == 0) : 1;
+        *launches = n;
+    }
     return FFBP_OK;
 }
 
@@ -341,6 +376,38 @@ int ffbp_level(const void *d_x, int Np, int P, int K, const void *d_phase, int C
     cudaError_t e = ffbp::launch_level(L, static_cast<cudaStream_t>(stream), &why);
     if (why) return fail(FFBP_E_UNSUPPORTED, "ffbp_level: %s", why);
     if (e != cudaSuccess) return cuda_fail(e, "ffbp_level");
+    return FFBP_OK;
+}
+
+size_t ffbp_level_tc_scratch_bytes(int Np, int C, int P, int Ko)
+{
+    if (Np < 1 || C < 1 || P < 1 || Ko < 1) return 0;
+    return ffbp::level_tc_scratch_bytes(Np, C, P, Ko);
+}
+
+int ffbp_level_tc(const void *d_x, int Np, int P, int K, const void *d_phase, int C, const float *d_tk, int Lk, int plk,
+                  int Dk, int Ko, double kc, const float *d_tp, int Lp, int plp, int Dp, int Po, const float *d_wp,
+                  const float *d_wk, void *d_out, int *d_bad, void *d_scratch, size_t scratch_bytes, int *d_status,
+                  void *stream)
+{
+    if (!d_x || !d_phase || !d_out || !d_scratch || !d_status) return fail(FFBP_E_ARG, "ffbp_level_tc: null buffer");
+    if (Np < 1 || P < 1 || K < 1 || C < 1 || Dk < 1 || Dp < 1 || Ko < 1 || Po < 1) return fail(FFBP_E_ARG, "ffbp_level_tc: non-positive size");
+    if ((Dk > 1 && (!d_tk || Lk < 1)) || (Dp > 1 && (!d_tp || Lp < 1))) return fail(FFBP_E_ARG, "ffbp_level_tc: taps missing");
+    if (((uintptr_t)d_scratch & 15) != 0) return fail(FFBP_E_ARG, "ffbp_level_tc: scratch must be 16-byte aligned");
+    const size_t need = ffbp::level_tc_scratch_bytes(Np, C, P, Ko);
+    if (scratch_bytes < need) return fail(FFBP_E_WORKSPACE, "ffbp_level_tc: scratch of %zu bytes, %zu needed", scratch_bytes, need);
+    ffbp::LevelLaunch L;
+    L.x = static_cast<const float2 *>(d_x); L.phase = static_cast<const float2 *>(d_phase); L.tk = d_tk; L.tp = d_tp;
+    L.wp = d_wp; L.wk = d_wk; L.out = static_cast<float2 *>(d_out); L.bad = d_bad;
+    L.Np = Np; L.C = C; L.P = P; L.K = K; L.Ko = Ko; L.Po = Po; L.Dk = Dk; L.Lk = Lk; L.plk = plk; L.Dp = Dp;
+    L.Lp = Lp; L.plp = plp; L.kc = kc; L.amax = d_status + 2;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e = ffbp::launch_amax(L.x, (size_t)Np * P * K, d_status + 1, s);
+    if (e != cudaSuccess) return cuda_fail(e, "ffbp_level_tc");
+    const char *why = nullptr;
+    e = ffbp::launch_level_tc(L, d_status + 1, d_scratch, d_status, s, &why);
+    if (why) return fail(FFBP_E_UNSUPPORTED, "ffbp_level_tc: %s", why);
+    if (e != cudaSuccess) return cuda_fail(e, "ffbp_level_tc");
     return FFBP_OK;
 }
 

@@ -535,9 +535,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
         // ------------------------------------------------------------------ epilogue (warps 0..3)
         float *P0 = sP, *P1 = sP + 32 * 65;
         const float oscale = a.scale / (BF ? 1.f : operand_scale(a.amax));
+        // after a failed wait a warp keeps stepping through the units (and the epilogue's named barriers, which all
+        // four warps must reach) without waiting, reading or writing
+        bool live = true;
         for (int ul = 0; ul < nul; ++ul) {
             const int ab = ul & 1;
-            if (!mbar_wait<EPILOGUE_HINT_NS>(&accf[ab], (uint32_t)((ul >> 1) & 1), &s_abort, a.err)) break;
+            if (live) live = mbar_wait<EPILOGUE_HINT_NS>(&accf[ab], (uint32_t)((ul >> 1) & 1), &s_abort, a.err);
+            live = __all_sync(0xffffffffu, live);
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t lanes = (uint32_t)(32 * warp) << 16;
             float *mine = (warp & 1) ? P1 : P0;                 // accumulator rows 32..63 (mod 64) are the Ai rows
@@ -558,7 +562,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
             if (BF) {
                 // warps 0, 1: hi rows (hi hi + hi lo); then warps 2, 3 add the lo rows (lo hi + lo lo)
                 float v[16];
-                if (warp < 2) {
+                if (live && warp < 2) {
 #pragma unroll
                     for (int c0 = 0; c0 < 64; c0 += 16) {
                         gather(c0, 64, v);
@@ -570,7 +574,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
                     if (lane == 0) mbar_arrive(&acce[ab]);
                 }
                 asm volatile("bar.sync 1, 128;" ::: "memory");
-                if (warp >= 2) {
+                if (live && warp >= 2) {
 #pragma unroll
                     for (int c0 = 0; c0 < 64; c0 += 16) {
                         gather(c0, 64, v);
@@ -582,12 +586,12 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
                     if (lane == 0) mbar_arrive(&acce[ab]);
                 }
                 asm volatile("bar.sync 1, 128;" ::: "memory");
-                tile_pixels(a, unit_tile<BF>(ul, 0), P0, P1, t, oscale);
+                if (live) tile_pixels(a, unit_tile<BF>(ul, 0), P0, P1, t, oscale);
                 asm volatile("bar.sync 1, 128;" ::: "memory");
             } else {
                 // tile slot ts: accumulator rows and columns [64 ts, 64 ts + 64), read by warps 2 ts and 2 ts + 1
                 for (int ts = 0; ts < 2; ++ts) {
-                    if ((warp >> 1) == ts) {
+                    if (live && (warp >> 1) == ts) {
                         float v[16];
 #pragma unroll
                         for (int c0 = 0; c0 < 64; c0 += 16) {
@@ -601,7 +605,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
                     }
                     asm volatile("bar.sync 1, 128;" ::: "memory");
                     const int tile = unit_tile<BF>(ul, ts);
-                    if (tile < a.B) tile_pixels(a, tile, P0, P1, t, oscale);
+                    if (live && tile < a.B) tile_pixels(a, tile, P0, P1, t, oscale);
                     asm volatile("bar.sync 1, 128;" ::: "memory");
                 }
             }

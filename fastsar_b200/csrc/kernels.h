@@ -23,6 +23,17 @@ struct LevelLaunch {
 // Returns cudaSuccess, or an error with *why set to a static message for shapes the kernels do not cover.
 cudaError_t launch_level(const LevelLaunch &L, cudaStream_t s, const char **why);
 
+// A level on the tensor cores (level_tc.cu): the frequency FIR of every child as one product per pulse (bfloat16
+// x 3, float32 accumulation) into a float16 intermediate in `scratch` (level_tc_scratch_bytes), then the pulse FIR
+// in float32. amax_in: the largest |component| of L.x (float bits), which sets the intermediate's scale; L.amax
+// receives the output's. err: set when a bounded wait runs out.
+bool level_tc_supported(int C, int Lk, int Dk);
+size_t level_tc_scratch_bytes(int Np, int C, int P, int Ko);
+cudaError_t launch_level_tc(const LevelLaunch &L, const int *amax_in, void *scratch, int *err, cudaStream_t s,
+                            const char **why);
+// The largest |component| of n complex samples into *amax (float bits, atomicMax; start at 0).
+cudaError_t launch_amax(const float2 *x, size_t n, int *amax, cudaStream_t s);
+
 // Child phases (geometry.cu).
 cudaError_t launch_phases(const double *ant, int P, const double *ref, int Np, const double *cen, int C,
                           const double *range, double k0c, double k1, int cancel_free, float2 *phase, cudaStream_t s);

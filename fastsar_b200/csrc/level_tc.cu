@@ -1,0 +1,666 @@
+// A level on the tcgen05 tensor cores (sm_100a): the chosen form of one merge stage of the FFBP (the reference's
+// rot_fir_k + fir_p: fastsar/ffbp_cpu.cpp:146-293, fastsar/ffbp_cuda.py:48-256), in two passes.
+//
+// The rotation of child c at input pulse p and sample k, exp(2 pi i (c0 + sl (k - kc))), followed by the frequency
+// FIR y[j] = sum_r hk[r] x[Dk j + r - plk] rot(Dk j + r - plk), factors as
+//     y_c[p, j] = R_c,p[j] sum_r m_c,p[r] x[p, Dk j + r - plk],
+//     m_c,p[r] = hk[r] exp(2 pi i sl r)                         (the child's modulated taps),
+//     R_c,p[j] = exp(2 pi i (c0 + sl (Dk j - plk - kc)))        (a ramp along the output columns).
+// Per pulse the sum is a dense product: the modulated taps of every child (children x taps) times the Hankel
+// windows of the parent's row (taps x output columns), shared by all children. The pulse FIR that follows acts on
+// the frequency-decimated columns.
+//
+// Pass 1 (level_tc_gemm): per parent and pulse the product on the tensor cores, three bfloat16 products (x = hi + lo:
+// hi hi + hi lo + lo hi) accumulated in float32; then the ramp, a power-of-two scale into float16's range, and the
+// intermediate y [Np, C, P, Kop] as float16 pairs. Real form: A' = [Mr_0; Mi_0; Mr_1; Mi_1; ...] (128 rows, two per
+// child, K = the taps padded to Lkp), B' = [Xr_j; Xi_j] (2 Nt rows: the real and imaginary Hankel rows of the tile's
+// Nt columns), D = A' B'^T: re = MrXr - MiXi, im = MrXi + MiXr.
+// Block roles: warps 16..23 produce, per pulse, the modulated taps (once per pulse, for all column tiles) and per
+// (pulse, tile) the bfloat16 hi/lo planes of the parent row's window and from them the Hankel rows; warp 24 issues the
+// MMAs (M = 128, N = 2 Nt, K = 16) into one of two TMEM accumulators; warps 0..15 read the accumulator (warp w reads
+// lane quarter w % 4, i.e. children 16 (w % 4) .. + 15, and a quarter of the columns), exchange halves between the
+// two rows of a child, apply the ramp and store.
+//
+// Pass 2 (level_fir): the pulse FIR of the intermediate on the CUDA cores in float32 (a thread per two columns with
+// the ceil(Lp / Dp) outputs it feeds in registers), written as complex64 with the largest component recorded.
+//
+// Every wait on a barrier is bounded in time; a wait that runs out sets *err and the block winds down.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace ffbp {
+
+namespace {
+
+constexpr int NCW = 16;                       // consumer warps 0..15
+constexpr int NPW = 8;                        // producer warps 16..23
+constexpr int MMAW = NCW + NPW;               // warp 24
+constexpr int NTHR = (NCW + NPW + 1) * 32;
+constexpr int NPT = NPW * 32;
+constexpr uint64_t WAIT_NS = 2000000000ull;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ uint32_t mbar_test(uint64_t *bar, uint32_t parity, uint32_t hint_ns)
+{
+    uint32_t done;
+    if (hint_ns)
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+                     : "=r"(done) : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns) : "memory");
+    else
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+                     : "=r"(done) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return done;
+}
+
+__device__ __forceinline__ uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait for the phase of parity `parity`: false (the block's abort flag and *err set) after WAIT_NS, or when
+// another thread of the block has aborted.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t hint_ns, volatile int *abort, int *err)
+{
+    if (mbar_test(bar, parity, 0)) return true;
+    const uint64_t t0 = global_ns();
+    for (uint32_t it = 1;; ++it) {
+        if (mbar_test(bar, parity, hint_ns)) return true;
+        if ((it & 255u) == 0) {
+            if (*abort) return false;
+            if (global_ns() - t0 > WAIT_NS) break;
+        }
+    }
+    *abort = 1;
+    if (err) atomicExch(err, 1);
+    return false;
+}
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
+{
+    // sm_100 shared-memory matrix descriptor: start address, leading (K) and stride (M/N) byte offsets in 16-byte
+    // units, version 1 at bit 46, no swizzle
+    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+                 :: "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :: "r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t addr, float *v)
+{
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(addr));
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// x = hi + lo with hi = bfloat16(x) and lo = bfloat16(x - hi), two values per 32-bit word (first value low)
+__device__ __forceinline__ void split2(float a, float b, uint32_t &hi, uint32_t &lo)
+{
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    const __nv_bfloat162 l = __floats2bfloat162_rn(a - __low2float(h), b - __high2float(h));
+    hi = *reinterpret_cast<const uint32_t *>(&h);
+    lo = *reinterpret_cast<const uint32_t *>(&l);
+}
+
+// byte offset of element (row, k) of a K-major operand without swizzle: core matrices of 8 rows x 8 elements
+__device__ __forceinline__ uint32_t core_off(int row, int kchunk, int nkc)
+{
+    return (uint32_t)(((row >> 3) * nkc + kchunk) * 128 + (row & 7) * 16);
+}
+
+struct GemmArgs {
+    const float2 *__restrict__ x;     // [Np, P, K]
+    const float2 *__restrict__ ph;    // [Np, C, P] (c0, sl)
+    const float *__restrict__ tk;     // [Lk]
+    const float *__restrict__ wp;     // [P] or null
+    const float *__restrict__ wk;     // [K] or null
+    int *bad;                         // first non-finite pulse (level 0) or null
+    const int *amax_in;               // largest |component| of x (float bits)
+    __half2 *y;                       // [Np, C, P, Kop]
+    int *err;
+    int Np, C, P, K, Ko, Kop, Dk, Lk, plk, Lkp, Nt, ntile, W, pseg, nseg, SB;
+    float kc;
+};
+
+// The power of two that brings values up to 4 amax (the taps' absolute sum is below 4 for the decimators of any
+// plan) below 2^13: the float16 intermediate then stays in range and keeps 11 significant bits.
+__device__ __forceinline__ float y_scale(const int *amax)
+{
+    const float m = amax ? __int_as_float(*amax) : 0.f;
+    if (!(m > 0.f) || !isfinite(m)) return 1.f;
+    int ex;
+    frexpf(4.f * m, &ex);
+    ex = ex < -100 ? -100 : (ex > 100 ? 100 : ex);
+    return ldexpf(1.f, 13 - ex);
+}
+
+__global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const int nkc = a.Lkp / 8;                               // core matrices along K
+    const uint32_t apart = 128u * a.Lkp * 2u;                // one part (hi or lo) of A'
+    const uint32_t bpart = 2u * a.Nt * a.Lkp * 2u;           // one part of B'
+    unsigned char *sA = smem;                                // [2 pulses][hi, lo]
+    unsigned char *sB = sA + 2 * 2 * apart;                  // [SB stages][hi, lo]
+    const int Wp = (a.W + 9) & ~1;                           // plane length in elements (even, with slack)
+    uint32_t *pl = reinterpret_cast<uint32_t *>(sB + (size_t)a.SB * 2 * bpart);   // [4][Wp / 2] words
+    float *s_tk = reinterpret_cast<float *>(pl + 4 * (Wp / 2));                   // [Lkp]
+    uint64_t *bars = reinterpret_cast<uint64_t *>(s_tk + a.Lkp + (a.Lkp & 1));
+    uint64_t *afull = bars, *aempty = bars + 2, *bfull = bars + 4, *bempty = bfull + a.SB, *dfull = bempty + a.SB,
+             *dempty = dfull + 2;
+    __shared__ uint32_t s_tmem;
+    __shared__ volatile int s_abort;
+    __shared__ float s_scale;
+
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int n = blockIdx.x / a.nseg, seg = blockIdx.x % a.nseg;
+    const int p0 = seg * a.pseg, p1 = min(a.P, p0 + a.pseg);
+    const int npl = p1 - p0;                                  // pulses of this block
+    const int nst = npl * a.ntile;                            // stages (pulse, tile)
+    const int ncol = 2 * a.Nt;                                // accumulator columns per stage
+
+    if (t == 0) {
+        s_abort = 0;
+        s_scale = y_scale(a.amax_in);
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&afull[i], NPW);
+            mbar_init(&aempty[i], 1);
+            mbar_init(&dfull[i], 1);
+            mbar_init(&dempty[i], NCW);
+        }
+        for (int i = 0; i < a.SB; ++i) {
+            mbar_init(&bfull[i], NPW);
+            mbar_init(&bempty[i], 1);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int i = t; i < a.Lkp; i += NTHR) s_tk[i] = i < a.Lk ? (a.tk ? a.tk[i] : 1.f) : 0.f;   // Dk = 1: one tap 1
+    // A' rows of no child stay zero: clear both pulses' buffers once
+    for (int i = t; i < (int)(4 * apart / 16); i += NTHR) reinterpret_cast<uint4 *>(sA)[i] = make_uint4(0, 0, 0, 0);
+    if (warp == MMAW) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" :: "r"(smem_u32(&s_tmem)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    const float scale = s_scale;
+
+    if (warp >= NCW && warp < MMAW) {
+        // ------------------------------------------------------------------ producers
+        const int pt = t - NCW * 32;
+        const float2 *__restrict__ xn = a.x + (size_t)n * a.P * a.K;
+        const float2 *__restrict__ phn = a.ph + (size_t)n * a.C * a.P;
+        const int npair = (a.W + 1) / 2;                      // window samples in pairs (2i, 2i + 1)
+        // the window of stage (pulse p, tile tt): samples k = kb + i, kb = Dk Nt tt - plk, i < W
+        float2 xv[4][2];                                      // this thread's pairs of the next stage (<= 4)
+        auto load = [&](int p, int tt) {
+            const int kb = a.Dk * a.Nt * tt - a.plk;
+            const float wpp = a.wp ? a.wp[p] : 1.f;
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                const int i = pt + m * NPT;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int k = kb + 2 * i + h;
+                    float2 v = make_float2(0.f, 0.f);
+                    if (i < npair && 2 * i + h < a.W && k >= 0 && k < a.K) {
+                        v = __ldg(&xn[(size_t)p * a.K + k]);
+                        if (a.wp) {
+                            const float w = wpp * a.wk[k];
+                            v.x *= w;
+                            v.y *= w;
+                        }
+                        if (a.bad && !(isfinite(v.x) && isfinite(v.y))) atomicMin(a.bad, p);
+                    }
+                    xv[m][h] = v;
+                }
+            }
+        };
+        if (nst > 0) load(p0, 0);
+        int sb = 0;
+        uint32_t sbpar = 0;
+        // after a failed wait a warp keeps stepping through the stages (and the producers' named barriers, which
+        // every producer warp must reach) without waiting or working
+        bool ok = true;
+        for (int s = 0; s < nst; ++s) {
+            const int pl_i = s / a.ntile, tt = s - pl_i * a.ntile, p = p0 + pl_i;
+            // modulated taps of pulse p (at its first tile), into A' buffer pl_i & 1
+            if (tt == 0 && ok) {
+                const int ab = pl_i & 1;
+                ok = mbar_wait(&aempty[ab], (uint32_t)(((pl_i >> 1) & 1) ^ 1), 1000, &s_abort, a.err);
+            }
+            if (tt == 0 && ok) {
+                const int ab = pl_i & 1;
+                unsigned char *Ab = sA + ab * 2 * apart;
+                for (int item = pt; item < a.C * nkc; item += NPT) {
+                    const int c = item / nkc, u = item - c * nkc;
+                    const float sl = __ldg(&phn[(size_t)c * a.P + p]).y;
+                    float2 z = cis_cycles(sl * (float)(8 * u));
+                    const float2 st = cis_cycles(sl);
+                    float mr[8], mi[8];
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) {
+                        const float h = s_tk[8 * u + e];
+                        mr[e] = h * z.x;
+                        mi[e] = h * z.y;
+                        z = cmul(z, st);
+                    }
+                    uint32_t rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        split2(mr[2 * e], mr[2 * e + 1], rh[e], rl[e]);
+                        split2(mi[2 * e], mi[2 * e + 1], ih[e], il[e]);
+                    }
+                    const uint32_t o0 = core_off(2 * c, u, nkc), o1 = core_off(2 * c + 1, u, nkc);
+                    *reinterpret_cast<uint4 *>(Ab + o0) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+                    *reinterpret_cast<uint4 *>(Ab + apart + o0) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+                    *reinterpret_cast<uint4 *>(Ab + o1) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+                    *reinterpret_cast<uint4 *>(Ab + apart + o1) = make_uint4(il[0], il[1], il[2], il[3]);
+                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&afull[ab]);
+            }
+            // the window's planes: xr hi, xr lo, xi hi, xi lo as bfloat16 pairs (word i = samples 2i, 2i + 1);
+            // the previous stage's Hankel rows have all been read from them (named barrier)
+            asm volatile("bar.sync 1, %0;" :: "n"(NPT) : "memory");
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                const int i = pt + m * NPT;
+                if (i < npair) {
+                    uint32_t rh, rl, ih, il;
+                    split2(xv[m][0].x, xv[m][1].x, rh, rl);
+                    split2(xv[m][0].y, xv[m][1].y, ih, il);
+                    pl[i] = rh;
+                    pl[Wp / 2 + i] = rl;
+                    pl[Wp + i] = ih;
+                    pl[3 * (Wp / 2) + i] = il;
+                }
+            }
+            // the next stage's samples while this one's Hankel rows are built
+            if (s + 1 < nst) {
+                const int s1 = s + 1, q = s1 / a.ntile;
+                load(p0 + q, s1 - q * a.ntile);
+            }
+            asm volatile("bar.sync 1, %0;" :: "n"(NPT) : "memory");
+            if (ok) ok = mbar_wait(&bempty[sb], sbpar ^ 1u, 1000, &s_abort, a.err);
+            // Hankel rows: row j < Nt: xr window from Dk j; row Nt + j: xi; 8 elements (16 bytes) per chunk
+            unsigned char *Bb = sB + sb * 2 * bpart;
+            const int nch = ncol * nkc;
+            for (int item = pt; ok && item < 2 * nch; item += NPT) {
+                const int part = item >= nch ? 1 : 0;
+                const int rem = item - part * nch;
+                const int row = rem / nkc, u = rem - row * nkc;
+                const int im = row >= a.Nt ? 1 : 0;
+                const int o = a.Dk * (row - im * a.Nt) + 8 * u;    // first element in the window
+                const uint32_t *src = pl + (2 * im + part) * (Wp / 2) + (o >> 1);
+                uint4 v;
+                if ((o & 1) == 0) {
+                    v = make_uint4(src[0], src[1], src[2], src[3]);
+                } else {
+                    const uint32_t w0 = src[0], w1 = src[1], w2 = src[2], w3 = src[3], w4 = src[4];
+                    v = make_uint4(__funnelshift_r(w0, w1, 16), __funnelshift_r(w1, w2, 16), __funnelshift_r(w2, w3, 16),
+                                   __funnelshift_r(w3, w4, 16));
+                }
+                *reinterpret_cast<uint4 *>(Bb + part * bpart + core_off(row, u, nkc)) = v;
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0 && ok) mbar_arrive(&bfull[sb]);
+            if (++sb == a.SB) { sb = 0; sbpar ^= 1u; }
+        }
+    } else if (warp == MMAW) {
+        // ------------------------------------------------------------------ MMA issue
+        if (lane == 0) {
+            const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(ncol >> 3) << 17) | ((128u >> 4) << 24);
+            const uint32_t sbo = (uint32_t)nkc * 128;
+            const uint32_t sA0 = smem_u32(sA), sB0 = smem_u32(sB);
+            int sb = 0;
+            uint32_t sbpar = 0;
+            for (int s = 0; s < nst; ++s) {
+                const int pl_i = s / a.ntile, tt = s - pl_i * a.ntile;
+                const int ab = pl_i & 1, db = s & 1;
+                if (tt == 0 && !mbar_wait(&afull[ab], (uint32_t)((pl_i >> 1) & 1), 0, &s_abort, a.err)) break;
+                if (!mbar_wait(&bfull[sb], sbpar, 0, &s_abort, a.err)) break;
+                if (!mbar_wait(&dempty[db], (uint32_t)(((s >> 1) & 1) ^ 1), 0, &s_abort, a.err)) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t dt = tmem + (uint32_t)(db * 256);
+                const uint32_t ah = sA0 + (uint32_t)ab * 2 * apart, al = ah + apart;
+                const uint32_t bh = sB0 + (uint32_t)sb * 2 * bpart, bl = bh + bpart;
+                for (int ks = 0; ks < a.Lkp / 16; ++ks) {
+                    const uint32_t ko = 256u * ks;
+                    mma_bf16(dt, smem_desc(ah + ko, 128, sbo), smem_desc(bh + ko, 128, sbo), idesc, ks > 0 ? 1u : 0u);
+                    mma_bf16(dt, smem_desc(ah + ko, 128, sbo), smem_desc(bl + ko, 128, sbo), idesc, 1u);
+                    mma_bf16(dt, smem_desc(al + ko, 128, sbo), smem_desc(bh + ko, 128, sbo), idesc, 1u);
+                }
+                mma_commit(&bempty[sb]);
+                mma_commit(&dfull[db]);
+                if (tt == a.ntile - 1) mma_commit(&aempty[ab]);
+                if (++sb == a.SB) { sb = 0; sbpar ^= 1u; }
+            }
+        }
+        __syncwarp();
+    } else {
+        // ------------------------------------------------------------------ consumers (warps 0..15)
+        const int q = warp & 3, g = warp >> 2;
+        const int c = 16 * q + (lane >> 1);                   // this lane's child (row 2c: Mr, row 2c + 1: Mi)
+        const bool odd = lane & 1;
+        const bool live = c < a.C;
+        const int cw = a.Nt / 4;                              // columns of this warp per tile
+        const float2 *__restrict__ phc = a.ph + ((size_t)n * a.C + (live ? c : 0)) * a.P;
+        __half2 *__restrict__ yc = a.y + ((size_t)n * a.C + (live ? c : 0)) * a.P * a.Kop;
+        float2 q0 = make_float2(0.f, 0.f);
+        for (int s = 0; s < nst; ++s) {
+            const int pl_i = s / a.ntile, tt = s - pl_i * a.ntile, p = p0 + pl_i;
+            const int db = s & 1;
+            if (tt == 0 && live) q0 = __ldg(&phc[p]);
+            // warp-uniform: the accumulator loads below are warp-collective
+            if (!__all_sync(0xffffffffu, mbar_wait(&dfull[db], (uint32_t)((s >> 1) & 1), 200, &s_abort, a.err))) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t base = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(db * 256);
+            const float2 st = cis_cycles(q0.y * (float)a.Dk);
+            for (int k8 = 0; k8 < cw; k8 += 8) {
+                const int cb = g * cw + k8;                   // first column of the chunk within the tile
+                float vr[8], vi[8];
+                tmem_ld8(base + (uint32_t)cb, vr);
+                tmem_ld8(base + (uint32_t)(a.Nt + cb), vi);
+                tmem_wait_ld();
+                if (k8 + 8 >= cw) {                           // the accumulator has been read
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&dempty[db]);
+                }
+                // even lane (Mr row) keeps columns 0..3 of the chunk, odd lane (Mi row) columns 4..7
+                float mr_r[4], mr_i[4], mi_r[4], mi_i[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const float sr = odd ? vr[i] : vr[4 + i], si = odd ? vi[i] : vi[4 + i];
+                    const float rr = __shfl_xor_sync(0xffffffffu, sr, 1), ri = __shfl_xor_sync(0xffffffffu, si, 1);
+                    const float orr = odd ? vr[4 + i] : vr[i], ori = odd ? vi[4 + i] : vi[i];
+                    mr_r[i] = odd ? rr : orr;
+                    mr_i[i] = odd ? ri : ori;
+                    mi_r[i] = odd ? orr : rr;
+                    mi_i[i] = odd ? ori : ri;
+                }
+                const int j0 = tt * a.Nt + cb + (odd ? 4 : 0);
+                if (live && j0 < a.Ko) {
+                    float2 w = cis_cycles(fmaf(q0.y, (float)(a.Dk * j0 - a.plk) - a.kc, q0.x));
+                    w.x *= scale;
+                    w.y *= scale;
+                    uint32_t outw[4];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        const float re = mr_r[i] - mi_i[i], im = mr_i[i] + mi_r[i];
+                        const float2 o = cmul(w, make_float2(re, im));
+                        const __half2 hv = __floats2half2_rn(o.x, o.y);
+                        outw[i] = *reinterpret_cast<const uint32_t *>(&hv);
+                        w = cmul(w, st);
+                    }
+                    *reinterpret_cast<uint4 *>(yc + (size_t)p * a.Kop + j0) = make_uint4(outw[0], outw[1], outw[2], outw[3]);
+                }
+            }
+        }
+    }
+
+    __syncthreads();
+    if (warp == MMAW) {
+        if (lane == 0) {
+            // drain: a commit on a fresh barrier completes once every earlier MMA of this thread has
+            uint64_t *dr = &afull[0];
+            mbar_init(dr, 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            mma_commit(dr);
+            const uint64_t t0 = global_ns();
+            while (!mbar_test(dr, 0, 0) && global_ns() - t0 < WAIT_NS) {
+            }
+        }
+        __syncwarp();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" :: "r"(tmem));
+    }
+}
+
+// --------------------------------------------------------------------------------------------------- pass 2
+struct FirArgs {
+    const __half2 *__restrict__ y;    // [rows, P, Kop]
+    const float *__restrict__ tp;     // [Lp]
+    float2 *__restrict__ out;         // [rows, Po, Ko]
+    int *amax;
+    const int *amax_in;
+    int rows, P, Kop, Ko, Po, Dp, Lp, plp, SEG, nseg, ncb;
+};
+
+template <int AP>
+__global__ void __launch_bounds__(128) level_fir(const FirArgs a)
+{
+    constexpr int APP = (AP + 3) & ~3;
+    extern __shared__ __align__(16) float s_tp[];             // [Dp][APP]: s_tp[b APP + s] = tp[Dp s + b]
+    int bid = blockIdx.x;
+    const int cb = bid % a.ncb;
+    bid /= a.ncb;
+    const int seg = bid % a.nseg;
+    const int row = bid / a.nseg;
+    const int t = threadIdx.x;
+    for (int r = t; r < a.Dp * APP; r += 128) {
+        const int b = r / APP, s = r - b * APP;
+        const int tap = a.Dp * s + b;
+        s_tp[r] = (s < AP && tap < a.Lp) ? (a.tp ? a.tp[tap] : 1.f) : 0.f;   // Dp = 1: one tap 1
+    }
+    __syncthreads();
+    const float inv = 1.f / y_scale(a.amax_in);
+    const int j = 2 * (cb * 128 + t);                          // two columns j, j + 1
+    const bool colok = j < a.Ko;
+    const int i_s = seg * a.SEG, i_e = min(a.Po, i_s + a.SEG);
+    const int g_end = i_e + AP - 1;
+    const __half2 *__restrict__ yr = a.y + (size_t)row * a.P * a.Kop + j;
+    float2 acc[2][AP];
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int s = 0; s < AP; ++s) acc[h][s] = make_float2(0.f, 0.f);
+    float vmax = 0.f;
+    int p = a.Dp * i_s - a.plp, b = 0;
+    for (int gi = i_s; gi < g_end;) {
+        if (p >= 0 && p < a.P && colok) {
+            const uint2 w = __ldg(reinterpret_cast<const uint2 *>(yr + (size_t)p * a.Kop));
+            const float2 v0 = __half22float2(*reinterpret_cast<const __half2 *>(&w.x));
+            const float2 v1 = __half22float2(*reinterpret_cast<const __half2 *>(&w.y));
+            float tb[APP];
+#pragma unroll
+            for (int s4 = 0; s4 < APP; s4 += 4) {
+                const float4 q4 = *reinterpret_cast<const float4 *>(&s_tp[b * APP + s4]);
+                tb[s4] = q4.x; tb[s4 + 1] = q4.y; tb[s4 + 2] = q4.z; tb[s4 + 3] = q4.w;
+            }
+#pragma unroll
+            for (int s = 0; s < AP; ++s) {
+                acc[0][s].x = fmaf(tb[s], v0.x, acc[0][s].x);
+                acc[0][s].y = fmaf(tb[s], v0.y, acc[0][s].y);
+                acc[1][s].x = fmaf(tb[s], v1.x, acc[1][s].x);
+                acc[1][s].y = fmaf(tb[s], v1.y, acc[1][s].y);
+            }
+        }
+        ++p;
+        if (++b == a.Dp) {                                    // group gi complete: output gi - (AP - 1) finished
+            b = 0;
+            const int i = gi - (AP - 1);
+            if (i >= i_s && colok) {
+                float2 *o = a.out + ((size_t)row * a.Po + i) * a.Ko + j;
+                const float2 o0 = make_float2(acc[0][AP - 1].x * inv, acc[0][AP - 1].y * inv);
+                const float2 o1 = make_float2(acc[1][AP - 1].x * inv, acc[1][AP - 1].y * inv);
+                o[0] = o0;
+                vmax = fmaxf(vmax, fmaxf(fabsf(o0.x), fabsf(o0.y)));
+                if (j + 1 < a.Ko) {
+                    o[1] = o1;
+                    vmax = fmaxf(vmax, fmaxf(fabsf(o1.x), fabsf(o1.y)));
+                }
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+#pragma unroll
+                for (int s = AP - 1; s > 0; --s) acc[h][s] = acc[h][s - 1];
+                acc[h][0] = make_float2(0.f, 0.f);
+            }
+            ++gi;
+        }
+    }
+    if (a.amax) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+        if ((t & 31) == 0 && vmax > 0.f) atomicMax(a.amax, __float_as_int(vmax));
+    }
+}
+
+template <int AP>
+cudaError_t launch_fir(FirArgs f, cudaStream_t s)
+{
+    constexpr int APP = (AP + 3) & ~3;
+    f.ncb = (f.Ko + 255) / 256;
+    const long base = (long)f.rows * f.ncb;
+    int nseg = 1;
+    while (base * nseg < 148L * 16 && f.Po / (nseg * 2) >= 8 * AP) nseg *= 2;
+    f.SEG = (f.Po + nseg - 1) / nseg;
+    f.nseg = (f.Po + f.SEG - 1) / f.SEG;
+    const long nb = base * f.nseg;
+    if (nb > 0x7fffffffL) return cudaErrorInvalidValue;
+    level_fir<AP><<<(unsigned)nb, 128, (size_t)f.Dp * APP * sizeof(float), s>>>(f);
+    return cudaGetLastError();
+}
+
+__global__ void amax_kernel(const float *__restrict__ v, size_t n, int *amax)
+{
+    float m = 0.f;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n / 4; i += (size_t)gridDim.x * blockDim.x) {
+        const float4 q = __ldg(reinterpret_cast<const float4 *>(v) + i);
+        m = fmaxf(m, fmaxf(fmaxf(fabsf(q.x), fabsf(q.y)), fmaxf(fabsf(q.z), fabsf(q.w))));
+    }
+    for (size_t i = (n / 4) * 4 + (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        m = fmaxf(m, fabsf(v[i]));
+    if (!isfinite(m)) m = 0.f;                                 // non-finite samples are reported by the level kernel
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(amax, __float_as_int(m));
+}
+
+}  // namespace
+
+size_t level_tc_scratch_bytes(int Np, int C, int P, int Ko)
+{
+    const int Kop = (Ko + 3) & ~3;
+    return (size_t)Np * C * P * Kop * sizeof(__half2);
+}
+
+bool level_tc_supported(int C, int Lk, int Dk)
+{
+    const int Lkp = ((Lk + 15) / 16) * 16;
+    return C >= 1 && C <= 64 && Lkp <= 64 && Dk >= 1;
+}
+
+cudaError_t launch_amax(const float2 *x, size_t n, int *amax, cudaStream_t s)
+{
+    amax_kernel<<<148 * 4, 256, 0, s>>>(reinterpret_cast<const float *>(x), 2 * n, amax);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_level_tc(const LevelLaunch &L, const int *amax_in, void *scratch, int *err, cudaStream_t s,
+                            const char **why)
+{
+    *why = nullptr;
+    const int Lk = L.Dk > 1 ? L.Lk : 1, plk = L.Dk > 1 ? L.plk : 0;
+    const int Lp = L.Dp > 1 ? L.Lp : 1, plp = L.Dp > 1 ? L.plp : 0;
+    if (!level_tc_supported(L.C, Lk, L.Dk)) { *why = "the tensor-core level takes C <= 64 children and Lk <= 64 taps"; return cudaErrorNotSupported; }
+    GemmArgs a;
+    a.x = L.x; a.ph = L.phase; a.tk = L.tk; a.wp = L.wp; a.wk = L.wk; a.bad = L.bad; a.amax_in = amax_in;
+    a.y = static_cast<__half2 *>(scratch); a.err = err;
+    a.Np = L.Np; a.C = L.C; a.P = L.P; a.K = L.K; a.Ko = L.Ko; a.Kop = (L.Ko + 3) & ~3; a.Dk = L.Dk; a.Lk = Lk;
+    a.plk = plk; a.Lkp = ((Lk + 15) / 16) * 16; a.kc = (float)L.kc;
+    // columns per tile: the multiple of 32 up to 128 that wastes the fewest columns on the last tile
+    int best = 128, bestw = 1 << 30;
+    for (int nt = 128; nt >= 32; nt -= 32) {
+        const int nti = (L.Ko + nt - 1) / nt, waste = nti * nt - L.Ko + nti * 8;   // a tile costs about 8 columns
+        if (waste < bestw) { bestw = waste; best = nt; }
+    }
+    a.Nt = best;
+    a.ntile = (L.Ko + a.Nt - 1) / a.Nt;
+    a.W = a.Dk * (a.Nt - 1) + a.Lkp;
+    if ((a.W + 1) / 2 > 4 * NPT) { *why = "a tile's window exceeds the producers' registers"; return cudaErrorNotSupported; }
+    // pulse segments: enough blocks for the device several times over
+    int nseg = 1;
+    while ((long)L.Np * nseg < 148L * 3 && L.P / (nseg * 2) >= 32) nseg *= 2;
+    a.pseg = (L.P + nseg - 1) / nseg;
+    a.nseg = (L.P + a.pseg - 1) / a.pseg;
+    int dev = 0, maxsmem = 227 * 1024;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const size_t apart = (size_t)128 * a.Lkp * 2, bpart = (size_t)2 * a.Nt * a.Lkp * 2;
+    const int Wp = (a.W + 9) & ~1;
+    auto need = [&](int sb) {
+        return 4 * apart + (size_t)sb * 2 * bpart + (size_t)4 * (Wp / 2) * 4 + (size_t)(a.Lkp + 1) * 4 + 8 +
+               (size_t)(6 + 2 * sb) * 8;
+    };
+    int SB = 4;
+    while (SB > 2 && need(SB) > (size_t)maxsmem - 1024) --SB;
+    if (need(SB) > (size_t)maxsmem - 1024) { *why = "the tensor-core level's operands do not fit shared memory"; return cudaErrorNotSupported; }
+    a.SB = SB;
+    cudaError_t e = cudaFuncSetAttribute(level_tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need(SB));
+    if (e != cudaSuccess) return e;
+    const long nb = (long)L.Np * a.nseg;
+    if (nb > 0x7fffffffL) return cudaErrorInvalidValue;
+    level_tc_gemm<<<(unsigned)nb, NTHR, need(SB), s>>>(a);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+
+    FirArgs f;
+    f.y = a.y; f.tp = L.tp; f.out = L.out; f.amax = L.amax; f.amax_in = amax_in;
+    f.rows = L.Np * L.C; f.P = L.P; f.Kop = a.Kop; f.Ko = L.Ko; f.Po = L.Po; f.Dp = L.Dp; f.Lp = Lp; f.plp = plp;
+    const int AP = (Lp + L.Dp - 1) / L.Dp;
+    switch (AP) {
+        case 1: return launch_fir<1>(f, s);
+        case 2: return launch_fir<2>(f, s);
+        case 3: return launch_fir<3>(f, s);
+        case 4: return launch_fir<4>(f, s);
+        case 5: return launch_fir<5>(f, s);
+        case 6: return launch_fir<6>(f, s);
+        case 7: return launch_fir<7>(f, s);
+        case 8: return launch_fir<8>(f, s);
+        case 9: return launch_fir<9>(f, s);
+        case 10: return launch_fir<10>(f, s);
+        case 11: return launch_fir<11>(f, s);
+        case 12: return launch_fir<12>(f, s);
+        default: *why = "pulse FIR spans more than 12 output pulses"; return cudaErrorNotSupported;
+    }
+}
+
+}  // namespace ffbp

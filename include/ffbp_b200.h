@@ -44,8 +44,13 @@ enum {
     FFBP_FINAL_TC_F16 = 1,  /* tcgen05 tensor cores, float16 operands, float32 accumulation; ffbp_form scales  */
                             /* the samples by a power of two into float16's range, ffbp_final takes them as    */
                             /* given (each component below 2^14 in magnitude)                                   */
-    FFBP_FINAL_TC_BF16X3 = 2 /* tcgen05 tensor cores, operands split x = hi + lo in bfloat16, the hi*hi, hi*lo,  */
-                             /* lo*hi and lo*lo products accumulated in float32                                */
+    FFBP_FINAL_TC_BF16X3 = 2, /* tcgen05 tensor cores, operands split x = hi + lo in bfloat16, the hi*hi, hi*lo, */
+                              /* lo*hi and lo*lo products accumulated in float32                               */
+    FFBP_LEVELS_TC = 0x100    /* flag, or-ed into ffbp_plan_desc.final_mode: the levels on the tensor cores     */
+                              /* (per pulse the children's modulated frequency taps times the parent row's      */
+                              /* Hankel windows, three bfloat16 products; a float16 intermediate; the pulse FIR */
+                              /* in float32). Levels of more than 64 children or 64 frequency taps stay on the  */
+                              /* float32 kernel. The workspace grows by the intermediate of the largest level.  */
 };
 
 /* One level of the plan (fastsar/ffbp2.py:192-250, make_plan's per-level record). All pointers are host memory. */
@@ -84,7 +89,7 @@ typedef struct {
     const float *h_wk;      /* [K0] Taylor window over samples, or NULL                                           */
     const float *h_wf;      /* aperture weights per (tile, final subaperture): [ntiles, Pf] (wf_ndim 2) or       */
     int wf_ndim;            /* [3, ntiles, Pf] weight and its gradients along e1, e2 (wf_ndim 3); NULL / 0 none  */
-    int final_mode;         /* FFBP_FINAL_*                                                                       */
+    int final_mode;         /* FFBP_FINAL_*, or-ed with FFBP_LEVELS_TC for the tensor-core levels                 */
 } ffbp_plan_desc;
 
 typedef struct ffbp_plan ffbp_plan;
@@ -144,6 +149,19 @@ int ffbp_plan_info(const ffbp_plan *plan, int *nlev, int *launches);
 int ffbp_level(const void *d_x, int Np, int P, int K, const void *d_phase, int C, const float *d_tk, int Lk, int plk,
                int Dk, int Ko, double kc, const float *d_tp, int Lp, int plp, int Dp, int Po, const float *d_wp,
                const float *d_wk, void *d_out, int *d_bad, void *stream);
+
+/* The same level on the tensor cores (the arithmetic of FFBP_LEVELS_TC): per pulse the children's modulated
+ * frequency taps tk[r] exp(2 pi i sl r) times the Hankel windows of the parent's row, three bfloat16 products
+ * accumulated in float32; the ramp exp(2 pi i (c0 + sl (Dk j - plk - kc))); a float16 intermediate in d_scratch
+ * (ffbp_level_tc_scratch_bytes, 16-byte aligned), scaled by a power of two from the input's largest component;
+ * the pulse FIR in float32. C <= 64 and Lk <= 64 (FFBP_E_UNSUPPORTED otherwise). d_status: 3 ints, zeroed by the
+ * caller: [0] set when a bounded wait of the kernel ran out, [1] the input's largest |component| (float bits,
+ * filled here), [2] the output's. No counterpart in the reference (its levels run in float32 only).            */
+size_t ffbp_level_tc_scratch_bytes(int Np, int C, int P, int Ko);
+int ffbp_level_tc(const void *d_x, int Np, int P, int K, const void *d_phase, int C, const float *d_tk, int Lk, int plk,
+                  int Dk, int Ko, double kc, const float *d_tp, int Lp, int plp, int Dp, int Po, const float *d_wp,
+                  const float *d_wk, void *d_out, int *d_bad, void *d_scratch, size_t scratch_bytes, int *d_status,
+                  void *stream);
 
 /* Child phases in float64 for one level (fastsar/ffbp2.py:329-339 / fastsar/ffbp_cuda.py:598-632): for parent n,
  * child c and pulse p, ddr = |cen[n,c] - ant[p]| - |ref[n] - ant[p]| (or - range[p] when d_range is given),

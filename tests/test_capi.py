@@ -12,7 +12,7 @@ from conftest import ROOT
 def _declared():
     with open(os.path.join(ROOT, 'include', 'ffbp_b200.h')) as fh:
         src = fh.read()
-    return sorted(set(re.findall(r'^\s*int\s+(ffbp_\w+)\s*\(', src, re.M)))
+    return sorted(set(re.findall(r'^\s*(?:int|size_t)\s+(ffbp_\w+)\s*\(', src, re.M)))
 
 
 def test_header_declares_the_binding_exports():
