@@ -41,6 +41,7 @@ constexpr int MMAW = NCW + NPW;               // warp 24
 constexpr int NTHR = (NCW + NPW + 1) * 32;
 constexpr int NPT = NPW * 32;
 constexpr uint64_t WAIT_NS = 2000000000ull;
+constexpr int XS = 4;                         // the producers' ring of parent-row windows, XS - 1 stages ahead
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -176,7 +177,8 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
     const int Wp = (a.W + 9) & ~1;                           // plane length in elements (even, with slack)
     uint32_t *pl = reinterpret_cast<uint32_t *>(sB + (size_t)a.SB * 2 * bpart);   // [4][Wp / 2] words
     float *s_tk = reinterpret_cast<float *>(pl + 4 * (Wp / 2));                   // [Lkp]
-    uint64_t *bars = reinterpret_cast<uint64_t *>(s_tk + a.Lkp + (a.Lkp & 1));
+    float2 *s_x = reinterpret_cast<float2 *>(s_tk + a.Lkp);                        // [XS][Wp] staged windows
+    uint64_t *bars = reinterpret_cast<uint64_t *>(s_x + (size_t)XS * Wp);
     uint64_t *afull = bars, *aempty = bars + 2, *bfull = bars + 4, *bempty = bfull + a.SB, *dfull = bempty + a.SB,
              *dempty = dfull + 2;
     __shared__ uint32_t s_tmem;
@@ -225,32 +227,25 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
         const float2 *__restrict__ xn = a.x + (size_t)n * a.P * a.K;
         const float2 *__restrict__ phn = a.ph + (size_t)n * a.C * a.P;
         const int npair = (a.W + 1) / 2;                      // window samples in pairs (2i, 2i + 1)
-        // the window of stage (pulse p, tile tt): samples k = kb + i, kb = Dk Nt tt - plk, i < W
-        float2 xv[4][2];                                      // this thread's pairs of the next stage (<= 4)
-        auto load = [&](int p, int tt) {
-            const int kb = a.Dk * a.Nt * tt - a.plk;
-            const float wpp = a.wp ? a.wp[p] : 1.f;
-#pragma unroll
-            for (int m = 0; m < 4; ++m) {
-                const int i = pt + m * NPT;
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int k = kb + 2 * i + h;
-                    float2 v = make_float2(0.f, 0.f);
-                    if (i < npair && 2 * i + h < a.W && k >= 0 && k < a.K) {
-                        v = __ldg(&xn[(size_t)p * a.K + k]);
-                        if (a.wp) {
-                            const float w = wpp * a.wk[k];
-                            v.x *= w;
-                            v.y *= w;
-                        }
-                        if (a.bad && !(isfinite(v.x) && isfinite(v.y))) atomicMin(a.bad, p);
-                    }
-                    xv[m][h] = v;
+        // the window of stage (pulse p, tile tt): samples k = kb + i, kb = Dk Nt tt - plk, i < W, copied XS - 1
+        // stages ahead into ring slot (stage % XS) (zero outside [0, K)); one cp.async group per stage
+        auto stage_x = [&](int st) {
+            if (st < nst) {
+                const int q = st / a.ntile, tt = st - q * a.ntile, p = p0 + q;
+                const int kb = a.Dk * a.Nt * tt - a.plk;
+                float2 *dst = s_x + (size_t)(st % XS) * Wp;
+                for (int i = pt; i < a.W; i += NPT) {
+                    const int k = kb + i;
+                    const bool v = k >= 0 && k < a.K;
+                    const float2 *src = v ? xn + (size_t)p * a.K + k : xn;
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;"
+                                 :: "r"(smem_u32(dst + i)), "l"(src), "r"(v ? 8 : 0) : "memory");
                 }
             }
+            asm volatile("cp.async.commit_group;" ::: "memory");
         };
-        if (nst > 0) load(p0, 0);
+#pragma unroll
+        for (int d = 0; d < XS - 1; ++d) stage_x(d);
         int sb = 0;
         uint32_t sbpar = 0;
         // after a failed wait a warp keeps stepping through the stages (and the producers' named barriers, which
@@ -258,6 +253,8 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
         bool ok = true;
         for (int s = 0; s < nst; ++s) {
             const int pl_i = s / a.ntile, tt = s - pl_i * a.ntile, p = p0 + pl_i;
+            stage_x(s + XS - 1);
+            asm volatile("cp.async.wait_group %0;" :: "n"(XS - 1) : "memory");   // this thread's copies of stage s
             // modulated taps of pulse p (at its first tile), into A' buffer pl_i & 1
             if (tt == 0 && ok) {
                 const int ab = pl_i & 1;
@@ -267,7 +264,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                 const int ab = pl_i & 1;
                 unsigned char *Ab = sA + ab * 2 * apart;
                 for (int item = pt; item < a.C * nkc; item += NPT) {
-                    const int c = item / nkc, u = item - c * nkc;
+                    const int u = item / a.C, c = item - u * a.C;   // consecutive threads: consecutive children
                     const float sl = __ldg(&phn[(size_t)c * a.P + p]).y;
                     float2 z = cis_cycles(sl * (float)(8 * u));
                     const float2 st = cis_cycles(sl);
@@ -296,25 +293,34 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                 if (lane == 0) mbar_arrive(&afull[ab]);
             }
             // the window's planes: xr hi, xr lo, xi hi, xi lo as bfloat16 pairs (word i = samples 2i, 2i + 1);
-            // the previous stage's Hankel rows have all been read from them (named barrier)
+            // the barrier also orders every producer's copies of this stage before the reads below and the
+            // previous stage's Hankel reads of the planes before these writes
             asm volatile("bar.sync 1, %0;" :: "n"(NPT) : "memory");
+            {
+                const float2 *xs = s_x + (size_t)(s % XS) * Wp;
+                const int kb = a.Dk * a.Nt * tt - a.plk;
+                const float wpp = a.wp ? a.wp[p] : 1.f;
+                for (int i = pt; i < npair; i += NPT) {
+                    float2 v[2];
 #pragma unroll
-            for (int m = 0; m < 4; ++m) {
-                const int i = pt + m * NPT;
-                if (i < npair) {
+                    for (int h = 0; h < 2; ++h) {
+                        const int e = 2 * i + h, k = kb + e;
+                        v[h] = e < a.W ? xs[e] : make_float2(0.f, 0.f);
+                        if (a.wp && k >= 0 && k < a.K && e < a.W) {
+                            const float w = wpp * a.wk[k];
+                            v[h].x *= w;
+                            v[h].y *= w;
+                        }
+                        if (a.bad && !(isfinite(v[h].x) && isfinite(v[h].y))) atomicMin(a.bad, p);
+                    }
                     uint32_t rh, rl, ih, il;
-                    split2(xv[m][0].x, xv[m][1].x, rh, rl);
-                    split2(xv[m][0].y, xv[m][1].y, ih, il);
+                    split2(v[0].x, v[1].x, rh, rl);
+                    split2(v[0].y, v[1].y, ih, il);
                     pl[i] = rh;
                     pl[Wp / 2 + i] = rl;
                     pl[Wp + i] = ih;
                     pl[3 * (Wp / 2) + i] = il;
                 }
-            }
-            // the next stage's samples while this one's Hankel rows are built
-            if (s + 1 < nst) {
-                const int s1 = s + 1, q = s1 / a.ntile;
-                load(p0 + q, s1 - q * a.ntile);
             }
             asm volatile("bar.sync 1, %0;" :: "n"(NPT) : "memory");
             if (ok) ok = mbar_wait(&bempty[sb], sbpar ^ 1u, 1000, &s_abort, a.err);
@@ -322,9 +328,12 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             unsigned char *Bb = sB + sb * 2 * bpart;
             const int nch = ncol * nkc;
             for (int item = pt; ok && item < 2 * nch; item += NPT) {
+                // eight consecutive threads take the eight rows of one core matrix (their 16-byte stores fill its
+                // 128 bytes: no bank conflicts), the next eight the next K chunk (their plane reads stay apart)
                 const int part = item >= nch ? 1 : 0;
                 const int rem = item - part * nch;
-                const int row = rem / nkc, u = rem - row * nkc;
+                const int r8 = rem & 7, rest = rem >> 3;
+                const int u = rest % nkc, row = (rest / nkc) * 8 + r8;
                 const int im = row >= a.Nt ? 1 : 0;
                 const int o = a.Dk * (row - im * a.Nt) + 8 * u;    // first element in the window
                 const uint32_t *src = pl + (2 * im + part) * (Wp / 2) + (o >> 1);
@@ -343,6 +352,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             if (lane == 0 && ok) mbar_arrive(&bfull[sb]);
             if (++sb == a.SB) { sb = 0; sbpar ^= 1u; }
         }
+        asm volatile("cp.async.wait_all;" ::: "memory");
     } else if (warp == MMAW) {
         // ------------------------------------------------------------------ MMA issue
         if (lane == 0) {
@@ -383,11 +393,15 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
         const int cw = a.Nt / 4;                              // columns of this warp per tile
         const float2 *__restrict__ phc = a.ph + ((size_t)n * a.C + (live ? c : 0)) * a.P;
         __half2 *__restrict__ yc = a.y + ((size_t)n * a.C + (live ? c : 0)) * a.P * a.Kop;
-        float2 q0 = make_float2(0.f, 0.f);
+        // the child's phase (c0, sl) of the current pulse, and of the next one loaded a pulse ahead
+        float2 q0 = make_float2(0.f, 0.f), qn = (live && npl > 0) ? __ldg(&phc[p0]) : make_float2(0.f, 0.f);
         for (int s = 0; s < nst; ++s) {
             const int pl_i = s / a.ntile, tt = s - pl_i * a.ntile, p = p0 + pl_i;
             const int db = s & 1;
-            if (tt == 0 && live) q0 = __ldg(&phc[p]);
+            if (tt == 0) {
+                q0 = qn;
+                if (live && pl_i + 1 < npl) qn = __ldg(&phc[p + 1]);
+            }
             // warp-uniform: the accumulator loads below are warp-collective
             if (!__all_sync(0xffffffffu, mbar_wait(&dfull[db], (uint32_t)((s >> 1) & 1), 200, &s_abort, a.err))) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -461,7 +475,7 @@ struct FirArgs {
     float2 *__restrict__ out;         // [rows, Po, Ko]
     int *amax;
     const int *amax_in;
-    int rows, P, Kop, Ko, Po, Dp, Lp, plp, SEG, nseg, ncb;
+    int rows, P, Kop, Ko, Po, Dp, Lp, plp, SEG, nseg;
 };
 
 template <int AP>
@@ -469,11 +483,8 @@ __global__ void __launch_bounds__(128) level_fir(const FirArgs a)
 {
     constexpr int APP = (AP + 3) & ~3;
     extern __shared__ __align__(16) float s_tp[];             // [Dp][APP]: s_tp[b APP + s] = tp[Dp s + b]
-    int bid = blockIdx.x;
-    const int cb = bid % a.ncb;
-    bid /= a.ncb;
-    const int seg = bid % a.nseg;
-    const int row = bid / a.nseg;
+    // thread -> (row, pair of columns j, j + 1), consecutive threads along a row's pairs and on into the next row;
+    // blockIdx.y: the segment of output pulses
     const int t = threadIdx.x;
     for (int r = t; r < a.Dp * APP; r += 128) {
         const int b = r / APP, s = r - b * APP;
@@ -481,9 +492,13 @@ __global__ void __launch_bounds__(128) level_fir(const FirArgs a)
         s_tp[r] = (s < AP && tap < a.Lp) ? (a.tp ? a.tp[tap] : 1.f) : 0.f;   // Dp = 1: one tap 1
     }
     __syncthreads();
+    const int npair = (a.Ko + 1) / 2;
+    const long gid = (long)blockIdx.x * 128 + t;
+    if (gid >= (long)a.rows * npair) return;
+    const int row = (int)(gid / npair), j = 2 * (int)(gid - (long)row * npair);
+    const int seg = blockIdx.y;
     const float inv = 1.f / y_scale(a.amax_in);
-    const int j = 2 * (cb * 128 + t);                          // two columns j, j + 1
-    const bool colok = j < a.Ko;
+    const bool colok = true;
     const int i_s = seg * a.SEG, i_e = min(a.Po, i_s + a.SEG);
     const int g_end = i_e + AP - 1;
     const __half2 *__restrict__ yr = a.y + (size_t)row * a.P * a.Kop + j;
@@ -493,12 +508,25 @@ __global__ void __launch_bounds__(128) level_fir(const FirArgs a)
 #pragma unroll
         for (int s = 0; s < AP; ++s) acc[h][s] = make_float2(0.f, 0.f);
     float vmax = 0.f;
-    int p = a.Dp * i_s - a.plp, b = 0;
-    for (int gi = i_s; gi < g_end;) {
-        if (p >= 0 && p < a.P && colok) {
-            const uint2 w = __ldg(reinterpret_cast<const uint2 *>(yr + (size_t)p * a.Kop));
-            const float2 v0 = __half22float2(*reinterpret_cast<const __half2 *>(&w.x));
-            const float2 v1 = __half22float2(*reinterpret_cast<const __half2 *>(&w.y));
+    // input pulses p_start .. p_stop - 1 in chunks of U, the next chunk's loads in flight while one is filtered
+    constexpr int U = 8;
+    const int p_start = a.Dp * i_s - a.plp, p_stop = a.Dp * g_end - a.plp;
+    auto ld = [&](int pp) -> uint2 {
+        return (pp >= 0 && pp < a.P && colok) ? __ldg(reinterpret_cast<const uint2 *>(yr + (size_t)pp * a.Kop))
+                                              : make_uint2(0u, 0u);
+    };
+    uint2 cur[U], nxt[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) cur[u] = ld(p_start + u);
+    int b = 0, gi = i_s;
+    for (int pc = p_start; pc < p_stop; pc += U) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) nxt[u] = ld(pc + U + u);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (pc + u >= p_stop) break;
+            const float2 v0 = __half22float2(*reinterpret_cast<const __half2 *>(&cur[u].x));
+            const float2 v1 = __half22float2(*reinterpret_cast<const __half2 *>(&cur[u].y));
             float tb[APP];
 #pragma unroll
             for (int s4 = 0; s4 < APP; s4 += 4) {
@@ -512,30 +540,31 @@ __global__ void __launch_bounds__(128) level_fir(const FirArgs a)
                 acc[1][s].x = fmaf(tb[s], v1.x, acc[1][s].x);
                 acc[1][s].y = fmaf(tb[s], v1.y, acc[1][s].y);
             }
-        }
-        ++p;
-        if (++b == a.Dp) {                                    // group gi complete: output gi - (AP - 1) finished
-            b = 0;
-            const int i = gi - (AP - 1);
-            if (i >= i_s && colok) {
-                float2 *o = a.out + ((size_t)row * a.Po + i) * a.Ko + j;
-                const float2 o0 = make_float2(acc[0][AP - 1].x * inv, acc[0][AP - 1].y * inv);
-                const float2 o1 = make_float2(acc[1][AP - 1].x * inv, acc[1][AP - 1].y * inv);
-                o[0] = o0;
-                vmax = fmaxf(vmax, fmaxf(fabsf(o0.x), fabsf(o0.y)));
-                if (j + 1 < a.Ko) {
-                    o[1] = o1;
-                    vmax = fmaxf(vmax, fmaxf(fabsf(o1.x), fabsf(o1.y)));
+            if (++b == a.Dp) {                                // group gi complete: output gi - (AP - 1) finished
+                b = 0;
+                const int i = gi - (AP - 1);
+                if (i >= i_s && colok) {
+                    float2 *o = a.out + ((size_t)row * a.Po + i) * a.Ko + j;
+                    const float2 o0 = make_float2(acc[0][AP - 1].x * inv, acc[0][AP - 1].y * inv);
+                    const float2 o1 = make_float2(acc[1][AP - 1].x * inv, acc[1][AP - 1].y * inv);
+                    o[0] = o0;
+                    vmax = fmaxf(vmax, fmaxf(fabsf(o0.x), fabsf(o0.y)));
+                    if (j + 1 < a.Ko) {
+                        o[1] = o1;
+                        vmax = fmaxf(vmax, fmaxf(fabsf(o1.x), fabsf(o1.y)));
+                    }
                 }
-            }
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
+                for (int h = 0; h < 2; ++h) {
 #pragma unroll
-                for (int s = AP - 1; s > 0; --s) acc[h][s] = acc[h][s - 1];
-                acc[h][0] = make_float2(0.f, 0.f);
+                    for (int s = AP - 1; s > 0; --s) acc[h][s] = acc[h][s - 1];
+                    acc[h][0] = make_float2(0.f, 0.f);
+                }
+                ++gi;
             }
-            ++gi;
         }
+#pragma unroll
+        for (int u = 0; u < U; ++u) cur[u] = nxt[u];
     }
     if (a.amax) {
 #pragma unroll
@@ -548,15 +577,13 @@ template <int AP>
 cudaError_t launch_fir(FirArgs f, cudaStream_t s)
 {
     constexpr int APP = (AP + 3) & ~3;
-    f.ncb = (f.Ko + 255) / 256;
-    const long base = (long)f.rows * f.ncb;
+    const long nb = ((long)f.rows * ((f.Ko + 1) / 2) + 127) / 128;
     int nseg = 1;
-    while (base * nseg < 148L * 16 && f.Po / (nseg * 2) >= 8 * AP) nseg *= 2;
+    while (nb * nseg < 148L * 16 && f.Po / (nseg * 2) >= 8 * AP) nseg *= 2;
     f.SEG = (f.Po + nseg - 1) / nseg;
     f.nseg = (f.Po + f.SEG - 1) / f.SEG;
-    const long nb = base * f.nseg;
-    if (nb > 0x7fffffffL) return cudaErrorInvalidValue;
-    level_fir<AP><<<(unsigned)nb, 128, (size_t)f.Dp * APP * sizeof(float), s>>>(f);
+    if (nb > 0x7fffffffL || f.nseg > 65535) return cudaErrorInvalidValue;
+    level_fir<AP><<<dim3((unsigned)nb, (unsigned)f.nseg), 128, (size_t)f.Dp * APP * sizeof(float), s>>>(f);
     return cudaGetLastError();
 }
 
@@ -607,39 +634,43 @@ cudaError_t launch_level_tc(const LevelLaunch &L, const int *amax_in, void *scra
     a.y = static_cast<__half2 *>(scratch); a.err = err;
     a.Np = L.Np; a.C = L.C; a.P = L.P; a.K = L.K; a.Ko = L.Ko; a.Kop = (L.Ko + 3) & ~3; a.Dk = L.Dk; a.Lk = Lk;
     a.plk = plk; a.Lkp = ((Lk + 15) / 16) * 16; a.kc = (float)L.kc;
-    // columns per tile: the multiple of 32 up to 128 that wastes the fewest columns on the last tile
-    int best = 128, bestw = 1 << 30;
+    int dev = 0, maxsmem = 227 * 1024;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const size_t avail = (size_t)maxsmem - 1024;              // static shared memory and slack
+    const size_t apart = (size_t)128 * a.Lkp * 2;
+    auto need = [&](int nt, int sb) {
+        const size_t bpart = (size_t)2 * nt * a.Lkp * 2;
+        const int W = a.Dk * (nt - 1) + a.Lkp, Wp = (W + 9) & ~1;
+        return 4 * apart + (size_t)sb * 2 * bpart + (size_t)4 * (Wp / 2) * 4 + (size_t)a.Lkp * 4 + (size_t)XS * Wp * 8 +
+               (size_t)(6 + 2 * sb) * 8;
+    };
+    // columns per tile: a multiple of 32 up to 128 whose operands fit shared memory with two B stages, the one that
+    // wastes the fewest columns on the last tile counting each tile as 32 columns of fixed cost
+    int best = 0, bestw = 1 << 30;
     for (int nt = 128; nt >= 32; nt -= 32) {
-        const int nti = (L.Ko + nt - 1) / nt, waste = nti * nt - L.Ko + nti * 8;   // a tile costs about 8 columns
+        if (need(nt, 2) > avail) continue;
+        const int nti = (L.Ko + nt - 1) / nt, waste = nti * nt - L.Ko + nti * 32;
         if (waste < bestw) { bestw = waste; best = nt; }
     }
+    if (!best) { *why = "the tensor-core level's operands do not fit shared memory"; return cudaErrorNotSupported; }
     a.Nt = best;
     a.ntile = (L.Ko + a.Nt - 1) / a.Nt;
     a.W = a.Dk * (a.Nt - 1) + a.Lkp;
-    if ((a.W + 1) / 2 > 4 * NPT) { *why = "a tile's window exceeds the producers' registers"; return cudaErrorNotSupported; }
     // pulse segments: enough blocks for the device several times over
     int nseg = 1;
     while ((long)L.Np * nseg < 148L * 3 && L.P / (nseg * 2) >= 32) nseg *= 2;
     a.pseg = (L.P + nseg - 1) / nseg;
     a.nseg = (L.P + a.pseg - 1) / a.pseg;
-    int dev = 0, maxsmem = 227 * 1024;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    const size_t apart = (size_t)128 * a.Lkp * 2, bpart = (size_t)2 * a.Nt * a.Lkp * 2;
-    const int Wp = (a.W + 9) & ~1;
-    auto need = [&](int sb) {
-        return 4 * apart + (size_t)sb * 2 * bpart + (size_t)4 * (Wp / 2) * 4 + (size_t)(a.Lkp + 1) * 4 + 8 +
-               (size_t)(6 + 2 * sb) * 8;
-    };
     int SB = 4;
-    while (SB > 2 && need(SB) > (size_t)maxsmem - 1024) --SB;
-    if (need(SB) > (size_t)maxsmem - 1024) { *why = "the tensor-core level's operands do not fit shared memory"; return cudaErrorNotSupported; }
+    while (SB > 2 && need(a.Nt, SB) > avail) --SB;
     a.SB = SB;
-    cudaError_t e = cudaFuncSetAttribute(level_tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need(SB));
+    const size_t smem = need(a.Nt, SB);
+    cudaError_t e = cudaFuncSetAttribute(level_tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const long nb = (long)L.Np * a.nseg;
     if (nb > 0x7fffffffL) return cudaErrorInvalidValue;
-    level_tc_gemm<<<(unsigned)nb, NTHR, need(SB), s>>>(a);
+    level_tc_gemm<<<(unsigned)nb, NTHR, smem, s>>>(a);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
 
     FirArgs f;
