@@ -166,17 +166,20 @@ __device__ __forceinline__ float y_scale(const int *amax)
     return ldexpf(1.f, 13 - ex);
 }
 
+template <int NKC>
 __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
-    const int nkc = a.Lkp / 8;                               // core matrices along K
+    constexpr int nkc = NKC;                                 // core matrices along K (Lkp = 8 NKC)
     const uint32_t apart = 128u * a.Lkp * 2u;                // one part (hi or lo) of A'
     const uint32_t bpart = 2u * a.Nt * a.Lkp * 2u;           // one part of B'
     unsigned char *sA = smem;                                // [2 pulses][hi, lo]
     unsigned char *sB = sA + 2 * 2 * apart;                  // [SB stages][hi, lo]
     const int Wp = (a.W + 9) & ~1;                           // plane length in elements (even, with slack)
-    uint32_t *pl = reinterpret_cast<uint32_t *>(sB + (size_t)a.SB * 2 * bpart);   // [4][Wp / 2] words
-    float *s_tk = reinterpret_cast<float *>(pl + 4 * (Wp / 2));                   // [Lkp]
+    // planes: [xr hi, xr lo, xi hi, xi lo][even, odd copy][Wp / 2] words; the even copy's word w holds samples
+    // 2w, 2w + 1, the odd copy's 2w + 1, 2w + 2, so that any 8 consecutive samples are 4 aligned words of one copy
+    uint32_t *pl = reinterpret_cast<uint32_t *>(sB + (size_t)a.SB * 2 * bpart);
+    float *s_tk = reinterpret_cast<float *>(pl + 8 * (Wp / 2));                   // [Lkp]
     float2 *s_x = reinterpret_cast<float2 *>(s_tk + a.Lkp);                        // [XS][Wp] staged windows
     uint64_t *bars = reinterpret_cast<uint64_t *>(s_x + (size_t)XS * Wp);
     uint64_t *afull = bars, *aempty = bars + 2, *bfull = bars + 4, *bempty = bfull + a.SB, *dfull = bempty + a.SB,
@@ -266,15 +269,19 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                 for (int item = pt; item < a.C * nkc; item += NPT) {
                     const int u = item / a.C, c = item - u * a.C;   // consecutive threads: consecutive children
                     const float sl = __ldg(&phn[(size_t)c * a.P + p]).y;
-                    float2 z = cis_cycles(sl * (float)(8 * u));
-                    const float2 st = cis_cycles(sl);
+                    // exp(2 pi i sl r) for r = 8u .. 8u + 7: two independent recurrences (even and odd r)
+                    const float2 st = cis_cycles(sl), st2 = cmul(st, st);
+                    float2 ze = cis_cycles(sl * (float)(8 * u)), zo = cmul(ze, st);
                     float mr[8], mi[8];
 #pragma unroll
-                    for (int e = 0; e < 8; ++e) {
-                        const float h = s_tk[8 * u + e];
-                        mr[e] = h * z.x;
-                        mi[e] = h * z.y;
-                        z = cmul(z, st);
+                    for (int e = 0; e < 8; e += 2) {
+                        const float h0 = s_tk[8 * u + e], h1 = s_tk[8 * u + e + 1];
+                        mr[e] = h0 * ze.x;
+                        mi[e] = h0 * ze.y;
+                        mr[e + 1] = h1 * zo.x;
+                        mi[e + 1] = h1 * zo.y;
+                        ze = cmul(ze, st2);
+                        zo = cmul(zo, st2);
                     }
                     uint32_t rh[4], rl[4], ih[4], il[4];
 #pragma unroll
@@ -301,9 +308,9 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                 const int kb = a.Dk * a.Nt * tt - a.plk;
                 const float wpp = a.wp ? a.wp[p] : 1.f;
                 for (int i = pt; i < npair; i += NPT) {
-                    float2 v[2];
+                    float2 v[3];                              // samples 2i, 2i + 1, 2i + 2 (windowed)
 #pragma unroll
-                    for (int h = 0; h < 2; ++h) {
+                    for (int h = 0; h < 3; ++h) {
                         const int e = 2 * i + h, k = kb + e;
                         v[h] = e < a.W ? xs[e] : make_float2(0.f, 0.f);
                         if (a.wp && k >= 0 && k < a.K && e < a.W) {
@@ -311,41 +318,65 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                             v[h].x *= w;
                             v[h].y *= w;
                         }
-                        if (a.bad && !(isfinite(v[h].x) && isfinite(v[h].y))) atomicMin(a.bad, p);
+                        if (h < 2 && a.bad && !(isfinite(v[h].x) && isfinite(v[h].y))) atomicMin(a.bad, p);
                     }
-                    uint32_t rh, rl, ih, il;
+                    uint32_t rh, rl, ih, il, orh, orl, oih, oil;
                     split2(v[0].x, v[1].x, rh, rl);
                     split2(v[0].y, v[1].y, ih, il);
+                    split2(v[1].x, v[2].x, orh, orl);
+                    split2(v[1].y, v[2].y, oih, oil);
+                    const int hw = Wp / 2;
                     pl[i] = rh;
-                    pl[Wp / 2 + i] = rl;
-                    pl[Wp + i] = ih;
-                    pl[3 * (Wp / 2) + i] = il;
+                    pl[hw + i] = orh;
+                    pl[2 * hw + i] = rl;
+                    pl[3 * hw + i] = orl;
+                    pl[4 * hw + i] = ih;
+                    pl[5 * hw + i] = oih;
+                    pl[6 * hw + i] = il;
+                    pl[7 * hw + i] = oil;
                 }
             }
             asm volatile("bar.sync 1, %0;" :: "n"(NPT) : "memory");
             if (ok) ok = mbar_wait(&bempty[sb], sbpar ^ 1u, 1000, &s_abort, a.err);
-            // Hankel rows: row j < Nt: xr window from Dk j; row Nt + j: xi; 8 elements (16 bytes) per chunk
+            // Hankel rows: row j < Nt: xr window from Dk j; row Nt + j: xi; 8 elements (16 bytes) per chunk.
+            // A warp takes 8 rows (lane % 8) x 4 K chunks (lane / 8) at a time: the 8 rows' 16-byte stores fill one
+            // 128-byte core matrix (no bank conflicts)
             unsigned char *Bb = sB + sb * 2 * bpart;
-            const int nch = ncol * nkc;
-            for (int item = pt; ok && item < 2 * nch; item += NPT) {
-                // eight consecutive threads take the eight rows of one core matrix (their 16-byte stores fill its
-                // 128 bytes: no bank conflicts), the next eight the next K chunk (their plane reads stay apart)
-                const int part = item >= nch ? 1 : 0;
-                const int rem = item - part * nch;
-                const int r8 = rem & 7, rest = rem >> 3;
-                const int u = rest % nkc, row = (rest / nkc) * 8 + r8;
-                const int im = row >= a.Nt ? 1 : 0;
-                const int o = a.Dk * (row - im * a.Nt) + 8 * u;    // first element in the window
-                const uint32_t *src = pl + (2 * im + part) * (Wp / 2) + (o >> 1);
-                uint4 v;
-                if ((o & 1) == 0) {
-                    v = make_uint4(src[0], src[1], src[2], src[3]);
-                } else {
-                    const uint32_t w0 = src[0], w1 = src[1], w2 = src[2], w3 = src[3], w4 = src[4];
-                    v = make_uint4(__funnelshift_r(w0, w1, 16), __funnelshift_r(w1, w2, 16), __funnelshift_r(w2, w3, 16),
-                                   __funnelshift_r(w3, w4, 16));
+            if (ok) {
+                // lane (r8 = lane % 8, uq = lane / 8) keeps its row within a block of 8 and its K chunk within a
+                // group of 4; warp pw takes the row blocks pw, pw + NPW, ... of each (part, re/im, chunk group).
+                // Along a warp's row blocks the window offset, the plane copy and the store move by constants.
+                constexpr int UB = (NKC + 3) / 4;
+                const int r8 = lane & 7, uq = lane >> 3, pw = warp - NCW;
+                const int nrb = a.Nt / 8;
+                const int nmine = nrb > pw ? (nrb - 1 - pw) / NPW + 1 : 0;
+                const int ostep = 8 * NPW * a.Dk, wstep = ostep >> 1;               // ostep is even
+                const uint32_t bstep = (uint32_t)(NPW * nkc * 128);
+#pragma unroll
+                for (int ub = 0; ub < UB; ++ub) {
+                    const int u = ub * 4 + uq;
+                    if (u >= NKC) continue;
+                    const int o0 = a.Dk * (8 * pw + r8) + 8 * u;                    // first element, first block
+                    const int cp = o0 & 1;
+#pragma unroll
+                    for (int pi = 0; pi < 4; ++pi) {                              // (part, re/im)
+                        const int part = pi & 1, im = pi >> 1;
+                        const uint32_t *src = pl + (2 * (2 * im + part) + cp) * (Wp / 2) + (o0 >> 1);
+                        unsigned char *dst = Bb + part * bpart + core_off(im * a.Nt + 8 * pw + r8, u, nkc);
+                        int m = 0;
+                        for (; m + 2 <= nmine; m += 2) {
+                            const uint32_t *s0 = src + m * wstep, *s1 = s0 + wstep;
+                            const uint4 v0 = make_uint4(s0[0], s0[1], s0[2], s0[3]);
+                            const uint4 v1 = make_uint4(s1[0], s1[1], s1[2], s1[3]);
+                            *reinterpret_cast<uint4 *>(dst + m * bstep) = v0;
+                            *reinterpret_cast<uint4 *>(dst + (m + 1) * bstep) = v1;
+                        }
+                        if (m < nmine) {
+                            const uint32_t *s0 = src + m * wstep;
+                            *reinterpret_cast<uint4 *>(dst + m * bstep) = make_uint4(s0[0], s0[1], s0[2], s0[3]);
+                        }
+                    }
                 }
-                *reinterpret_cast<uint4 *>(Bb + part * bpart + core_off(row, u, nkc)) = v;
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
@@ -406,17 +437,29 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             if (!__all_sync(0xffffffffu, mbar_wait(&dfull[db], (uint32_t)((s >> 1) & 1), 200, &s_abort, a.err))) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t base = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(db * 256);
-            const float2 st = cis_cycles(q0.y * (float)a.Dk);
+            const float2 st = cis_cycles(q0.y * (float)a.Dk), st8 = cis_cycles(q0.y * (float)(8 * a.Dk));
+            // this lane's ramp at its first column of the chunk: seeded at the first chunk, then 8 columns on
+            float2 wc = cis_cycles(fmaf(q0.y, (float)(a.Dk * (tt * a.Nt + g * cw + (odd ? 4 : 0)) - a.plk) - a.kc, q0.x));
+            wc.x *= scale;
+            wc.y *= scale;
+            // chunks of 8 columns; the next chunk's accumulator loads are in flight while one is processed
+            float vr[8], vi[8], nr[8], ni[8];
+            tmem_ld8(base + (uint32_t)(g * cw), vr);
+            tmem_ld8(base + (uint32_t)(a.Nt + g * cw), vi);
+            tmem_wait_ld();
+            // the accumulator is released as soon as its last chunk is in registers
+            auto release = [&]() {
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&dempty[db]);
+            };
+            if (cw == 8) release();
             for (int k8 = 0; k8 < cw; k8 += 8) {
                 const int cb = g * cw + k8;                   // first column of the chunk within the tile
-                float vr[8], vi[8];
-                tmem_ld8(base + (uint32_t)cb, vr);
-                tmem_ld8(base + (uint32_t)(a.Nt + cb), vi);
-                tmem_wait_ld();
-                if (k8 + 8 >= cw) {                           // the accumulator has been read
-                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(&dempty[db]);
+                const bool more = k8 + 8 < cw;
+                if (more) {
+                    tmem_ld8(base + (uint32_t)(cb + 8), nr);
+                    tmem_ld8(base + (uint32_t)(a.Nt + cb + 8), ni);
                 }
                 // even lane (Mr row) keeps columns 0..3 of the chunk, odd lane (Mi row) columns 4..7
                 float mr_r[4], mr_i[4], mi_r[4], mi_i[4];
@@ -431,10 +474,9 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                     mi_i[i] = odd ? ori : ri;
                 }
                 const int j0 = tt * a.Nt + cb + (odd ? 4 : 0);
+                float2 w = wc;
+                wc = cmul(wc, st8);
                 if (live && j0 < a.Ko) {
-                    float2 w = cis_cycles(fmaf(q0.y, (float)(a.Dk * j0 - a.plk) - a.kc, q0.x));
-                    w.x *= scale;
-                    w.y *= scale;
                     uint32_t outw[4];
 #pragma unroll
                     for (int i = 0; i < 4; ++i) {
@@ -445,6 +487,13 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                         w = cmul(w, st);
                     }
                     *reinterpret_cast<uint4 *>(yc + (size_t)p * a.Kop + j0) = make_uint4(outw[0], outw[1], outw[2], outw[3]);
+                }
+                tmem_wait_ld();
+                if (more && k8 + 16 >= cw) release();
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    vr[i] = nr[i];
+                    vi[i] = ni[i];
                 }
             }
         }
@@ -642,7 +691,7 @@ cudaError_t launch_level_tc(const LevelLaunch &L, const int *amax_in, void *scra
     auto need = [&](int nt, int sb) {
         const size_t bpart = (size_t)2 * nt * a.Lkp * 2;
         const int W = a.Dk * (nt - 1) + a.Lkp, Wp = (W + 9) & ~1;
-        return 4 * apart + (size_t)sb * 2 * bpart + (size_t)4 * (Wp / 2) * 4 + (size_t)a.Lkp * 4 + (size_t)XS * Wp * 8 +
+        return 4 * apart + (size_t)sb * 2 * bpart + (size_t)8 * (Wp / 2) * 4 + (size_t)a.Lkp * 4 + (size_t)XS * Wp * 8 +
                (size_t)(6 + 2 * sb) * 8;
     };
     // columns per tile: a multiple of 32 up to 128 whose operands fit shared memory with two B stages, the one that
@@ -666,12 +715,22 @@ cudaError_t launch_level_tc(const LevelLaunch &L, const int *amax_in, void *scra
     while (SB > 2 && need(a.Nt, SB) > avail) --SB;
     a.SB = SB;
     const size_t smem = need(a.Nt, SB);
-    cudaError_t e = cudaFuncSetAttribute(level_tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
     const long nb = (long)L.Np * a.nseg;
     if (nb > 0x7fffffffL) return cudaErrorInvalidValue;
-    level_tc_gemm<<<(unsigned)nb, NTHR, smem, s>>>(a);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    auto run = [&](auto kern) -> cudaError_t {
+        cudaError_t r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (r != cudaSuccess) return r;
+        kern<<<(unsigned)nb, NTHR, smem, s>>>(a);
+        return cudaGetLastError();
+    };
+    cudaError_t e;
+    switch (a.Lkp / 8) {
+        case 2: e = run(level_tc_gemm<2>); break;
+        case 4: e = run(level_tc_gemm<4>); break;
+        case 6: e = run(level_tc_gemm<6>); break;
+        default: e = run(level_tc_gemm<8>); break;
+    }
+    if (e != cudaSuccess) return e;
 
     FirArgs f;
     f.y = a.y; f.tp = L.tp; f.out = L.out; f.amax = L.amax; f.amax_in = amax_in;
