@@ -12,6 +12,12 @@ bracketed by a barrier and a synchronize; the 1.07 GB history is larger than the
 `e2e` repeats the timing through the public call with host buffers: each step copies the history from pinned host
 memory to the device and the image back.
 
+The chosen form is ImageFormer(precision='float16'): the levels on the tensor cores (split-bfloat16 products of
+the children's modulated frequency taps and the parent rows' Hankel windows, a float16 intermediate, the pulse FIR
+in float32), the final stage on the tensor cores (float16 operands, float32 accumulation), and 80 dB filters. The
+plain form is precision='float32' with the reference's 70 dB filters. Both errors are measured against the float64
+exact backprojection at 64x on random pixels.
+
 --gpus N (torchrun, one process per GPU): every rank forms its own collection (independent replicas; weak
 scaling); the step time is the maximum over ranks and the value counts every rank's backprojections.
 
@@ -86,25 +92,47 @@ class Clocks:
                     samples=len(rows))
 
 
-def plan_work(plan):
-    """Algorithmic bytes and flops of each launch of a form call (the level kernels, then the final stage):
-    bytes = the launch's compulsory reads and writes (its input samples, its child phases, its output samples);
-    flops = the rotation (8 per input sample and child) and the two FIRs (4 per tap and output sample, complex
-    data by real taps) of a level, and 8 T^2 Pf Qf per final tile (the separable tile sum as a real product)."""
-    out = []
-    B = 1
-    for lv in plan['levels']:
-        N = B * lv['C']
-        Lk = lv['fir_k']['L'] if lv['fir_k'] else 1
-        Lp = lv['fir_p']['L'] if lv['fir_p'] else 1
-        byt = 8 * (B * lv['P'] * lv['K'] + N * lv['P'] + N * lv['Po'] * lv['Ko'])
-        fl = N * lv['P'] * (8.0 * lv['K'] + 4.0 * Lk * lv['Ko']) + N * lv['Po'] * lv['Ko'] * 4.0 * Lp
-        out.append(dict(bytes=float(byt), flops=float(fl), kind='level'))
-        B = N
+def launch_work(plan, launches):
+    """Algorithmic bytes and flops of each launch of a form call, from the plan and the launch list
+    [(kind, level, ms)]:
+      level_fp32     bytes: the input samples, the child phases, the output samples; flops: the rotation (8 per
+                     input sample and child) and the two FIRs (4 per tap and output sample, complex by real);
+      level_tc_gemm  bytes: the input samples, the phases, the float16 intermediate written (4 per sample); flops:
+                     the children's frequency FIR as a complex product, 8 C Lk Ko per parent and pulse;
+      level_tc_fir   bytes: the intermediate read and the output written; flops: 4 Lp per output sample;
+      amax           bytes: the history read;
+      final_*        bytes: the final samples read and the image written; flops: 8 T^2 Pf Qf per tile.
+    'units' says which peak applies: 'tensor' (bf16 tensor), 'fp32' (CUDA cores) or None (bytes only)."""
+    lv = plan['levels']
+    nb = [1]
+    for l in lv:
+        nb.append(nb[-1] * l['C'])
     fin = plan['final']
-    T = plan['T']
-    out.append(dict(bytes=float(8 * (B * fin['P'] * fin['K'] + plan['nx'] * plan['ny'])),
-                    flops=float(8.0 * T * T * fin['P'] * fin['K'] * B), kind='final'))
+    out = []
+    for kind, l, ms in launches:
+        if kind == 'amax':
+            out.append(dict(bytes=8.0 * lv[0]['P'] * lv[0]['K'], flops=0.0, units=None))
+            continue
+        if kind.startswith('final'):
+            B = nb[-1]
+            out.append(dict(bytes=float(8 * (B * fin['P'] * fin['K'] + plan['nx'] * plan['ny'])),
+                            flops=float(8.0 * plan['T'] ** 2 * fin['P'] * fin['K'] * B),
+                            units='tensor' if kind == 'final_tc' else 'fp32'))
+            continue
+        L = lv[l]
+        Np, C, P, K, Ko, Po = nb[l], L['C'], L['P'], L['K'], L['Ko'], L['Po']
+        Lk = L['fir_k']['L'] if L['fir_k'] else 1
+        Lp = L['fir_p']['L'] if L['fir_p'] else 1
+        N = Np * C
+        if kind == 'level_fp32':
+            out.append(dict(bytes=float(8 * (Np * P * K + N * P + N * Po * Ko)),
+                            flops=float(N * P * (8.0 * K + 4.0 * Lk * Ko) + N * Po * Ko * 4.0 * Lp), units='fp32'))
+        elif kind == 'level_tc_gemm':
+            out.append(dict(bytes=float(8 * (Np * P * K + N * P) + 4 * N * P * Ko),
+                            flops=float(8.0 * N * P * Lk * Ko), units='tensor'))
+        else:
+            out.append(dict(bytes=float(4 * N * P * Ko + 8 * N * Po * Ko), flops=float(4.0 * N * Po * Ko * Lp),
+                            units='fp32'))
     return out
 
 
@@ -179,22 +207,13 @@ def main():
     col = w['col']
     log(f'[bench] history {tuple(S.shape)} from {w["n_scatterers"]} scatterers in {time.time() - t0:.1f} s')
 
-    # the chosen form and the plain float32 FFBP
-    modes = {'plain': 'fp32'}
-    try:
-        os.environ['FASTSAR_FINAL'] = 'tc3'
-        chosen = ImageFormer(col.ant, col.fmin, col.df, col.K, w['nx'], w['ny'], w['spx'], w['spy'], w['e1'], w['e2'])
-        probe = chosen.form_device(S)
-        torch.cuda.synchronize()
-        modes['chosen'] = 'tc3'
-    except ValueError as e:
-        log(f'[bench] tensor-core final stage unavailable ({e}); the chosen form is the plain float32 FFBP')
-        chosen = None
-    os.environ['FASTSAR_FINAL'] = 'fp32'
-    plain = ImageFormer(col.ant, col.fmin, col.df, col.K, w['nx'], w['ny'], w['spx'], w['spy'], w['e1'], w['e2'])
-    if chosen is None:
-        chosen, modes['chosen'] = plain, 'fp32'
-    plan = plain._plan
+    # the chosen form (precision='float16': tensor-core levels and final stage, 80 dB filters) and the plain
+    # float32 FFBP (the reference's arithmetic and filters)
+    mk = lambda prec: ImageFormer(col.ant, col.fmin, col.df, col.K, w['nx'], w['ny'], w['spx'], w['spy'], w['e1'],
+                                  w['e2'], precision=prec)
+    chosen = mk('float16')
+    plain = mk('float32')
+    plan = chosen._plan
     npix, P = w['nx'] * w['ny'], col.Np
     out = torch.empty((w['nx'], w['ny']), dtype=torch.complex64, device='cuda')
     out_plain = torch.empty_like(out)
@@ -217,11 +236,12 @@ def main():
         return max_over_ranks(e0.elapsed_time(e1) / steps), c
 
     ms, clocks = timed(chosen, out, args.steps, args.warmup, clocks=True)
-    ms_plain = ms if chosen is plain else timed(plain, out_plain, args.steps, args.warmup)[0]
-    if chosen is plain:
-        out_plain = out
+    ms_plain = timed(plain, out_plain, args.steps, args.warmup)[0]
     stages = chosen._dev.form_timed(S, out)
-    stages_plain = stages if chosen is plain else plain._dev.form_timed(S, out_plain)
+    stages_plain = plain._dev.form_timed(S, out_plain)
+    # every launch of the chosen form, timed by events on its stream (the median of three calls)
+    profs = [chosen._dev.form_profile(S, out) for _ in range(3)]
+    launches = [(k, l, float(np.median([p[i][2] for p in profs]))) for i, (k, l, _) in enumerate(profs[0])]
     torch.cuda.synchronize()
 
     # end to end through the public call: pinned host history -> device -> image -> pinned host
@@ -265,29 +285,30 @@ def main():
     log(f'[bench] float64 BP 64x on {len(idx)} pixels in {time.time() - t1:.1f} s: chosen {err_chosen:.1f} dB, '
         f'plain {err_plain:.1f} dB')
 
-    # roofline of the dominant launch of the chosen form
+    # roofline of the dominant launch of the chosen form: achieved = its algorithmic bytes (or flops) / its time;
+    # of the HBM and compute rooflines the one it comes closer to
     hbm, bf16, src = peaks()
-    work = plan_work(chosen._plan)
-    k = int(np.argmax(stages))
-    names = [f'level{i}' for i in range(len(stages) - 1)] + ['final']
+    work = launch_work(chosen._plan, launches)
+    k = int(np.argmax([x[2] for x in launches]))
+    kname = f'{launches[k][0]}[{launches[k][1]}]'
+    kms = launches[k][2]
     traffic = None
     try:
         with open(os.path.join(ROOT, 'profiles', 'traffic.json')) as fh:
-            traffic = json.load(fh).get(args.workload, {}).get(names[k])
+            traffic = json.load(fh).get(args.workload, {}).get(kname)
     except (OSError, ValueError):
         pass
-    is_tc = names[k] == 'final' and modes['chosen'] != 'fp32'
-    if is_tc:
-        ach = work[k]['flops'] / (stages[k] * 1e-3) / 1e12
-        roof = dict(bound='tensor', achieved=ach, peak=bf16, unit='TFLOP/s', frac=ach / bf16, traffic=traffic)
+    gbs = work[k]['bytes'] / (kms * 1e-3) / 1e9
+    fl = work[k]['flops'] / (kms * 1e-3) / 1e12
+    fpk = bf16 if work[k]['units'] == 'tensor' else FP32_PEAK_NOMINAL
+    if work[k]['units'] and fl / fpk > gbs / hbm:
+        roof = dict(bound='tensor' if work[k]['units'] == 'tensor' else 'fp32', achieved=fl, peak=fpk,
+                    unit='TFLOP/s', frac=fl / fpk, traffic=traffic)
     else:
-        ach = work[k]['bytes'] / (stages[k] * 1e-3) / 1e9
-        tf = work[k]['flops'] / (stages[k] * 1e-3) / 1e12
-        roof = dict(bound='hbm', achieved=ach, peak=hbm, unit='GB/s', frac=ach / hbm, traffic=traffic,
-                    fp32_cores=dict(achieved_tflops=tf, peak_tflops_nominal=FP32_PEAK_NOMINAL,
-                                    frac=tf / FP32_PEAK_NOMINAL))
-    roof.update(kernel=names[k], peak_source=src, ms=stages[k], algorithmic_bytes=work[k]['bytes'],
-                algorithmic_flops=work[k]['flops'])
+        roof = dict(bound='hbm', achieved=gbs, peak=hbm, unit='GB/s', frac=gbs / hbm, traffic=traffic)
+    roof.update(kernel=kname, peak_source=src if roof['bound'] != 'fp32' else 'nominal FP32 FMA at 1965 MHz',
+                ms=kms, algorithmic_bytes=work[k]['bytes'], algorithmic_flops=work[k]['flops'],
+                hbm_frac=gbs / hbm, compute_frac=(fl / fpk) if work[k]['units'] else None)
 
     # the reference CPU former on this host, bounded sample
     cpu = None
@@ -303,27 +324,29 @@ def main():
             log(f'[bench] cpu baseline failed: {type(e).__name__}: {e}')
 
     value = world * npix * P / (ms * 1e-3) / 1e9
-    launches = chosen._dev.launches()
+    nlaunch = chosen._dev.launches()
     line = dict(
         metric=METRIC, value=value, unit='GBP/s', n_gpus=world, steps=args.steps, warmup=args.warmup,
         ms_per_step=ms, higher_is_better=True, scaling='weak', vs_baseline=None,
-        dtype='f32' if modes['chosen'] == 'fp32' else 'f32+bf16x3',
+        dtype='mixed: bf16x3 and f16 tensor products, f16 intermediate, f32 accumulation',
         data=f'synthetic: {w["n_scatterers"]} seeded scatterers simulated on the GPU in float64, noise -40 dB',
         config=dict(workload=f'{args.workload}: {P} pulses x {col.K} samples -> {w["nx"]} x {w["ny"]} px at '
-                             f'{w["spx"]} m', final=modes['chosen'], T=plain.T,
+                             f'{w["spx"]} m', form="precision='float16'", T=chosen.T, atten_db=chosen.atten,
                     levels=[(l['C'], l['Dk'], l['Dp']) for l in plan['levels']],
                     l2='inputs larger than L2 (1.07 GB history per step), no flush',
                     parallelism=f'replicas x{world}' if world > 1 else 'single GPU'),
         err_db=dict(chosen=err_chosen, plain=err_plain, reference='float64 exact backprojection, 64x, linear, '
                     f'{len(idx)} random pixels, one complex gain fitted'),
-        plain_fp32=dict(value=world * npix * P / (ms_plain * 1e-3) / 1e9, ms_per_step=ms_plain, stages_ms=stages_plain),
+        plain_fp32=dict(value=world * npix * P / (ms_plain * 1e-3) / 1e9, ms_per_step=ms_plain, stages_ms=stages_plain,
+                        atten_db=plain.atten),
         speedup_vs_plain=ms_plain / ms,
-        stages_ms=dict(zip(names, stages)),
+        stages_ms=stages,
+        launches_ms=[(f'{kk}[{ll}]', round(m, 3)) for kk, ll, m in launches],
         roofline=roof,
         cpu_baseline=cpu,
         e2e=dict(value=world * npix * P / (ms_e2e * 1e-3) / 1e9, unit='GBP/s', ms_per_step=ms_e2e,
                  h2d_bytes_per_step=int(S.numel() * 8), d2h_bytes_per_step=int(npix * 8)),
-        gpu_launches=launches * args.steps,
+        gpu_launches=nlaunch * args.steps,
         clocks=clocks)
     if rank == 0:
         print(json.dumps(line), flush=True)

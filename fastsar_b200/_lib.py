@@ -12,11 +12,13 @@ LIB_PATH = os.path.join(HERE, 'libffbp_b200.so')
 FFBP_OK, FFBP_E_ARG, FFBP_E_CUDA, FFBP_E_NOMEM, FFBP_E_WORKSPACE, FFBP_E_UNSUPPORTED = 0, -1, -2, -3, -4, -5
 FFBP_FINAL_FP32, FFBP_FINAL_TC_F16, FFBP_FINAL_TC_BF16X3 = 0, 1, 2
 FFBP_LEVELS_TC = 0x100
+KIND_NAMES = {1: 'amax', 2: 'level_fp32', 3: 'level_tc_gemm', 4: 'level_tc_fir', 5: 'final_fp32', 6: 'final_tc'}
 
 # every symbol include/ffbp_b200.h declares
 EXPORTS = ('ffbp_last_error', 'ffbp_abi_version', 'ffbp_plan_create', 'ffbp_plan_destroy', 'ffbp_plan_workspace_bytes',
            'ffbp_form', 'ffbp_form_timed', 'ffbp_plan_info', 'ffbp_level', 'ffbp_phases', 'ffbp_final',
-           'ffbp_bp_points_f64', 'ffbp_simulate', 'ffbp_form_static', 'ffbp_level_tc', 'ffbp_level_tc_scratch_bytes')
+           'ffbp_bp_points_f64', 'ffbp_simulate', 'ffbp_form_static', 'ffbp_level_tc', 'ffbp_level_tc_scratch_bytes',
+           'ffbp_form_profile')
 
 _c_int, _c_double, _vp = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
 
@@ -65,6 +67,8 @@ def load():
     L.ffbp_form_static.argtypes = [_vp, _vp, _vp, _vp, ctypes.POINTER(_c_int)]
     L.ffbp_form_timed.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_size_t, _vp, ctypes.POINTER(ctypes.c_float), _c_int]
     L.ffbp_plan_info.argtypes = [_vp, ctypes.POINTER(_c_int), ctypes.POINTER(_c_int)]
+    L.ffbp_form_profile.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_size_t, _vp, ctypes.POINTER(ctypes.c_float),
+                                    ctypes.POINTER(_c_int), _c_int]
     L.ffbp_level.argtypes = [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_int, _c_double,
                              _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp]
     L.ffbp_level_tc.argtypes = [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_int,

@@ -214,6 +214,18 @@ class DevicePlan:
                                      ctypes.c_void_p(stream.cuda_stream), ms, n), 'ffbp_form_timed')
         return list(ms)
 
+    def form_profile(self, S_dev, img_dev, stream=None):
+        """form with the device time (ms) of every launch: [(kind name, level, ms), ...] in launch order."""
+        import torch
+        L = _lib.load()
+        stream = torch.cuda.current_stream(self.device) if stream is None else stream
+        n = self.launches()
+        ms, kind = (ctypes.c_float * n)(), (ctypes.c_int * n)()
+        _lib.check(L.ffbp_form_profile(self.handle, ctypes.c_void_p(S_dev.data_ptr()), ctypes.c_void_p(img_dev.data_ptr()),
+                                       ctypes.c_void_p(self.workspace()), ctypes.c_size_t(self.ws_bytes),
+                                       ctypes.c_void_p(stream.cuda_stream), ms, kind, n), 'ffbp_form_profile')
+        return [(_lib.KIND_NAMES.get(k >> 8, '?'), k & 0xff, float(m)) for k, m in zip(kind, ms)]
+
     def launches(self):
         """Kernels one form call launches."""
         L = _lib.load()

@@ -255,8 +255,16 @@ int ffbp_plan_workspace_bytes(const ffbp_plan *p, size_t *bytes)
     return FFBP_OK;
 }
 
+// One form call. When `prof` is given, an event is recorded after every launch (and one before the first):
+// prof->kind[i] = FFBP_KIND_* << 8 | level of launch i.
+struct FormProfile {
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> kind;
+    ~FormProfile() { for (auto &x : ev) cudaEventDestroy(x); }
+};
+
 static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, size_t ws_bytes, void *stream_, int *h_bad,
-                     float *stage_ms, int n_stage)
+                     FormProfile *prof)
 {
     if (!p || !d_S || !d_img || !d_ws) return fail(FFBP_E_ARG, "ffbp_form: null argument");
     size_t need;
@@ -275,19 +283,19 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
     cudaError_t e = cudaMemsetAsync(bad, 0x7f, sizeof(int), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(bad + 1, 0, (size_t)(p->nlev + 2) * sizeof(int), s);
     if (e != cudaSuccess) return cuda_fail(e, "status reset");
-    const bool timed = stage_ms != nullptr;
-    if (timed && n_stage < p->nlev + 1) return fail(FFBP_E_ARG, "stage_ms holds %d entries, %d needed", n_stage, p->nlev + 1);
-    std::vector<cudaEvent_t> ev;
-    if (timed) {
-        ev.resize(p->nlev + 2);
-        for (auto &x : ev) cudaEventCreate(&x);
-        cudaEventRecord(ev[0], s);
-    }
-    auto destroy_events = [&]() { for (auto &x : ev) cudaEventDestroy(x); };
+    auto mark = [&](int kind) {
+        if (!prof) return;
+        cudaEvent_t x;
+        cudaEventCreate(&x);
+        cudaEventRecord(x, s);
+        prof->ev.push_back(x);
+        prof->kind.push_back(kind);
+    };
+    mark(0);
     const float2 *in = static_cast<const float2 *>(d_S);
-    if (level_on_tc(p, 0) && (e = ffbp::launch_amax(in, (size_t)p->lv[0].P * p->lv[0].K, amax, s)) != cudaSuccess) {
-        destroy_events();
-        return cuda_fail(e, "history scan");
+    if (level_on_tc(p, 0)) {
+        if ((e = ffbp::launch_amax(in, (size_t)p->lv[0].P * p->lv[0].K, amax, s)) != cudaSuccess) return cuda_fail(e, "history scan");
+        mark(FFBP_KIND_AMAX << 8);
     }
     for (int l = 0; l < p->nlev; ++l) {
         const DevLevel &v = p->lv[l];
@@ -300,10 +308,19 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
         L.Dp = v.Dp; L.Lp = v.Lp; L.plp = v.plp; L.kc = v.kc;
         L.amax = amax + l + 1;
         const char *why = nullptr;
-        e = level_on_tc(p, l) ? ffbp::launch_level_tc(L, amax + l, scratch, bad + 1, s, &why) : ffbp::launch_level(L, s, &why);
-        if (why) { destroy_events(); return fail(FFBP_E_UNSUPPORTED, "level %d: %s", l, why); }
-        if (e != cudaSuccess) { destroy_events(); return cuda_fail(e, "level kernel"); }
-        if (timed) cudaEventRecord(ev[l + 1], s);
+        if (level_on_tc(p, l)) {
+            e = ffbp::launch_level_tc_gemm(L, amax + l, scratch, bad + 1, s, &why);
+            if (!why && e == cudaSuccess) {
+                mark(FFBP_KIND_LEVEL_TC_GEMM << 8 | l);
+                e = ffbp::launch_level_tc_fir(L, amax + l, scratch, s, &why);
+                if (!why && e == cudaSuccess) mark(FFBP_KIND_LEVEL_TC_FIR << 8 | l);
+            }
+        } else {
+            e = ffbp::launch_level(L, s, &why);
+            if (!why && e == cudaSuccess) mark(FFBP_KIND_LEVEL << 8 | l);
+        }
+        if (why) return fail(FFBP_E_UNSUPPORTED, "level %d: %s", l, why);
+        if (e != cudaSuccess) return cuda_fail(e, "level kernel");
         in = outp;
     }
     ffbp::FinalLaunch F;
@@ -315,13 +332,11 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
     const int fm = p->final_mode & 0xff;
     const char *why = nullptr;
     e = fm == FFBP_FINAL_FP32 ? ffbp::launch_final_fp32(F, s, &why) : ffbp::launch_final_tc(F, fm, s, &why);
-    if (why) { destroy_events(); return fail(FFBP_E_UNSUPPORTED, "final stage: %s", why); }
-    if (e != cudaSuccess) { destroy_events(); return cuda_fail(e, "final kernel"); }
-    if (timed) {
-        cudaEventRecord(ev[p->nlev + 1], s);
-        if ((e = cudaEventSynchronize(ev[p->nlev + 1])) != cudaSuccess) { destroy_events(); return cuda_fail(e, "form"); }
-        for (int l = 0; l <= p->nlev; ++l) cudaEventElapsedTime(&stage_ms[l], ev[l], ev[l + 1]);
-        destroy_events();
+    if (why) return fail(FFBP_E_UNSUPPORTED, "final stage: %s", why);
+    if (e != cudaSuccess) return cuda_fail(e, "final kernel");
+    mark((fm == FFBP_FINAL_FP32 ? FFBP_KIND_FINAL : FFBP_KIND_FINAL_TC) << 8 | p->nlev);
+    if (prof) {
+        if ((e = cudaEventSynchronize(prof->ev.back())) != cudaSuccess) return cuda_fail(e, "form");
         int st = 0;
         if ((e = cudaMemcpy(&st, bad + 1, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess) return cuda_fail(e, "status read");
         if (st) return fail(FFBP_E_CUDA, "a tensor-core kernel stopped waiting on its pipeline (a bounded wait ran out)");
@@ -338,14 +353,52 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
 
 int ffbp_form(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, size_t ws_bytes, void *stream, int *h_bad)
 {
-    return form_impl(p, d_S, d_img, d_ws, ws_bytes, stream, h_bad, nullptr, 0);
+    return form_impl(p, d_S, d_img, d_ws, ws_bytes, stream, h_bad, nullptr);
 }
 
 int ffbp_form_timed(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, size_t ws_bytes, void *stream,
                     float *h_stage_ms, int n_stage)
 {
     if (!h_stage_ms) return fail(FFBP_E_ARG, "ffbp_form_timed: null stage_ms");
-    return form_impl(p, d_S, d_img, d_ws, ws_bytes, stream, nullptr, h_stage_ms, n_stage);
+    if (!p) return fail(FFBP_E_ARG, "ffbp_form_timed: null plan");
+    if (n_stage < p->nlev + 1) return fail(FFBP_E_ARG, "stage_ms holds %d entries, %d needed", n_stage, p->nlev + 1);
+    FormProfile prof;
+    const int rc = form_impl(p, d_S, d_img, d_ws, ws_bytes, stream, nullptr, &prof);
+    if (rc != FFBP_OK) return rc;
+    // a stage runs from the event before its first launch to the one after its last (the history scan goes to
+    // level 0)
+    for (int l = 0; l <= p->nlev; ++l) h_stage_ms[l] = 0.f;
+    size_t i0 = 0;
+    for (size_t i = 1; i < prof.ev.size(); ++i) {
+        const int lv = prof.kind[i] & 0xff, k = prof.kind[i] >> 8;
+        const int next = i + 1 < prof.ev.size() ? (prof.kind[i + 1] & 0xff) : -1;
+        if (k == FFBP_KIND_AMAX) continue;
+        if (next != lv) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, prof.ev[i0], prof.ev[i]);
+            h_stage_ms[lv] = ms;
+            i0 = i;
+        }
+    }
+    return FFBP_OK;
+}
+
+int ffbp_form_profile(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, size_t ws_bytes, void *stream,
+                      float *h_ms, int *h_kind, int n)
+{
+    if (!p || !h_ms || !h_kind) return fail(FFBP_E_ARG, "ffbp_form_profile: null argument");
+    int nl = 0, nk = 0;
+    ffbp_plan_info(p, &nl, &nk);
+    if (n < nk) return fail(FFBP_E_ARG, "ffbp_form_profile: %d entries, %d launches", n, nk);
+    FormProfile prof;
+    const int rc = form_impl(p, d_S, d_img, d_ws, ws_bytes, stream, nullptr, &prof);
+    if (rc != FFBP_OK) return rc;
+    for (int i = 0; i < n; ++i) { h_ms[i] = 0.f; h_kind[i] = 0; }
+    for (size_t i = 1; i < prof.ev.size() && (int)i <= n; ++i) {
+        cudaEventElapsedTime(&h_ms[i - 1], prof.ev[i - 1], prof.ev[i]);
+        h_kind[i - 1] = prof.kind[i];
+    }
+    return FFBP_OK;
 }
 
 int ffbp_plan_info(const ffbp_plan *p, int *nlev, int *launches)
@@ -472,7 +525,7 @@ namespace ffbp {
 // ffbp_form on a workspace the caller names, for the entry points of other translation units.
 int form_on_workspace(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, size_t ws_bytes, void *stream, int *h_bad)
 {
-    return form_impl(p, d_S, d_img, d_ws, ws_bytes, stream, h_bad, nullptr, 0);
+    return form_impl(p, d_S, d_img, d_ws, ws_bytes, stream, h_bad, nullptr);
 }
 
 int set_error(int code, const char *msg)

@@ -31,6 +31,11 @@ bool level_tc_supported(int C, int Lk, int Dk);
 size_t level_tc_scratch_bytes(int Np, int C, int P, int Ko);
 cudaError_t launch_level_tc(const LevelLaunch &L, const int *amax_in, void *scratch, int *err, cudaStream_t s,
                             const char **why);
+// its two passes, for callers that time them apart
+cudaError_t launch_level_tc_gemm(const LevelLaunch &L, const int *amax_in, void *scratch, int *err, cudaStream_t s,
+                                 const char **why);
+cudaError_t launch_level_tc_fir(const LevelLaunch &L, const int *amax_in, const void *scratch, cudaStream_t s,
+                                const char **why);
 // The largest |component| of n complex samples into *amax (float bits, atomicMax; start at 0).
 cudaError_t launch_amax(const float2 *x, size_t n, int *amax, cudaStream_t s);
 

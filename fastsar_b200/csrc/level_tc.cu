@@ -671,12 +671,11 @@ cudaError_t launch_amax(const float2 *x, size_t n, int *amax, cudaStream_t s)
     return cudaGetLastError();
 }
 
-cudaError_t launch_level_tc(const LevelLaunch &L, const int *amax_in, void *scratch, int *err, cudaStream_t s,
-                            const char **why)
+cudaError_t launch_level_tc_gemm(const LevelLaunch &L, const int *amax_in, void *scratch, int *err, cudaStream_t s,
+                                 const char **why)
 {
     *why = nullptr;
     const int Lk = L.Dk > 1 ? L.Lk : 1, plk = L.Dk > 1 ? L.plk : 0;
-    const int Lp = L.Dp > 1 ? L.Lp : 1, plp = L.Dp > 1 ? L.plp : 0;
     if (!level_tc_supported(L.C, Lk, L.Dk)) { *why = "the tensor-core level takes C <= 64 children and Lk <= 64 taps"; return cudaErrorNotSupported; }
     GemmArgs a;
     a.x = L.x; a.ph = L.phase; a.tk = L.tk; a.wp = L.wp; a.wk = L.wk; a.bad = L.bad; a.amax_in = amax_in;
@@ -731,10 +730,17 @@ cudaError_t launch_level_tc(const LevelLaunch &L, const int *amax_in, void *scra
         default: e = run(level_tc_gemm<8>); break;
     }
     if (e != cudaSuccess) return e;
+    return cudaSuccess;
+}
 
+cudaError_t launch_level_tc_fir(const LevelLaunch &L, const int *amax_in, const void *scratch, cudaStream_t s,
+                                const char **why)
+{
+    *why = nullptr;
+    const int Lp = L.Dp > 1 ? L.Lp : 1, plp = L.Dp > 1 ? L.plp : 0;
     FirArgs f;
-    f.y = a.y; f.tp = L.tp; f.out = L.out; f.amax = L.amax; f.amax_in = amax_in;
-    f.rows = L.Np * L.C; f.P = L.P; f.Kop = a.Kop; f.Ko = L.Ko; f.Po = L.Po; f.Dp = L.Dp; f.Lp = Lp; f.plp = plp;
+    f.y = static_cast<const __half2 *>(scratch); f.tp = L.tp; f.out = L.out; f.amax = L.amax; f.amax_in = amax_in;
+    f.rows = L.Np * L.C; f.P = L.P; f.Kop = (L.Ko + 3) & ~3; f.Ko = L.Ko; f.Po = L.Po; f.Dp = L.Dp; f.Lp = Lp; f.plp = plp;
     const int AP = (Lp + L.Dp - 1) / L.Dp;
     switch (AP) {
         case 1: return launch_fir<1>(f, s);
@@ -751,6 +757,18 @@ cudaError_t launch_level_tc(const LevelLaunch &L, const int *amax_in, void *scra
         case 12: return launch_fir<12>(f, s);
         default: *why = "pulse FIR spans more than 12 output pulses"; return cudaErrorNotSupported;
     }
+}
+
+}  // namespace ffbp
+
+namespace ffbp {
+
+cudaError_t launch_level_tc(const LevelLaunch &L, const int *amax_in, void *scratch, int *err, cudaStream_t s,
+                            const char **why)
+{
+    cudaError_t e = launch_level_tc_gemm(L, amax_in, scratch, err, s, why);
+    if (e != cudaSuccess || *why) return e;
+    return launch_level_tc_fir(L, amax_in, scratch, s, why);
 }
 
 }  // namespace ffbp

@@ -134,6 +134,20 @@ int ffbp_form_static(ffbp_plan *plan, const void *d_S, void *d_img, void *stream
 int ffbp_form_timed(ffbp_plan *plan, const void *d_S, void *d_img, void *d_ws, size_t ws_bytes, void *stream,
                     float *h_stage_ms, int n_stage);
 
+/* ffbp_form with the device time of every launch, in launch order: h_ms[i] (ms, CUDA events recorded on `stream`
+ * after each launch) and h_kind[i] = FFBP_KIND_* << 8 | level (nlev for the final stage). n >= the launch count
+ * of ffbp_plan_info. Waits for the stream. No counterpart in the reference (it times stages, not launches).       */
+enum {
+    FFBP_KIND_AMAX = 1,            /* the history's largest component (ahead of tensor-core levels)               */
+    FFBP_KIND_LEVEL = 2,           /* a float32 level kernel                                                       */
+    FFBP_KIND_LEVEL_TC_GEMM = 3,   /* a tensor-core level's first pass (products, ramp, float16 intermediate)     */
+    FFBP_KIND_LEVEL_TC_FIR = 4,    /* a tensor-core level's pulse FIR                                              */
+    FFBP_KIND_FINAL = 5,           /* the float32 final stage                                                      */
+    FFBP_KIND_FINAL_TC = 6         /* the tensor-core final stage                                                  */
+};
+int ffbp_form_profile(ffbp_plan *plan, const void *d_S, void *d_img, void *d_ws, size_t ws_bytes, void *stream,
+                      float *h_ms, int *h_kind, int n);
+
 /* Levels and launches of a plan: *nlev, and the kernels one ffbp_form launches (*launches).                  */
 int ffbp_plan_info(const ffbp_plan *plan, int *nlev, int *launches);
 
