@@ -464,6 +464,36 @@ int ffbp_level_tc(const void *d_x, int Np, int P, int K, const void *d_phase, in
     return FFBP_OK;
 }
 
+int ffbp_exact_pad(const void *d_S, int n, int K, const float *d_wp, const float *d_wk, int nfft, void *d_pad,
+                   int *d_bad, int p_off, void *stream)
+{
+    if (!d_S || !d_pad) return fail(FFBP_E_ARG, "ffbp_exact_pad: null buffer");
+    if (n < 0 || K < 2 || nfft < K || p_off < 0) return fail(FFBP_E_ARG, "ffbp_exact_pad: bad sizes");
+    cudaError_t e = ffbp::launch_exact_pad(static_cast<const float2 *>(d_S), n, K, d_wp, d_wk, nfft,
+                                           static_cast<float2 *>(d_pad), d_bad, p_off, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "ffbp_exact_pad");
+    return FFBP_OK;
+}
+
+int ffbp_exact_backproject(const void *d_prof, int n, int nfft, int W, const long long *d_blo, const int *d_lo,
+                           const double *d_ant, const double *d_ref, const double *d_cen, int ntx, int nty, int tx,
+                           int ty, int nx, int ny, double spx, double spy, const double *e1, const double *e2,
+                           double inv_dr, double kcyc, int cubic, int along1, void *d_win, void *d_out, void *stream)
+{
+    if (!d_prof || !d_blo || !d_lo || !d_ant || !d_ref || !d_cen || !e1 || !e2 || !d_win || !d_out)
+        return fail(FFBP_E_ARG, "ffbp_exact_backproject: null buffer");
+    if (n < 0 || W > nfft || ntx < 1 || nty < 1 || nx < 1 || ny < 1 || ntx * tx < nx || nty * ty < ny)
+        return fail(FFBP_E_ARG, "ffbp_exact_backproject: bad sizes");
+    const char *why = nullptr;
+    cudaError_t e = ffbp::launch_exact_tiles(static_cast<const float2 *>(d_prof), n, nfft, W, d_blo, d_lo, d_ant, d_ref,
+                                             d_cen, ntx, nty, tx, ty, nx, ny, spx, spy, e1, e2, inv_dr, kcyc, cubic,
+                                             along1, static_cast<float2 *>(d_win), static_cast<float2 *>(d_out),
+                                             static_cast<cudaStream_t>(stream), &why);
+    if (why) return fail(FFBP_E_ARG, "ffbp_exact_backproject: %s", why);
+    if (e != cudaSuccess) return cuda_fail(e, "ffbp_exact_backproject");
+    return FFBP_OK;
+}
+
 int ffbp_phases(const double *d_ant, int P, const double *d_ref, int Np, const double *d_cen, int C,
                 const double *d_range, double k0c, double k1, int cancel_free, void *d_phase, void *stream)
 {

@@ -76,4 +76,14 @@ cudaError_t launch_bp_points_f64(const double2 *prof, int P, int nfft, const dou
 cudaError_t launch_simulate(const double *ant, int P, int K, double fmin, double df, const double *pos,
                             const double2 *amp, int N, float2 *S, cudaStream_t s);
 
+// Exact backprojection onto a grid's tiles (exact_tiles.cu): the windowed, zero-padded history of a chunk of pulses
+// (its fftshift folded in), and the crop plus tiled backprojection of its inverse-FFT profiles.
+cudaError_t launch_exact_pad(const float2 *s, int n, int K, const float *wp, const float *wk, int nfft, float2 *pad,
+                             int *bad, int p_off, cudaStream_t st);
+cudaError_t launch_exact_tiles(const float2 *prof, int n, int nfft, int W, const long long *blo, const int *lo,
+                               const double *ant, const double *ref, const double *cen, int ntx, int nty, int tx,
+                               int ty, int nx, int ny, double spx, double spy, const double *e1, const double *e2,
+                               double inv_dr, double kcyc, int cubic, int along1, float2 *win, float2 *out,
+                               cudaStream_t st, const char **why);
+
 }  // namespace ffbp

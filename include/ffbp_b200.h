@@ -177,6 +177,23 @@ int ffbp_level_tc(const void *d_x, int Np, int P, int K, const void *d_phase, in
                   const float *d_wk, void *d_out, int *d_bad, void *d_scratch, size_t scratch_bytes, int *d_status,
                   void *stream);
 
+/* Exact backprojection onto a grid (ExactFormer, fastsar/exact.py:404-801), in two calls per chunk of n pulses:
+ * ffbp_exact_pad writes the windowed samples S[p, k] wp[p_off + p] wk[k] of d_S [n, K] complex64 into d_pad [n, nfft]
+ * at bin k - K/2 (mod nfft) (fastsar/exact.py:186-194 pad_window; the other bins are the caller's, zeroed once)
+ * and records in d_bad (optional, atomic min) the first pulse p_off + p with a non-finite sample; after the caller's
+ * inverse FFT of length nfft (cuFFT, normalised by 1/nfft), ffbp_exact_backproject crops each profile's W reachable
+ * bins from blo[p] (circularly, scaled by nfft: fastsar/exact.py:196-205 crop) into d_win [n, W] and adds the tiled
+ * backprojection (fastsar/exact.py:58-162 bp_tiles) onto d_out [nx, ny] complex64. Tiles tx x ty in {32 x 32,
+ * 16 x 16, 8 x 16, 8 x 8}; d_cen [ntx nty, 3] their centres (float64), tile (bx, by) at index bx nty + by; lo[p] =
+ * blo[p] - nfft/2; e1, e2 host pointers to 3 doubles; cubic 1 (Lagrange, 4 samples) or 0 (linear); along1 1 to run
+ * consecutive blocks along e1.                                                                                    */
+int ffbp_exact_pad(const void *d_S, int n, int K, const float *d_wp, const float *d_wk, int nfft, void *d_pad,
+                   int *d_bad, int p_off, void *stream);
+int ffbp_exact_backproject(const void *d_prof, int n, int nfft, int W, const long long *d_blo, const int *d_lo,
+                           const double *d_ant, const double *d_ref, const double *d_cen, int ntx, int nty, int tx,
+                           int ty, int nx, int ny, double spx, double spy, const double *e1, const double *e2,
+                           double inv_dr, double kcyc, int cubic, int along1, void *d_win, void *d_out, void *stream);
+
 /* Child phases in float64 for one level (fastsar/ffbp2.py:329-339 / fastsar/ffbp_cuda.py:598-632): for parent n,
  * child c and pulse p, ddr = |cen[n,c] - ant[p]| - |ref[n] - ant[p]| (or - range[p] when d_range is given),
  * c0 = ddr k0c - rint(ddr k0c), sl = ddr k1, stored as float pairs into d_phase [Np, C, P]. cancel_free selects

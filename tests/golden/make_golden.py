@@ -14,6 +14,8 @@ Fixtures:
   fir.npz             decimator_fir kernels for a spread of (n_in, D, pass) values
   kernels.npz         the reference C++ kernels rot_fir_k_cplx, rot_fir_k, fir_p, final_tiles on seeded small inputs
   image_<case>.npz    ImageFormer(backend='cpu') images (history, image), ExactFormer(cpu) and backproject(cpu, 64x)
+  exact_setup.npz     ExactFormer's set-up (tile, centres, reachable bins) on geometries that pick 32 x 32 and 16 x 16
+                      tiles (python tests/golden/make_golden.py --only exact writes this file alone)
 """
 import argparse
 import os
@@ -92,11 +94,39 @@ def plan_record(ffbp2, col, nx, ny, spx, spy, e1, e2, T, nlev, pmax=0.4, full_li
     return plan, coll, rec
 
 
+def exact_setup(sim, ExactFormer):
+    """ExactFormer(backend='cpu')'s geometry-only set-up: the tile, the tile centres, the window of bins per pulse."""
+    rec = {}
+    cases = {'r5k': (sim.make_collect(res=0.5, scene=60.0, r0=5e3), 128, 128, 0.5, 0.5),
+             'r1k': (sim.make_collect(res=0.5, scene=60.0, r0=1e3), 96, 80, 0.5, 0.5),
+             'wide': (sim.make_collect(res=0.3, scene=100.0, r0=2e4), 300, 200, 0.3, 0.25)}
+    for name, (col, nx, ny, spx, spy) in cases.items():
+        f = ExactFormer(col.ant, col.fmin, col.df, col.K, nx, ny, spx, spy, backend='cpu')
+        rec[f'{name}_ant'] = col.ant
+        rec[f'{name}_scal'] = np.array([col.fmin, col.df, col.K, nx, ny, spx, spy], np.float64)
+        rec[f'{name}_tile'] = np.array(f.tile, np.int64)
+        rec[f'{name}_err'] = np.array(f.predicted_error_db)
+        rec[f'{name}_cen'] = f.cen
+        rec[f'{name}_blo'] = np.asarray(f.blo, np.int64)
+        rec[f'{name}_W'] = np.array(f.W, np.int64)
+        rec[f'{name}_nfft'] = np.array(f.nfft, np.int64)
+        rec[f'{name}_inv_dr'] = np.array(f.inv_dr)
+        rec[f'{name}_kcyc'] = np.array(f.kcyc)
+        print('exact setup', name, f.tile, f.W, f.nfft)
+    np.savez_compressed(os.path.join(HERE, 'exact_setup.npz'), **rec)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--ref', default='/root/reference')
+    ap.add_argument('--only', choices=('exact',), default=None)
     args = ap.parse_args()
     fs = import_reference(args.ref)
+    if args.only == 'exact':
+        from fastsar import sim
+        from fastsar.exact import ExactFormer
+        exact_setup(sim, ExactFormer)
+        return
     from fastsar import sim, ffbp2, ffbp_cpu, bp
     from fastsar.api import ImageFormer, _window
     from fastsar.exact import ExactFormer
@@ -243,6 +273,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, 'image_spot512.npz'), S=S, ffbp=img, bp64_idx=sub, bp64=ref64,
                         T=np.array(f.T), err=np.array(f.predicted_error_db))
     print('image_spot512 done', f.T, f.predicted_error_db)
+    exact_setup(sim, ExactFormer)
 
 
 if __name__ == '__main__':
