@@ -12,11 +12,12 @@ bracketed by a barrier and a synchronize; the 1.07 GB history is larger than the
 `e2e` repeats the timing through the public call with host buffers: each step copies the history from pinned host
 memory to the device and the image back.
 
-The chosen form is ImageFormer(precision='float16'): the levels on the tensor cores (split-bfloat16 products of
-the children's modulated frequency taps and the parent rows' Hankel windows, a float16 intermediate, the pulse FIR
-in float32), the final stage on the tensor cores (float16 operands, float32 accumulation), and 80 dB filters. The
-plain form is precision='float32' with the reference's 70 dB filters. Both errors are measured against the float64
-exact backprojection at 64x on random pixels.
+The chosen form is ImageFormer(precision='float16', taps='learned'): the levels on the tensor cores (split-bfloat16
+products of the children's modulated frequency taps and the parent rows' Hankel windows, a float16 intermediate,
+the pulse FIR in float32), the final stage on the tensor cores (float16 operands, float32 accumulation), and the
+learned decimation taps (fastsar_b200.learned: 8-output-sample filters from the packaged network, shorter than the
+80 dB Kaiser-sinc ones and more accurate). The plain form is precision='float32' with the reference's 70 dB
+Kaiser-sinc filters. Both errors are measured against the float64 exact backprojection at 64x on random pixels.
 
 --gpus N (torchrun, one process per GPU): every rank forms its own collection (independent replicas; weak
 scaling); the step time is the maximum over ranks and the value counts every rank's backprojections.
@@ -207,11 +208,11 @@ def main():
     col = w['col']
     log(f'[bench] history {tuple(S.shape)} from {w["n_scatterers"]} scatterers in {time.time() - t0:.1f} s')
 
-    # the chosen form (precision='float16': tensor-core levels and final stage, 80 dB filters) and the plain
-    # float32 FFBP (the reference's arithmetic and filters)
-    mk = lambda prec: ImageFormer(col.ant, col.fmin, col.df, col.K, w['nx'], w['ny'], w['spx'], w['spy'], w['e1'],
-                                  w['e2'], precision=prec)
-    chosen = mk('float16')
+    # the chosen form (precision='float16': tensor-core levels and final stage; learned decimation taps) and the
+    # plain float32 FFBP (the reference's arithmetic and filters)
+    mk = lambda prec, **kw: ImageFormer(col.ant, col.fmin, col.df, col.K, w['nx'], w['ny'], w['spx'], w['spy'],
+                                        w['e1'], w['e2'], precision=prec, **kw)
+    chosen = mk('float16', taps='learned')
     plain = mk('float32')
     plan = chosen._plan
     npix, P = w['nx'] * w['ny'], col.Np
@@ -277,11 +278,12 @@ def main():
     ref64 = backproject_device(S, col.ant, col.fmin, col.df, pts, upsample=64).cpu().numpy()
     it = torch.from_numpy(idx).cuda()
 
-    def rel_db(a):
+    def rel_db(a, fit=True):
         a = a.reshape(-1)[it].cpu().numpy().astype(np.complex128)
-        g = np.vdot(a, ref64) / np.vdot(a, a)
+        g = np.vdot(a, ref64) / np.vdot(a, a) if fit else 1.0
         return float(10 * np.log10(np.sum(np.abs(g * a - ref64) ** 2) / np.sum(np.abs(ref64) ** 2)))
     err_chosen, err_plain = rel_db(out), rel_db(out_plain)
+    err_nofit = dict(chosen=rel_db(out, False), plain=rel_db(out_plain, False))
     log(f'[bench] float64 BP 64x on {len(idx)} pixels in {time.time() - t1:.1f} s: chosen {err_chosen:.1f} dB, '
         f'plain {err_plain:.1f} dB')
 
@@ -331,12 +333,13 @@ def main():
         dtype='mixed: bf16x3 and f16 tensor products, f16 intermediate, f32 accumulation',
         data=f'synthetic: {w["n_scatterers"]} seeded scatterers simulated on the GPU in float64, noise -40 dB',
         config=dict(workload=f'{args.workload}: {P} pulses x {col.K} samples -> {w["nx"]} x {w["ny"]} px at '
-                             f'{w["spx"]} m', form="precision='float16'", T=chosen.T, atten_db=chosen.atten,
+                             f'{w["spx"]} m', form="precision='float16', taps='learned'", T=chosen.T,
+                    taps=[(l['kind_k'], l['kind_p']) for l in plan['levels']], atten_db_fallback=chosen.atten,
                     levels=[(l['C'], l['Dk'], l['Dp']) for l in plan['levels']],
                     l2='inputs larger than L2 (1.07 GB history per step), no flush',
                     parallelism=f'replicas x{world}' if world > 1 else 'single GPU'),
         err_db=dict(chosen=err_chosen, plain=err_plain, reference='float64 exact backprojection, 64x, linear, '
-                    f'{len(idx)} random pixels, one complex gain fitted'),
+                    f'{len(idx)} random pixels, one complex gain fitted', no_gain_fitted=err_nofit),
         plain_fp32=dict(value=world * npix * P / (ms_plain * 1e-3) / 1e9, ms_per_step=ms_plain, stages_ms=stages_plain,
                         atten_db=plain.atten),
         speedup_vs_plain=ms_plain / ms,

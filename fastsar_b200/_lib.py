@@ -18,7 +18,8 @@ KIND_NAMES = {1: 'amax', 2: 'level_fp32', 3: 'level_tc_gemm', 4: 'level_tc_fir',
 EXPORTS = ('ffbp_last_error', 'ffbp_abi_version', 'ffbp_plan_create', 'ffbp_plan_destroy', 'ffbp_plan_workspace_bytes',
            'ffbp_form', 'ffbp_form_timed', 'ffbp_plan_info', 'ffbp_level', 'ffbp_phases', 'ffbp_final',
            'ffbp_bp_points_f64', 'ffbp_simulate', 'ffbp_form_static', 'ffbp_level_tc', 'ffbp_level_tc_scratch_bytes',
-           'ffbp_form_profile', 'ffbp_exact_pad', 'ffbp_exact_backproject')
+           'ffbp_form_profile', 'ffbp_exact_pad', 'ffbp_exact_backproject', 'ffbp_mlp_param_count',
+           'ffbp_mlp_max_decimation', 'ffbp_mlp_work_bytes', 'ffbp_mlp_taps', 'ffbp_mlp_grad', 'ffbp_mlp_train_step')
 
 _c_int, _c_double, _vp = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
 
@@ -75,6 +76,14 @@ def load():
                                 _c_double, _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t,
                                 _vp, _vp]
     L.ffbp_level_tc_scratch_bytes.argtypes = [_c_int, _c_int, _c_int, _c_int]
+    L.ffbp_mlp_param_count.argtypes = []
+    L.ffbp_mlp_work_bytes.argtypes = [_c_int]
+    L.ffbp_mlp_taps.argtypes = [_vp, _vp, _c_int, _vp, _vp, _vp]
+    L.ffbp_mlp_max_decimation.argtypes = []
+    L.ffbp_mlp_grad.argtypes = [_vp, _vp, _c_int, _vp, ctypes.c_float, _vp, _c_int, _vp, _vp, _c_int, _vp, _vp, _vp,
+                                _vp]
+    L.ffbp_mlp_train_step.argtypes = [_vp, _vp, _vp, _c_int, _vp, ctypes.c_float, _vp, _c_int, _vp, _vp, _c_int,
+                                      ctypes.c_float, _c_int, _vp, _vp, _vp]
     L.ffbp_exact_pad.argtypes = [_vp, _c_int, _c_int, _vp, _vp, _c_int, _vp, _vp, _c_int, _vp]
     L.ffbp_exact_backproject.argtypes = [_vp, _c_int, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int,
                                          _c_int, _c_int, _c_int, _c_double, _c_double, _vp, _vp, _c_double, _c_double,
@@ -88,6 +97,7 @@ def load():
     for name in EXPORTS:
         getattr(L, name).restype = _c_int
     L.ffbp_level_tc_scratch_bytes.restype = ctypes.c_size_t
+    L.ffbp_mlp_work_bytes.restype = ctypes.c_size_t
     _LIB = L
     return L
 

@@ -254,11 +254,14 @@ class ImageFormer:
     precision='float32' runs the float32 kernels with the reference's filters (70 dB stop band); 'float16' is the
     mixed-precision form: the levels and the final stage on the tensor cores (split bfloat16 products, a float16
     intermediate, float16 final operands, float32 accumulation) with 80 dB filters, whose smaller error leaves room
-    for the reduced-precision arithmetic. atten (an extension of this package) sets the filters' stop band in dB."""
+    for the reduced-precision arithmetic. atten (an extension of this package) sets the filters' stop band in dB.
+    taps (an extension too): 'kaiser' (default, the reference's Kaiser-sinc decimators), 'learned' (the packaged
+    learned decimation taps, fastsar_b200.learned: 8-output-sample filters where the network covers a level's
+    decimation and pass fraction, Kaiser-sinc ones elsewhere) or a LearnedTaps instance."""
 
     def __init__(self, ant, fmin, df, K, nx, ny, spx, spy, e1=(1.0, 0.0, 0.0), e2=(0.0, 1.0, 0.0), *, backend='auto',
                  precision='float32', window=True, T='auto', levels=None, pmax=0.4, target_db=-40.0, aperture_weight=None,
-                 ref=None, range_gate='auto', padded=None, atten=None):
+                 ref=None, range_gate='auto', padded=None, atten=None, taps='kaiser'):
         self.ant = _check_positions(ant)
         self.P, self.K = self.ant.shape[0], int(K)
         if self.K < 2:
@@ -275,6 +278,17 @@ class ImageFormer:
         if not (np.isfinite(atten) and 20.0 <= float(atten) <= 200.0):
             raise ValueError(f'atten must be a stop-band attenuation in dB between 20 and 200, got {atten!r}')
         self.atten = float(atten)
+        if isinstance(taps, str):
+            if taps not in ('kaiser', 'learned'):
+                raise ValueError(f"taps must be 'kaiser', 'learned' or a LearnedTaps, got {taps!r}")
+            if taps == 'learned':
+                from .learned import LearnedTaps
+                taps = LearnedTaps.load()
+            else:
+                taps = None
+        elif not hasattr(taps, 'decimator'):
+            raise ValueError(f"taps must be 'kaiser', 'learned' or a LearnedTaps, got {taps!r}")
+        self.taps = taps
         self.window = window
         self.nx, self.ny = nx, ny
         self.predicted_error_db = None
@@ -311,7 +325,7 @@ class ImageFormer:
         while True:
             try:
                 plan = _plan.make_plan(col, nx, ny, spx, spy, T=T, nlev=nlev, pmax=pmax, e1=e1, e2=e2,
-                                       pulse=padded and padded[2], atten=self.atten)
+                                       pulse=padded and padded[2], atten=self.atten, taps=self.taps)
                 break
             except ValueError as e:
                 if levels is not None or 'cannot split' not in str(e) or nlev >= 8:

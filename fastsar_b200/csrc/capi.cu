@@ -9,6 +9,7 @@
 // intermediate at once, so the reference's first-level groups and batches (fastsar/ffbp_cuda.py:1154-1198) are not
 // needed for the workloads of record and the launches cover all children of a level.
 #include <climits>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -491,6 +492,53 @@ int ffbp_exact_backproject(const void *d_prof, int n, int nfft, int W, const lon
                                              static_cast<cudaStream_t>(stream), &why);
     if (why) return fail(FFBP_E_ARG, "ffbp_exact_backproject: %s", why);
     if (e != cudaSuccess) return cuda_fail(e, "ffbp_exact_backproject");
+    return FFBP_OK;
+}
+
+int ffbp_mlp_param_count(void) { return ffbp::mlp_param_count(); }
+
+int ffbp_mlp_max_decimation(void) { return ffbp::mlp_max_decimation(); }
+
+size_t ffbp_mlp_work_bytes(int nq) { return nq > 0 ? ffbp::mlp_work_bytes(nq) : 0; }
+
+int ffbp_mlp_taps(const float *d_params, const float *d_x, int nq, float *d_out, void *d_work, void *stream)
+{
+    if (!d_params || !d_x || !d_out || !d_work || nq < 1) return fail(FFBP_E_ARG, "ffbp_mlp_taps: bad arguments");
+    cudaError_t e = ffbp::mlp_taps(d_params, d_x, nq, d_out, static_cast<float *>(d_work), static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "ffbp_mlp_taps");
+    return FFBP_OK;
+}
+
+static bool mlp_pairs_ok(const float *d_x, int nq, const float *d_prior, float scale, const int *d_inst, int ninst,
+                         const double *d_f, const void *d_y, int S)
+{
+    return d_x && d_prior && d_inst && d_f && d_y && nq >= 1 && ninst >= 1 && ninst <= 65535 && S >= 1 &&
+           (long long)ninst * S <= (1LL << 31) && std::isfinite(scale);
+}
+
+int ffbp_mlp_grad(const float *d_params, const float *d_x, int nq, const float *d_prior, float scale,
+                  const int *d_inst, int ninst, const double *d_f, const void *d_y, int S, float *d_grad,
+                  float *d_loss, void *d_work, void *stream)
+{
+    if (!d_params || !d_loss || !d_work || !mlp_pairs_ok(d_x, nq, d_prior, scale, d_inst, ninst, d_f, d_y, S))
+        return fail(FFBP_E_ARG, "ffbp_mlp_grad: bad arguments");
+    cudaError_t e = ffbp::mlp_grad(d_params, d_x, nq, d_prior, scale, d_inst, ninst, d_f, static_cast<const float2 *>(d_y),
+                                   S, d_grad, d_loss, static_cast<float *>(d_work), static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "ffbp_mlp_grad");
+    return FFBP_OK;
+}
+
+int ffbp_mlp_train_step(float *d_params, float *d_adam, const float *d_x, int nq, const float *d_prior, float scale,
+                        const int *d_inst, int ninst, const double *d_f, const void *d_y, int S, float lr, int t,
+                        float *d_loss, void *d_work, void *stream)
+{
+    if (!d_params || !d_adam || !d_loss || !d_work || t < 1 || !std::isfinite(lr) ||
+        !mlp_pairs_ok(d_x, nq, d_prior, scale, d_inst, ninst, d_f, d_y, S))
+        return fail(FFBP_E_ARG, "ffbp_mlp_train_step: bad arguments");
+    cudaError_t e = ffbp::mlp_train_step(d_params, d_adam, d_x, nq, d_prior, scale, d_inst, ninst, d_f,
+                                         static_cast<const float2 *>(d_y), S, lr, t, d_loss, static_cast<float *>(d_work),
+                                         static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "ffbp_mlp_train_step");
     return FFBP_OK;
 }
 

@@ -86,4 +86,17 @@ cudaError_t launch_exact_tiles(const float2 *prof, int n, int nfft, int W, const
                                double inv_dr, double kcyc, int cubic, int along1, float2 *win, float2 *out,
                                cudaStream_t st, const char **why);
 
+// The learned-tap network (mlp.cu): parameter count, work-buffer bytes for nq queries, the outputs of nq feature
+// rows, and the gradient / Adam step of the decimation loss over ninst instances of S point-target pairs each.
+int mlp_param_count();
+int mlp_max_decimation();
+size_t mlp_work_bytes(int nq);
+cudaError_t mlp_taps(const float *params, const float *x, int nq, float *taps, float *work, cudaStream_t s);
+cudaError_t mlp_grad(const float *params, const float *x, int nq, const float *prior, float scale, const int *inst,
+                     int ninst, const double *f, const float2 *y, int S, float *grad, float *loss, float *work,
+                     cudaStream_t s);
+cudaError_t mlp_train_step(float *params, float *adam, const float *x, int nq, const float *prior, float scale,
+                           const int *inst, int ninst, const double *f, const float2 *y, int S, float lr, int t,
+                           float *loss, float *work, cudaStream_t s);
+
 }  // namespace ffbp

@@ -131,7 +131,7 @@ def positions(ant, idx):
 # ------------------------------------------------------------------------------------------------ plan
 
 def make_plan(col, nx, ny, spx, spy, T=32, nlev=3, pmax=0.4, atten=70.0, splits=None, e1=(1.0, 0.0, 0.0),
-              e2=(0.0, 1.0, 0.0), pulse=None):
+              e2=(0.0, 1.0, 0.0), pulse=None, taps=None):
     """The plan of an nx x ny image of spacings spx, spy along the orthonormal e1, e2 about the origin, for the
     collection col (fmin, df, K, ant). Returns a dict with the padded grid (Nx, Ny, ox, oy), the per-level records
     (splits sx, sy and children C; decimations Dk, Dp; sizes K, P in and Ko, Po out; filters fir_k, fir_p; the band
@@ -139,7 +139,10 @@ def make_plan(col, nx, ny, spx, spy, T=32, nlev=3, pmax=0.4, atten=70.0, splits=
     points ref [B, 3], the child offsets d [C, 3], the child centres cen [B, C, 3], the output pulse positions pidx)
     and the final-stage record (fastsar/ffbp2.py:192-250), which adds the tiles' first pixels and the antenna path
     of the final subapertures to the reference's.
-    pulse: per-level (Dp, pass_p) that replace the ones this aperture would get."""
+    pulse: per-level (Dp, pass_p) that replace the ones this aperture would get.
+    taps: None (the reference's Kaiser-sinc decimators) or learned decimation taps (fastsar_b200.learned.LearnedTaps):
+    an axis whose decimation and pass fraction the network covers takes its 8-output-sample filter (margin m = 4),
+    the others keep the Kaiser-sinc one; the level records which in kind_k / kind_p."""
     e1, e2 = np.asarray(e1, np.float64), np.asarray(e2, np.float64)
     if splits is None:
         sxs, sys_ = choose_splits(nx, T, nlev), choose_splits(ny, T, nlev)
@@ -174,21 +177,24 @@ def make_plan(col, nx, ny, spx, spy, T=32, nlev=3, pmax=0.4, atten=70.0, splits=
         if pulse is not None:
             Dp, pass_p = int(pulse[lev][0]), float(pulse[lev][1])
         ak, ap = min(pass_k, 0.95), min(pass_p, 0.95)
-        Ko, mk = decimator_shape(K, Dk, ak, atten)
-        Po, mp = decimator_shape(P, Dp, ap, atten)
+        lk = taps.decimator(K, Dk, ak, lev, 0) if taps is not None and Dk > 1 else None
+        lp = taps.decimator(P, Dp, ap, lev, 1) if taps is not None and Dp > 1 else None
+        Ko, mk = (lk[0]['n_out'], lk[1]) if lk else decimator_shape(K, Dk, ak, atten)
+        Po, mp = (lp[0]['n_out'], lp[1]) if lp else decimator_shape(P, Dp, ap, atten)
         # an axis shorter than its decimation kernel is not decimated (late levels of small collections)
         if Dk > 1 and K < 2 * mk * Dk + Dk:
-            Dk, pass_k, ak = 1, rk / (C / (2.0 * df) / 2.0), 0.95
+            Dk, pass_k, ak, lk = 1, rk / (C / (2.0 * df) / 2.0), 0.95, None
             Ko, mk = K, 0
         if Dp > 1 and P < 2 * mp * Dp + Dp:
-            Dp, pass_p, ap = 1, 2.0 * kmax * dop, 0.95
+            Dp, pass_p, ap, lp = 1, 2.0 * kmax * dop, 0.95, None
             Po, mp = P, 0
         pidx = Dp * (np.arange(Po) - mp) + (Dp - 1) / 2.0
         plan['levels'].append(dict(
             sx=sx, sy=sy, C=sx * sy, Dk=Dk, Dp=Dp, K=K, P=P, Ko=Ko, Po=Po, mk=mk, mp=mp,
-            fir_k=decimator_fir(K, Dk, ak, atten)[0] if Dk > 1 else None,
-            fir_p=decimator_fir(P, Dp, ap, atten)[0] if Dp > 1 else None,
-            dec_k=(K, Dk, ak, atten), dec_p=(P, Dp, ap, atten),
+            fir_k=(lk[0] if lk else decimator_fir(K, Dk, ak, atten)[0]) if Dk > 1 else None,
+            fir_p=(lp[0] if lp else decimator_fir(P, Dp, ap, atten)[0]) if Dp > 1 else None,
+            kind_k='learned' if lk else 'kaiser', kind_p='learned' if lp else 'kaiser',
+            dec_k=(K, Dk, ak, taps.ident if lk else atten), dec_p=(P, Dp, ap, taps.ident if lp else atten),
             f0=f0, df=df, ant=ant, ref=ref, d=cen[0] - ref[0], cen=cen, pidx=pidx,
             pass_k=float(pass_k), pass_p=float(pass_p)))
         ant = positions(ant, pidx)

@@ -194,6 +194,33 @@ int ffbp_exact_backproject(const void *d_prof, int n, int nfft, int W, const lon
                            int ty, int nx, int ny, double spx, double spy, const double *e1, const double *e2,
                            double inv_dr, double kcyc, int cubic, int along1, void *d_win, void *d_out, void *stream);
 
+/* The learned-tap network (no counterpart in the reference): an MLP 5 -> 64 -> 64 -> 64 -> 16 (GELU, bfloat16
+ * weights and activations, float32 sums) that stands in for the Kaiser-sinc decimation taps of the merge stages
+ * (fastsar/ffbp2.py:101-137). A query is one phase q of one axis of a stage's decimation by D: features (phase
+ * phi_q, pass fraction of the axis, 1 / D, stage, axis, each scaled by the caller); outputs 0..7 correct the 8 range-axis taps of that
+ * phase and 8..15 the 8 angle-axis taps (a query uses the ones of its axis): tap n, at offset phi_q - 4 + n output
+ * samples, = prior + scale * output, with phi_q = (q + 1/2) / D for even D and q / D for odd D.
+ * d_params: ffbp_mlp_param_count floats, per layer W [out, in] then b [out]; d_x [nq, 5] float32; d_work:
+ * ffbp_mlp_work_bytes(nq) bytes. ffbp_mlp_taps writes the outputs d_out [nq, 16].
+ * Training pairs: instance i of d_inst [ninst, 3] (first query, D in 1..ffbp_mlp_max_decimation(), axis 0 or 1)
+ * owns queries first .. first + D - 1 with prior taps d_prior [nq, 8]; its S samples are point targets at
+ * frequencies d_f [ninst, S] (float64, cycles per output sample), whose parent samples are e^{2 pi i f t}, and their
+ * exact child values d_y [ninst, S] (complex64); the decimated value is v = (1 / D) sum over the instance's taps of
+ * tap e^{2 pi i f t}. ffbp_mlp_grad writes the gradient of mean |v - y|^2 over all pairs (d_grad, param count
+ * floats, or NULL) and the sum |v - y|^2 (*d_loss; NaN when an instance is outside the query table);
+ * ffbp_mlp_train_step takes one Adam step (lr, step t >= 1, b1 0.9, b2 0.999, eps 1e-8) with d_adam (2 x param
+ * count floats: first then second moments, zeroed at t = 1). */
+int ffbp_mlp_param_count(void);
+int ffbp_mlp_max_decimation(void);
+size_t ffbp_mlp_work_bytes(int nq);
+int ffbp_mlp_taps(const float *d_params, const float *d_x, int nq, float *d_out, void *d_work, void *stream);
+int ffbp_mlp_grad(const float *d_params, const float *d_x, int nq, const float *d_prior, float scale,
+                  const int *d_inst, int ninst, const double *d_f, const void *d_y, int S, float *d_grad,
+                  float *d_loss, void *d_work, void *stream);
+int ffbp_mlp_train_step(float *d_params, float *d_adam, const float *d_x, int nq, const float *d_prior, float scale,
+                        const int *d_inst, int ninst, const double *d_f, const void *d_y, int S, float lr, int t,
+                        float *d_loss, void *d_work, void *stream);
+
 /* Child phases in float64 for one level (fastsar/ffbp2.py:329-339 / fastsar/ffbp_cuda.py:598-632): for parent n,
  * child c and pulse p, ddr = |cen[n,c] - ant[p]| - |ref[n] - ant[p]| (or - range[p] when d_range is given),
  * c0 = ddr k0c - rint(ddr k0c), sl = ddr k1, stored as float pairs into d_phase [Np, C, P]. cancel_free selects

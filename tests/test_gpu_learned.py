@@ -1,0 +1,161 @@
+"""The learned decimation taps on a B200: the network's kernels (ffbp_mlp_*) against the CPU oracle
+(oracle/mlp_oracle.py) — outputs, loss, gradients, the Adam step —, training on the GPU lowering the loss, and what
+the packaged network (fastsar_b200/data/learned_taps.npz) gains over the Kaiser-sinc decimators it stands in for:
+per filter on held-out instances, and per image against the float64 exact backprojection.
+Tolerances: outputs within 1e-2, the loss within 1e-3 and gradients within 2e-2 (relative L2 per layer) of the
+oracle, which rounds the same weights to bfloat16 but sums in float64 (a float32 sum that lands on the other side
+of a bfloat16 rounding boundary moves an activation by one bfloat16 step, about 4e-3 relative, and the move passes
+on through the later layers)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import mlp_oracle as M
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip('torch')
+if not torch.cuda.is_available():
+    pytest.skip('no CUDA device', allow_module_level=True)
+
+
+def _flat(params):
+    return np.concatenate([np.concatenate([W.ravel(), b.ravel()]) for W, b in params]).astype(np.float32)
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, np.float64).ravel(), np.asarray(b, np.float64).ravel()
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _random_net(seed):
+    """Oracle-layout parameters with a non-zero last layer (so that the outputs move the taps)."""
+    ps = M.init_params(seed)
+    rng = np.random.default_rng(seed + 100)
+    return [(W, (0.1 * rng.standard_normal(b.shape)).astype(np.float32)) for W, b in ps]
+
+
+def test_outputs_match_oracle():
+    from fastsar_b200 import learned
+    ps = _random_net(1)
+    x = np.concatenate([learned.features(D, w, st, ax) for D, w, st, ax in learned.instances(3, 40)])
+    got = learned.LearnedTaps(_flat(ps)).outputs(x)
+    want, _ = M.forward(ps, x)
+    assert got.shape == want.shape
+    assert _rel(got, want) < 1e-2
+
+
+@pytest.mark.parametrize('S', [200, 512])
+def test_gradient_matches_oracle(S):
+    from fastsar_b200 import learned
+    ps = _random_net(2)
+    pairs = learned.make_pairs(learned.instances(4, 6), S, seed=5)
+    loss, grad = learned.LearnedTaps(_flat(ps)).grad(pairs)
+    want_loss, want = M.loss_and_grad(ps, pairs[0], pairs[1], learned.SCALE, pairs[2], pairs[3], pairs[4])
+    assert abs(loss - want_loss) <= 1e-3 * want_loss
+    for li, (gp, (dW, db)) in enumerate(zip(learned.unpack(grad), want)):
+        assert _rel(gp[0], dW) < 2e-2, (li, 'W', _rel(gp[0], dW))
+        assert _rel(gp[1], db) < 2e-2, (li, 'b', _rel(gp[1], db))
+
+
+def test_adam_step_matches_oracle():
+    """One ffbp_mlp_train_step (t = 1, second moments preset to 1e-6 so that the step is smooth in the gradient)
+    against the oracle's Adam step on the oracle's gradient."""
+    from fastsar_b200 import _lib, learned
+    L = _lib.load()
+    ps = _random_net(3)
+    pairs = learned.make_pairs(learned.instances(6, 5), 256, seed=7)
+    x, pr, inst, f, y = (torch.as_tensor(np.ascontiguousarray(a)).cuda() for a in pairs)
+    p = torch.from_numpy(_flat(ps)).cuda()
+    adam = torch.zeros(2 * learned.N_PARAMS, dtype=torch.float32, device='cuda')
+    adam[learned.N_PARAMS:] = 1e-6
+    work = torch.empty(int(L.ffbp_mlp_work_bytes(x.shape[0])) // 4 + 16, dtype=torch.float32, device='cuda')
+    loss = torch.zeros(1, dtype=torch.float32, device='cuda')
+    lr = 1e-3
+    _lib.check(L.ffbp_mlp_train_step(p.data_ptr(), adam.data_ptr(), x.data_ptr(), x.shape[0], pr.data_ptr(),
+                                     ctypes.c_float(learned.SCALE), inst.data_ptr(), inst.shape[0], f.data_ptr(),
+                                     y.data_ptr(), f.shape[1], ctypes.c_float(lr), 1, loss.data_ptr(), work.data_ptr(),
+                                     torch.cuda.current_stream().cuda_stream), 'ffbp_mlp_train_step')
+    _, g = M.loss_and_grad(ps, *pairs[:2], learned.SCALE, *pairs[2:])
+    state = [(np.zeros_like(W, np.float64), np.full(W.shape, 1e-6), np.zeros_like(b, np.float64), np.full(b.shape, 1e-6))
+             for W, b in ps]
+    want = M.adam_step(ps, g, state, lr=lr, t=1)
+    got = learned.unpack(p.cpu().numpy())
+    for (W0, b0), (Wg, bg), (Ww, bw) in zip(ps, got, want):
+        assert _rel(Wg - W0, Ww - W0) < 2e-2
+        assert _rel(bg - b0, bw - b0) < 2e-2
+
+
+def test_bad_instance_gives_nan_loss():
+    from fastsar_b200 import learned
+    pairs = list(learned.make_pairs(learned.instances(8, 3), 64, seed=9))
+    inst = pairs[2].copy()
+    inst[1, 0] = pairs[0].shape[0]                  # past the query table
+    pairs[2] = inst
+    loss, _ = learned.LearnedTaps().grad(tuple(pairs))
+    assert np.isnan(loss)
+    loss, _ = learned.LearnedTaps().grad(learned.make_pairs(learned.instances(8, 3), 64, seed=9))
+    assert np.isfinite(loss)
+
+
+def test_training_lowers_the_loss():
+    """A short run from the prior (the untrained network's last layer is zero) on 128 instances lowers the loss."""
+    from fastsar_b200 import learned
+    pairs = learned.make_pairs(learned.instances(11, 128), 128, seed=12)
+    m = learned.LearnedTaps(seed=3)
+    hist = m.train(pairs, steps=400, lr=1e-3, lr_end=1e-4, every=100)
+    first, last = hist[0][1], hist[-1][1]
+    print('loss %.2f dB -> %.2f dB' % (10 * np.log10(first), 10 * np.log10(last)))
+    assert np.isfinite(last) and last < first / 2
+
+
+def test_packaged_taps_beat_the_kaiser_filters():
+    """On held-out filter instances the packaged network's 8-output-sample taps have a smaller band error than the
+    prior alone and than the reference's 80 dB Kaiser-sinc decimators, with no more taps."""
+    from fastsar_b200 import learned
+    m = learned.LearnedTaps.load()
+    rows = learned.evaluate(m, learned.instances(10 ** 6, 48))
+    mean = {k: float(np.mean([r[k] for r in rows])) for k in ('learned', 'prior', 'kaiser', 'taps', 'kaiser_taps')}
+    print(mean)
+    assert mean['learned'] < mean['prior'] - 5.0
+    assert mean['learned'] < mean['kaiser'] - 5.0
+    assert mean['taps'] <= mean['kaiser_taps']
+
+
+def test_learned_taps_image_against_float64(golden, oracle_lib):
+    """The 512-pulse spotlight formed with the packaged learned taps (plain float32 former): its error against the
+    float64 exact backprojection (64x) is below the Kaiser-sinc former's at 70 dB (the reference's filters) and at
+    80 dB."""
+    from fastsar_b200 import ImageFormer, sim
+    g = golden('image_spot512')
+    w = sim.workload('spotlight_512')
+    col = w['col']
+    errs = {}
+    for name, kw in (('kaiser70', {}), ('kaiser80', dict(atten=80.0)), ('learned', dict(taps='learned'))):
+        f = ImageFormer(col.ant, col.fmin, col.df, col.K, 512, 512, 0.25, 0.25, w['e1'], w['e2'], **kw)
+        img = f(g['S'])
+        errs[name] = oracle_lib.rel_db(img.ravel()[g['bp64_idx']], g['bp64'])
+        if name == 'learned':
+            kinds = [(lv['kind_k'], lv['kind_p']) for lv in f._plan['levels']]
+    print(errs, kinds)
+    assert any('learned' in k for k in kinds)
+    assert errs['learned'] < errs['kaiser70'] - 1.0
+    assert errs['learned'] < errs['kaiser80']
+
+
+def test_learned_taps_mixed_precision_image_against_float64(golden, oracle_lib):
+    """The chosen form, precision='float16' with the learned taps, on the 512-pulse spotlight: below -60 dB against
+    the float64 exact backprojection and no worse than precision='float16' with the 80 dB Kaiser-sinc filters."""
+    from fastsar_b200 import ImageFormer, sim
+    g = golden('image_spot512')
+    w = sim.workload('spotlight_512')
+    col = w['col']
+    errs = {}
+    for name, kw in (('kaiser80', {}), ('learned', dict(taps='learned'))):
+        f = ImageFormer(col.ant, col.fmin, col.df, col.K, 512, 512, 0.25, 0.25, w['e1'], w['e2'], precision='float16',
+                        **kw)
+        errs[name] = oracle_lib.rel_db(f(g['S']).ravel()[g['bp64_idx']], g['bp64'])
+    print(errs)
+    assert errs['learned'] < -60.0
+    assert errs['learned'] < errs['kaiser80'] + 0.5
