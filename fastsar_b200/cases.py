@@ -1,0 +1,131 @@
+"""Single-stage cases of a workload's plan, for timing one kernel at a time and for small profiler captures:
+
+    python -m fastsar_b200.cases level L1 [--parents 8] [--pulses 2048] [--form tc|fp32] [--taps learned|80|70]
+    python -m fastsar_b200.cases final [--tiles 20000] [--mode f16|bf16x3|fp32] [--taps learned|80|70]
+
+`level`: one merge stage of the plan (its children, decimations and filters) on `--parents` parents of random
+samples and random child phases, through ffbp_level_tc (tensor cores: its two launches, level_tc_gemm and
+level_fir) or ffbp_level (float32: level_kernel); `--pulses` shortens the pulse axis (the pulse filter is then
+designed for the shorter axis by the same rule). `final`: the final stage through ffbp_final on `--tiles` tiles of
+the plan's final shape with random samples and geometry. Each prints the event-timed duration of every repetition.
+The defaults are the 16,384 x 8,192 -> 12,288 x 8,832 spotlight (workload spotlight_12k) with the learned taps.
+"""
+import argparse
+
+import numpy as np
+
+from . import _lib
+from . import plan as _plan
+from . import sim
+
+
+def workload_plan(name='spotlight_12k', taps='learned'):
+    """The plan of a named workload with learned taps ('learned', Kaiser-sinc fallback at 80 dB) or Kaiser-sinc
+    filters at the given attenuation."""
+    w = sim.workload(name)
+    model = None
+    atten = 80.0
+    if taps == 'learned':
+        from .learned import LearnedTaps
+        model = LearnedTaps.load()
+    else:
+        atten = float(taps)
+    return w, _plan.make_plan(w['col'], w['nx'], w['ny'], w['spx'], w['spy'], T=32, nlev=3, atten=atten, e1=w['e1'],
+                              e2=w['e2'], taps=model)
+
+
+def level_case(level, parents, pulses=0, form='tc', taps='learned', reps=3, seed=1):
+    import torch
+    L = _lib.load()
+    w, pl = workload_plan(taps=taps)
+    lv = pl['levels'][level]
+    P, K, C, Ko, Po, Dk, Dp = lv['P'], lv['K'], lv['C'], lv['Ko'], lv['Po'], lv['Dk'], lv['Dp']
+    fk, fp = lv['fir_k'], lv['fir_p']
+    if pulses:
+        P = int(pulses)
+        if lv['kind_p'] == 'learned':
+            from .learned import LearnedTaps
+            fp = LearnedTaps.load().decimator(P, Dp, min(lv['pass_p'], 0.95), level, 1)[0]
+        else:
+            fp = _plan.decimator_fir(P, Dp, min(lv['pass_p'], 0.95), lv['dec_p'][3])[0]
+        Po = fp['n_out']
+    g = torch.Generator(device='cuda')
+    g.manual_seed(seed)
+    x = torch.view_as_complex(torch.randn((parents, P, K, 2), device='cuda', generator=g)).contiguous()
+    ph = torch.stack([torch.rand((parents, C, P), device='cuda', generator=g) - 0.5,
+                      (torch.rand((parents, C, P), device='cuda', generator=g) - 0.5) * 0.004], -1).contiguous()
+    tk = torch.tensor(np.asarray(fk['kern'], np.float32), device='cuda')
+    tp = torch.tensor(np.asarray(fp['kern'], np.float32), device='cuda')
+    out = torch.empty((parents * C, Po, Ko), dtype=torch.complex64, device='cuda')
+    st = torch.zeros(3, dtype=torch.int32, device='cuda')
+    s = torch.cuda.current_stream().cuda_stream
+    nb = int(L.ffbp_level_tc_scratch_bytes(parents, C, P, Ko))
+    scr = torch.empty(nb // 4 + 4, dtype=torch.int32, device='cuda') if form == 'tc' else None
+
+    def run():
+        if form == 'tc':
+            _lib.check(L.ffbp_level_tc(x.data_ptr(), parents, P, K, ph.data_ptr(), C, tk.data_ptr(), fk['L'], fk['pl'],
+                                       Dk, Ko, (K - 1) / 2.0, tp.data_ptr(), fp['L'], fp['pl'], Dp, Po, None, None,
+                                       out.data_ptr(), None, scr.data_ptr(), nb, st.data_ptr(), s), 'ffbp_level_tc')
+        else:
+            _lib.check(L.ffbp_level(x.data_ptr(), parents, P, K, ph.data_ptr(), C, tk.data_ptr(), fk['L'], fk['pl'], Dk,
+                                    Ko, (K - 1) / 2.0, tp.data_ptr(), fp['L'], fp['pl'], Dp, Po, None, None,
+                                    out.data_ptr(), None, s), 'ffbp_level')
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        run()
+        e1.record()
+        torch.cuda.synchronize()
+        print(f'level {level} ({form}, taps {taps}) parents={parents} P={P} K={K} C={C} Ko={Ko} Po={Po} '
+              f'Lk={fk["L"]} Lp={fp["L"]}: {e0.elapsed_time(e1):.3f} ms', flush=True)
+
+
+def final_case(tiles, mode='f16', taps='learned', reps=2, seed=2):
+    import torch
+    L = _lib.load()
+    w, pl = workload_plan(taps=taps)
+    f = pl['final']
+    Pf, Qf, T = f['P'], f['K'], pl['T']
+    m = {'fp32': _lib.FFBP_FINAL_FP32, 'f16': _lib.FFBP_FINAL_TC_F16, 'bf16x3': _lib.FFBP_FINAL_TC_BF16X3}[mode]
+    g = torch.Generator(device='cuda')
+    g.manual_seed(seed)
+    d = torch.view_as_complex(torch.randn((tiles, Pf, Qf, 2), device='cuda', generator=g)).contiguous()
+    ux = (torch.rand((tiles, Pf), device='cuda', generator=g, dtype=torch.float64) - 0.5) * 0.1
+    uy = (torch.rand((tiles, Pf), device='cuda', generator=g, dtype=torch.float64) - 0.5) * 1.6
+    ucx, ucy = ux.mean(1).contiguous(), uy.mean(1).contiguous()
+    rc = torch.full((tiles,), 5e5, device='cuda', dtype=torch.float64)
+    out = torch.empty((tiles, T, T), dtype=torch.complex64, device='cuda')
+    s = torch.cuda.current_stream().cuda_stream
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _lib.check(L.ffbp_final(d.data_ptr(), tiles, Pf, Qf, T, ux.data_ptr(), uy.data_ptr(), 0.2, 0.2, 64.0, 0.0085,
+                                ucx.data_ptr(), ucy.data_ptr(), rc.data_ptr(), 64.5, None, m, out.data_ptr(), s),
+                   'ffbp_final')
+        e1.record()
+        torch.cuda.synchronize()
+        print(f'final ({mode}, taps {taps}) tiles={tiles} Pf={Pf} Qf={Qf} T={T}: {e0.elapsed_time(e1):.3f} ms',
+              flush=True)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description='time one stage of a workload plan')
+    ap.add_argument('stage', choices=('level', 'final'))
+    ap.add_argument('level', nargs='?', default='L1', choices=('L0', 'L1', 'L2'))
+    ap.add_argument('--parents', type=int, default=8)
+    ap.add_argument('--pulses', type=int, default=0)
+    ap.add_argument('--form', choices=('tc', 'fp32'), default='tc')
+    ap.add_argument('--tiles', type=int, default=20000)
+    ap.add_argument('--mode', choices=('f16', 'bf16x3', 'fp32'), default='f16')
+    ap.add_argument('--taps', default='learned', help="'learned' or a Kaiser-sinc attenuation in dB (70, 80)")
+    ap.add_argument('--reps', type=int, default=3)
+    a = ap.parse_args(argv)
+    if a.stage == 'level':
+        level_case(int(a.level[1]), a.parents, a.pulses, a.form, a.taps, a.reps)
+    else:
+        final_case(a.tiles, a.mode, a.taps, a.reps)
+
+
+if __name__ == '__main__':
+    main()
