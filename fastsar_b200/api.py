@@ -176,6 +176,7 @@ class DevicePlan:
         _lib.check(L.ffbp_plan_workspace_bytes(h, ctypes.byref(n)), 'ffbp_plan_workspace_bytes')
         self.ws_bytes = int(n.value)
         self._ws = None
+        self._stage = None
 
     def workspace(self):
         import torch
@@ -186,6 +187,28 @@ class DevicePlan:
 
     def release_workspace(self):
         self._ws = None
+        self._stage = None
+
+    def form_host(self, S_ptrs, img_ptrs, stream=None):
+        """ffbp_form_host on host buffers (addresses of [P, K] and [nx, ny] complex64 arrays, page-locked for the
+        overlap): the images formed in turn, each upload and download overlapping the neighbours' formation.
+        Returns each image's first non-finite pulse (-1: none)."""
+        import torch
+        L = _lib.load()
+        n = len(S_ptrs)
+        if self._stage is None:
+            nb = ctypes.c_size_t()
+            _lib.check(L.ffbp_plan_host_bytes(self.handle, ctypes.byref(nb)), 'ffbp_plan_host_bytes')
+            self._stage_bytes = int(nb.value)
+            self._stage = torch.empty(self._stage_bytes + 256, dtype=torch.uint8, device=self.device)
+        stage = self._stage.data_ptr() + (-self._stage.data_ptr()) % 256
+        stream = torch.cuda.current_stream(self.device) if stream is None else stream
+        bad = (ctypes.c_int * n)()
+        _lib.check(L.ffbp_form_host(self.handle, (ctypes.c_void_p * n)(*S_ptrs), (ctypes.c_void_p * n)(*img_ptrs), n,
+                                    ctypes.c_void_p(stage), ctypes.c_size_t(self._stage_bytes),
+                                    ctypes.c_void_p(self.workspace()), ctypes.c_size_t(self.ws_bytes),
+                                    ctypes.c_void_p(stream.cuda_stream), bad), 'ffbp_form_host')
+        return list(bad)
 
     def form(self, S_dev, img_dev, stream=None, check=True):
         """S_dev [P, K] complex64 torch tensor on the device -> img_dev [nx, ny] complex64 (written). check: read back
@@ -396,6 +419,46 @@ class ImageFormer:
         if out is None:
             out = torch.empty((self.nx, self.ny), dtype=torch.complex64, device=self._dev.device)
         return self._dev.form(S_dev, out, check=check)
+
+    def form_many(self, histories, images=None):
+        """Form a sequence of images from host memory: histories [P, K] complex64 (torch CPU tensors or numpy
+        arrays; page-locked torch tensors, `pin_memory=True`, let the copies overlap the formation) -> images
+        [nx, ny] complex64 in host memory (the given `images`, or new page-locked tensors), returned as numpy
+        arrays. Each history's upload and each image's download run on their own streams while the neighbouring
+        images form (ffbp_form_host). Raises ValueError naming the first image with non-finite samples."""
+        import torch
+        hs = []
+        for S in histories:
+            if isinstance(S, torch.Tensor):
+                if S.is_cuda:
+                    raise ValueError('form_many takes host histories; use form_device for device ones')
+                if tuple(S.shape) != (self.P, self.K) or S.dtype != torch.complex64 or not S.is_contiguous():
+                    raise ValueError(f'host phase history must be a contiguous complex64 {(self.P, self.K)} tensor, '
+                                     f'got {S.dtype} {tuple(S.shape)}')
+                hs.append(S)
+            else:
+                S = _check_history(np.asarray(S), self.P)
+                if S.shape != (self.P, self.K):
+                    raise ValueError(f'phase history must be {(self.P, self.K)}, got {S.shape}')
+                hs.append(torch.from_numpy(np.ascontiguousarray(S, np.complex64)))
+        if images is None:
+            images = [torch.empty((self.nx, self.ny), dtype=torch.complex64, pin_memory=True) for _ in hs]
+        outs = []
+        for im in images:
+            t = im if isinstance(im, torch.Tensor) else torch.from_numpy(im)
+            if tuple(t.shape) != (self.nx, self.ny) or t.dtype != torch.complex64 or not t.is_contiguous() or t.is_cuda:
+                raise ValueError(f'images must be contiguous complex64 {(self.nx, self.ny)} host arrays')
+            outs.append(t)
+        if len(outs) != len(hs):
+            raise ValueError(f'{len(hs)} histories but {len(outs)} images')
+        if not hs:
+            return []
+        bad = self._dev.form_host([h.data_ptr() for h in hs], [o.data_ptr() for o in outs])
+        for i, b in enumerate(bad):
+            if b >= 0:
+                raise ValueError(f'phase history {i} has non-finite samples (NaN or inf), the first in pulse {b}; '
+                                 'zero them (S[~np.isfinite(S)] = 0) or drop the pulses')
+        return [o.numpy() for o in outs]
 
     def __call__(self, S):
         """S [P, K] complex phase history (numpy, or a torch tensor) -> complex64 image [nx, ny] (numpy)."""

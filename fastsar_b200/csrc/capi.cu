@@ -61,6 +61,13 @@ struct ffbp_plan {
     int2 *first = nullptr;
     size_t bufA = 0, bufB = 0;
     std::vector<void *> owned;
+    // the host-memory pipeline of ffbp_form_host, made at its first call: an upload and a download stream, per
+    // device buffer pair b the events "history b uploaded", "image b formed", "image b downloaded", and a pinned
+    // array of per-image status words
+    cudaStream_t up = nullptr, down = nullptr;
+    cudaEvent_t ev_up[2] = {}, ev_formed[2] = {}, ev_down[2] = {};
+    int *h_status = nullptr;
+    int n_status = 0;
 
     template <class T_>
     cudaError_t alloc(T_ **p, size_t count)
@@ -76,6 +83,14 @@ struct ffbp_plan {
     ~ffbp_plan()
     {
         for (void *q : owned) cudaFree(q);
+        for (int b = 0; b < 2; ++b) {
+            if (ev_up[b]) cudaEventDestroy(ev_up[b]);
+            if (ev_formed[b]) cudaEventDestroy(ev_formed[b]);
+            if (ev_down[b]) cudaEventDestroy(ev_down[b]);
+        }
+        if (up) cudaStreamDestroy(up);
+        if (down) cudaStreamDestroy(down);
+        if (h_status) cudaFreeHost(h_status);
     }
 };
 
@@ -348,6 +363,80 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
         if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "form");
         *h_bad = (v[0] == 0x7f7f7f7f) ? -1 : v[0];
         if (v[1]) return fail(FFBP_E_CUDA, "a tensor-core kernel stopped waiting on its pipeline (a bounded wait ran out)");
+    }
+    return FFBP_OK;
+}
+
+int ffbp_plan_host_bytes(const ffbp_plan *p, size_t *bytes)
+{
+    if (!p || !bytes) return fail(FFBP_E_ARG, "ffbp_plan_host_bytes: null argument");
+    *bytes = 2 * align256((size_t)p->lv[0].P * p->lv[0].K * sizeof(float2)) +
+             2 * align256((size_t)p->nx * p->ny * sizeof(float2));
+    return FFBP_OK;
+}
+
+int ffbp_form_host(ffbp_plan *p, const void *const *h_S, void *const *h_img, int n, void *d_stage,
+                   size_t stage_bytes, void *d_ws, size_t ws_bytes, void *stream, int *h_bad)
+{
+    if (!p || !h_S || !h_img || !d_stage || !d_ws || !h_bad || n < 1) return fail(FFBP_E_ARG, "ffbp_form_host: bad arguments");
+    for (int i = 0; i < n; ++i)
+        if (!h_S[i] || !h_img[i]) return fail(FFBP_E_ARG, "ffbp_form_host: null host buffer %d", i);
+    size_t need;
+    ffbp_plan_host_bytes(p, &need);
+    if (stage_bytes < need) return fail(FFBP_E_WORKSPACE, "staging buffer of %zu bytes, %zu needed", stage_bytes, need);
+    if (((uintptr_t)d_stage & 255) != 0) return fail(FFBP_E_ARG, "staging buffer must be 256-byte aligned");
+    cudaError_t e = cudaSuccess;
+    if (!p->up) {
+        if ((e = cudaStreamCreateWithFlags(&p->up, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaStreamCreateWithFlags(&p->down, cudaStreamNonBlocking)) != cudaSuccess)
+            return cuda_fail(e, "ffbp_form_host: streams");
+        for (int b = 0; b < 2; ++b)
+            if ((e = cudaEventCreateWithFlags(&p->ev_up[b], cudaEventDisableTiming)) != cudaSuccess ||
+                (e = cudaEventCreateWithFlags(&p->ev_formed[b], cudaEventDisableTiming)) != cudaSuccess ||
+                (e = cudaEventCreateWithFlags(&p->ev_down[b], cudaEventDisableTiming)) != cudaSuccess)
+                return cuda_fail(e, "ffbp_form_host: events");
+    }
+    if (p->n_status < 2 * n) {
+        if (p->h_status) cudaFreeHost(p->h_status);
+        p->h_status = nullptr;
+        p->n_status = 0;
+        if ((e = cudaHostAlloc(reinterpret_cast<void **>(&p->h_status), 2 * (size_t)n * sizeof(int), cudaHostAllocDefault)) != cudaSuccess)
+            return cuda_fail(e, "ffbp_form_host: status array");
+        p->n_status = 2 * n;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t sb = (size_t)p->lv[0].P * p->lv[0].K * sizeof(float2), ib = (size_t)p->nx * p->ny * sizeof(float2);
+    char *st = static_cast<char *>(d_stage);
+    void *dS[2] = {st, st + align256(sb)};
+    void *dI[2] = {st + 2 * align256(sb), st + 2 * align256(sb) + align256(ib)};
+    const int *bad = static_cast<const int *>(d_ws);           // form_impl's status words
+    int rc = FFBP_OK;
+    // image i: upload on `up` once image i - 2 no longer reads history buffer i % 2; form on `stream` once the upload
+    // is done and image i - 2 has left image buffer i % 2; download on `down` once formed. Up to two images are in
+    // flight, so the uploads and downloads of one image overlap the formation of its neighbours.
+    for (int i = 0; i < n && rc == FFBP_OK; ++i) {
+        const int b = i & 1;
+        if (i >= 2 && (e = cudaStreamWaitEvent(p->up, p->ev_formed[b], 0)) != cudaSuccess) { rc = cuda_fail(e, "ffbp_form_host"); break; }
+        if ((e = cudaMemcpyAsync(dS[b], h_S[i], sb, cudaMemcpyHostToDevice, p->up)) != cudaSuccess ||
+            (e = cudaEventRecord(p->ev_up[b], p->up)) != cudaSuccess ||
+            (e = cudaStreamWaitEvent(s, p->ev_up[b], 0)) != cudaSuccess ||
+            (i >= 2 && (e = cudaStreamWaitEvent(s, p->ev_down[b], 0)) != cudaSuccess)) { rc = cuda_fail(e, "ffbp_form_host"); break; }
+        if ((rc = form_impl(p, dS[b], dI[b], d_ws, ws_bytes, stream, nullptr, nullptr)) != FFBP_OK) break;
+        if ((e = cudaMemcpyAsync(p->h_status + 2 * i, bad, 2 * sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+            (e = cudaEventRecord(p->ev_formed[b], s)) != cudaSuccess ||
+            (e = cudaStreamWaitEvent(p->down, p->ev_formed[b], 0)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(h_img[i], dI[b], ib, cudaMemcpyDeviceToHost, p->down)) != cudaSuccess ||
+            (e = cudaEventRecord(p->ev_down[b], p->down)) != cudaSuccess) { rc = cuda_fail(e, "ffbp_form_host"); break; }
+    }
+    // wait for everything queued (the host buffers are in use until then), also after an error
+    const cudaError_t e1 = cudaStreamSynchronize(p->up), e2 = cudaStreamSynchronize(s), e3 = cudaStreamSynchronize(p->down);
+    if (rc != FFBP_OK) return rc;
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
+        return cuda_fail(e1 != cudaSuccess ? e1 : e2 != cudaSuccess ? e2 : e3, "ffbp_form_host");
+    for (int i = 0; i < n; ++i) {
+        h_bad[i] = p->h_status[2 * i] == 0x7f7f7f7f ? -1 : p->h_status[2 * i];
+        if (p->h_status[2 * i + 1])
+            return fail(FFBP_E_CUDA, "image %d: a tensor-core kernel stopped waiting on its pipeline (a bounded wait ran out)", i);
     }
     return FFBP_OK;
 }

@@ -118,6 +118,17 @@ int ffbp_plan_workspace_bytes(const ffbp_plan *plan, size_t *bytes);
 int ffbp_form(ffbp_plan *plan, const void *d_S, void *d_img, void *d_ws, size_t ws_bytes, void *stream,
               int *h_bad_pulse);
 
+/* Form n images from host memory, overlapping each history's upload and each image's download with the
+ * formation of its neighbours (the reference's pinned double-buffered upload, fastsar/ffbp_cuda.py:692-765,
+ * carried across images): h_S[i] [P0, K0] complex64 and h_img[i] [nx, ny] complex64 in page-locked host memory
+ * (pageable memory works, without the overlap). d_stage: two device histories and two device images,
+ * ffbp_plan_host_bytes bytes, 256-byte aligned; d_ws: the form workspace. The formation runs on `stream`, the copies
+ * on two streams of the plan. Returns when every image is in host memory; h_bad[i] is image i's first non-finite
+ * pulse (or -1). No counterpart in the reference's API.                                                         */
+int ffbp_plan_host_bytes(const ffbp_plan *plan, size_t *bytes);
+int ffbp_form_host(ffbp_plan *plan, const void *const *h_S, void *const *h_img, int n, void *d_stage,
+                   size_t stage_bytes, void *d_ws, size_t ws_bytes, void *stream, int *h_bad);
+
 /* ffbp_form without a caller-allocated workspace, for callers that cannot allocate device memory when they form an
  * image (a device pool they do not control, a real-time loop that must not enter the CUDA allocator). No counterpart
  * in the reference. The scratch is a static device array of this library, FFBP_STATIC_WS_BYTES (64 MiB), held by

@@ -443,3 +443,28 @@ def test_image_float16_large_amplitudes(golden, oracle_lib):
     print(f'float16 at 2^24 x amplitude: {r:.1e} from the unscaled image; {e64:.1f} dB vs float64 BP 64x')
     assert r < 1e-6
     assert e64 < -60.0
+
+
+def test_form_many_matches_device_forming(golden):
+    """ImageFormer.form_many (ffbp_form_host: uploads and downloads on their own streams, two images in flight) gives
+    bit for bit the images of form_device, for page-locked and pageable host histories, float32 and the tensor-core
+    form; a history with a non-finite sample raises naming that history and its pulse."""
+    from fastsar_b200 import ImageFormer, sim
+    g = golden('image_spot512')
+    w = sim.workload('spotlight_512')
+    col = w['col']
+    rng = np.random.default_rng(3)
+    Ss = [g['S'].astype(np.complex64)] + [(g['S'] * (rng.standard_normal() + 1j * rng.standard_normal())).astype(np.complex64)
+                                          for _ in range(4)]
+    for prec in ('float32', 'float16'):
+        f = ImageFormer(col.ant, col.fmin, col.df, col.K, 512, 512, 0.25, 0.25, w['e1'], w['e2'], precision=prec)
+        want = [f.form_device(torch.from_numpy(S).cuda()).cpu().numpy() for S in Ss]
+        pinned = [torch.from_numpy(S).pin_memory() for S in Ss]
+        got = f.form_many(pinned)
+        assert all(np.array_equal(a, b) for a, b in zip(got, want))
+        got = f.form_many(Ss[:3])                               # pageable numpy histories
+        assert all(np.array_equal(a, b) for a, b in zip(got, want[:3]))
+        bad = [S.copy() for S in Ss[:3]]
+        bad[2][37, 5] = np.nan
+        with pytest.raises(ValueError, match='phase history 2 .*pulse 37'):
+            f.form_many(bad)
