@@ -83,9 +83,9 @@ def load():
     L.ffbp_mlp_work_bytes.argtypes = [_c_int]
     L.ffbp_mlp_taps.argtypes = [_vp, _vp, _c_int, _vp, _vp, _vp]
     L.ffbp_mlp_max_decimation.argtypes = []
-    L.ffbp_mlp_grad.argtypes = [_vp, _vp, _c_int, _vp, ctypes.c_float, _vp, _c_int, _vp, _vp, _c_int, _vp, _vp, _vp,
-                                _vp]
-    L.ffbp_mlp_train_step.argtypes = [_vp, _vp, _vp, _c_int, _vp, ctypes.c_float, _vp, _c_int, _vp, _vp, _c_int,
+    L.ffbp_mlp_grad.argtypes = [_vp, _vp, _c_int, _vp, ctypes.c_float, _vp, _vp, _c_int, _vp, _vp, _c_int, _vp, _vp,
+                                _vp, _vp]
+    L.ffbp_mlp_train_step.argtypes = [_vp, _vp, _vp, _c_int, _vp, ctypes.c_float, _vp, _vp, _c_int, _vp, _vp, _c_int,
                                       ctypes.c_float, _c_int, _vp, _vp, _vp]
     L.ffbp_exact_pad.argtypes = [_vp, _c_int, _c_int, _vp, _vp, _c_int, _vp, _vp, _c_int, _vp]
     L.ffbp_exact_backproject.argtypes = [_vp, _c_int, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int,

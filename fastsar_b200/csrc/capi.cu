@@ -606,25 +606,25 @@ static bool mlp_pairs_ok(const float *d_x, int nq, const float *d_prior, float s
 }
 
 int ffbp_mlp_grad(const float *d_params, const float *d_x, int nq, const float *d_prior, float scale,
-                  const int *d_inst, int ninst, const double *d_f, const void *d_y, int S, float *d_grad,
-                  float *d_loss, void *d_work, void *stream)
+                  const int *d_inst, const float *d_weight, int ninst, const double *d_f, const void *d_y, int S,
+                  float *d_grad, float *d_loss, void *d_work, void *stream)
 {
     if (!d_params || !d_loss || !d_work || !mlp_pairs_ok(d_x, nq, d_prior, scale, d_inst, ninst, d_f, d_y, S))
         return fail(FFBP_E_ARG, "ffbp_mlp_grad: bad arguments");
-    cudaError_t e = ffbp::mlp_grad(d_params, d_x, nq, d_prior, scale, d_inst, ninst, d_f, static_cast<const float2 *>(d_y),
+    cudaError_t e = ffbp::mlp_grad(d_params, d_x, nq, d_prior, scale, d_inst, d_weight, ninst, d_f, static_cast<const float2 *>(d_y),
                                    S, d_grad, d_loss, static_cast<float *>(d_work), static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return cuda_fail(e, "ffbp_mlp_grad");
     return FFBP_OK;
 }
 
 int ffbp_mlp_train_step(float *d_params, float *d_adam, const float *d_x, int nq, const float *d_prior, float scale,
-                        const int *d_inst, int ninst, const double *d_f, const void *d_y, int S, float lr, int t,
-                        float *d_loss, void *d_work, void *stream)
+                        const int *d_inst, const float *d_weight, int ninst, const double *d_f, const void *d_y, int S,
+                        float lr, int t, float *d_loss, void *d_work, void *stream)
 {
     if (!d_params || !d_adam || !d_loss || !d_work || t < 1 || !std::isfinite(lr) ||
         !mlp_pairs_ok(d_x, nq, d_prior, scale, d_inst, ninst, d_f, d_y, S))
         return fail(FFBP_E_ARG, "ffbp_mlp_train_step: bad arguments");
-    cudaError_t e = ffbp::mlp_train_step(d_params, d_adam, d_x, nq, d_prior, scale, d_inst, ninst, d_f,
+    cudaError_t e = ffbp::mlp_train_step(d_params, d_adam, d_x, nq, d_prior, scale, d_inst, d_weight, ninst, d_f,
                                          static_cast<const float2 *>(d_y), S, lr, t, d_loss, static_cast<float *>(d_work),
                                          static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return cuda_fail(e, "ffbp_mlp_train_step");

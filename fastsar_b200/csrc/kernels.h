@@ -93,10 +93,10 @@ int mlp_max_decimation();
 size_t mlp_work_bytes(int nq);
 cudaError_t mlp_taps(const float *params, const float *x, int nq, float *taps, float *work, cudaStream_t s);
 cudaError_t mlp_grad(const float *params, const float *x, int nq, const float *prior, float scale, const int *inst,
-                     int ninst, const double *f, const float2 *y, int S, float *grad, float *loss, float *work,
-                     cudaStream_t s);
+                     const float *wt, int ninst, const double *f, const float2 *y, int S, float *grad, float *loss,
+                     float *work, cudaStream_t s);
 cudaError_t mlp_train_step(float *params, float *adam, const float *x, int nq, const float *prior, float scale,
-                           const int *inst, int ninst, const double *f, const float2 *y, int S, float lr, int t,
-                           float *loss, float *work, cudaStream_t s);
+                           const int *inst, const float *wt, int ninst, const double *f, const float2 *y, int S,
+                           float lr, int t, float *loss, float *work, cudaStream_t s);
 
 }  // namespace ffbp

@@ -659,10 +659,23 @@ size_t level_tc_scratch_bytes(int Np, int C, int P, int Ko)
     return (size_t)Np * C * P * Kop * sizeof(__half2);
 }
 
+// Dynamic shared memory of level_tc_gemm: both pulses' A' (hi, lo), sb stages of B' (hi, lo), the window planes, the
+// taps, the staged windows and the barriers.
+static size_t gemm_smem(int Lkp, int Dk, int nt, int sb)
+{
+    const size_t apart = (size_t)128 * Lkp * 2, bpart = (size_t)2 * nt * Lkp * 2;
+    const int W = Dk * (nt - 1) + Lkp, Wp = (W + 9) & ~1;
+    // barriers: afull[2], aempty[2], bfull[sb], bempty[sb], dfull[2], dempty[2]
+    return 4 * apart + (size_t)sb * 2 * bpart + (size_t)8 * (Wp / 2) * 4 + (size_t)Lkp * 4 + (size_t)XS * Wp * 8 +
+           (size_t)(8 + 2 * sb) * 8;
+}
+
+constexpr size_t GEMM_SMEM_MAX = 226 * 1024;                 // the opt-in limit less static shared memory and slack
+
 bool level_tc_supported(int C, int Lk, int Dk)
 {
     const int Lkp = ((Lk + 15) / 16) * 16;
-    return C >= 1 && C <= 64 && Lkp <= 64 && Dk >= 1;
+    return C >= 1 && C <= 64 && Lkp <= 96 && Dk >= 1 && gemm_smem(Lkp, Dk, 32, 2) <= GEMM_SMEM_MAX;
 }
 
 cudaError_t launch_amax(const float2 *x, size_t n, int *amax, cudaStream_t s)
@@ -676,7 +689,7 @@ cudaError_t launch_level_tc_gemm(const LevelLaunch &L, const int *amax_in, void 
 {
     *why = nullptr;
     const int Lk = L.Dk > 1 ? L.Lk : 1, plk = L.Dk > 1 ? L.plk : 0;
-    if (!level_tc_supported(L.C, Lk, L.Dk)) { *why = "the tensor-core level takes C <= 64 children and Lk <= 64 taps"; return cudaErrorNotSupported; }
+    if (!level_tc_supported(L.C, Lk, L.Dk)) { *why = "the tensor-core level takes C <= 64 children and Lk <= 96 taps"; return cudaErrorNotSupported; }
     GemmArgs a;
     a.x = L.x; a.ph = L.phase; a.tk = L.tk; a.wp = L.wp; a.wk = L.wk; a.bad = L.bad; a.amax_in = amax_in;
     a.y = static_cast<__half2 *>(scratch); a.err = err;
@@ -685,14 +698,8 @@ cudaError_t launch_level_tc_gemm(const LevelLaunch &L, const int *amax_in, void 
     int dev = 0, maxsmem = 227 * 1024;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    const size_t avail = (size_t)maxsmem - 1024;              // static shared memory and slack
-    const size_t apart = (size_t)128 * a.Lkp * 2;
-    auto need = [&](int nt, int sb) {
-        const size_t bpart = (size_t)2 * nt * a.Lkp * 2;
-        const int W = a.Dk * (nt - 1) + a.Lkp, Wp = (W + 9) & ~1;
-        return 4 * apart + (size_t)sb * 2 * bpart + (size_t)8 * (Wp / 2) * 4 + (size_t)a.Lkp * 4 + (size_t)XS * Wp * 8 +
-               (size_t)(6 + 2 * sb) * 8;
-    };
+    const size_t avail = std::min((size_t)maxsmem - 1024, GEMM_SMEM_MAX);
+    auto need = [&](int nt, int sb) { return gemm_smem(a.Lkp, a.Dk, nt, sb); };
     // columns per tile: a multiple of 32 up to 128 whose operands fit shared memory with two B stages, the one that
     // wastes the fewest columns on the last tile counting each tile as 32 columns of fixed cost
     int best = 0, bestw = 1 << 30;
@@ -727,7 +734,9 @@ cudaError_t launch_level_tc_gemm(const LevelLaunch &L, const int *amax_in, void 
         case 2: e = run(level_tc_gemm<2>); break;
         case 4: e = run(level_tc_gemm<4>); break;
         case 6: e = run(level_tc_gemm<6>); break;
-        default: e = run(level_tc_gemm<8>); break;
+        case 8: e = run(level_tc_gemm<8>); break;
+        case 10: e = run(level_tc_gemm<10>); break;
+        default: e = run(level_tc_gemm<12>); break;
     }
     if (e != cudaSuccess) return e;
     return cudaSuccess;

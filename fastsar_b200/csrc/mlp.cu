@@ -104,8 +104,9 @@ __global__ void dense_bwd_x(const float *__restrict__ dZ, const float *__restric
 // queries q0 .. q0 + D - 1; query q holds the 8 taps of phase q at offsets t = phi_q - 4 + n (n = 0..7) in output
 // samples, phi_q = (q + 1/2) / D for even D and q / D for odd D, each tap = prior + scale * (output 8 a + n of the
 // network). A sample is a point target's parent samples e^{2 pi i f t} (f in cycles per output sample, float64) and
-// its exact child value y; the decimated value is v = (1 / D) sum_{q, n} tap x. Block (x, i) takes samples
-// 256 x .. of instance i: the loss sum |v - y|^2 (atomic) and d (mean |v - y|^2) / d output, reduced per tap over the
+// its exact child value y; the decimated value is v = (1 / D) sum_{q, n} tap x; instance i's pairs weigh wt[i] (1
+// without wt). Block (x, i) takes samples 256 x .. of instance i: the loss sum wt |v - y|^2 (atomic) and
+// d (mean wt |v - y|^2) / d output, reduced per tap over the
 // block in shared memory before one atomic per tap. An instance outside the query table (or D outside 1..32, or an
 // axis other than 0 or 1) adds NaN to the loss and is skipped.
 constexpr int LOSS_THREADS = 256;
@@ -119,7 +120,8 @@ __device__ __forceinline__ float2 cis_frac(double c)       // e^{2 pi i c}, the 
 }
 
 __global__ void __launch_bounds__(LOSS_THREADS) fir_loss(const float *__restrict__ out, const float *__restrict__ prior,
-                                                         float scale, const int *__restrict__ inst, int nq, int S,
+                                                         float scale, const int *__restrict__ inst,
+                                                         const float *__restrict__ wt, int nq, int S,
                                                          const double *__restrict__ f, const float2 *__restrict__ y,
                                                          float gscale, float *__restrict__ dout, float *__restrict__ loss)
 {
@@ -151,14 +153,14 @@ __global__ void __launch_bounds__(LOSS_THREADS) fir_loss(const float *__restrict
             x = make_float2(x.x * step.x - x.y * step.y, x.x * step.y + x.y * step.x);
         }
     }
-    const float invD = 1.f / (float)D;
+    const float invD = 1.f / (float)D, wi = wt ? wt[i] : 1.f;
     float ex = 0.f, ey = 0.f;
     if (live) {
         const float2 yy = y[(long)i * S + s];
         ex = vx * invD - yy.x;
         ey = vy * invD - yy.y;
     }
-    float l = ex * ex + ey * ey;
+    float l = wi * (ex * ex + ey * ey);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
     if ((threadIdx.x & 31) == 0) atomicAdd(loss, l);
@@ -175,7 +177,7 @@ __global__ void __launch_bounds__(LOSS_THREADS) fir_loss(const float *__restrict
         }
     }
     __syncthreads();
-    const float g = gscale * scale * invD;
+    const float g = gscale * scale * invD * wi;
     for (int j = threadIdx.x; j < L; j += blockDim.x)
         atomicAdd(&dout[(long)(q0 + (j >> 3)) * 16 + 8 * ax + (j & 7)], g * s_g[j]);
 }
@@ -275,8 +277,8 @@ cudaError_t mlp_taps(const float *params, const float *x, int B, float *taps, fl
 }
 
 cudaError_t mlp_grad(const float *params, const float *x, int nq, const float *prior, float scale, const int *inst,
-                     int ninst, const double *f, const float2 *y, int S, float *grad, float *loss, float *work,
-                     cudaStream_t s)
+                     const float *wt, int ninst, const double *f, const float2 *y, int S, float *grad, float *loss,
+                     float *work, cudaStream_t s)
 {
     Work k = carve(work, nq);
     cudaError_t e = forward(params, x, nq, k, s);
@@ -284,7 +286,7 @@ cudaError_t mlp_grad(const float *params, const float *x, int nq, const float *p
     if ((e = cudaMemsetAsync(loss, 0, sizeof(float), s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(k.dtaps, 0, (size_t)nq * 16 * sizeof(float), s)) != cudaSuccess) return e;
     fir_loss<<<dim3((S + LOSS_THREADS - 1) / LOSS_THREADS, ninst), LOSS_THREADS, 0, s>>>(
-        k.H[NL - 1], prior, scale, inst, nq, S, f, y, 2.f / ((float)ninst * (float)S), k.dtaps, loss);
+        k.H[NL - 1], prior, scale, inst, wt, nq, S, f, y, 2.f / ((float)ninst * (float)S), k.dtaps, loss);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = backward(x, nq, k, s)) != cudaSuccess) return e;
     if (grad) return cudaMemcpyAsync(grad, k.grad, param_count() * sizeof(float), cudaMemcpyDeviceToDevice, s);
@@ -292,10 +294,10 @@ cudaError_t mlp_grad(const float *params, const float *x, int nq, const float *p
 }
 
 cudaError_t mlp_train_step(float *params, float *adam, const float *x, int nq, const float *prior, float scale,
-                           const int *inst, int ninst, const double *f, const float2 *y, int S, float lr, int t,
-                           float *loss, float *work, cudaStream_t s)
+                           const int *inst, const float *wt, int ninst, const double *f, const float2 *y, int S,
+                           float lr, int t, float *loss, float *work, cudaStream_t s)
 {
-    cudaError_t e = mlp_grad(params, x, nq, prior, scale, inst, ninst, f, y, S, nullptr, loss, work, s);
+    cudaError_t e = mlp_grad(params, x, nq, prior, scale, inst, wt, ninst, f, y, S, nullptr, loss, work, s);
     if (e != cudaSuccess) return e;
     Work k = carve(work, nq);
     const int P = param_count();

@@ -34,8 +34,8 @@ LAYERS = ((5, 64), (64, 64), (64, 64), (64, 16))
 WIDTH = 8                      # output samples spanned by the filter: 8 taps per phase
 BETA = 7.0                     # Kaiser parameter of the prior
 SCALE = 1.0 / 32.0             # output -> tap correction
-D_RANGE = (2, 24)              # decimations and pass fractions the network is trained for
-W_RANGE = (0.25, 0.5)
+D_RANGE = (2, 32)              # decimations and pass fractions the network is trained for
+W_RANGE = (0.25, 0.65)
 
 
 # --------------------------------------------------------------------------------------------- filter geometry
@@ -179,10 +179,11 @@ class LearnedTaps:
     def _device_pairs(self, pairs):
         import torch
         dev = torch.device('cuda', torch.cuda.current_device())
-        x, prior_, inst, f, y = pairs
+        x, prior_, inst, wt, f, y = pairs
         return (torch.as_tensor(np.ascontiguousarray(x, np.float32)).to(dev),
                 torch.as_tensor(np.ascontiguousarray(prior_, np.float32)).to(dev),
                 torch.as_tensor(np.ascontiguousarray(inst, np.int32)).to(dev),
+                torch.as_tensor(np.ascontiguousarray(wt, np.float32)).to(dev),
                 torch.as_tensor(np.ascontiguousarray(f, np.float64)).to(dev),
                 torch.as_tensor(np.ascontiguousarray(y, np.complex64)).to(dev))
 
@@ -191,14 +192,14 @@ class LearnedTaps:
         import torch
         L = _lib.load()
         dev = torch.device('cuda', torch.cuda.current_device())
-        x, pr, inst, f, y = self._device_pairs(pairs)
+        x, pr, inst, wt, f, y = self._device_pairs(pairs)
         p = torch.from_numpy(self.params).to(dev)
         nq, (ninst, S) = x.shape[0], f.shape
         grad = torch.empty(N_PARAMS, dtype=torch.float32, device=dev)
         loss = torch.zeros(1, dtype=torch.float32, device=dev)
         work = torch.empty(int(L.ffbp_mlp_work_bytes(nq)) // 4 + 16, dtype=torch.float32, device=dev)
         _lib.check(L.ffbp_mlp_grad(p.data_ptr(), x.data_ptr(), nq, pr.data_ptr(), ctypes.c_float(SCALE), inst.data_ptr(),
-                                   ninst, f.data_ptr(), y.data_ptr(), S, grad.data_ptr(), loss.data_ptr(),
+                                   wt.data_ptr(), ninst, f.data_ptr(), y.data_ptr(), S, grad.data_ptr(), loss.data_ptr(),
                                    work.data_ptr(), torch.cuda.current_stream(dev).cuda_stream), 'ffbp_mlp_grad')
         return float(loss.item()), grad.cpu().numpy()
 
@@ -208,7 +209,7 @@ class LearnedTaps:
         import torch
         L = _lib.load()
         dev = torch.device('cuda', torch.cuda.current_device())
-        x, pr, inst, f, y = self._device_pairs(pairs)
+        x, pr, inst, wt, f, y = self._device_pairs(pairs)
         nq, (ninst, S) = x.shape[0], f.shape
         p = torch.from_numpy(self.params.copy()).to(dev)
         adam = torch.zeros(2 * N_PARAMS, dtype=torch.float32, device=dev)
@@ -219,7 +220,8 @@ class LearnedTaps:
         for t in range(1, steps + 1):
             rate = lr * (lr_end / lr) ** ((t - 1) / max(1, steps - 1))
             _lib.check(L.ffbp_mlp_train_step(p.data_ptr(), adam.data_ptr(), x.data_ptr(), nq, pr.data_ptr(),
-                                             ctypes.c_float(SCALE), inst.data_ptr(), ninst, f.data_ptr(), y.data_ptr(),
+                                             ctypes.c_float(SCALE), inst.data_ptr(), wt.data_ptr(), ninst, f.data_ptr(),
+                                             y.data_ptr(),
                                              S, ctypes.c_float(rate), t, loss.data_ptr(), work.data_ptr(), s),
                        'ffbp_mlp_train_step')
             if t % every == 0 or t == 1 or t == steps:
@@ -253,9 +255,10 @@ def instances(seed, n):
 
 
 def make_pairs(insts, S, seed):
-    """Training pairs of filter instances: (x [nq, 5], prior [nq, 8], inst [ninst, 3], f [ninst, S], y [ninst, S]).
-    Per instance S point targets: the first half in the child's band (child value 1), the rest spread over the
-    folds onto it inside the input band (child value 0)."""
+    """Training pairs of filter instances: (x [nq, 5], prior [nq, 8], inst [ninst, 3], weight [ninst], f [ninst, S],
+    y [ninst, S]). Per instance S point targets: the first half in the child's band (child value 1), the rest
+    spread over the folds onto it inside the input band (child value 0). An instance weighs the inverse of the
+    prior's loss on its pairs (normalised to a mean of 1), so that narrow and wide bands count alike."""
     rng = np.random.default_rng(seed)
     xs, ps, inst = [], [], []
     f = np.empty((len(insts), S))
@@ -272,20 +275,42 @@ def make_pairs(insts, S, seed):
         folds = np.array([k for k in range(-(D // 2), D // 2 + 1) if k != 0], np.float64)
         g = folds[rng.integers(0, len(folds), S - h)] + rng.uniform(-w / 2, w / 2, S - h)
         f[i, h:] = np.clip(g, -D / 2, D / 2)
-    return (np.concatenate(xs), np.concatenate(ps).astype(np.float32), np.asarray(inst, np.int32), f, y)
+    wt = np.empty(len(insts))
+    for i, (D, w, st, ax) in enumerate(insts):
+        v = np.exp(2j * np.pi * f[i][:, None, None] * tap_offsets(D)[None]).reshape(S, -1) @ prior(D).ravel() / D
+        wt[i] = 1.0 / max(np.mean(np.abs(v - y[i]) ** 2), 1e-30)
+    wt /= wt.mean()
+    return (np.concatenate(xs), np.concatenate(ps).astype(np.float32), np.asarray(inst, np.int32),
+            wt.astype(np.float32), f, y)
+
+
+def kaiser_of_length(D, w, L):
+    """The reference's Kaiser-sinc decimator (fastsar/ffbp2.py:101-137) with the highest stop-band attenuation
+    (0.25 dB steps) whose kernel has at most L taps."""
+    from .plan import decimator_fir
+    lo, hi = 20.0, 200.0
+    while hi - lo > 0.25:
+        mid = 0.5 * (lo + hi)
+        if decimator_fir(4096, D, w, mid)[0]['L'] <= L:
+            lo = mid
+        else:
+            hi = mid
+    return decimator_fir(4096, D, w, lo)[0]['kern']
 
 
 def evaluate(model, insts, atten=80.0):
-    """Per instance the band error (dB) of the learned taps, the prior alone and the reference's Kaiser-sinc
-    decimator at `atten` (its length in taps too): a list of dicts."""
+    """Per instance the band error (dB) of the learned taps, the prior alone, the reference's Kaiser-sinc decimator
+    of no more taps than the learned filter (kaiser_same) and the one at `atten` (kaiser, with its length in
+    taps): a list of dicts."""
     from .plan import decimator_fir
     rows = []
     for D, w, st, ax in insts:
         k = kern_from_phases(model.phase_taps(D, w, st, ax))
         kp = kern_from_phases(prior(D))
         kr = decimator_fir(4096, D, w, atten)[0]['kern']
+        ks = kaiser_of_length(D, w, len(k))
         rows.append(dict(D=D, w=w, stage=st, axis=ax, learned=band_error_db(k, D, w, centre(D)),
-                         prior=band_error_db(kp, D, w, centre(D)),
+                         prior=band_error_db(kp, D, w, centre(D)), kaiser_same=band_error_db(ks, D, w),
                          kaiser=band_error_db(kr, D, w), taps=len(k), kaiser_taps=len(kr)))
     return rows
 
@@ -295,7 +320,7 @@ def main(argv=None):
     import time
     ap = argparse.ArgumentParser(description='train the learned decimation taps on the GPU')
     ap.add_argument('cmd', choices=('train', 'eval'))
-    ap.add_argument('--instances', type=int, default=4096)
+    ap.add_argument('--instances', type=int, default=8192)
     ap.add_argument('--pairs', type=int, default=256, help='point targets per instance')
     ap.add_argument('--steps', type=int, default=60000)
     ap.add_argument('--lr', type=float, default=3e-3)
@@ -313,7 +338,7 @@ def main(argv=None):
                instances=args.instances, pairs=args.pairs)
     m = LearnedTaps.load(args.out)
     rows = evaluate(m, instances(10 ** 6, 64))
-    for key in ('learned', 'prior', 'kaiser'):
+    for key in ('learned', 'prior', 'kaiser_same', 'kaiser'):
         print(key, round(float(np.mean([r[key] for r in rows])), 2), 'dB')
     print('taps', np.mean([r['taps'] for r in rows]), 'kaiser 80 dB taps', np.mean([r['kaiser_taps'] for r in rows]))
 

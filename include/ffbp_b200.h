@@ -179,7 +179,7 @@ int ffbp_level(const void *d_x, int Np, int P, int K, const void *d_phase, int C
  * frequency taps tk[r] exp(2 pi i sl r) times the Hankel windows of the parent's row, three bfloat16 products
  * accumulated in float32; the ramp exp(2 pi i (c0 + sl (Dk j - plk - kc))); a float16 intermediate in d_scratch
  * (ffbp_level_tc_scratch_bytes, 16-byte aligned), scaled by a power of two from the input's largest component;
- * the pulse FIR in float32. C <= 64 and Lk <= 64 (FFBP_E_UNSUPPORTED otherwise). d_status: 3 ints, zeroed by the
+ * the pulse FIR in float32. C <= 64 and Lk <= 96 (FFBP_E_UNSUPPORTED otherwise). d_status: 3 ints, zeroed by the
  * caller: [0] set when a bounded wait of the kernel ran out, [1] the input's largest |component| (float bits,
  * filled here), [2] the output's. No counterpart in the reference (its levels run in float32 only).            */
 size_t ffbp_level_tc_scratch_bytes(int Np, int C, int P, int Ko);
@@ -217,8 +217,9 @@ int ffbp_exact_backproject(const void *d_prof, int n, int nfft, int W, const lon
  * owns queries first .. first + D - 1 with prior taps d_prior [nq, 8]; its S samples are point targets at
  * frequencies d_f [ninst, S] (float64, cycles per output sample), whose parent samples are e^{2 pi i f t}, and their
  * exact child values d_y [ninst, S] (complex64); the decimated value is v = (1 / D) sum over the instance's taps of
- * tap e^{2 pi i f t}. ffbp_mlp_grad writes the gradient of mean |v - y|^2 over all pairs (d_grad, param count
- * floats, or NULL) and the sum |v - y|^2 (*d_loss; NaN when an instance is outside the query table);
+ * tap e^{2 pi i f t}; instance i's pairs weigh d_weight[i] (float32; NULL: all 1). ffbp_mlp_grad writes the
+ * gradient of mean weight |v - y|^2 over all pairs (d_grad, param count floats, or NULL) and the sum
+ * weight |v - y|^2 (*d_loss; NaN when an instance is outside the query table);
  * ffbp_mlp_train_step takes one Adam step (lr, step t >= 1, b1 0.9, b2 0.999, eps 1e-8) with d_adam (2 x param
  * count floats: first then second moments, zeroed at t = 1). */
 int ffbp_mlp_param_count(void);
@@ -226,11 +227,11 @@ int ffbp_mlp_max_decimation(void);
 size_t ffbp_mlp_work_bytes(int nq);
 int ffbp_mlp_taps(const float *d_params, const float *d_x, int nq, float *d_out, void *d_work, void *stream);
 int ffbp_mlp_grad(const float *d_params, const float *d_x, int nq, const float *d_prior, float scale,
-                  const int *d_inst, int ninst, const double *d_f, const void *d_y, int S, float *d_grad,
-                  float *d_loss, void *d_work, void *stream);
+                  const int *d_inst, const float *d_weight, int ninst, const double *d_f, const void *d_y, int S,
+                  float *d_grad, float *d_loss, void *d_work, void *stream);
 int ffbp_mlp_train_step(float *d_params, float *d_adam, const float *d_x, int nq, const float *d_prior, float scale,
-                        const int *d_inst, int ninst, const double *d_f, const void *d_y, int S, float lr, int t,
-                        float *d_loss, void *d_work, void *stream);
+                        const int *d_inst, const float *d_weight, int ninst, const double *d_f, const void *d_y, int S,
+                        float lr, int t, float *d_loss, void *d_work, void *stream);
 
 /* Child phases in float64 for one level (fastsar/ffbp2.py:329-339 / fastsar/ffbp_cuda.py:598-632): for parent n,
  * child c and pulse p, ddr = |cen[n,c] - ant[p]| - |ref[n] - ant[p]| (or - range[p] when d_range is given),

@@ -52,7 +52,7 @@ def test_gradient_matches_oracle(S):
     ps = _random_net(2)
     pairs = learned.make_pairs(learned.instances(4, 6), S, seed=5)
     loss, grad = learned.LearnedTaps(_flat(ps)).grad(pairs)
-    want_loss, want = M.loss_and_grad(ps, pairs[0], pairs[1], learned.SCALE, pairs[2], pairs[3], pairs[4])
+    want_loss, want = M.loss_and_grad(ps, pairs[0], pairs[1], learned.SCALE, *pairs[2:])
     assert abs(loss - want_loss) <= 1e-3 * want_loss
     for li, (gp, (dW, db)) in enumerate(zip(learned.unpack(grad), want)):
         assert _rel(gp[0], dW) < 2e-2, (li, 'W', _rel(gp[0], dW))
@@ -66,7 +66,7 @@ def test_adam_step_matches_oracle():
     L = _lib.load()
     ps = _random_net(3)
     pairs = learned.make_pairs(learned.instances(6, 5), 256, seed=7)
-    x, pr, inst, f, y = (torch.as_tensor(np.ascontiguousarray(a)).cuda() for a in pairs)
+    x, pr, inst, wt, f, y = (torch.as_tensor(np.ascontiguousarray(a)).cuda() for a in pairs)
     p = torch.from_numpy(_flat(ps)).cuda()
     adam = torch.zeros(2 * learned.N_PARAMS, dtype=torch.float32, device='cuda')
     adam[learned.N_PARAMS:] = 1e-6
@@ -74,7 +74,8 @@ def test_adam_step_matches_oracle():
     loss = torch.zeros(1, dtype=torch.float32, device='cuda')
     lr = 1e-3
     _lib.check(L.ffbp_mlp_train_step(p.data_ptr(), adam.data_ptr(), x.data_ptr(), x.shape[0], pr.data_ptr(),
-                                     ctypes.c_float(learned.SCALE), inst.data_ptr(), inst.shape[0], f.data_ptr(),
+                                     ctypes.c_float(learned.SCALE), inst.data_ptr(), wt.data_ptr(), inst.shape[0],
+                                     f.data_ptr(),
                                      y.data_ptr(), f.shape[1], ctypes.c_float(lr), 1, loss.data_ptr(), work.data_ptr(),
                                      torch.cuda.current_stream().cuda_stream), 'ffbp_mlp_train_step')
     _, g = M.loss_and_grad(ps, *pairs[:2], learned.SCALE, *pairs[2:])
@@ -112,15 +113,17 @@ def test_training_lowers_the_loss():
 
 def test_packaged_taps_beat_the_kaiser_filters():
     """On held-out filter instances the packaged network's 8-output-sample taps have a smaller band error than the
-    prior alone and than the reference's 80 dB Kaiser-sinc decimators, with no more taps."""
+    prior alone and than the reference's Kaiser-sinc decimator of the same length (its attenuation raised as far as
+    the length allows): by 5 dB on average, and on at least three quarters of the instances."""
     from fastsar_b200 import learned
     m = learned.LearnedTaps.load()
     rows = learned.evaluate(m, learned.instances(10 ** 6, 48))
-    mean = {k: float(np.mean([r[k] for r in rows])) for k in ('learned', 'prior', 'kaiser', 'taps', 'kaiser_taps')}
+    mean = {k: float(np.mean([r[k] for r in rows])) for k in ('learned', 'prior', 'kaiser_same', 'kaiser', 'taps',
+                                                               'kaiser_taps')}
     print(mean)
     assert mean['learned'] < mean['prior'] - 5.0
-    assert mean['learned'] < mean['kaiser'] - 5.0
-    assert mean['taps'] <= mean['kaiser_taps']
+    assert mean['learned'] < mean['kaiser_same'] - 5.0
+    assert np.mean([r['learned'] < r['kaiser_same'] for r in rows]) >= 0.75
 
 
 def test_learned_taps_image_against_float64(golden, oracle_lib):
@@ -145,17 +148,19 @@ def test_learned_taps_image_against_float64(golden, oracle_lib):
 
 
 def test_learned_taps_mixed_precision_image_against_float64(golden, oracle_lib):
-    """The chosen form, precision='float16' with the learned taps, on the 512-pulse spotlight: below -60 dB against
-    the float64 exact backprojection and no worse than precision='float16' with the 80 dB Kaiser-sinc filters."""
+    """precision='float16' with the learned taps on the 512-pulse spotlight: below -60 dB against the float64 exact
+    backprojection and no worse than precision='float16' with the 80 dB Kaiser-sinc filters; with the child data
+    oversampled 2x instead of 2.5x (pmax 0.5, the benchmark's chosen form) still below -60 dB."""
     from fastsar_b200 import ImageFormer, sim
     g = golden('image_spot512')
     w = sim.workload('spotlight_512')
     col = w['col']
     errs = {}
-    for name, kw in (('kaiser80', {}), ('learned', dict(taps='learned'))):
+    for name, kw in (('kaiser80', {}), ('learned', dict(taps='learned')), ('learned_p05', dict(taps='learned', pmax=0.5))):
         f = ImageFormer(col.ant, col.fmin, col.df, col.K, 512, 512, 0.25, 0.25, w['e1'], w['e2'], precision='float16',
                         **kw)
         errs[name] = oracle_lib.rel_db(f(g['S']).ravel()[g['bp64_idx']], g['bp64'])
     print(errs)
     assert errs['learned'] < -60.0
     assert errs['learned'] < errs['kaiser80'] + 0.5
+    assert errs['learned_p05'] < -60.0

@@ -158,6 +158,8 @@ TC_LEVEL_CASES = [
     (1, 200, 900, 64, 3, 10, 0.6),    # 64 children (every accumulator row), several column tiles
     (2, 120, 700, 56, 7, 8, 0.45),    # 56 children, 57 frequency taps
     (8, 90, 160, 30, 5, 6, 0.6),      # many parents, 30 children
+    (2, 100, 800, 56, 9, 8, 0.45),    # 73 frequency taps (K padded to 80)
+    (1, 90, 1200, 40, 10, 6, 0.5),    # 90 frequency taps (K padded to 96)
 ]
 
 
@@ -184,7 +186,7 @@ def test_level_tensor_cores_match_oracle(lib, oracle_lib, case):
 
 def test_level_tensor_cores_window_nonfinite_and_limits(lib, oracle_lib):
     """The first level's window and the non-finite scan on the tensor-core level, and the shapes it leaves to the
-    float32 kernel (more than 64 frequency taps) refused with FFBP_E_UNSUPPORTED."""
+    float32 kernel (more than 96 frequency taps) refused with FFBP_E_UNSUPPORTED."""
     rng = np.random.default_rng(5)
     x, c0, sl, fk, fp, Ko, Po = _level_case(rng, 1, 120, 256, 12, 3, 2)
     from fastsar_b200.api import _window
@@ -197,9 +199,9 @@ def test_level_tensor_cores_window_nonfinite_and_limits(lib, oracle_lib):
     bad = torch.full((1,), 2 ** 31 - 1, dtype=torch.int32, device='cuda')
     _run_level_tc(lib, x, c0, sl, fk, fp, Ko, Po, 3, 2, window=w, bad=bad)
     assert int(bad.item()) == 77
-    x, c0, sl, fk, fp, Ko, Po = _level_case(rng, 1, 50, 700, 2, 7, 2)       # Lk = 79
-    with pytest.raises(ValueError, match='64'):
-        _run_level_tc(lib, x, c0, sl, fk, fp, Ko, Po, 7, 2)
+    x, c0, sl, fk, fp, Ko, Po = _level_case(rng, 1, 50, 1200, 2, 11, 2)     # Lk = 121
+    with pytest.raises(ValueError, match='96'):
+        _run_level_tc(lib, x, c0, sl, fk, fp, Ko, Po, 11, 2)
 
 
 @pytest.mark.parametrize('T', [16, 32])

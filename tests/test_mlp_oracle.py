@@ -37,9 +37,9 @@ def test_bf16_rounding_matches_torch():
 def test_oracle_gradient_matches_central_differences(layer):
     from fastsar_b200 import learned
     params = M.init_params(seed=1)
-    x, prior, inst, f, y = _pairs(3, 16, seed=2)
-    mean = lambda P: M.loss_and_grad(P, x, prior, learned.SCALE, inst, f, y, rounding=False)[0] / f.size
-    _, grads = M.loss_and_grad(params, x, prior, learned.SCALE, inst, f, y, rounding=False)
+    x, prior, inst, wt, f, y = _pairs(3, 16, seed=2)
+    mean = lambda P: M.loss_and_grad(P, x, prior, learned.SCALE, inst, wt, f, y, rounding=False)[0] / f.size
+    _, grads = M.loss_and_grad(params, x, prior, learned.SCALE, inst, wt, f, y, rounding=False)
     rng = np.random.default_rng(5)
     W, b = params[layer]
     h = 1e-3
@@ -58,8 +58,8 @@ def test_oracle_gradient_matches_central_differences(layer):
 def test_oracle_adam_step():
     from fastsar_b200 import learned
     params = M.init_params(seed=4)
-    x, prior, inst, f, y = _pairs(4, 32, seed=6)
-    _, g = M.loss_and_grad(params, x, prior, learned.SCALE, inst, f, y)
+    x, prior, inst, wt, f, y = _pairs(4, 32, seed=6)
+    _, g = M.loss_and_grad(params, x, prior, learned.SCALE, inst, wt, f, y)
     state = [(np.zeros_like(W, np.float64), np.zeros_like(W, np.float64), np.zeros_like(b, np.float64),
               np.zeros_like(b, np.float64)) for W, b in params]
     new = M.adam_step(params, g, state, lr=1e-2, t=1)
