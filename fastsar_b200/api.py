@@ -343,28 +343,45 @@ class ImageFormer:
                                    or not 0 <= padded[0] <= self.P - padded[1]):
             raise ValueError('padded=(first, count, pulse) goes with an aperture_weight, the levels of the plan that '
                              f'pulse is from and an aperture within the {self.P} pulses, got {padded!r}')
+        def planned(col):
+            nlev = 3 if levels is None else levels
+            while True:
+                try:
+                    return _plan.make_plan(col, nx, ny, spx, spy, T=T, nlev=nlev, pmax=pmax, e1=e1, e2=e2,
+                                           pulse=padded and padded[2], atten=self.atten, taps=self.taps), nlev
+                except ValueError as e:
+                    if levels is not None or 'cannot split' not in str(e) or nlev >= 8:
+                        raise
+                    nlev += 1
+
         col = Collect(fmin=float(fmin), df=float(df), K=self.K, ant=self.ant, res=0.5)
-        nlev = 3 if levels is None else levels
-        while True:
-            try:
-                plan = _plan.make_plan(col, nx, ny, spx, spy, T=T, nlev=nlev, pmax=pmax, e1=e1, e2=e2,
-                                       pulse=padded and padded[2], atten=self.atten, taps=self.taps)
-                break
-            except ValueError as e:
-                if levels is not None or 'cannot split' not in str(e) or nlev >= 8:
-                    raise
-                nlev += 1
+        plan, nlev = planned(col)
+        # the range gate (fastsar/api.py:398-416): 'auto' where the first level's frequency filter would not fit the
+        # level kernel (more than 256 taps: an image narrow in range from a wide-band collection), True wherever it
+        # keeps fewer than half of the samples
+        self.range_gate = None
+        lk = plan['levels'][0]['fir_k']['L'] if plan['levels'][0]['fir_k'] else 1
+        why = None
+        if range_gate == 'auto' and aperture_weight is None and lk > 256:
+            why = (f"the first level's frequency filter would have {lk} taps (range decimation "
+                   f"{plan['levels'][0]['Dk']}), more than the level kernel holds (256)")
+        if why or range_gate is True:
+            g = _plan.gate_plan(self.ant, ref, float(fmin), float(df), self.K, nx, ny, spx, spy, e1, e2)
+            kept = g['k1'] - g['k0']
+            if g['N'] < g['Kp'] and kept < (self.K if why else self.K // 2):
+                col = Collect(fmin=g['fmin'], df=g['df'], K=kept, ant=self.ant, res=0.5)
+                plan, nlev = planned(col)
+                self.range_gate = dict(g, K=self.K, kept=kept, note=(
+                    f'range gate: each pulse cut to the {g["N"]} range bins about the image before formation, '
+                    f'{kept} samples for {self.K}' + (f' ({why})' if why else '')))
+                lk = plan['levels'][0]['fir_k']['L'] if plan['levels'][0]['fir_k'] else 1
         self.levels = nlev
         self._plan = plan
-        self.range_gate = None
-        if range_gate is True:
-            raise ValueError('range_gate=True: the range gate is not part of this version; form with range_gate=False')
-        lk = plan['levels'][0]['fir_k']['L'] if plan['levels'][0]['fir_k'] else 1
         if lk > 256:
             raise ValueError(f'the first level\'s frequency filter has {lk} taps (range decimation '
                              f"{plan['levels'][0]['Dk']}: an image narrow in range from a wide-band collection), more "
-                             'than the level kernel holds (256); the range gate that shortens it is not part of this '
-                             'version: form a wider image or several')
+                             'than the level kernel holds (256); form with range_gate=True (or \'auto\', without an '
+                             'aperture_weight), a wider image, or several')
         wf = None
         if aperture_weight is not None:
             wspan = dict(P=self.P) if padded is None else dict(P=int(padded[1]), first=int(padded[0]))
@@ -377,10 +394,12 @@ class ImageFormer:
         wp = wk = None
         if window:
             self.wp, self.wk = wp, wk = _window(self.P, self.K)
-        self._dev = DevicePlan(plan, wp, wk, wf, None if ref is None else np.asarray(ref, np.float64),
-                               _final_mode(precision))
+        # a gated history is windowed in the gate, before its transforms; the former then takes it as it is
+        self._dev = DevicePlan(plan, None if self.range_gate else wp, None if self.range_gate else wk, wf,
+                               None if ref is None else np.asarray(ref, np.float64), _final_mode(precision))
         self._S = None
         self._img = None
+        self._gate_dev = None
 
     # ------------------------------------------------------------------------------------------------ calls
     def memory(self):
@@ -413,11 +432,60 @@ class ImageFormer:
         self._S.copy_(torch.from_numpy(S), non_blocking=False)
         return self._S
 
+    def _gate(self, S_dev):
+        """The range gate on the device (fastsar/api.py:525-564, fastsar/ffbp_cuda.py:767-864): S_dev [P, K]
+        complex64 -> the gated history [P, kept] complex64 (a buffer of the former), windowed; in blocks of pulses
+        whose padded rows stay within 256 MB; the transforms by cuFFT. Raises ValueError naming the first pulse with
+        a non-finite sample."""
+        import torch
+        L = _lib.load()
+        g = self.range_gate
+        dev = self._dev.device
+        P, K, kept = self.P, self.K, g['kept']
+        npl, Kp, N, k0, k1 = g['npl'], g['Kp'], g['N'], g['k0'], g['k1']
+        if self._gate_dev is None:
+            win = self.window
+            self._gate_dev = dict(
+                taper=torch.from_numpy(np.ascontiguousarray(g['taper'], np.float32)).to(dev),
+                wp=torch.from_numpy(np.ascontiguousarray(self.wp, np.float32)).to(dev) if win else None,
+                wk=torch.from_numpy(np.ascontiguousarray(self.wk, np.float32)).to(dev) if win else None,
+                out=torch.empty((P, kept), dtype=torch.complex64, device=dev),
+                bad=torch.empty(1, dtype=torch.int32, device=dev))
+        gd = self._gate_dev
+        S_dev = S_dev.contiguous()
+        gd['bad'].fill_(2 ** 31 - 1)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        nb = int(max(1, min(P, (1 << 28) // (Kp * 8))))
+        tp = _lib.tptr
+        for p0 in range(0, P, nb):
+            r = min(nb, P - p0)
+            z = torch.empty((r, Kp), dtype=torch.complex64, device=dev)
+            _lib.check(L.ffbp_gate_pad(S_dev.data_ptr() + p0 * K * 8, r, K, tp(gd['wp']), tp(gd['wk']), npl, Kp,
+                                       z.data_ptr(), gd['bad'].data_ptr(), p0, stream), 'ffbp_gate_pad')
+            q = torch.fft.ifft(z, dim=1)
+            del z
+            u = torch.empty((r, N), dtype=torch.complex64, device=dev)
+            _lib.check(L.ffbp_gate_fold(q.data_ptr(), r, Kp, N, u.data_ptr(), stream), 'ffbp_gate_fold')
+            del q
+            v = torch.fft.fft(u, dim=1)
+            _lib.check(L.ffbp_gate_taper(v.data_ptr(), r, N, k0, k1, gd['taper'].data_ptr(),
+                                         gd['out'].data_ptr() + p0 * kept * 8, stream), 'ffbp_gate_taper')
+        b = int(gd['bad'].item())
+        if b != 2 ** 31 - 1:
+            raise ValueError(f'phase history has non-finite samples (NaN or inf), the first in pulse {b}; '
+                             'zero them (S[~np.isfinite(S)] = 0) or drop the pulses')
+        return gd['out']
+
     def form_device(self, S_dev, out=None, check=True):
-        """S_dev [P, K] complex64 on the device -> the image [nx, ny] complex64 on the device (torch)."""
+        """S_dev [P, K] complex64 on the device -> the image [nx, ny] complex64 on the device (torch). With a range
+        gate the history is gated first (and always checked for non-finite samples there)."""
         import torch
         if out is None:
             out = torch.empty((self.nx, self.ny), dtype=torch.complex64, device=self._dev.device)
+        if self.range_gate is not None:
+            if tuple(S_dev.shape) != (self.P, self.K):
+                raise ValueError(f'phase history must be {(self.P, self.K)}, got {tuple(S_dev.shape)}')
+            S_dev = self._gate(S_dev)
         return self._dev.form(S_dev, out, check=check)
 
     def form_many(self, histories, images=None):
@@ -453,6 +521,13 @@ class ImageFormer:
             raise ValueError(f'{len(hs)} histories but {len(outs)} images')
         if not hs:
             return []
+        if self.range_gate is not None:                         # gated: one image after the other
+            for i, (h, o) in enumerate(zip(hs, outs)):
+                try:
+                    o.copy_(self.form_device(h.to(self._dev.device)))
+                except ValueError as e:
+                    raise ValueError(str(e).replace('phase history', f'phase history {i}', 1)) from None
+            return [o.numpy() for o in outs]
         bad = self._dev.form_host([h.data_ptr() for h in hs], [o.data_ptr() for o in outs])
         for i, b in enumerate(bad):
             if b >= 0:

@@ -584,6 +584,35 @@ int ffbp_exact_backproject(const void *d_prof, int n, int nfft, int W, const lon
     return FFBP_OK;
 }
 
+int ffbp_gate_pad(const void *d_S, int n, int K, const float *d_wp, const float *d_wk, int npl, int Kp, void *d_z,
+                  int *d_bad, int p_off, void *stream)
+{
+    if (!d_S || !d_z || n < 0 || K < 1 || npl < 0 || Kp < K + npl || (!d_wp) != (!d_wk) || p_off < 0)
+        return fail(FFBP_E_ARG, "ffbp_gate_pad: bad arguments");
+    cudaError_t e = ffbp::launch_gate_pad(static_cast<const float2 *>(d_S), n, K, d_wp, d_wk, npl, Kp,
+                                          static_cast<float2 *>(d_z), d_bad, p_off, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "ffbp_gate_pad");
+    return FFBP_OK;
+}
+
+int ffbp_gate_fold(const void *d_q, int n, int Kp, int N, void *d_u, void *stream)
+{
+    if (!d_q || !d_u || n < 0 || N < 2 || N > Kp) return fail(FFBP_E_ARG, "ffbp_gate_fold: bad arguments");
+    cudaError_t e = ffbp::launch_gate_fold(static_cast<const float2 *>(d_q), n, Kp, N, static_cast<float2 *>(d_u),
+                                           static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "ffbp_gate_fold");
+    return FFBP_OK;
+}
+
+int ffbp_gate_taper(const void *d_u, int n, int N, int k0, int k1, const float *d_taper, void *d_out, void *stream)
+{
+    if (!d_u || !d_taper || !d_out || n < 0 || k0 < 0 || k1 <= k0 || k1 > N) return fail(FFBP_E_ARG, "ffbp_gate_taper: bad arguments");
+    cudaError_t e = ffbp::launch_gate_taper(static_cast<const float2 *>(d_u), n, N, k0, k1, d_taper,
+                                            static_cast<float2 *>(d_out), static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "ffbp_gate_taper");
+    return FFBP_OK;
+}
+
 int ffbp_mlp_param_count(void) { return ffbp::mlp_param_count(); }
 
 int ffbp_mlp_max_decimation(void) { return ffbp::mlp_max_decimation(); }

@@ -86,6 +86,13 @@ cudaError_t launch_exact_tiles(const float2 *prof, int n, int nfft, int W, const
                                double inv_dr, double kcyc, int cubic, int along1, float2 *win, float2 *out,
                                cudaStream_t st, const char **why);
 
+// The range gate (gate.cu): pad and window a block of pulses, gather the bins about bin 0, taper the kept samples.
+cudaError_t launch_gate_pad(const float2 *S, int n, int K, const float *wp, const float *wk, int npl, int Kp,
+                            float2 *z, int *bad, int p_off, cudaStream_t s);
+cudaError_t launch_gate_fold(const float2 *q, int n, int Kp, int N, float2 *u, cudaStream_t s);
+cudaError_t launch_gate_taper(const float2 *u, int n, int N, int k0, int k1, const float *taper, float2 *out,
+                              cudaStream_t s);
+
 // The learned-tap network (mlp.cu): parameter count, work-buffer bytes for nq queries, the outputs of nq feature
 // rows, and the gradient / Adam step of the decimation loss over ninst instances of S point-target pairs each.
 int mlp_param_count();

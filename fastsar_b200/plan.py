@@ -11,6 +11,7 @@ This is the planner of the reference's factorized backprojection, restated:
 * `positions`           fastsar/ffbp.py:122-125
 * `final_weights`       fastsar/api.py:203-244
 * `plan_signature`      fastsar/ffbp2.py:259-273, `pulse_plan` fastsar/ffbp2.py:252-256
+* `gate_plan`           fastsar/api.py:272-300 (the range gate), with `taper` fastsar/patches.py:156-159
 
 Integers (splits, decimations, filter lengths and offsets, sizes) must equal the reference's exactly and floats to
 1e-12: the level kernels index with them and the image's tile order depends on them. The arithmetic below follows
@@ -261,6 +262,44 @@ def choose_T(ant, fmax, nx, ny, spx, spy, e1, e2, target_db=-40.0, choices=(32, 
         if err <= target_db:
             return T, err
     return choices[-1], err
+
+
+# ------------------------------------------------------------------------------------------------ range gate
+
+def taper(f, band, guard):
+    """1 over the band, a raised cosine to 0 across the guard on either side (fastsar/patches.py:156-159)."""
+    t = np.clip(np.maximum(band[0] - f, f - band[1]) / guard, 0, 1)
+    return 0.5 * (1 + np.cos(np.pi * t))
+
+
+def gate_plan(ant, ref, fmin, df, K, nx, ny, spx, spy, e1, e2):
+    """The range gate of an nx x ny image centred on the origin (fastsar/api.py:272-300): the spectrum padded by a
+    guard of an eighth of the band on either side (npl samples below, Kp in all, a fast FFT length), each pulse's
+    inverse transform cut to the N range bins about its reference range that the image's points span over the
+    aperture (sampled at up to 257 pulses) with a margin of 6 range resolutions of the guard, and the transform back
+    kept over the band and its guards (samples k0 .. k1 - 1 of N), tapered to 0 across the guards. -> dict(npl, Kp,
+    N, k0, k1, taper [k1 - k0] float32 (with the scale Kp / N), fmin, df: of the gated history)."""
+    from scipy.fft import next_fast_len
+    ant = np.asarray(ant, np.float64)
+    e1, e2 = np.asarray(e1, np.float64), np.asarray(e2, np.float64)
+    band = (fmin, fmin + (K - 1) * df)
+    guard = 0.125 * (band[1] - band[0])
+    npl = int(np.ceil(guard / df))
+    Kp = next_fast_len(K + 2 * npl)
+    idx = np.unique(np.linspace(0, len(ant) - 1, min(len(ant), 257)).astype(np.int64))
+    a = ant[idx]
+    r0 = np.linalg.norm(a, axis=1) if ref is None else np.asarray(ref, np.float64)[idx]
+    t = np.linspace(-0.5, 0.5, 5)
+    pts = ((t * nx * spx)[:, None, None] * e1 + (t * ny * spy)[None, :, None] * e2).reshape(-1, 3)
+    half = np.abs(np.linalg.norm(pts[None] - a[:, None], axis=2) - r0[:, None]).max() + 6 * C / (2 * guard)
+    N = next_fast_len(2 * int(np.ceil(half * 2 * Kp * df / C)))
+    N += N % 2
+    df2, f0 = Kp * df / N, fmin - npl * df
+    T = taper(f0 + df2 * np.arange(N), band, guard)
+    keep = np.nonzero(T > 0)[0]
+    k0, k1 = int(keep[0]), int(keep[-1]) + 1
+    return dict(npl=npl, Kp=int(Kp), N=int(N), k0=k0, k1=k1, taper=(T[k0:k1] * (Kp / N)).astype(np.float32),
+                fmin=float(f0 + k0 * df2), df=float(df2))
 
 
 # ------------------------------------------------------------------------------------------------ geometry

@@ -205,6 +205,18 @@ int ffbp_exact_backproject(const void *d_prof, int n, int nfft, int W, const lon
                            int ty, int nx, int ny, double spx, double spy, const double *e1, const double *e2,
                            double inv_dr, double kcyc, int cubic, int along1, void *d_win, void *d_out, void *stream);
 
+/* The range gate (fastsar/ffbp_cuda.py:767-864 and ImageFormer._gate fastsar/api.py:525-564), three steps around the
+ * caller's two FFTs (cuFFT) per block of n pulses: ffbp_gate_pad writes d_z [n, Kp] complex64: zeros, and at
+ * npl .. npl + K - 1 the pulses' samples d_S [n, K] times the window d_wp[p_off + p] d_wk[k] (both or neither), and
+ * lowers *d_bad to the first pulse (p_off + p) with a non-finite sample (d_bad may be NULL); the caller takes the
+ * inverse FFT of each row (scaled by 1 / Kp); ffbp_gate_fold gathers the N bins about bin 0, d_u[p, i] =
+ * d_q[p, i] for i < N - N/2 and d_q[p, Kp - N + i] above; the caller takes the forward FFT of each row;
+ * ffbp_gate_taper writes d_out [n, k1 - k0] = d_u[p, k0 + k] d_taper[k] (the gated history's rows).            */
+int ffbp_gate_pad(const void *d_S, int n, int K, const float *d_wp, const float *d_wk, int npl, int Kp, void *d_z,
+                  int *d_bad, int p_off, void *stream);
+int ffbp_gate_fold(const void *d_q, int n, int Kp, int N, void *d_u, void *stream);
+int ffbp_gate_taper(const void *d_u, int n, int N, int k0, int k1, const float *d_taper, void *d_out, void *stream);
+
 /* The learned-tap network (no counterpart in the reference): an MLP 5 -> 64 -> 64 -> 64 -> 16 (GELU, bfloat16
  * weights and activations, float32 sums) that stands in for the Kaiser-sinc decimation taps of the merge stages
  * (fastsar/ffbp2.py:101-137). A query is one phase q of one axis of a stage's decimation by D: features (phase

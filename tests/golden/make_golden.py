@@ -16,6 +16,9 @@ Fixtures:
   image_<case>.npz    ImageFormer(backend='cpu') images (history, image), ExactFormer(cpu) and backproject(cpu, 64x)
   exact_setup.npz     ExactFormer's set-up (tile, centres, reachable bins) on geometries that pick 32 x 32 and 16 x 16
                       tiles (python tests/golden/make_golden.py --only exact writes this file alone)
+  gate.npz            the range gate: _gate_plan on wide-band and spotlight geometries, the gated history of a seeded
+                      random history (first pulses), and ImageFormer(backend='cpu', range_gate=True)'s image of a
+                      simulated wide-band scene (python tests/golden/make_golden.py --only gate writes this file alone)
 """
 import argparse
 import os
@@ -116,16 +119,80 @@ def exact_setup(sim, ExactFormer):
     np.savez_compressed(os.path.join(HERE, 'exact_setup.npz'), **rec)
 
 
+def wide_band_collection(sim_mod, K=24000, P=384):
+    """An image narrow in range from a wide-band collection (the reference's wide_band case of tests/test_api.py:
+    0.5 m resolution, 30 km, 40 deg grazing)."""
+    res, r0 = 0.5, 30e3
+    df = 299792458.0 / (2 * res) / K
+    y = (np.arange(P) - (P - 1) / 2) * (r0 * 299792458.0 / 9.6e9 / (2 * res) / P)
+    psi = np.radians(40.0)
+    ant = np.stack([np.full(P, -r0 * np.cos(psi)), y, np.full(P, r0 * np.sin(psi))], 1)
+    return sim_mod.Collect(fmin=9.6e9 - (K // 2) * df, df=df, K=K, ant=ant, res=res)
+
+
+def wide_band_scene(seed=3):
+    """5 bright points in the 96 x 96 image at 0.4 m and 200 clutter scatterers over 3 km of range around it."""
+    rng = np.random.default_rng(seed)
+    pts = np.array([[0.0, 0.0, 0], [11.3, -7.1, 0], [-14.2, 12.4, 0], [15.1, 16.2, 0], [-9.3, -15.7, 0]])
+    cl = np.stack([(rng.random(200) - 0.5) * 3000, (rng.random(200) - 0.5) * 60, np.zeros(200)], 1)
+    amp = np.concatenate([np.full(5, 30.0), (rng.standard_normal(200) + 1j * rng.standard_normal(200)) / np.sqrt(2)])
+    return np.concatenate([pts, cl]), amp
+
+
+def gate(fastsar):
+    """The range gate's plan, gated history and a gated image from the reference (fastsar/api.py:272-300, 525-564)."""
+    from fastsar import sim, api
+    from fastsar_b200 import sim as mysim
+    rec = {}
+    col = wide_band_collection(sim)
+    grid = dict(nx=96, ny=96, spx=0.4, spy=0.4, e1=(0.0, 1.0, 0.0), e2=(1.0, 0.0, 0.0))
+    w4 = mysim.workload('spotlight_4k')
+    cases = {'wide': (col, None, grid),
+             'wide_ref': (col, np.linalg.norm(col.ant, axis=1) + 3.0, grid),
+             'wide_rect': (col, None, dict(nx=160, ny=48, spx=0.3, spy=0.5, e1=(0.0, 1.0, 0.0), e2=(1.0, 0.0, 0.0))),
+             'spot4k': (w4['col'], None, dict(nx=256, ny=256, spx=0.25, spy=0.25, e1=w4['e1'], e2=w4['e2']))}
+    for name, (c, ref, g) in cases.items():
+        gp = api._gate_plan(c.ant, ref, float(c.fmin), float(c.df), c.K, g['nx'], g['ny'], g['spx'], g['spy'],
+                            np.asarray(g['e1'], float), np.asarray(g['e2'], float))
+        rec[f'{name}_ant'] = c.ant
+        rec[f'{name}_ref'] = np.zeros(0) if ref is None else ref
+        rec[f'{name}_scal'] = np.array([c.fmin, c.df, c.K, g['nx'], g['ny'], g['spx'], g['spy']], np.float64)
+        rec[f'{name}_e'] = np.array([g['e1'], g['e2']], np.float64)
+        rec[f'{name}_ints'] = np.array([gp['npl'], gp['Kp'], gp['N'], gp['k0'], gp['k1']], np.int64)
+        rec[f'{name}_fl'] = np.array([gp['fmin'], gp['df']])
+        rec[f'{name}_taper'] = gp['taper']
+        print('gate plan', name, rec[f'{name}_ints'])
+    # the gated history of a seeded random history (windowed), its first 8 pulses
+    args = (col.ant, col.fmin, col.df, col.K)
+    f = api.ImageFormer(*args, **grid, backend='cpu', range_gate=True)
+    rng = np.random.default_rng(21)
+    S = (rng.standard_normal((col.ant.shape[0], col.K)) + 1j * rng.standard_normal((col.ant.shape[0], col.K))).astype(np.complex64)
+    rec['hist_gated'] = np.asarray(f._gate(S))[:8]
+    rec['hist_kept'] = np.array(f.range_gate['kept'])
+    # a gated image of a simulated scene (float64 direct sum on the host)
+    pos, amp = wide_band_scene()
+    S = mysim.simulate_brute(wide_band_collection(mysim), pos, amp).astype(np.complex64)
+    rec['img_pos'], rec['img_amp'] = pos, amp
+    rec['img'] = f(S)
+    rec['img_levels'] = np.array(f.levels)
+    rec['img_Dk0'] = np.array(f._plan['levels'][0]['Dk'])
+    print('gated image', rec['img'].shape, 'kept', f.range_gate['kept'], 'levels', f.levels)
+    np.savez_compressed(os.path.join(HERE, 'gate.npz'), **rec)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--ref', default='/root/reference')
-    ap.add_argument('--only', choices=('exact',), default=None)
+    ap.add_argument('--only', choices=('exact', 'gate'), default=None)
     args = ap.parse_args()
     fs = import_reference(args.ref)
     if args.only == 'exact':
         from fastsar import sim
         from fastsar.exact import ExactFormer
         exact_setup(sim, ExactFormer)
+        return
+    if args.only == 'gate':
+        gate(fs)
         return
     from fastsar import sim, ffbp2, ffbp_cpu, bp
     from fastsar.api import ImageFormer, _window
