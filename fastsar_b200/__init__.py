@@ -12,7 +12,7 @@ from .exact import plane_points  # noqa: F401
 
 def __getattr__(name):
     # the formers import torch and load the CUDA library: only when asked for
-    if name in ('ImageFormer', 'form_image'):
+    if name in ('ImageFormer', 'form_image', 'BatchFormer'):
         from . import api
         return getattr(api, name)
     if name in ('ExactFormer', 'backproject'):

@@ -20,7 +20,7 @@ EXPORTS = ('ffbp_last_error', 'ffbp_abi_version', 'ffbp_plan_create', 'ffbp_plan
            'ffbp_bp_points_f64', 'ffbp_simulate', 'ffbp_form_static', 'ffbp_level_tc', 'ffbp_level_tc_scratch_bytes',
            'ffbp_form_profile', 'ffbp_exact_pad', 'ffbp_exact_backproject', 'ffbp_mlp_param_count',
            'ffbp_mlp_max_decimation', 'ffbp_mlp_work_bytes', 'ffbp_plan_host_bytes', 'ffbp_form_host', 'ffbp_gate_pad',
-           'ffbp_gate_fold', 'ffbp_gate_taper', 'ffbp_mlp_taps', 'ffbp_mlp_grad', 'ffbp_mlp_train_step')
+           'ffbp_gate_fold', 'ffbp_gate_taper', 'ffbp_batch_create', 'ffbp_batch_form', 'ffbp_batch_destroy', 'ffbp_mlp_taps', 'ffbp_mlp_grad', 'ffbp_mlp_train_step')
 
 _c_int, _c_double, _vp = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
 
@@ -68,6 +68,10 @@ def load():
     L.ffbp_form.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_size_t, _vp, ctypes.POINTER(_c_int)]
     L.ffbp_form_static.argtypes = [_vp, _vp, _vp, _vp, ctypes.POINTER(_c_int)]
     L.ffbp_plan_host_bytes.argtypes = [_vp, ctypes.POINTER(ctypes.c_size_t)]
+    L.ffbp_batch_create.argtypes = [ctypes.POINTER(_vp), _c_int, ctypes.POINTER(_vp), ctypes.POINTER(_vp),
+                                    ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_size_t), _vp, ctypes.POINTER(_vp)]
+    L.ffbp_batch_form.argtypes = [_vp, _vp, ctypes.POINTER(_c_int)]
+    L.ffbp_batch_destroy.argtypes = [_vp]
     L.ffbp_gate_pad.argtypes = [_vp, _c_int, _c_int, _vp, _vp, _c_int, _c_int, _vp, _vp, _c_int, _vp]
     L.ffbp_gate_fold.argtypes = [_vp, _c_int, _c_int, _c_int, _vp, _vp]
     L.ffbp_gate_taper.argtypes = [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _vp]

@@ -542,6 +542,96 @@ class ImageFormer:
         return img.cpu().numpy()
 
 
+class BatchFormer:
+    """Several formers (patches of uneven sizes, from one or several collections; any precision and taps) formed
+    together by one CUDA graph (ffbp_batch_create): each former's launches on a branch of their own, so that small
+    images' kernels run side by side instead of one image after another, and one graph launch per batch. No
+    counterpart in the reference, which forms a mosaic's patches one at a time (fastsar/patches.py:619-972).
+
+    batch = BatchFormer([former_a, former_b, ...]); images = batch(histories) with host histories (numpy or torch
+    CPU, each [P_i, K_i] complex) -> numpy images; or batch.form_device(device histories or None) -> the device
+    images (None forms what batch.histories hold). The batch owns a device history, image and workspace per
+    former (they run at once). Range-gated formers are not batched (the gate's transforms run outside the graph)."""
+
+    def __init__(self, formers):
+        import torch
+        L = _lib.load()
+        self.formers = list(formers)
+        if not self.formers:
+            raise ValueError('BatchFormer needs at least one former')
+        for i, f in enumerate(self.formers):
+            if not isinstance(f, ImageFormer):
+                raise TypeError(f'former {i} is not an ImageFormer')
+            if f.range_gate is not None:
+                raise ValueError(f'former {i} gates its history in range, which a batch does not run; '
+                                 'form it alone')
+        devs = {f._dev.device for f in self.formers}
+        if len(devs) != 1:
+            raise ValueError('the formers of a batch must be on one device')
+        self.device = devs.pop()
+        n = len(self.formers)
+        self.histories = [torch.empty((f.P, f.K), dtype=torch.complex64, device=self.device) for f in self.formers]
+        self.images = [torch.empty((f.nx, f.ny), dtype=torch.complex64, device=self.device) for f in self.formers]
+        vp = ctypes.c_void_p
+        plans = (vp * n)(*[f._dev.handle.value for f in self.formers])
+        S = (vp * n)(*[h.data_ptr() for h in self.histories])
+        I = (vp * n)(*[m.data_ptr() for m in self.images])
+        W = (vp * n)(*[f._dev.workspace() for f in self.formers])
+        nb = (ctypes.c_size_t * n)(*[f._dev.ws_bytes for f in self.formers])
+        h = vp()
+        with torch.cuda.device(self.device):
+            stream = torch.cuda.current_stream(self.device)
+            _lib.check(L.ffbp_batch_create(plans, n, S, I, W, nb, vp(stream.cuda_stream), ctypes.byref(h)),
+                       'ffbp_batch_create')
+        self.handle = h
+
+    def __del__(self):
+        if getattr(self, 'handle', None) is not None and self.handle.value:
+            try:
+                _lib.load().ffbp_batch_destroy(self.handle)
+            except Exception:
+                pass
+            self.handle = None
+
+    def form_device(self, histories=None, check=True):
+        """Device histories (torch tensors [P_i, K_i], complex) copied into the batch's buffers, or None for what
+        they hold; one graph launch forms every image -> the batch's device images. check: wait and raise
+        ValueError naming the first image with a non-finite sample."""
+        import torch
+        L = _lib.load()
+        if histories is not None:
+            if len(histories) != len(self.formers):
+                raise ValueError(f'{len(self.formers)} formers but {len(histories)} histories')
+            for i, (S, buf) in enumerate(zip(histories, self.histories)):
+                if tuple(S.shape) != tuple(buf.shape):
+                    raise ValueError(f'phase history {i} must be {tuple(buf.shape)}, got {tuple(S.shape)}')
+                buf.copy_(S, non_blocking=True)
+        n = len(self.formers)
+        stream = torch.cuda.current_stream(self.device)
+        bad = (ctypes.c_int * n)() if check else None
+        _lib.check(L.ffbp_batch_form(self.handle, ctypes.c_void_p(stream.cuda_stream), bad), 'ffbp_batch_form')
+        if check:
+            for i, b in enumerate(bad):
+                if b >= 0:
+                    raise ValueError(f'phase history {i} has non-finite samples (NaN or inf), the first in pulse {b}; '
+                                     'zero them (S[~np.isfinite(S)] = 0) or drop the pulses')
+        return self.images
+
+    def __call__(self, histories):
+        """Host histories -> numpy images."""
+        import torch
+        ts = []
+        for i, (S, f) in enumerate(zip(histories, self.formers)):
+            if not isinstance(S, torch.Tensor):
+                S = _check_history(np.asarray(S), f.P)
+                S = torch.from_numpy(np.ascontiguousarray(S, np.complex64))
+            ts.append(S)
+        if len(ts) != len(self.formers):
+            raise ValueError(f'{len(self.formers)} formers but {len(ts)} histories')
+        imgs = self.form_device([t.to(self.device, torch.complex64) for t in ts])
+        return [m.cpu().numpy() for m in imgs]
+
+
 def form_image(S, ant, fmin, df, nx, ny, spx, spy, e1=(1.0, 0.0, 0.0), e2=(0.0, 1.0, 0.0), *, algorithm='ffbp',
                backend='auto', precision='float32', window=True, T='auto', levels=None, pmax=0.4, pfa_guard=300.0,
                pfa_support='union', target_db=-40.0, ref=None, interp=None, upsample=None, center=None,

@@ -441,6 +441,113 @@ int ffbp_form_host(ffbp_plan *p, const void *const *h_S, void *const *h_img, int
     return FFBP_OK;
 }
 
+}  // extern "C"
+
+// A batch: the form calls of n plans captured once into a CUDA graph, each plan's launches on a branch of its own
+// (forked from and joined to the capturing stream), so that the kernels of different plans run side by side and one
+// graph launch replaces them all.
+struct ffbp_batch {
+    int n = 0;
+    std::vector<const int *> status;     // each plan's workspace status words (first non-finite pulse, wait status)
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int *h_status = nullptr;             // page-locked, 2 n ints
+    ~ffbp_batch()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (h_status) cudaFreeHost(h_status);
+    }
+};
+
+extern "C" {
+
+int ffbp_batch_create(ffbp_plan *const *plans, int n, const void *const *d_S, void *const *d_img, void *const *d_ws,
+                      const size_t *ws_bytes, void *stream, ffbp_batch **out)
+{
+    if (!plans || !d_S || !d_img || !d_ws || !ws_bytes || !out || n < 1) return fail(FFBP_E_ARG, "ffbp_batch_create: bad arguments");
+    *out = nullptr;
+    for (int i = 0; i < n; ++i) {
+        if (!plans[i] || !d_S[i] || !d_img[i] || !d_ws[i]) return fail(FFBP_E_ARG, "ffbp_batch_create: null entry %d", i);
+        size_t need;
+        ffbp_plan_workspace_bytes(plans[i], &need);
+        if (ws_bytes[i] < need) return fail(FFBP_E_WORKSPACE, "plan %d: workspace of %zu bytes, %zu needed", i, ws_bytes[i], need);
+        if (((uintptr_t)d_ws[i] & 255) != 0) return fail(FFBP_E_ARG, "plan %d: workspace must be 256-byte aligned", i);
+    }
+    (void)stream;                        // nothing runs here: the graph is captured on a stream of the call's own
+    ffbp_batch *b = new ffbp_batch;
+    b->n = n;
+    cudaStream_t s = nullptr;            // the capturing stream (the legacy default stream cannot capture)
+    std::vector<cudaStream_t> br(n, nullptr);
+    std::vector<cudaEvent_t> joined(n, nullptr);
+    cudaEvent_t fork = nullptr;
+    cudaError_t e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    for (int i = 0; i < n && e == cudaSuccess; ++i) {
+        e = cudaStreamCreateWithFlags(&br[i], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&joined[i], cudaEventDisableTiming);
+    }
+    auto cleanup = [&]() {
+        for (int i = 0; i < n; ++i) {
+            if (joined[i]) cudaEventDestroy(joined[i]);
+            if (br[i]) cudaStreamDestroy(br[i]);
+        }
+        if (fork) cudaEventDestroy(fork);
+        if (s) cudaStreamDestroy(s);
+    };
+    if (e != cudaSuccess) { cleanup(); delete b; return cuda_fail(e, "ffbp_batch_create: streams"); }
+    int rc = FFBP_OK;
+    // capture: relaxed, since the tensor-core launchers set their kernels' shared-memory attribute as they launch
+    if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed)) != cudaSuccess) { cleanup(); delete b; return cuda_fail(e, "ffbp_batch_create: capture"); }
+    e = cudaEventRecord(fork, s);
+    for (int i = 0; i < n && e == cudaSuccess && rc == FFBP_OK; ++i) {
+        if ((e = cudaStreamWaitEvent(br[i], fork, 0)) != cudaSuccess) break;
+        rc = form_impl(plans[i], d_S[i], d_img[i], d_ws[i], ws_bytes[i], br[i], nullptr, nullptr);
+        if (rc != FFBP_OK) break;
+        if ((e = cudaEventRecord(joined[i], br[i])) != cudaSuccess) break;
+        e = cudaStreamWaitEvent(s, joined[i], 0);
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(s, &g);
+    if (rc == FFBP_OK && e == cudaSuccess && e2 == cudaSuccess) e = cudaGraphInstantiate(&b->exec, g, 0);
+    b->graph = g;
+    cleanup();
+    if (rc != FFBP_OK) { delete b; return rc; }
+    if (e != cudaSuccess || e2 != cudaSuccess) { delete b; return cuda_fail(e != cudaSuccess ? e : e2, "ffbp_batch_create: graph"); }
+    for (int i = 0; i < n; ++i) b->status.push_back(static_cast<const int *>(d_ws[i]));
+    if ((e = cudaHostAlloc(reinterpret_cast<void **>(&b->h_status), 2 * (size_t)n * sizeof(int), cudaHostAllocDefault)) != cudaSuccess) {
+        delete b;
+        return cuda_fail(e, "ffbp_batch_create: status array");
+    }
+    *out = b;
+    return FFBP_OK;
+}
+
+int ffbp_batch_form(ffbp_batch *b, void *stream, int *h_bad)
+{
+    if (!b) return fail(FFBP_E_ARG, "ffbp_batch_form: null batch");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaGraphLaunch(b->exec, s);
+    if (e != cudaSuccess) return cuda_fail(e, "ffbp_batch_form");
+    if (!h_bad) return FFBP_OK;
+    for (int i = 0; i < b->n && e == cudaSuccess; ++i)
+        e = cudaMemcpyAsync(b->h_status + 2 * i, b->status[i], 2 * sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(e, "ffbp_batch_form");
+    for (int i = 0; i < b->n; ++i) {
+        h_bad[i] = b->h_status[2 * i] == 0x7f7f7f7f ? -1 : b->h_status[2 * i];
+        if (b->h_status[2 * i + 1])
+            return fail(FFBP_E_CUDA, "image %d: a tensor-core kernel stopped waiting on its pipeline (a bounded wait ran out)", i);
+    }
+    return FFBP_OK;
+}
+
+int ffbp_batch_destroy(ffbp_batch *b)
+{
+    delete b;
+    return FFBP_OK;
+}
+
 int ffbp_form(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, size_t ws_bytes, void *stream, int *h_bad)
 {
     return form_impl(p, d_S, d_img, d_ws, ws_bytes, stream, h_bad, nullptr);

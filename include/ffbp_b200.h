@@ -129,6 +129,19 @@ int ffbp_plan_host_bytes(const ffbp_plan *plan, size_t *bytes);
 int ffbp_form_host(ffbp_plan *plan, const void *const *h_S, void *const *h_img, int n, void *d_stage,
                    size_t stage_bytes, void *d_ws, size_t ws_bytes, void *stream, int *h_bad);
 
+/* A batch: n plans (patches of uneven sizes, of one or several collections) formed together. ffbp_batch_create
+ * captures the n form calls once into a CUDA graph, each plan's launches on a branch of its own so that the kernels
+ * of different plans run side by side, on the buffers given here: d_S[i] (plan i's history), d_img[i] (its image),
+ * d_ws[i] (its workspace of ws_bytes[i], 256-byte aligned; one per plan, they run at once). The call runs no
+ * kernel (it captures on a stream of its own; `stream` is unused). ffbp_batch_form launches the graph on `stream` (the buffers' current contents are formed); with h_bad
+ * (n ints) it waits and writes each image's first non-finite pulse (or -1). No counterpart in the reference,
+ * which forms patches one after the other (fastsar/patches.py:619-972).                                      */
+typedef struct ffbp_batch ffbp_batch;
+int ffbp_batch_create(ffbp_plan *const *plans, int n, const void *const *d_S, void *const *d_img, void *const *d_ws,
+                      const size_t *ws_bytes, void *stream, ffbp_batch **out);
+int ffbp_batch_form(ffbp_batch *batch, void *stream, int *h_bad);
+int ffbp_batch_destroy(ffbp_batch *batch);
+
 /* ffbp_form without a caller-allocated workspace, for callers that cannot allocate device memory when they form an
  * image (a device pool they do not control, a real-time loop that must not enter the CUDA allocator). No counterpart
  * in the reference. The scratch is a static device array of this library, FFBP_STATIC_WS_BYTES (64 MiB), held by
