@@ -64,13 +64,14 @@ def tap_offsets(D):
     return phases(D)[:, None] - 4.0 + np.arange(8)[None, :]
 
 
-def loss_and_grad(params, x, prior, scale, inst, f, y, rounding=True):
-    """The decimation loss of the learned taps and its gradients [(dW, db), ...] (float64): returns (sum |v - y|^2,
-    grads of the mean). Instance i = (first query q0, D, axis) of inst [ninst, 3] uses the taps prior[q0 + q, n] +
-    scale * out[q0 + q, 8 axis + n] at offsets tap_offsets(D)[q, n]; pair s of the instance (f [ninst, S] cycles per
-    output sample, y [ninst, S] complex) decimates to v = (1 / D) sum_{q, n} tap e^{2 pi i f t}. The rounding of the
-    forward pass is passed straight through: the gradient is that of the smooth network evaluated at the rounded
-    weights and activations."""
+def loss_and_grad(params, x, prior, scale, inst, weight, f, y, rounding=True):
+    """The decimation loss of the learned taps and its gradients [(dW, db), ...] (float64): returns
+    (sum weight |v - y|^2, grads of the mean). Instance i = (first query q0, D, axis) of inst [ninst, 3] uses the taps
+    prior[q0 + q, n] + scale * out[q0 + q, 8 axis + n] at offsets tap_offsets(D)[q, n]; pair s of the instance
+    (f [ninst, S] cycles per output sample, y [ninst, S] complex) decimates to v = (1 / D) sum_{q, n} tap
+    e^{2 pi i f t}; the instance's pairs weigh weight[i] (None: 1). The rounding of the forward pass is passed
+    straight through: the gradient is that of the smooth network evaluated at the rounded weights and
+    activations."""
     out, cache = forward(params, x, rounding)
     ninst, S = f.shape
     dout = np.zeros_like(out)
@@ -80,8 +81,9 @@ def loss_and_grad(params, x, prior, scale, inst, f, y, rounding=True):
         X = np.exp(2j * np.pi * f[i][:, None, None] * tap_offsets(D)[None])          # [S, D, 8]
         v = np.einsum('sqn,qn->s', X, taps) / D
         e = v - y[i]
-        total += float(np.sum(np.abs(e) ** 2))
-        g = np.real(np.conj(e)[:, None, None] * X).sum(0) * (2.0 / (ninst * S)) / D
+        wi = 1.0 if weight is None else float(weight[i])
+        total += wi * float(np.sum(np.abs(e) ** 2))
+        g = wi * np.real(np.conj(e)[:, None, None] * X).sum(0) * (2.0 / (ninst * S)) / D
         dout[q0:q0 + D, 8 * ax:8 * ax + 8] += scale * g
     d = dout
     grads = [None] * len(params)
