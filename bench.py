@@ -25,6 +25,9 @@ backprojection at 64x on random pixels.
 --gpus N (torchrun, one process per GPU): every rank forms its own collection (independent replicas; weak
 scaling); the step time is the maximum over ranks and the value counts every rank's backprojections.
 
+--workload patches_48: the batched form instead (run_patches): 48 autotuned patches of uneven sizes from 6
+collections formed by one CUDA graph, against the same formers one after another and patch-by-patch plain FFBP.
+
 --impl reference: the reference's own CPU implementation (its fastsar/ffbp_cpu.cpp kernels, compiled from its
 sources by oracle/Makefile, driven by the oracle's restatement of its host orchestration) on this host's cores, on
 a bounded sample of the same workload: a fixed subset of the first level's children, whose work is a fixed
@@ -43,6 +46,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+C = 299792458.0
 METRIC = 'giga-backprojections/s at ≤-60 dB vs FP64: chosen form vs plain FFBP on B200'
 CHOSEN_PMAX = 0.5           # the chosen form's oversampling parameter (the reference's default is 0.4)
 FP32_PEAK_NOMINAL = 148 * 128 * 2 * 1.965e9 / 1e12      # TFLOP/s, FP32 FMA on the CUDA cores at the maximum clock
@@ -185,6 +189,8 @@ def main():
 
     if args.impl == 'reference':
         return run_reference(args, world, rank)
+    if args.workload.startswith('patches'):
+        return run_patches(args)
 
     import torch
     import torch.distributed as dist
@@ -353,6 +359,120 @@ def main():
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def run_patches(args):
+    """--workload patches_48: a batch of 48 uneven patches from 6 collections (sim.patch_workload). Each patch's plan
+    is autotuned (fastsar_b200.tune: the chosen form's candidates where its predicted error meets -60 dB, the float32
+    former's with learned taps otherwise); the batch is formed by one CUDA graph (BatchFormer) and timed against the same formers one
+    patch after another and against patch-by-patch plain float32 FFBP with the reference's plans. Errors per patch
+    against the float64 exact backprojection (64x) on random pixels. One GPU; prints one JSON line."""
+    import torch
+    from fastsar_b200 import sim, ImageFormer, BatchFormer, tune
+    from fastsar_b200.exact import backproject_device, plane_points
+    torch.cuda.set_device(0)
+    wl = sim.patch_workload(args.workload, seed=args.seed)
+    t0 = time.time()
+    hist, specs = [], []
+    for ci, c in enumerate(wl):
+        col = c['col']
+        ea, er = c['extent']
+        rng = np.random.default_rng(args.seed + 7 * ci)
+        sc = c['scene']
+        res = (C / (2.0 * col.K * col.df), c['sp'])
+        pos, amp = sim.scene(rng, ea / c['sp'], er / c['sp'], c['sp'], c['sp'], c['e1'], c['e2'],
+                             n_points=sc['n_points'], rcs_sigma_db=sc['rcs_sigma_db'], n_corners=sc['n_corners'],
+                             clutter_db=sc['clutter_db'], res=res, col=col, fill=1.0, max_clutter=100000)
+        g = torch.Generator(device='cuda')
+        g.manual_seed(args.seed + ci)
+        S = torch.view_as_complex(torch.randn((col.Np, col.K, 2), device='cuda', generator=g) *
+                                  (10.0 ** (sc['noise_db'] / 20.0) / np.sqrt(2.0))).contiguous()
+        sim.simulate(col, pos, amp, out=S)
+        hist.append(S)
+        r0 = np.linalg.norm(col.ant, axis=1)
+        for (ca, cr, na, nr) in c['patches']:
+            cen = ca * np.asarray(c['e1']) + cr * np.asarray(c['e2'])
+            specs.append(dict(ci=ci, cen=cen, nx=na, ny=nr, sp=c['sp'], e1=c['e1'], e2=c['e2'], ant=col.ant - cen,
+                              r0=r0, col=col))
+    torch.cuda.synchronize()
+    log(f'[bench] {len(wl)} histories, {len(specs)} patches in {time.time() - t0:.1f} s')
+
+    def make(sp, **kw):
+        col = sp['col']
+        return ImageFormer(sp['ant'], col.fmin, col.df, col.K, sp['nx'], sp['ny'], sp['sp'], sp['sp'], sp['e1'],
+                           sp['e2'], ref=sp['r0'], **kw)
+
+    t1 = time.time()
+    chosen, choices = [], []
+    for sp in specs:
+        f, kw, _ = tune.tune_former(lambda **kw: make(sp, **kw), tune.CHOSEN + tune.FLOAT32, hist[sp['ci']],
+                                    target_db=-60.0, reps=2)
+        chosen.append(f)
+        choices.append(kw)
+    log(f'[bench] autotuned {len(specs)} patches in {time.time() - t1:.1f} s')
+    plain = [make(sp) for sp in specs]
+    bp = sum(sp['nx'] * sp['ny'] * sp['col'].Np for sp in specs)
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    outs_c = [torch.empty((f.nx, f.ny), dtype=torch.complex64, device='cuda') for f in chosen]
+    outs_p = [torch.empty((f.nx, f.ny), dtype=torch.complex64, device='cuda') for f in plain]
+
+    def seq(formers, outs):
+        def run():
+            for f, sp, o in zip(formers, specs, outs):
+                f.form_device(hist[sp['ci']], o, check=False)
+        return run
+    ms_plain = timed(seq(plain, outs_p), args.steps, args.warmup)
+    for f in plain:
+        f.release()
+    del outs_p
+    torch.cuda.empty_cache()
+    ms_seq = timed(seq(chosen, outs_c), args.steps, args.warmup)
+    batch = BatchFormer(chosen, sources=[sp['ci'] for sp in specs])
+    for k, S in enumerate(hist):
+        batch.histories[k].copy_(S)
+    ms_batch = timed(lambda: batch.form_device(check=False), args.steps, args.warmup)
+    imgs = batch.form_device()
+    # errors against float64 64x on random pixels of every patch
+    errs = []
+    rng = np.random.default_rng(5)
+    for f, sp, img in zip(chosen, specs, imgs):
+        n = f.nx * f.ny
+        idx = rng.choice(n, size=min(256, n), replace=False)
+        pts = plane_points(f.nx, f.ny, sp['sp'], sp['sp'], sp['e1'], sp['e2']).reshape(-1, 3)[idx] + sp['cen']
+        ref = backproject_device(hist[sp['ci']], sp['col'].ant, sp['col'].fmin, sp['col'].df, pts,
+                                 upsample=64).cpu().numpy()
+        a = img.reshape(-1)[torch.from_numpy(idx).cuda()].cpu().numpy().astype(np.complex128)
+        errs.append(float(10 * np.log10(np.sum(np.abs(a - ref) ** 2) / np.sum(np.abs(ref) ** 2))))
+    kinds = {}
+    for kw in choices:
+        key = f"{kw['precision']}" + (f"+{kw['taps']}" if 'taps' in kw else '') + f" T{kw['T']} L{kw['levels']}"
+        kinds[key] = kinds.get(key, 0) + 1
+    line = dict(
+        metric='aggregate giga-backprojections/s of 48 uneven patches from 6 collections, one CUDA graph',
+        value=bp / (ms_batch * 1e-3) / 1e9, unit='GBP/s', n_gpus=1, steps=args.steps, warmup=args.warmup,
+        ms_per_step=ms_batch, higher_is_better=True, scaling='weak', vs_baseline=None,
+        dtype='per patch: the chosen form (bf16x3 / f16 tensor products, f32 accumulation) or float32',
+        data='synthetic: 6 seeded spotlight collections simulated on the GPU in float64, noise -40 dB',
+        config=dict(workload='patches_48: 48 patches, sides 256-4096 px (log-uniform, within the unambiguous '
+                             'extents), from 6 collections of 2048-16384 pulses x 2048-8192 samples',
+                    patches=len(specs), collections=len(wl), backprojections=bp, plans=kinds),
+        sequential_ms=ms_seq, plain_fp32_patch_by_patch=dict(ms_per_step=ms_plain, value=bp / (ms_plain * 1e-3) / 1e9),
+        speedup_vs_plain=ms_plain / ms_batch, speedup_vs_sequential=ms_seq / ms_batch,
+        err_db=dict(max=max(errs), median=float(np.median(errs)), per_patch=[round(e, 1) for e in errs],
+                    reference='float64 exact backprojection, 64x, 256 random pixels per patch, no gain fitted'))
+    print(json.dumps(line), flush=True)
 
 
 def run_reference(args, world, rank):

@@ -432,6 +432,13 @@ class ImageFormer:
         self._S.copy_(torch.from_numpy(S), non_blocking=False)
         return self._S
 
+    def release(self):
+        """Return the former's device buffers (workspace, staging, gate) to the allocator; the next call makes
+        them again."""
+        self._dev.release_workspace()
+        self._S = None
+        self._gate_dev = None
+
     def _gate(self, S_dev):
         """The range gate on the device (fastsar/api.py:525-564, fastsar/ffbp_cuda.py:767-864): S_dev [P, K]
         complex64 -> the gated history [P, kept] complex64 (a buffer of the former), windowed; in blocks of pulses
@@ -550,10 +557,12 @@ class BatchFormer:
 
     batch = BatchFormer([former_a, former_b, ...]); images = batch(histories) with host histories (numpy or torch
     CPU, each [P_i, K_i] complex) -> numpy images; or batch.form_device(device histories or None) -> the device
-    images (None forms what batch.histories hold). The batch owns a device history, image and workspace per
-    former (they run at once). Range-gated formers are not batched (the gate's transforms run outside the graph)."""
+    images (None forms what batch.histories hold). sources[i]: the history former i forms from (formers of patches
+    of one collection share it; default: a history per former); the histories passed are then one per source. The
+    batch owns a device history per source and an image and a workspace per former (they run at once).
+    Range-gated formers are not batched (the gate's transforms run outside the graph)."""
 
-    def __init__(self, formers):
+    def __init__(self, formers, sources=None):
         import torch
         L = _lib.load()
         self.formers = list(formers)
@@ -570,11 +579,20 @@ class BatchFormer:
             raise ValueError('the formers of a batch must be on one device')
         self.device = devs.pop()
         n = len(self.formers)
-        self.histories = [torch.empty((f.P, f.K), dtype=torch.complex64, device=self.device) for f in self.formers]
+        self.sources = list(range(n)) if sources is None else [int(x) for x in sources]
+        if len(self.sources) != n or min(self.sources) < 0:
+            raise ValueError(f'sources must give each of the {n} formers a history index')
+        shapes = {}
+        for f, src in zip(self.formers, self.sources):
+            if shapes.setdefault(src, (f.P, f.K)) != (f.P, f.K):
+                raise ValueError(f'formers sharing history {src} differ in pulses or samples')
+        if sorted(shapes) != list(range(len(shapes))):
+            raise ValueError('sources must number the histories 0, 1, ... without gaps')
+        self.histories = [torch.empty(shapes[k], dtype=torch.complex64, device=self.device) for k in range(len(shapes))]
         self.images = [torch.empty((f.nx, f.ny), dtype=torch.complex64, device=self.device) for f in self.formers]
         vp = ctypes.c_void_p
         plans = (vp * n)(*[f._dev.handle.value for f in self.formers])
-        S = (vp * n)(*[h.data_ptr() for h in self.histories])
+        S = (vp * n)(*[self.histories[k].data_ptr() for k in self.sources])
         I = (vp * n)(*[m.data_ptr() for m in self.images])
         W = (vp * n)(*[f._dev.workspace() for f in self.formers])
         nb = (ctypes.c_size_t * n)(*[f._dev.ws_bytes for f in self.formers])
@@ -600,8 +618,8 @@ class BatchFormer:
         import torch
         L = _lib.load()
         if histories is not None:
-            if len(histories) != len(self.formers):
-                raise ValueError(f'{len(self.formers)} formers but {len(histories)} histories')
+            if len(histories) != len(self.histories):
+                raise ValueError(f'{len(self.histories)} histories expected, got {len(histories)}')
             for i, (S, buf) in enumerate(zip(histories, self.histories)):
                 if tuple(S.shape) != tuple(buf.shape):
                     raise ValueError(f'phase history {i} must be {tuple(buf.shape)}, got {tuple(S.shape)}')
@@ -613,21 +631,22 @@ class BatchFormer:
         if check:
             for i, b in enumerate(bad):
                 if b >= 0:
-                    raise ValueError(f'phase history {i} has non-finite samples (NaN or inf), the first in pulse {b}; '
-                                     'zero them (S[~np.isfinite(S)] = 0) or drop the pulses')
+                    raise ValueError(f'phase history {self.sources[i]} (image {i}) has non-finite samples (NaN or '
+                                     f'inf), the first in pulse {b}; zero them (S[~np.isfinite(S)] = 0) or drop the '
+                                     'pulses')
         return self.images
 
     def __call__(self, histories):
-        """Host histories -> numpy images."""
+        """Host histories (one per source) -> numpy images."""
         import torch
         ts = []
-        for i, (S, f) in enumerate(zip(histories, self.formers)):
+        for i, (S, buf) in enumerate(zip(histories, self.histories)):
             if not isinstance(S, torch.Tensor):
-                S = _check_history(np.asarray(S), f.P)
+                S = _check_history(np.asarray(S), buf.shape[0])
                 S = torch.from_numpy(np.ascontiguousarray(S, np.complex64))
             ts.append(S)
-        if len(ts) != len(self.formers):
-            raise ValueError(f'{len(self.formers)} formers but {len(ts)} histories')
+        if len(ts) != len(self.histories):
+            raise ValueError(f'{len(self.histories)} histories expected, got {len(ts)}')
         imgs = self.form_device([t.to(self.device, torch.complex64) for t in ts])
         return [m.cpu().numpy() for m in imgs]
 

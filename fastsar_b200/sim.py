@@ -204,6 +204,49 @@ def workload(name):
     raise ValueError(f'unknown workload {name!r}')
 
 
+def patch_workload(name='patches_48', seed=0):
+    """A batch of uneven image patches from several spotlight collections -> list of dict(col, e1, e2, sp, extent,
+    patches=[(ca, cr, na, nr)] (centre along e1 and e2 in metres, pixels along e1 and e2), scene).
+
+    patches_48: 48 patches (8 per collection) with sides drawn log-uniform from 256 to 4,096 pixels (seeded, each side
+    held within 80 % of the range and cross-range extents the collection leaves unambiguous), cut from 6 X-band
+    spotlight collections of 2,048-16,384 pulses x 2,048-8,192 samples (powers of two), apertures of 1-4 deg,
+    bandwidths of 0.6-1.2 GHz, 20-500 km, 35-55 deg grazing; pixel spacing the coarser of the two resolutions (in
+    steps of 5 cm); each collection's scene 2,000 log-normal targets (sigma 10 dB) and 10 corners at +40 dB over
+    -25 dB clutter across its patches' extent, noise -40 dB."""
+    if name != 'patches_48':
+        raise ValueError(f'unknown patch workload {name!r}')
+    rng = np.random.default_rng(1000 + seed)
+    out = []
+    for ci in range(6):
+        P = int(2 ** rng.integers(11, 15))
+        K = int(2 ** rng.integers(11, 14))
+        ap = float(rng.uniform(1.0, 4.0))
+        bw = float(rng.uniform(0.6e9, 1.2e9))
+        r0 = float(rng.choice([20e3, 100e3, 500e3]))
+        graze = float(rng.uniform(35.0, 55.0))
+        col = spotlight(P, K, 9.6e9, bw, r0, graze, ap)
+        res_r = C / (2.0 * bw) / np.cos(np.deg2rad(graze))
+        lam = C / 9.6e9
+        res_a = lam / (2.0 * np.deg2rad(ap))
+        sp = float(np.ceil(max(res_r, res_a) / 0.05) * 0.05)
+        swath_r = K * (C / (2.0 * bw)) / np.cos(np.deg2rad(graze))      # unambiguous ground range
+        swath_a = lam / (2.0 * np.deg2rad(ap) / P)                        # unambiguous cross range
+        lim_r, lim_a = int(0.8 * swath_r / sp), int(0.8 * swath_a / sp)
+        ext_r, ext_a = 0.8 * swath_r, 0.8 * swath_a
+        patches = []
+        for _ in range(8):
+            na = int(min(lim_a, np.exp(rng.uniform(np.log(256), np.log(4096)))))
+            nr = int(min(lim_r, np.exp(rng.uniform(np.log(256), np.log(4096)))))
+            ca = float(rng.uniform(-0.5, 0.5) * max(0.0, ext_a - na * sp))
+            cr = float(rng.uniform(-0.5, 0.5) * max(0.0, ext_r - nr * sp))
+            patches.append((ca, cr, na, nr))
+        out.append(dict(col=col, e1=(0.0, 1.0, 0.0), e2=(1.0, 0.0, 0.0), sp=sp, extent=(ext_a, ext_r),
+                        patches=patches, scene=dict(n_points=2000, rcs_sigma_db=10.0, n_corners=10,
+                                                    clutter_db=-25.0, noise_db=-40.0)))
+    return out
+
+
 def simulate(col, pos, amp, out=None, device=None, chunk=65536):
     """Phase history [P, K] complex64 on the GPU (a torch tensor) by the direct sum over scatterers, float64 ranges
     and phases, through ffbp_simulate (fastsar/sim.py:69-90 computes the same sum with a NUFFT). out: a tensor to add

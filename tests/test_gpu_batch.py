@@ -49,6 +49,12 @@ def test_batch_matches_formers_alone(golden):
     hs[3][11, 7] = np.nan
     with pytest.raises(ValueError, match='phase history 3 .*pulse 11'):
         batch(hs)
+    # the spotlight's patches sharing one device history
+    shared = BatchFormer([f for f, _ in pairs], sources=[0, 0, 0, 0, 0, 1])
+    got = shared([pairs[0][1], pairs[-1][1]])
+    assert all(np.array_equal(a, b) for a, b in zip(got, want))
+    with pytest.raises(ValueError, match='differ'):
+        BatchFormer([f for f, _ in pairs], sources=[0, 0, 0, 0, 0, 0])
 
 
 def test_batch_refuses_gated_formers():
