@@ -8,7 +8,8 @@ samples and random child phases, through ffbp_level_tc (tensor cores: its two la
 level_fir) or ffbp_level (float32: level_kernel); `--pulses` shortens the pulse axis (the pulse filter is then
 designed for the shorter axis by the same rule). `final`: the final stage through ffbp_final on `--tiles` tiles of
 the plan's final shape with random samples and geometry. Each prints the event-timed duration of every repetition.
-The defaults are the 16,384 x 8,192 -> 12,288 x 8,832 spotlight (workload spotlight_12k) with the learned taps.
+The defaults are the 16,384 x 8,192 -> 12,288 x 8,832 spotlight (workload spotlight_12k) planned as the chosen form
+(learned taps, pmax 0.5); --pmax 0.4 --taps 70 gives the reference's plan.
 """
 import argparse
 
@@ -19,9 +20,10 @@ from . import plan as _plan
 from . import sim
 
 
-def workload_plan(name='spotlight_12k', taps='learned'):
+def workload_plan(name='spotlight_12k', taps='learned', pmax=0.5):
     """The plan of a named workload with learned taps ('learned', Kaiser-sinc fallback at 80 dB) or Kaiser-sinc
-    filters at the given attenuation."""
+    filters at the given attenuation, at oversampling parameter pmax (0.5: the chosen form's; 0.4: the
+    reference's default)."""
     w = sim.workload(name)
     model = None
     atten = 80.0
@@ -30,14 +32,14 @@ def workload_plan(name='spotlight_12k', taps='learned'):
         model = LearnedTaps.load()
     else:
         atten = float(taps)
-    return w, _plan.make_plan(w['col'], w['nx'], w['ny'], w['spx'], w['spy'], T=32, nlev=3, atten=atten, e1=w['e1'],
-                              e2=w['e2'], taps=model)
+    return w, _plan.make_plan(w['col'], w['nx'], w['ny'], w['spx'], w['spy'], T=32, nlev=3, pmax=pmax, atten=atten,
+                              e1=w['e1'], e2=w['e2'], taps=model)
 
 
-def level_case(level, parents, pulses=0, form='tc', taps='learned', reps=3, seed=1):
+def level_case(level, parents, pulses=0, form='tc', taps='learned', reps=3, seed=1, pmax=0.5):
     import torch
     L = _lib.load()
-    w, pl = workload_plan(taps=taps)
+    w, pl = workload_plan(taps=taps, pmax=pmax)
     lv = pl['levels'][level]
     P, K, C, Ko, Po, Dk, Dp = lv['P'], lv['K'], lv['C'], lv['Ko'], lv['Po'], lv['Dk'], lv['Dp']
     fk, fp = lv['fir_k'], lv['fir_p']
@@ -81,10 +83,10 @@ def level_case(level, parents, pulses=0, form='tc', taps='learned', reps=3, seed
               f'Lk={fk["L"]} Lp={fp["L"]}: {e0.elapsed_time(e1):.3f} ms', flush=True)
 
 
-def final_case(tiles, mode='f16', taps='learned', reps=2, seed=2):
+def final_case(tiles, mode='f16', taps='learned', reps=2, seed=2, pmax=0.5):
     import torch
     L = _lib.load()
-    w, pl = workload_plan(taps=taps)
+    w, pl = workload_plan(taps=taps, pmax=pmax)
     f = pl['final']
     Pf, Qf, T = f['P'], f['K'], pl['T']
     m = {'fp32': _lib.FFBP_FINAL_FP32, 'f16': _lib.FFBP_FINAL_TC_F16, 'bf16x3': _lib.FFBP_FINAL_TC_BF16X3}[mode]
@@ -120,11 +122,12 @@ def main(argv=None):
     ap.add_argument('--mode', choices=('f16', 'bf16x3', 'fp32'), default='f16')
     ap.add_argument('--taps', default='learned', help="'learned' or a Kaiser-sinc attenuation in dB (70, 80)")
     ap.add_argument('--reps', type=int, default=3)
+    ap.add_argument('--pmax', type=float, default=0.5)
     a = ap.parse_args(argv)
     if a.stage == 'level':
-        level_case(int(a.level[1]), a.parents, a.pulses, a.form, a.taps, a.reps)
+        level_case(int(a.level[1]), a.parents, a.pulses, a.form, a.taps, a.reps, pmax=a.pmax)
     else:
-        final_case(a.tiles, a.mode, a.taps, a.reps)
+        final_case(a.tiles, a.mode, a.taps, a.reps, pmax=a.pmax)
 
 
 if __name__ == '__main__':
