@@ -28,6 +28,9 @@ scaling); the step time is the maximum over ranks and the value counts every ran
 --workload patches_48: the batched form instead (run_patches): 48 autotuned patches of uneven sizes from 6
 collections formed by one CUDA graph, against the same formers one after another and patch-by-patch plain FFBP.
 
+--workload stack_8: a repeat-pass stack (run_stack): 8 passes of one scene formed to a common 8,192 x 8,192 grid by
+one CUDA graph, with per-pass errors and pairwise coherence against float64.
+
 --impl reference: the reference's own CPU implementation (its fastsar/ffbp_cpu.cpp kernels, compiled from its
 sources by oracle/Makefile, driven by the oracle's restatement of its host orchestration) on this host's cores, on
 a bounded sample of the same workload: a fixed subset of the first level's children, whose work is a fixed
@@ -191,6 +194,8 @@ def main():
         return run_reference(args, world, rank)
     if args.workload.startswith('patches'):
         return run_patches(args)
+    if args.workload.startswith('stack'):
+        return run_stack(args)
 
     import torch
     import torch.distributed as dist
@@ -472,6 +477,119 @@ def run_patches(args):
         speedup_vs_plain=ms_plain / ms_batch, speedup_vs_sequential=ms_seq / ms_batch,
         err_db=dict(max=max(errs), median=float(np.median(errs)), per_patch=[round(e, 1) for e in errs],
                     reference='float64 exact backprojection, 64x, 256 random pixels per patch, no gain fitted'))
+    print(json.dumps(line), flush=True)
+
+
+def run_stack(args):
+    """--workload stack_8: a repeat-pass stack of 8 collections of one scene formed to 8,192 x 8,192 pixels on a
+    common grid (sim.stack_workload). The chosen form (float16, learned taps, pmax 0.5) of every pass is formed by one
+    CUDA graph (BatchFormer) and timed against the passes formed one after another by the plain float32 former.
+    Per pass, the error against the float64 exact backprojection (64x) on random pixels; per pair of passes, the
+    complex coherence over those pixels against the float64 images' coherence. One GPU; prints one JSON line."""
+    import torch
+    from fastsar_b200 import sim, ImageFormer, BatchFormer
+    from fastsar_b200.exact import backproject_device, plane_points
+    torch.cuda.set_device(0)
+    w = sim.stack_workload(args.workload, seed=args.seed)
+    passes, sc = w['passes'], w['scene']
+    nx, ny, sp = w['nx'], w['ny'], w['spx']
+    t0 = time.time()
+    rng = np.random.default_rng(args.seed + 11)
+    res = (C / (2.0 * passes[0].K * passes[0].df), sp)
+    pos, amp = sim.scene(rng, nx, ny, sp, sp, w['e1'], w['e2'], n_points=sc['n_points'], rcs_sigma_db=sc['rcs_sigma_db'],
+                         n_corners=sc['n_corners'], clutter_db=sc['clutter_db'], res=res, fill=1.0, max_clutter=100000)
+    keep = np.ones(len(pos), bool)
+    for col in passes:
+        keep &= sim.unambiguous_mask(col, pos)
+    pos, amp = pos[keep], amp[keep]
+    hist = []
+    for k, col in enumerate(passes):
+        g = torch.Generator(device='cuda')
+        g.manual_seed(args.seed + 100 + k)
+        S = torch.view_as_complex(torch.randn((col.Np, col.K, 2), device='cuda', generator=g) *
+                                  (10.0 ** (sc['noise_db'] / 20.0) / np.sqrt(2.0))).contiguous()
+        sim.simulate(col, pos, amp, out=S)
+        hist.append(S)
+    torch.cuda.synchronize()
+    log(f'[bench] {len(passes)} passes of {len(amp)} scatterers simulated in {time.time() - t0:.1f} s')
+    bp = len(passes) * nx * ny * passes[0].Np
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    mk = lambda col, **kw: ImageFormer(col.ant, col.fmin, col.df, col.K, nx, ny, sp, sp, w['e1'], w['e2'], **kw)
+    # plain float32, the passes one after another (each former's buffers returned after its turn)
+    out = torch.empty((nx, ny), dtype=torch.complex64, device='cuda')
+    ms_plain = 0.0
+    for col, S in zip(passes, hist):
+        f = mk(col)
+        ms_plain += timed(lambda: f.form_device(S, out, check=False), max(1, args.steps // 2), 1)
+        f.release()
+        del f
+        torch.cuda.empty_cache()
+    del out
+    chosen = [mk(col, precision='float16', taps='learned', pmax=0.5) for col in passes]
+    # one graph over all passes; where the device cannot hold every pass's buffers at once, graphs of fewer
+    group = len(chosen)
+    while True:
+        try:
+            batches = [BatchFormer(chosen[i:i + group]) for i in range(0, len(chosen), group)]
+            break
+        except (MemoryError, RuntimeError) as e:
+            if group == 1 or 'memory' not in str(e).lower():
+                raise
+            batches = None
+            torch.cuda.empty_cache()
+            group = (group + 1) // 2
+    for b, i in zip(batches, range(0, len(chosen), group)):
+        for buf, S in zip(b.histories, hist[i:i + group]):
+            buf.copy_(S)
+    ms_batch = timed(lambda: [b.form_device(check=False) for b in batches], args.steps, args.warmup)
+    imgs = [m for b in batches for m in b.form_device()]
+    # errors and coherence against float64 64x on random pixels
+    n_pix = min(args.err_pixels, nx * ny)
+    idx = np.random.default_rng(5).choice(nx * ny, size=n_pix, replace=False)
+    pts = plane_points(nx, ny, sp, sp, w['e1'], w['e2']).reshape(-1, 3)[idx]
+    it = torch.from_numpy(idx).cuda()
+    ours, refs, errs = [], [], []
+    for col, S, img in zip(passes, hist, imgs):
+        ref = backproject_device(S, col.ant, col.fmin, col.df, pts, upsample=64).cpu().numpy()
+        a = img.reshape(-1)[it].cpu().numpy().astype(np.complex128)
+        ours.append(a)
+        refs.append(ref)
+        errs.append(float(10 * np.log10(np.sum(np.abs(a - ref) ** 2) / np.sum(np.abs(ref) ** 2))))
+
+    def coh(a, b):
+        return float(np.abs(np.vdot(b, a)) / np.sqrt(np.vdot(a, a).real * np.vdot(b, b).real))
+    pairs = [(i, j) for i in range(len(passes)) for j in range(i + 1, len(passes))]
+    dcoh = [abs(coh(ours[i], ours[j]) - coh(refs[i], refs[j])) for i, j in pairs]
+    cref = [coh(refs[i], refs[j]) for i, j in pairs]
+    line = dict(
+        metric='aggregate giga-backprojections/s of an 8-pass repeat-pass stack, one CUDA graph',
+        value=bp / (ms_batch * 1e-3) / 1e9, unit='GBP/s', n_gpus=1, steps=args.steps, warmup=args.warmup,
+        ms_per_step=ms_batch, higher_is_better=True, scaling='weak', vs_baseline=None,
+        dtype='mixed: bf16x3 and f16 tensor products, f16 intermediate, f32 accumulation',
+        data=f'synthetic: one seeded scene of {len(amp)} scatterers, 8 passes simulated on the GPU in float64, '
+             'noise -40 dB',
+        config=dict(workload='stack_8: 8 passes, 32768 pulses x 4096 samples, Ku 16 GHz, 800 MHz, 6 deg, 50 km, '
+                             'baselines up to +-50 m -> 8192 x 8192 px at 0.15 m on a common grid',
+                    form="precision='float16', taps='learned', pmax=0.5", backprojections=bp, passes_per_graph=group,
+                    baselines_m=[round(float(np.linalg.norm(o)), 1) for o in w['offsets']]),
+        plain_fp32_pass_by_pass=dict(ms_per_step=ms_plain, value=bp / (ms_plain * 1e-3) / 1e9),
+        speedup_vs_plain=ms_plain / ms_batch,
+        err_db=dict(per_pass=[round(e, 2) for e in errs], max=max(errs),
+                    reference=f'float64 exact backprojection, 64x, {n_pix} random pixels, no gain fitted'),
+        coherence=dict(max_abs_diff_vs_float64=max(dcoh), float64_range=[round(min(cref), 4), round(max(cref), 4)],
+                       pairs=len(pairs)))
     print(json.dumps(line), flush=True)
 
 

@@ -247,6 +247,28 @@ def patch_workload(name='patches_48', seed=0):
     return out
 
 
+def stack_workload(name='stack_8', seed=0):
+    """A repeat-pass stack: passes of one scene on a common grid -> dict(passes=[Collect], offsets [n, 3], nx, ny,
+    spx, spy, e1, e2, scene).
+
+    stack_8: 8 wide-angle Ku-band spotlight collections (16 GHz, 800 MHz, 6 deg aperture, 50 km, 45 deg grazing,
+    32,768 pulses x 4,096 samples each), the tracks offset from a nominal one by seeded baselines of up to +-50 m
+    across track (in height and ground range), each formed to 8,192 x 8,192 pixels at 0.15 m on the grid about the
+    common scene origin; the scene 2,000 log-normal targets (sigma 10 dB) and 10 corners at +40 dB over -25 dB
+    clutter, noise -40 dB, scatterers kept inside the range band every pass leaves unambiguous."""
+    if name != 'stack_8':
+        raise ValueError(f'unknown stack workload {name!r}')
+    rng = np.random.default_rng(2000 + seed)
+    base = spotlight(32768, 4096, 16e9, 800e6, 50e3, 45.0, 6.0)
+    offsets = np.zeros((8, 3))
+    offsets[1:, 0] = rng.uniform(-50.0, 50.0, 7) / np.sqrt(2.0)
+    offsets[1:, 2] = rng.uniform(-50.0, 50.0, 7) / np.sqrt(2.0)
+    passes = [Collect(fmin=base.fmin, df=base.df, K=base.K, ant=base.ant + o[None, :], res=base.res) for o in offsets]
+    return dict(passes=passes, offsets=offsets, nx=8192, ny=8192, spx=0.15, spy=0.15, e1=(0.0, 1.0, 0.0),
+                e2=(1.0, 0.0, 0.0), scene=dict(n_points=2000, rcs_sigma_db=10.0, n_corners=10, clutter_db=-25.0,
+                                               noise_db=-40.0))
+
+
 def simulate(col, pos, amp, out=None, device=None, chunk=65536):
     """Phase history [P, K] complex64 on the GPU (a torch tensor) by the direct sum over scatterers, float64 ranges
     and phases, through ffbp_simulate (fastsar/sim.py:69-90 computes the same sum with a NUFFT). out: a tensor to add
