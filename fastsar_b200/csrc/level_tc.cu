@@ -531,14 +531,16 @@ template <int AP>
 __global__ void __launch_bounds__(128) level_fir(const FirArgs a)
 {
     constexpr int APP = (AP + 3) & ~3;
-    extern __shared__ __align__(16) float s_tp[];             // [Dp][APP]: s_tp[b APP + s] = tp[Dp s + b]
+    // [Dp][APP] pairs: s_tp[b APP + s] = (tp[Dp s + b], tp[Dp s + b]), a tap twice for the packed multiply-adds
+    extern __shared__ __align__(16) float2 s_tp[];
     // thread -> (row, pair of columns j, j + 1), consecutive threads along a row's pairs and on into the next row;
     // blockIdx.y: the segment of output pulses
     const int t = threadIdx.x;
     for (int r = t; r < a.Dp * APP; r += 128) {
         const int b = r / APP, s = r - b * APP;
         const int tap = a.Dp * s + b;
-        s_tp[r] = (s < AP && tap < a.Lp) ? (a.tp ? a.tp[tap] : 1.f) : 0.f;   // Dp = 1: one tap 1
+        const float v = (s < AP && tap < a.Lp) ? (a.tp ? a.tp[tap] : 1.f) : 0.f;   // Dp = 1: one tap 1
+        s_tp[r] = make_float2(v, v);
     }
     __syncthreads();
     const int npair = (a.Ko + 1) / 2;
@@ -576,18 +578,17 @@ __global__ void __launch_bounds__(128) level_fir(const FirArgs a)
             if (pc + u >= p_stop) break;
             const float2 v0 = __half22float2(*reinterpret_cast<const __half2 *>(&cur[u].x));
             const float2 v1 = __half22float2(*reinterpret_cast<const __half2 *>(&cur[u].y));
-            float tb[APP];
+            float2 tb[APP];
 #pragma unroll
-            for (int s4 = 0; s4 < APP; s4 += 4) {
-                const float4 q4 = *reinterpret_cast<const float4 *>(&s_tp[b * APP + s4]);
-                tb[s4] = q4.x; tb[s4 + 1] = q4.y; tb[s4 + 2] = q4.z; tb[s4 + 3] = q4.w;
+            for (int s2 = 0; s2 < APP; s2 += 2) {
+                const float4 q4 = *reinterpret_cast<const float4 *>(&s_tp[b * APP + s2]);
+                tb[s2] = make_float2(q4.x, q4.y);
+                tb[s2 + 1] = make_float2(q4.z, q4.w);
             }
 #pragma unroll
             for (int s = 0; s < AP; ++s) {
-                acc[0][s].x = fmaf(tb[s], v0.x, acc[0][s].x);
-                acc[0][s].y = fmaf(tb[s], v0.y, acc[0][s].y);
-                acc[1][s].x = fmaf(tb[s], v1.x, acc[1][s].x);
-                acc[1][s].y = fmaf(tb[s], v1.y, acc[1][s].y);
+                acc[0][s] = ffma2(tb[s], v0, acc[0][s]);
+                acc[1][s] = ffma2(tb[s], v1, acc[1][s]);
             }
             if (++b == a.Dp) {                                // group gi complete: output gi - (AP - 1) finished
                 b = 0;
@@ -632,7 +633,7 @@ cudaError_t launch_fir(FirArgs f, cudaStream_t s)
     f.SEG = (f.Po + nseg - 1) / nseg;
     f.nseg = (f.Po + f.SEG - 1) / f.SEG;
     if (nb > 0x7fffffffL || f.nseg > 65535) return cudaErrorInvalidValue;
-    level_fir<AP><<<dim3((unsigned)nb, (unsigned)f.nseg), 128, (size_t)f.Dp * APP * sizeof(float), s>>>(f);
+    level_fir<AP><<<dim3((unsigned)nb, (unsigned)f.nseg), 128, (size_t)f.Dp * APP * sizeof(float2), s>>>(f);
     return cudaGetLastError();
 }
 
