@@ -15,11 +15,12 @@
 // intermediate y [Np, C, P, Kop] as float16 pairs. Real form: A' = [Mr_0; Mi_0; Mr_1; Mi_1; ...] (128 rows, two per
 // child, K = the taps padded to Lkp), B' = [Xr_j; Xi_j] (2 Nt rows: the real and imaginary Hankel rows of the tile's
 // Nt columns), D = A' B'^T: re = MrXr - MiXi, im = MrXi + MiXr.
-// Block roles: warps 16..23 produce, per pulse, the modulated taps (once per pulse, for all column tiles) and per
+// Block roles: warps 8..23 produce, per pulse, the modulated taps (once per pulse, for all column tiles) and per
 // (pulse, tile) the bfloat16 hi/lo planes of the parent row's window and from them the Hankel rows; warp 24 issues the
-// MMAs (M = 128, N = 2 Nt, K = 16) into one of two TMEM accumulators; warps 0..15 read the accumulator (warp w reads
-// lane quarter w % 4, i.e. children 16 (w % 4) .. + 15, and a quarter of the columns), exchange halves between the
-// two rows of a child, apply the ramp and store.
+// MMAs (M = 128, N = 2 Nt, K = 16) into one of two TMEM accumulators; warps 0..7 read the accumulator (warp w reads
+// lane quarter w % 4, i.e. children 16 (w % 4) .. + 15, and half of the columns), exchange halves between the
+// two rows of a child, apply the ramp and store. The producers' phases bound a stage, so they get two warps of
+// every three (with 16 consumer and 8 producer warps a stage took 8-10 % longer at the second and third levels).
 //
 // Pass 2 (level_fir): the pulse FIR of the intermediate on the CUDA cores in float32 (a thread per two columns with
 // the ceil(Lp / Dp) outputs it feeds in registers), written as complex64 with the largest component recorded.
@@ -35,8 +36,8 @@ namespace ffbp {
 
 namespace {
 
-constexpr int NCW = 16;                       // consumer warps 0..15
-constexpr int NPW = 8;                        // producer warps 16..23
+constexpr int NCW = 8;                        // consumer warps 0..7 (a multiple of 4: the TMEM lane quarters)
+constexpr int NPW = 16;                       // producer warps 8..23
 constexpr int MMAW = NCW + NPW;               // warp 24
 constexpr int NTHR = (NCW + NPW + 1) * 32;
 constexpr int NPT = NPW * 32;
@@ -416,12 +417,12 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
         }
         __syncwarp();
     } else {
-        // ------------------------------------------------------------------ consumers (warps 0..15)
+        // ------------------------------------------------------------------ consumers (warps 0..7)
         const int q = warp & 3, g = warp >> 2;
         const int c = 16 * q + (lane >> 1);                   // this lane's child (row 2c: Mr, row 2c + 1: Mi)
         const bool odd = lane & 1;
         const bool live = c < a.C;
-        const int cw = a.Nt / 4;                              // columns of this warp per tile
+        const int cw = a.Nt / (NCW / 4);                      // columns of this warp per tile
         const float2 *__restrict__ phc = a.ph + ((size_t)n * a.C + (live ? c : 0)) * a.P;
         __half2 *__restrict__ yc = a.y + ((size_t)n * a.C + (live ? c : 0)) * a.P * a.Kop;
         // the child's phase (c0, sl) of the current pulse, and of the next one loaded a pulse ahead
