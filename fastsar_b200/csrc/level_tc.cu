@@ -37,10 +37,12 @@ namespace ffbp {
 namespace {
 
 constexpr int NCW = 8;                        // consumer warps 0..7 (a multiple of 4: the TMEM lane quarters)
-constexpr int NPW = 16;                       // producer warps 8..23
+constexpr int NPW = 16;                       // producer warps 8..23:
+constexpr int NAW = 4;                        //   warps 8..11 build the modulated taps (A'),
+constexpr int NBW = NPW - NAW;                //   warps 12..23 the planes and Hankel rows (B')
+constexpr int NAT = NAW * 32, NBT = NBW * 32;
 constexpr int MMAW = NCW + NPW;               // warp 24
 constexpr int NTHR = (NCW + NPW + 1) * 32;
-constexpr int NPT = NPW * 32;
 constexpr uint64_t WAIT_NS = 2000000000ull;
 constexpr int XS = 4;                         // the producers' ring of parent-row windows, XS - 1 stages ahead
 
@@ -200,13 +202,13 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
         s_abort = 0;
         s_scale = y_scale(a.amax_in);
         for (int i = 0; i < 2; ++i) {
-            mbar_init(&afull[i], NPW);
+            mbar_init(&afull[i], NAW);
             mbar_init(&aempty[i], 1);
             mbar_init(&dfull[i], 1);
             mbar_init(&dempty[i], NCW);
         }
         for (int i = 0; i < a.SB; ++i) {
-            mbar_init(&bfull[i], NPW);
+            mbar_init(&bfull[i], NBW);
             mbar_init(&bempty[i], 1);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -225,11 +227,53 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
     const uint32_t tmem = s_tmem;
     const float scale = s_scale;
 
-    if (warp >= NCW && warp < MMAW) {
-        // ------------------------------------------------------------------ producers
-        const int pt = t - NCW * 32;
-        const float2 *__restrict__ xn = a.x + (size_t)n * a.P * a.K;
+    if (warp >= NCW && warp < NCW + NAW) {
+        // ------------------------------------------------------------------ A' producers
+        // the modulated taps of each pulse into A' buffer pulse & 1, a pulse ahead of the B' producers (the
+        // buffer is free once the MMAs of the pulse two back have completed); no named barrier
+        const int at = t - NCW * 32;
         const float2 *__restrict__ phn = a.ph + (size_t)n * a.C * a.P;
+        for (int pl_i = 0; pl_i < npl; ++pl_i) {
+            const int ab = pl_i & 1, p = p0 + pl_i;
+            if (!mbar_wait(&aempty[ab], (uint32_t)(((pl_i >> 1) & 1) ^ 1), 1000, &s_abort, a.err)) break;
+            unsigned char *Ab = sA + ab * 2 * apart;
+            for (int item = at; item < a.C * nkc; item += NAT) {
+                const int u = item / a.C, c = item - u * a.C;   // consecutive threads: consecutive children
+                const float sl = __ldg(&phn[(size_t)c * a.P + p]).y;
+                // exp(2 pi i sl r) for r = 8u .. 8u + 7: two independent recurrences (even and odd r)
+                const float2 st = cis_cycles(sl), st2 = cmul(st, st);
+                float2 ze = cis_cycles(sl * (float)(8 * u)), zo = cmul(ze, st);
+                float mr[8], mi[8];
+#pragma unroll
+                for (int e = 0; e < 8; e += 2) {
+                    const float h0 = s_tk[8 * u + e], h1 = s_tk[8 * u + e + 1];
+                    mr[e] = h0 * ze.x;
+                    mi[e] = h0 * ze.y;
+                    mr[e + 1] = h1 * zo.x;
+                    mi[e + 1] = h1 * zo.y;
+                    ze = cmul(ze, st2);
+                    zo = cmul(zo, st2);
+                }
+                uint32_t rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    split2(mr[2 * e], mr[2 * e + 1], rh[e], rl[e]);
+                    split2(mi[2 * e], mi[2 * e + 1], ih[e], il[e]);
+                }
+                const uint32_t o0 = core_off(2 * c, u, nkc), o1 = core_off(2 * c + 1, u, nkc);
+                *reinterpret_cast<uint4 *>(Ab + o0) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+                *reinterpret_cast<uint4 *>(Ab + apart + o0) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+                *reinterpret_cast<uint4 *>(Ab + o1) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+                *reinterpret_cast<uint4 *>(Ab + apart + o1) = make_uint4(il[0], il[1], il[2], il[3]);
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&afull[ab]);
+        }
+    } else if (warp >= NCW + NAW && warp < MMAW) {
+        // ------------------------------------------------------------------ B' producers
+        const int pt = t - (NCW + NAW) * 32;
+        const float2 *__restrict__ xn = a.x + (size_t)n * a.P * a.K;
         const int npair = (a.W + 1) / 2;                      // window samples in pairs (2i, 2i + 1)
         // the window of stage (pulse p, tile tt): samples k = kb + i, kb = Dk Nt tt - plk, i < W, copied XS - 1
         // stages ahead into ring slot (stage % XS) (zero outside [0, K)); one cp.async group per stage
@@ -238,7 +282,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                 const int q = st / a.ntile, tt = st - q * a.ntile, p = p0 + q;
                 const int kb = a.Dk * a.Nt * tt - a.plk;
                 float2 *dst = s_x + (size_t)(st % XS) * Wp;
-                for (int i = pt; i < a.W; i += NPT) {
+                for (int i = pt; i < a.W; i += NBT) {
                     const int k = kb + i;
                     const bool v = k >= 0 && k < a.K;
                     const float2 *src = v ? xn + (size_t)p * a.K + k : xn;
@@ -259,56 +303,15 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             const int pl_i = s / a.ntile, tt = s - pl_i * a.ntile, p = p0 + pl_i;
             stage_x(s + XS - 1);
             asm volatile("cp.async.wait_group %0;" :: "n"(XS - 1) : "memory");   // this thread's copies of stage s
-            // modulated taps of pulse p (at its first tile), into A' buffer pl_i & 1
-            if (tt == 0 && ok) {
-                const int ab = pl_i & 1;
-                ok = mbar_wait(&aempty[ab], (uint32_t)(((pl_i >> 1) & 1) ^ 1), 1000, &s_abort, a.err);
-            }
-            if (tt == 0 && ok) {
-                const int ab = pl_i & 1;
-                unsigned char *Ab = sA + ab * 2 * apart;
-                for (int item = pt; item < a.C * nkc; item += NPT) {
-                    const int u = item / a.C, c = item - u * a.C;   // consecutive threads: consecutive children
-                    const float sl = __ldg(&phn[(size_t)c * a.P + p]).y;
-                    // exp(2 pi i sl r) for r = 8u .. 8u + 7: two independent recurrences (even and odd r)
-                    const float2 st = cis_cycles(sl), st2 = cmul(st, st);
-                    float2 ze = cis_cycles(sl * (float)(8 * u)), zo = cmul(ze, st);
-                    float mr[8], mi[8];
-#pragma unroll
-                    for (int e = 0; e < 8; e += 2) {
-                        const float h0 = s_tk[8 * u + e], h1 = s_tk[8 * u + e + 1];
-                        mr[e] = h0 * ze.x;
-                        mi[e] = h0 * ze.y;
-                        mr[e + 1] = h1 * zo.x;
-                        mi[e + 1] = h1 * zo.y;
-                        ze = cmul(ze, st2);
-                        zo = cmul(zo, st2);
-                    }
-                    uint32_t rh[4], rl[4], ih[4], il[4];
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        split2(mr[2 * e], mr[2 * e + 1], rh[e], rl[e]);
-                        split2(mi[2 * e], mi[2 * e + 1], ih[e], il[e]);
-                    }
-                    const uint32_t o0 = core_off(2 * c, u, nkc), o1 = core_off(2 * c + 1, u, nkc);
-                    *reinterpret_cast<uint4 *>(Ab + o0) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
-                    *reinterpret_cast<uint4 *>(Ab + apart + o0) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
-                    *reinterpret_cast<uint4 *>(Ab + o1) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
-                    *reinterpret_cast<uint4 *>(Ab + apart + o1) = make_uint4(il[0], il[1], il[2], il[3]);
-                }
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&afull[ab]);
-            }
             // the window's planes: xr hi, xr lo, xi hi, xi lo as bfloat16 pairs (word i = samples 2i, 2i + 1);
             // the barrier also orders every producer's copies of this stage before the reads below and the
             // previous stage's Hankel reads of the planes before these writes
-            asm volatile("bar.sync 1, %0;" :: "n"(NPT) : "memory");
+            asm volatile("bar.sync 1, %0;" :: "n"(NBT) : "memory");
             {
                 const float2 *xs = s_x + (size_t)(s % XS) * Wp;
                 const int kb = a.Dk * a.Nt * tt - a.plk;
                 const float wpp = a.wp ? a.wp[p] : 1.f;
-                for (int i = pt; i < npair; i += NPT) {
+                for (int i = pt; i < npair; i += NBT) {
                     float2 v[3];                              // samples 2i, 2i + 1, 2i + 2 (windowed)
 #pragma unroll
                     for (int h = 0; h < 3; ++h) {
@@ -337,7 +340,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                     pl[7 * hw + i] = oil;
                 }
             }
-            asm volatile("bar.sync 1, %0;" :: "n"(NPT) : "memory");
+            asm volatile("bar.sync 1, %0;" :: "n"(NBT) : "memory");
             if (ok) ok = mbar_wait(&bempty[sb], sbpar ^ 1u, 1000, &s_abort, a.err);
             // Hankel rows: row j < Nt: xr window from Dk j; row Nt + j: xi; 8 elements (16 bytes) per chunk.
             // A warp takes 8 rows (lane % 8) x 4 K chunks (lane / 8) at a time: the 8 rows' 16-byte stores fill one
@@ -345,14 +348,14 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             unsigned char *Bb = sB + sb * 2 * bpart;
             if (ok) {
                 // lane (r8 = lane % 8, uq = lane / 8) keeps its row within a block of 8 and its K chunk within a
-                // group of 4; warp pw takes the row blocks pw, pw + NPW, ... of each (part, re/im, chunk group).
+                // group of 4; warp pw takes the row blocks pw, pw + NBW, ... of each (part, re/im, chunk group).
                 // Along a warp's row blocks the window offset, the plane copy and the store move by constants.
                 constexpr int UB = (NKC + 3) / 4;
-                const int r8 = lane & 7, uq = lane >> 3, pw = warp - NCW;
+                const int r8 = lane & 7, uq = lane >> 3, pw = warp - NCW - NAW;
                 const int nrb = a.Nt / 8;
-                const int nmine = nrb > pw ? (nrb - 1 - pw) / NPW + 1 : 0;
-                const int ostep = 8 * NPW * a.Dk, wstep = ostep >> 1;               // ostep is even
-                const uint32_t bstep = (uint32_t)(NPW * nkc * 128);
+                const int nmine = nrb > pw ? (nrb - 1 - pw) / NBW + 1 : 0;
+                const int ostep = 8 * NBW * a.Dk, wstep = ostep >> 1;               // ostep is even
+                const uint32_t bstep = (uint32_t)(NBW * nkc * 128);
 #pragma unroll
                 for (int ub = 0; ub < UB; ++ub) {
                     const int u = ub * 4 + uq;
