@@ -39,8 +39,9 @@ namespace {
 constexpr int NCW = 8;                        // consumer warps 0..7 (a multiple of 4: the TMEM lane quarters)
 constexpr int NPW = 16;                       // producer warps 8..23:
 constexpr int NAW = 4;                        //   warps 8..11 build the modulated taps (A'),
-constexpr int NBW = NPW - NAW;                //   warps 12..23 the planes and Hankel rows (B')
-constexpr int NAT = NAW * 32, NBT = NBW * 32;
+constexpr int NBW = NPW - NAW;                //   warps 12..23 B': 12..15 the planes, 16..23 the Hankel rows
+constexpr int NLW = 4, NHW = NBW - NLW;
+constexpr int NAT = NAW * 32, NLT = NLW * 32, NHT = NHW * 32;
 constexpr int MMAW = NCW + NPW;               // warp 24
 constexpr int NTHR = (NCW + NPW + 1) * 32;
 constexpr uint64_t WAIT_NS = 2000000000ull;
@@ -181,12 +182,12 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
     const int Wp = (a.W + 9) & ~1;                           // plane length in elements (even, with slack)
     // planes: [xr hi, xr lo, xi hi, xi lo][even, odd copy][Wp / 2] words; the even copy's word w holds samples
     // 2w, 2w + 1, the odd copy's 2w + 1, 2w + 2, so that any 8 consecutive samples are 4 aligned words of one copy
-    uint32_t *pl = reinterpret_cast<uint32_t *>(sB + (size_t)a.SB * 2 * bpart);
-    float *s_tk = reinterpret_cast<float *>(pl + 8 * (Wp / 2));                   // [Lkp]
+    uint32_t *pl = reinterpret_cast<uint32_t *>(sB + (size_t)a.SB * 2 * bpart);   // two stages' planes
+    float *s_tk = reinterpret_cast<float *>(pl + 16 * (Wp / 2));                  // [Lkp]
     float2 *s_x = reinterpret_cast<float2 *>(s_tk + a.Lkp);                        // [XS][Wp] staged windows
     uint64_t *bars = reinterpret_cast<uint64_t *>(s_x + (size_t)XS * Wp);
     uint64_t *afull = bars, *aempty = bars + 2, *bfull = bars + 4, *bempty = bfull + a.SB, *dfull = bempty + a.SB,
-             *dempty = dfull + 2;
+             *dempty = dfull + 2, *pfull = dempty + 2, *pempty = pfull + 2;
     __shared__ uint32_t s_tmem;
     __shared__ volatile int s_abort;
     __shared__ float s_scale;
@@ -208,8 +209,12 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             mbar_init(&dempty[i], NCW);
         }
         for (int i = 0; i < a.SB; ++i) {
-            mbar_init(&bfull[i], NBW);
+            mbar_init(&bfull[i], NHW);
             mbar_init(&bempty[i], 1);
+        }
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&pfull[i], NLT);
+            mbar_init(&pempty[i], NHT);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -270,8 +275,8 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             __syncwarp();
             if (lane == 0) mbar_arrive(&afull[ab]);
         }
-    } else if (warp >= NCW + NAW && warp < MMAW) {
-        // ------------------------------------------------------------------ B' producers
+    } else if (warp >= NCW + NAW && warp < NCW + NAW + NLW) {
+        // ------------------------------------------------------------------ B' producers: planes
         const int pt = t - (NCW + NAW) * 32;
         const float2 *__restrict__ xn = a.x + (size_t)n * a.P * a.K;
         const int npair = (a.W + 1) / 2;                      // window samples in pairs (2i, 2i + 1)
@@ -282,7 +287,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                 const int q = st / a.ntile, tt = st - q * a.ntile, p = p0 + q;
                 const int kb = a.Dk * a.Nt * tt - a.plk;
                 float2 *dst = s_x + (size_t)(st % XS) * Wp;
-                for (int i = pt; i < a.W; i += NBT) {
+                for (int i = pt; i < a.W; i += NLT) {
                     const int k = kb + i;
                     const bool v = k >= 0 && k < a.K;
                     const float2 *src = v ? xn + (size_t)p * a.K + k : xn;
@@ -294,24 +299,25 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
         };
 #pragma unroll
         for (int d = 0; d < XS - 1; ++d) stage_x(d);
-        int sb = 0;
-        uint32_t sbpar = 0;
-        // after a failed wait a warp keeps stepping through the stages (and the producers' named barriers, which
-        // every producer warp must reach) without waiting or working
+        // after a failed wait a warp keeps stepping through the stages (and the named barrier, which every planes
+        // warp must reach) without waiting or working
         bool ok = true;
         for (int s = 0; s < nst; ++s) {
             const int pl_i = s / a.ntile, tt = s - pl_i * a.ntile, p = p0 + pl_i;
+            asm volatile("cp.async.wait_group %0;" :: "n"(XS - 2) : "memory");   // this thread's copies of stage s
+            // every planes thread's copies of stage s are in, and its reads of stage s - 1's window done: that
+            // ring slot takes the window XS - 1 stages ahead
+            asm volatile("bar.sync 1, %0;" :: "n"(NLT) : "memory");
             stage_x(s + XS - 1);
-            asm volatile("cp.async.wait_group %0;" :: "n"(XS - 1) : "memory");   // this thread's copies of stage s
-            // the window's planes: xr hi, xr lo, xi hi, xi lo as bfloat16 pairs (word i = samples 2i, 2i + 1);
-            // the barrier also orders every producer's copies of this stage before the reads below and the
-            // previous stage's Hankel reads of the planes before these writes
-            asm volatile("bar.sync 1, %0;" :: "n"(NBT) : "memory");
-            {
+            if (ok) ok = mbar_wait(&pempty[s & 1], (uint32_t)(((s >> 1) & 1) ^ 1), 1000, &s_abort, a.err);
+            // the window's planes: xr hi, xr lo, xi hi, xi lo as bfloat16 pairs (word i = samples 2i, 2i + 1), into
+            // plane buffer s & 1
+            if (ok) {
+                uint32_t *plb = pl + (s & 1) * 8 * (Wp / 2);
                 const float2 *xs = s_x + (size_t)(s % XS) * Wp;
                 const int kb = a.Dk * a.Nt * tt - a.plk;
                 const float wpp = a.wp ? a.wp[p] : 1.f;
-                for (int i = pt; i < npair; i += NBT) {
+                for (int i = pt; i < npair; i += NLT) {
                     float2 v[3];                              // samples 2i, 2i + 1, 2i + 2 (windowed)
 #pragma unroll
                     for (int h = 0; h < 3; ++h) {
@@ -330,32 +336,41 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                     split2(v[1].x, v[2].x, orh, orl);
                     split2(v[1].y, v[2].y, oih, oil);
                     const int hw = Wp / 2;
-                    pl[i] = rh;
-                    pl[hw + i] = orh;
-                    pl[2 * hw + i] = rl;
-                    pl[3 * hw + i] = orl;
-                    pl[4 * hw + i] = ih;
-                    pl[5 * hw + i] = oih;
-                    pl[6 * hw + i] = il;
-                    pl[7 * hw + i] = oil;
+                    plb[i] = rh;
+                    plb[hw + i] = orh;
+                    plb[2 * hw + i] = rl;
+                    plb[3 * hw + i] = orl;
+                    plb[4 * hw + i] = ih;
+                    plb[5 * hw + i] = oih;
+                    plb[6 * hw + i] = il;
+                    plb[7 * hw + i] = oil;
                 }
+                mbar_arrive(&pfull[s & 1]);
             }
-            asm volatile("bar.sync 1, %0;" :: "n"(NBT) : "memory");
-            if (ok) ok = mbar_wait(&bempty[sb], sbpar ^ 1u, 1000, &s_abort, a.err);
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+    } else if (warp >= NCW + NAW + NLW && warp < MMAW) {
+        // ------------------------------------------------------------------ B' producers: Hankel rows
+        int sb = 0;
+        uint32_t sbpar = 0;
+        for (int s = 0; s < nst; ++s) {
+            if (!mbar_wait(&pfull[s & 1], (uint32_t)((s >> 1) & 1), 1000, &s_abort, a.err)) break;
+            if (!mbar_wait(&bempty[sb], sbpar ^ 1u, 1000, &s_abort, a.err)) break;
             // Hankel rows: row j < Nt: xr window from Dk j; row Nt + j: xi; 8 elements (16 bytes) per chunk.
             // A warp takes 8 rows (lane % 8) x 4 K chunks (lane / 8) at a time: the 8 rows' 16-byte stores fill one
             // 128-byte core matrix (no bank conflicts)
             unsigned char *Bb = sB + sb * 2 * bpart;
-            if (ok) {
+            const uint32_t *plb = pl + (s & 1) * 8 * (Wp / 2);
+            {
                 // lane (r8 = lane % 8, uq = lane / 8) keeps its row within a block of 8 and its K chunk within a
-                // group of 4; warp pw takes the row blocks pw, pw + NBW, ... of each (part, re/im, chunk group).
+                // group of 4; warp pw takes the row blocks pw, pw + NHW, ... of each (part, re/im, chunk group).
                 // Along a warp's row blocks the window offset, the plane copy and the store move by constants.
                 constexpr int UB = (NKC + 3) / 4;
-                const int r8 = lane & 7, uq = lane >> 3, pw = warp - NCW - NAW;
+                const int r8 = lane & 7, uq = lane >> 3, pw = warp - NCW - NAW - NLW;
                 const int nrb = a.Nt / 8;
-                const int nmine = nrb > pw ? (nrb - 1 - pw) / NBW + 1 : 0;
-                const int ostep = 8 * NBW * a.Dk, wstep = ostep >> 1;               // ostep is even
-                const uint32_t bstep = (uint32_t)(NBW * nkc * 128);
+                const int nmine = nrb > pw ? (nrb - 1 - pw) / NHW + 1 : 0;
+                const int ostep = 8 * NHW * a.Dk, wstep = ostep >> 1;               // ostep is even
+                const uint32_t bstep = (uint32_t)(NHW * nkc * 128);
 #pragma unroll
                 for (int ub = 0; ub < UB; ++ub) {
                     const int u = ub * 4 + uq;
@@ -365,7 +380,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
 #pragma unroll
                     for (int pi = 0; pi < 4; ++pi) {                              // (part, re/im)
                         const int part = pi & 1, im = pi >> 1;
-                        const uint32_t *src = pl + (2 * (2 * im + part) + cp) * (Wp / 2) + (o0 >> 1);
+                        const uint32_t *src = plb + (2 * (2 * im + part) + cp) * (Wp / 2) + (o0 >> 1);
                         unsigned char *dst = Bb + part * bpart + core_off(im * a.Nt + 8 * pw + r8, u, nkc);
                         int m = 0;
                         for (; m + 2 <= nmine; m += 2) {
@@ -384,10 +399,10 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
-            if (lane == 0 && ok) mbar_arrive(&bfull[sb]);
+            mbar_arrive(&pempty[s & 1]);                      // this thread's reads of the planes are done
+            if (lane == 0) mbar_arrive(&bfull[sb]);
             if (++sb == a.SB) { sb = 0; sbpar ^= 1u; }
         }
-        asm volatile("cp.async.wait_all;" ::: "memory");
     } else if (warp == MMAW) {
         // ------------------------------------------------------------------ MMA issue
         if (lane == 0) {
@@ -670,9 +685,10 @@ static size_t gemm_smem(int Lkp, int Dk, int nt, int sb)
 {
     const size_t apart = (size_t)128 * Lkp * 2, bpart = (size_t)2 * nt * Lkp * 2;
     const int W = Dk * (nt - 1) + Lkp, Wp = (W + 9) & ~1;
-    // barriers: afull[2], aempty[2], bfull[sb], bempty[sb], dfull[2], dempty[2]
-    return 4 * apart + (size_t)sb * 2 * bpart + (size_t)8 * (Wp / 2) * 4 + (size_t)Lkp * 4 + (size_t)XS * Wp * 8 +
-           (size_t)(8 + 2 * sb) * 8;
+    // two stages' planes; barriers: afull[2], aempty[2], bfull[sb], bempty[sb], dfull[2], dempty[2], pfull[2],
+    // pempty[2]
+    return 4 * apart + (size_t)sb * 2 * bpart + (size_t)16 * (Wp / 2) * 4 + (size_t)Lkp * 4 + (size_t)XS * Wp * 8 +
+           (size_t)(12 + 2 * sb) * 8;
 }
 
 constexpr size_t GEMM_SMEM_MAX = 226 * 1024;                 // the opt-in limit less static shared memory and slack
