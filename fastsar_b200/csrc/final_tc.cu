@@ -17,7 +17,8 @@
 // shape does two or four times the work per instruction; two issuing warps double the rate again.
 //
 // Block roles (persistent over units; one block per SM):
-//   warps 6..17  producers: per final subaperture they build A' and B' (128 rows x Qfp each) in shared memory, a
+//   warps 6..    producers (10 or 12 warps, by shape): per final subaperture they build A' and B' (128 rows x Qfp
+//                each) in shared memory, a
 //                row's ramp by a complex recurrence along q seeded in float64, converted to the operand type, into a
 //                ring of S stages (K-major, no swizzle: core matrices of 8 rows x 16 bytes). Each warp stages the
 //                samples and geometry it needs RS - 1 stages ahead with cp.async into its own ring;
@@ -44,15 +45,14 @@ namespace {
 constexpr int TT = 32;                     // tile side
 constexpr int NEPI = 4;                    // epilogue warps 0..3 (TMEM lane quarters 0..3)
 constexpr int NISS = 2;                    // MMA issuing warps 4, 5
-constexpr int NPW = 12;                    // producer warps 6..17
-constexpr int PW0 = NEPI + NISS;
-constexpr int NTHREADS = (NEPI + NISS + NPW) * 32;
+constexpr int PW0 = NEPI + NISS;           // producer warps PW0 .. PW0 + NPW - 1 (NPW = 10 or 12, a template
+                                           // parameter of the kernel, chosen per shape by the launcher)
 constexpr int RS = 8;                      // depth of each producer warp's staging ring (a power of 2)
 constexpr int SLOT_BYTES = 160;            // staging of one warp item: 16 float2 samples, u (double), 3 weights
 constexpr int TMEM_COLS = 512;             // NISS issuers x 2 accumulators x 128 columns
 constexpr uint64_t WAIT_NS = 2000000000ull;   // a barrier that has not completed after 2 s counts as stuck
 constexpr uint32_t PRODUCER_HINT_NS = 1000;   // suspend-time hints of the waits: producers on a free stage,
-constexpr uint32_t ISSUER_HINT_NS = 0;        // the issuers poll without one,
+constexpr uint32_t ISSUER_HINT_NS = 2000;     // the issuers on a filled stage,
 constexpr uint32_t EPILOGUE_HINT_NS = 4000;   // the epilogue on a finished accumulator
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -169,6 +169,7 @@ struct TcArgs {
     float scale;
     int *err;
     const int *amax;
+    int interleave;                        // the order of the producer warps' items (final_tc_kernel)
 };
 
 // The power of two s that brings samples whose components are at most *amax (a float's bits; null: unknown) to
@@ -259,8 +260,8 @@ __device__ __forceinline__ void tile_pixels(const TcArgs &a, int tile, const flo
     }
 }
 
-template <bool BF, bool WEIGHTED, int MAXWI>
-__global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
+template <bool BF, bool WEIGHTED, int MAXWI, int NPW>
+__global__ void __launch_bounds__((NEPI + NISS + NPW) * 32, 1) final_tc_kernel(const TcArgs a)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
     const int ng = a.Qfp / 8;                                   // core matrices along K per operand
@@ -328,10 +329,20 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
         int it_ts[MAXWI], it_op[MAXWI], it_gp[MAXWI];
 #pragma unroll
         for (int k = 0; k < MAXWI; ++k) {
-            const int wi = pw + k * NPW;
-            it_ts[k] = wi < nwi ? wi / (2 * hg) : -1;
-            it_op[k] = (wi / hg) & 1;
-            it_gp[k] = wi % hg;
+            if (a.interleave) {
+                // A items first, then B items, dealt out to the warps forwards and backwards in turn, so that
+                // with an even count per warp each warp builds as many A items (the heavier) as B items
+                const int j = (k & 1) ? k * NPW + (NPW - 1 - pw) : k * NPW + pw;
+                const int half = nwi / 2;
+                it_ts[k] = j < nwi ? (j % half) / hg : -1;
+                it_op[k] = j >= half ? 1 : 0;
+                it_gp[k] = (j % half) % hg;
+            } else {
+                const int wi = pw + k * NPW;
+                it_ts[k] = wi < nwi ? wi / (2 * hg) : -1;
+                it_op[k] = (wi / hg) & 1;
+                it_gp[k] = wi % hg;
+            }
         }
         // copies of the stage (unit ul, subaperture p) into ring slot `slot`, one cp.async group per stage
         // (empty past the last stage)
@@ -648,14 +659,19 @@ cudaError_t launch_final_tc(const FinalLaunch &F, int mode, cudaStream_t s, cons
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    // warp items per producer warp and stage: (tile slots) x (A, B) x (pairs of 8-sample groups) over NPW warps
+    // warp items per stage: (tile slots) x (A, B) x (pairs of 8-sample groups), over 10 producer warps when that
+    // needs no more items per warp than 12 do (fewer warps contend for the issue slots; measured 7 % faster at
+    // 38 x 71 in float16, 5 % in split bfloat16), else over 12; with 10 the items are interleaved (A and B items
+    // on every warp: 2 % faster at 38 x 71), with 12 they are not (2 % slower interleaved at 47 x 91)
     const int ng = a.Qfp / 8, hg = (ng + 1) / 2;
     const int nwi = (bf ? 1 : 2) * 2 * hg;
-    const int maxwi = (nwi + NPW - 1) / NPW;
+    const int npw = (nwi + 9) / 10 == (nwi + 11) / 12 ? 10 : 12;
+    a.interleave = npw == 10 ? 1 : 0;
+    const int maxwi = (nwi + npw - 1) / npw;
     if (maxwi > 4) { *why = "more than 256 frequency samples per final tile"; return cudaErrorNotSupported; }
     const int mw = maxwi <= 1 ? 1 : (maxwi <= 2 ? 2 : 4);
     const size_t stage = (size_t)4 * 64 * a.Qfp * 2;
-    const size_t fixed = (size_t)2 * 32 * 65 * 4 + (size_t)NPW * RS * mw * SLOT_BYTES + (size_t)(2 * 4 + 6) * 8;
+    const size_t fixed = (size_t)2 * 32 * 65 * 4 + (size_t)npw * RS * mw * SLOT_BYTES + (size_t)(2 * 4 + 6) * 8;
     const size_t avail = (size_t)maxsmem - 1024;                // static shared memory and slack
     // stages: a multiple of the issuers (each owns S / nis of them)
     int S = 4;
@@ -670,17 +686,20 @@ cudaError_t launch_final_tc(const FinalLaunch &F, int mode, cudaStream_t s, cons
     auto run = [&](auto kern) -> cudaError_t {
         cudaError_t r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (r != cudaSuccess) return r;
-        kern<<<grid, NTHREADS, smem, s>>>(a);
+        kern<<<grid, (NEPI + NISS + npw) * 32, smem, s>>>(a);
         return cudaGetLastError();
     };
 #define FFBP_TC_RUN(MW)                                                                                    \
-    (bf ? (a.w ? run(final_tc_kernel<true, true, MW>) : run(final_tc_kernel<true, false, MW>))             \
-        : (a.w ? run(final_tc_kernel<false, true, MW>) : run(final_tc_kernel<false, false, MW>)))
+    (npw == 10 ? FFBP_TC_RUN_NPW(MW, 10) : FFBP_TC_RUN_NPW(MW, 12))
+#define FFBP_TC_RUN_NPW(MW, N)                                                                                \
+    (bf ? (a.w ? run(final_tc_kernel<true, true, MW, N>) : run(final_tc_kernel<true, false, MW, N>))       \
+        : (a.w ? run(final_tc_kernel<false, true, MW, N>) : run(final_tc_kernel<false, false, MW, N>)))
     cudaError_t e;
     if (mw == 1) e = FFBP_TC_RUN(1);
     else if (mw == 2) e = FFBP_TC_RUN(2);
     else e = FFBP_TC_RUN(4);
 #undef FFBP_TC_RUN
+#undef FFBP_TC_RUN_NPW
     return e;
 }
 

@@ -335,13 +335,13 @@ def test_torch_input_matches_numpy(golden):
 
 @pytest.mark.parametrize('mode,tol', [(2, 2e-4), (1, 3e-3)], ids=['bf16x3', 'f16'])
 @pytest.mark.parametrize('weighted', [False, True])
-@pytest.mark.parametrize('shape', [(5, 13, 57), (300, 7, 96), (3, 40, 130), (4, 1, 40), (301, 44, 88), (400, 59, 113)],
+@pytest.mark.parametrize('shape', [(5, 13, 57), (300, 7, 96), (3, 40, 130), (4, 1, 40), (301, 38, 71), (400, 59, 113)],
                          ids=['small', 'many-tiles', 'long-q', 'one-subaperture', 'spotlight-12k-final', 'two-stages'])
 def test_final_tensor_cores_match_oracle(lib, oracle_lib, mode, tol, weighted, shape):
     """The tcgen05 final stage (T = 32) against the float64 oracle: split bfloat16 products within 2e-4, one
     float16 product within 3e-3 (its operands carry 11 bits); units beyond one per multiprocessor, an odd tile count
     (the float16 form pairs tiles), one final subaperture (one MMA issuer), padding of Qf to a multiple of 16,
-    aperture weights, the final stage's shape at the 12,288 x 8,832 spotlight (Pf 44, Qf 88), and a shape whose
+    aperture weights, the chosen form's final stage shape at the 12,288 x 8,832 spotlight (Pf 38, Qf 71), and a shape whose
     operands leave room for two pipeline stages only, with an odd subaperture count and several units per block."""
     T = 32
     rng = np.random.default_rng(7 * mode + weighted + shape[0])
