@@ -17,11 +17,12 @@
 // shape does two or four times the work per instruction; two issuing warps double the rate again.
 //
 // Block roles (persistent over units; one block per SM):
-//   warps 6..    producers (10 or 12 warps, by shape): per final subaperture they build A' and B' (128 rows x Qfp
-//                each) in shared memory, a
-//                row's ramp by a complex recurrence along q seeded in float64, converted to the operand type, into a
-//                ring of S stages (K-major, no swizzle: core matrices of 8 rows x 16 bytes). Each warp stages the
-//                samples and geometry it needs RS - 1 stages ahead with cp.async into its own ring;
+//   warp 6       loader: stages each final subaperture's samples and geometry by cp.async into a ring of LS
+//                slots, LS - 1 subapertures ahead (its copies' completion arrives on the slot's barrier);
+//   warps 7..18  producers: per final subaperture they build A' and B' (128 rows x Qfp
+//                each) in shared memory from the staged slot, a row's ramp by a complex recurrence along q seeded in
+//                float64, converted to the operand type, into a ring of S stages (K-major, no swizzle: core
+//                matrices of 8 rows x 16 bytes);
 //   warps 4, 5   one thread each issues tcgen05.mma: warp 4 + k takes the final subapertures p = k mod 2 of every
 //                unit into its own accumulator (two 128-column accumulators per issuer, 512 TMEM columns), from its
 //                own stages k, k + 2, ... of the ring (a stage with one consumer, so that no parity wait can run two
@@ -45,13 +46,15 @@ namespace {
 constexpr int TT = 32;                     // tile side
 constexpr int NEPI = 4;                    // epilogue warps 0..3 (TMEM lane quarters 0..3)
 constexpr int NISS = 2;                    // MMA issuing warps 4, 5
-constexpr int PW0 = NEPI + NISS;           // producer warps PW0 .. PW0 + NPW - 1 (NPW = 10 or 12, a template
-                                           // parameter of the kernel, chosen per shape by the launcher)
-constexpr int RS = 8;                      // depth of each producer warp's staging ring (a power of 2)
-constexpr int SLOT_BYTES = 160;            // staging of one warp item: 16 float2 samples, u (double), 3 weights
+constexpr int NLD = 1;                     // loader warp 6
+constexpr int NPW = 12;                    // producer warps 7..18
+constexpr int PW0 = NEPI + NISS + NLD;
+constexpr int NTHREADS = (NEPI + NISS + NLD + NPW) * 32;
+constexpr int LS = 8;                      // the loader's ring of staged final subapertures
 constexpr int TMEM_COLS = 512;             // NISS issuers x 2 accumulators x 128 columns
 constexpr uint64_t WAIT_NS = 2000000000ull;   // a barrier that has not completed after 2 s counts as stuck
-constexpr uint32_t PRODUCER_HINT_NS = 1000;   // suspend-time hints of the waits: producers on a free stage,
+constexpr uint32_t PRODUCER_HINT_NS = 1000;   // suspend-time hints of the waits: producers on a free stage or
+                                              // a staged subaperture, the loader on a free ring slot,
 constexpr uint32_t ISSUER_HINT_NS = 2000;     // the issuers on a filled stage,
 constexpr uint32_t EPILOGUE_HINT_NS = 4000;   // the epilogue on a finished accumulator
 
@@ -260,17 +263,21 @@ __device__ __forceinline__ void tile_pixels(const TcArgs &a, int tile, const flo
     }
 }
 
-template <bool BF, bool WEIGHTED, int MAXWI, int NPW>
-__global__ void __launch_bounds__((NEPI + NISS + NPW) * 32, 1) final_tc_kernel(const TcArgs a)
+template <bool BF, bool WEIGHTED, int MAXWI>
+__global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
     const int ng = a.Qfp / 8;                                   // core matrices along K per operand
     const uint32_t H = 64u * a.Qfp * 2u;                        // 64 operand rows
     const uint32_t stagebytes = 4u * H;                         // A' (128 rows), B' (128 rows)
     float *sP = reinterpret_cast<float *>(smem + (size_t)a.S * stagebytes);             // [2][32][65]
-    unsigned char *stg0 = reinterpret_cast<unsigned char *>(sP + 2 * 32 * 65);          // producer staging
-    uint64_t *bars = reinterpret_cast<uint64_t *>(stg0 + (size_t)NPW * RS * MAXWI * SLOT_BYTES);
+    // the loader's ring: per slot and tile slot, the subaperture's Qfp samples (zero past Qf), ux, uy and the
+    // three weights (tsb bytes)
+    unsigned char *ring = reinterpret_cast<unsigned char *>(sP + 2 * 32 * 65);
+    const uint32_t tsb = 8u * a.Qfp + 32u, slotbytes = (BF ? 1u : 2u) * tsb;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(ring + (size_t)LS * slotbytes);
     uint64_t *full = bars, *empty = bars + a.S, *accf = bars + 2 * a.S, *acce = accf + 2, *drain = acce + 2;
+    uint64_t *lfull = drain + 2, *lempty = lfull + LS;
     __shared__ uint32_t s_tmem;
     __shared__ volatile int s_abort;
 
@@ -289,6 +296,10 @@ __global__ void __launch_bounds__((NEPI + NISS + NPW) * 32, 1) final_tc_kernel(c
             mbar_init(&acce[k], NEPI);
             mbar_init(&drain[k], 1);
         }
+        for (int k = 0; k < LS; ++k) {
+            mbar_init(&lfull[k], 32);                      // the loader's 32 threads, once their copies have landed
+            mbar_init(&lempty[k], NPW);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == NEPI) {
@@ -302,7 +313,57 @@ __global__ void __launch_bounds__((NEPI + NISS + NPW) * 32, 1) final_tc_kernel(c
     const uint32_t tmem = s_tmem;
     const uint32_t smem0 = smem_u32(smem);
 
-    if (warp >= PW0) {
+    if (warp == NEPI + NISS) {
+        // ------------------------------------------------------------------ loader
+        // Stages every final subaperture of this block's units LS - 1 ahead of the producers: per tile slot the
+        // Qfp samples (8 bytes each, zero past Qf and for a tile past the last), ux, uy and the weights, by cp.async
+        // into ring slot it % LS; the copies' completion arrives on lfull (each thread's, .noinc), the producers'
+        // reads of the slot on lempty. The next unit's samples and geometry are prefetched into L2 a unit ahead.
+        const int nts = BF ? 1 : 2;
+        const int ntot = nul * a.Pf;
+        const size_t nbp = (size_t)a.B * a.Pf;
+        auto prefetch_unit = [&](int ul) {
+            if (ul >= nul) return;
+            for (int ts = 0; ts < nts; ++ts) {
+                const int tile = unit_tile<BF>(ul, ts);
+                if (tile >= a.B) break;
+                const char *dbeg = reinterpret_cast<const char *>(a.d + (size_t)tile * a.Pf * a.Qf);
+                const int dbytes = a.Pf * a.Qf * (int)sizeof(float2);
+                for (int o = lane * 128; o < dbytes; o += 32 * 128)
+                    asm volatile("prefetch.global.L2 [%0];" :: "l"(dbeg + o));
+                const double *src = (lane < 16 ? a.ux : a.uy) + (size_t)tile * a.Pf;
+                const int ub = a.Pf * (int)sizeof(double);
+                for (int o = (lane & 15) * 128; o < ub; o += 16 * 128)
+                    asm volatile("prefetch.global.L2 [%0];" :: "l"(reinterpret_cast<const char *>(src) + o));
+            }
+        };
+        int ul = 0, p = 0;
+        for (int it = 0; it < ntot; ++it) {
+            const int ls = it % LS;
+            if (it >= LS && !mbar_wait<PRODUCER_HINT_NS>(&lempty[ls], (uint32_t)((it / LS - 1) & 1), &s_abort, a.err))
+                break;
+            if (p == 0) prefetch_unit(ul + 1);
+            const uint32_t sl = smem_u32(ring) + (uint32_t)ls * slotbytes;
+            for (int ts = 0; ts < nts; ++ts) {
+                const int tile = unit_tile<BF>(ul, ts);
+                const bool tv = tile < a.B;
+                const size_t bp = tv ? (size_t)tile * a.Pf + p : 0;
+                const float2 *src = a.d + bp * a.Qf;
+                const uint32_t dst = sl + (uint32_t)ts * tsb;
+                for (int q = lane; q < a.Qfp; q += 32) {
+                    const bool v = tv && q < a.Qf;
+                    cp_async(dst + 8u * q, v ? (const void *)(src + q) : (const void *)a.d, 8, v);
+                }
+                const uint32_t gd = dst + 8u * a.Qfp;
+                if (lane < 2) cp_async(gd + 8u * lane, (const void *)((lane ? a.uy : a.ux) + bp), 8, tv);
+                else if (WEIGHTED && lane < 5)
+                    cp_async(gd + 16u + 4u * (lane - 2), (const void *)(a.w + (size_t)(lane - 2) * nbp + bp), 4, tv);
+            }
+            asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" :: "r"(smem_u32(&lfull[ls])) : "memory");
+            if (++p == a.Pf) { p = 0; ++ul; }
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+    } else if (warp >= PW0) {
         // ------------------------------------------------------------------ producers
         // Warp items: (tile slot ts, operand A or B, pair of 8-sample groups gp). Lane l of the warp takes pixel
         // row pair r = l % 16 (rows r and 31 - r, whose offsets are dl and -dl, so that their ramps are complex
@@ -315,9 +376,6 @@ __global__ void __launch_bounds__((NEPI + NISS + NPW) * 32, 1) final_tc_kernel(c
         const int nwi = nts * 2 * hg;
         const int ntot = nul * a.Pf;
         const int r = lane & 15, sub = lane >> 4;
-        const size_t nbp = (size_t)a.B * a.Pf;
-        const uint32_t stg_me = smem_u32(stg0) + (uint32_t)(pw * RS * MAXWI * SLOT_BYTES);
-        const float *stg_me_p = reinterpret_cast<const float *>(stg0 + (size_t)pw * RS * MAXWI * SLOT_BYTES);
         // byte offsets (without the group) of rows r, r + 32, 31 - r, 63 - r within a 64-row half operand
         uint32_t roff[4];
         {
@@ -344,62 +402,6 @@ __global__ void __launch_bounds__((NEPI + NISS + NPW) * 32, 1) final_tc_kernel(c
                 it_gp[k] = wi % hg;
             }
         }
-        // copies of the stage (unit ul, subaperture p) into ring slot `slot`, one cp.async group per stage
-        // (empty past the last stage)
-        auto issue = [&](int ul, int p, int slot) {
-            if (ul < nul) {
-#pragma unroll
-                for (int k = 0; k < MAXWI; ++k) {
-                    if (it_ts[k] < 0) break;
-                    const int tile = unit_tile<BF>(ul, it_ts[k]);
-                    const bool tv = tile < a.B;
-                    const size_t bp = tv ? (size_t)tile * a.Pf + p : 0;
-                    const uint32_t sl = stg_me + (uint32_t)((slot * MAXWI + k) * SLOT_BYTES);
-                    if (lane < 16) {
-                        if (it_op[k] == 0) {
-                            const int q = 16 * it_gp[k] + lane;
-                            const bool v = tv && q < a.Qf;
-                            cp_async(sl + 8u * lane, v ? (const void *)(a.d + bp * a.Qf + q) : (const void *)a.d, 8, v);
-                        }
-                    } else if (lane == 16) {
-                        cp_async(sl + 128u, it_op[k] == 0 ? (const void *)(a.ux + bp) : (const void *)(a.uy + bp), 8, tv);
-                    } else if (WEIGHTED && lane < 20) {
-                        cp_async(sl + 136u + 4u * (lane - 17), (const void *)(a.w + (size_t)(lane - 17) * nbp + bp), 4,
-                                 tv);
-                    }
-                }
-            }
-            asm volatile("cp.async.commit_group;" ::: "memory");
-        };
-        // the next unit's samples and geometry into L2 while this one is formed
-        auto prefetch_unit = [&](int ul) {
-            if (ul >= nul) return;
-            const int pt = t - PW0 * 32;
-            for (int ts = 0; ts < nts; ++ts) {
-                const int tile = unit_tile<BF>(ul, ts);
-                if (tile >= a.B) break;
-                const char *dbeg = reinterpret_cast<const char *>(a.d + (size_t)tile * a.Pf * a.Qf);
-                const int dbytes = a.Pf * a.Qf * (int)sizeof(float2);
-                for (int o = pt * 128; o < dbytes; o += NPW * 32 * 128)
-                    asm volatile("prefetch.global.L2 [%0];" :: "l"(dbeg + o));
-                if (pt < 16) {
-                    const double *src = (pt < 8 ? a.ux : a.uy) + (size_t)tile * a.Pf;
-                    const int ub = a.Pf * (int)sizeof(double);
-                    for (int o = (pt & 7) * 128; o < ub; o += 8 * 128)
-                        asm volatile("prefetch.global.L2 [%0];" :: "l"(reinterpret_cast<const char *>(src) + o));
-                }
-            }
-        };
-        prefetch_unit(0);
-        // stage counters, advanced by one per stage: (ul2, p2, slot2) the next stage to stage RS - 1 ahead;
-        // (ul, p) the stage being built, stg its ring stage and par that stage's phase parity, slot its staging
-        int ul2 = 0, p2 = 0, slot2 = 0;
-#pragma unroll
-        for (int i = 0; i < RS - 1; ++i) {
-            issue(ul2, p2, slot2);
-            if (++p2 == a.Pf) { p2 = 0; ++ul2; }
-            slot2 = (slot2 + 1) & (RS - 1);
-        }
         const float sp32x = (float)a.spx, sp32y = (float)a.spy;
         // the float16 operands carry d scaled by a power of two that keeps them inside the format's range
         const float dscale = BF ? 1.f : operand_scale(a.amax);
@@ -408,17 +410,14 @@ __global__ void __launch_bounds__((NEPI + NISS + NPW) * 32, 1) final_tc_kernel(c
         const int rs = a.S / nis;
         int ps0 = 0, ps1 = 0;
         uint32_t pp0 = 0, pp1 = 0;
-        int ul = 0, p = 0, slot = 0;
+        int p = 0;
         for (int it = 0; it < ntot; ++it) {
-            issue(ul2, p2, slot2);
-            if (++p2 == a.Pf) { p2 = 0; ++ul2; }
-            slot2 = (slot2 + 1) & (RS - 1);
-            asm volatile("cp.async.wait_group %0;" :: "n"(RS - 1) : "memory");
-            __syncwarp();
-            if (p == 0) prefetch_unit(ul + 1);
+            const int ls = it % LS;
             const int kq = nis == 2 ? (p & 1) : 0;
             const int stg = kq + nis * (kq ? ps1 : ps0);
+            if (!mbar_wait<PRODUCER_HINT_NS>(&lfull[ls], (uint32_t)((it / LS) & 1), &s_abort, a.err)) break;
             if (!mbar_wait<PRODUCER_HINT_NS>(&empty[stg], (kq ? pp1 : pp0) ^ 1u, &s_abort, a.err)) break;
+            const unsigned char *slotb = ring + (size_t)ls * slotbytes;
             unsigned char *sbase = smem + (size_t)stg * stagebytes;
 #pragma unroll
             for (int k = 0; k < MAXWI; ++k) {
@@ -426,9 +425,10 @@ __global__ void __launch_bounds__((NEPI + NISS + NPW) * 32, 1) final_tc_kernel(c
                 const int ts = it_ts[k], op = it_op[k];
                 const int g = 2 * it_gp[k] + sub;
                 if (g >= ng) continue;
-                const float *slotp = stg_me_p + (slot * MAXWI + k) * (SLOT_BYTES / 4);
+                const unsigned char *tsp = slotb + (uint32_t)ts * tsb;
+                const float *gw = reinterpret_cast<const float *>(tsp + 8 * a.Qfp + 16);   // the weights
                 const bool isA = op == 0;
-                const double u = *reinterpret_cast<const double *>(slotp + 32);
+                const double u = *reinterpret_cast<const double *>(tsp + 8 * a.Qfp + (isA ? 0 : 8));
                 const float dlf = ((float)r - 0.5f * (TT - 1)) * (isA ? sp32x : sp32y);      // r < 16: dl < 0
                 const double dl = ((double)r - 0.5 * (TT - 1)) * (isA ? a.spx : a.spy);
                 const double ud = -(u * dl);
@@ -437,14 +437,14 @@ __global__ void __launch_bounds__((NEPI + NISS + NPW) * 32, 1) final_tc_kernel(c
                 const float2 st = cis_cycles_d(ud * a.a1);
                 float w1 = 1.f, w2 = 1.f;                       // the weights of rows r and 31 - r
                 if (WEIGHTED) {
-                    if (isA) { w1 = slotp[34] + slotp[35] * dlf; w2 = slotp[34] - slotp[35] * dlf; }
-                    else { w1 = 1.f + slotp[36] * dlf; w2 = 1.f - slotp[36] * dlf; }
+                    if (isA) { w1 = gw[0] + gw[1] * dlf; w2 = gw[0] - gw[1] * dlf; }
+                    else { w1 = 1.f + gw[2] * dlf; w2 = 1.f - gw[2] * dlf; }
                 }
                 // operand base: A' or B'; half: bfloat16 hi (lo one half further), float16 the tile slot's; group g
                 unsigned char *ob = sbase + (isA ? 0u : 2u * H) + (BF ? 0u : (uint32_t)ts * H) + (uint32_t)g * 128u;
                 float r1[8], i1[8], r2[8], i2[8];
                 if (isA) {
-                    const float4 *dq = reinterpret_cast<const float4 *>(slotp + 16 * sub);
+                    const float4 *dq = reinterpret_cast<const float4 *>(tsp + 64 * g);
 #pragma unroll
                     for (int e2 = 0; e2 < 4; ++e2) {
                         const float4 dd = dq[e2];
@@ -493,17 +493,18 @@ __global__ void __launch_bounds__((NEPI + NISS + NPW) * 32, 1) final_tc_kernel(c
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
-            if (lane == 0) mbar_arrive(&full[stg]);
+            if (lane == 0) {
+                mbar_arrive(&full[stg]);
+                mbar_arrive(&lempty[ls]);
+            }
             if (kq) {
                 if (++ps1 == rs) { ps1 = 0; pp1 ^= 1u; }
             } else if (++ps0 == rs) {
                 ps0 = 0;
                 pp0 ^= 1u;
             }
-            if (++p == a.Pf) { p = 0; ++ul; }
-            slot = (slot + 1) & (RS - 1);
+            if (++p == a.Pf) p = 0;
         }
-        asm volatile("cp.async.wait_all;" ::: "memory");
     } else if (warp >= NEPI) {
         // ------------------------------------------------------------------ MMA issue
         const int k = warp - NEPI;
@@ -659,19 +660,18 @@ cudaError_t launch_final_tc(const FinalLaunch &F, int mode, cudaStream_t s, cons
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    // warp items per stage: (tile slots) x (A, B) x (pairs of 8-sample groups), over 10 producer warps when that
-    // needs no more items per warp than 12 do (fewer warps contend for the issue slots; measured 7 % faster at
-    // 38 x 71 in float16, 5 % in split bfloat16), else over 12; with 10 the items are interleaved (A and B items
-    // on every warp: 2 % faster at 38 x 71), with 12 they are not (2 % slower interleaved at 47 x 91)
+    // warp items per stage: (tile slots) x (A, B) x (pairs of 8-sample groups) over the NPW producer warps; when
+    // every warp gets the same even number of items they are interleaved (as many A items, the heavier, as B
+    // items on each warp: 3 % faster at 47 x 91 in float16; 1 % slower at 38 x 71, whose count is uneven)
     const int ng = a.Qfp / 8, hg = (ng + 1) / 2;
     const int nwi = (bf ? 1 : 2) * 2 * hg;
-    const int npw = (nwi + 9) / 10 == (nwi + 11) / 12 ? 10 : 12;
-    a.interleave = npw == 10 ? 1 : 0;
-    const int maxwi = (nwi + npw - 1) / npw;
+    a.interleave = nwi % (2 * NPW) == 0 ? 1 : 0;
+    const int maxwi = (nwi + NPW - 1) / NPW;
     if (maxwi > 4) { *why = "more than 256 frequency samples per final tile"; return cudaErrorNotSupported; }
     const int mw = maxwi <= 1 ? 1 : (maxwi <= 2 ? 2 : 4);
     const size_t stage = (size_t)4 * 64 * a.Qfp * 2;
-    const size_t fixed = (size_t)2 * 32 * 65 * 4 + (size_t)npw * RS * mw * SLOT_BYTES + (size_t)(2 * 4 + 6) * 8;
+    const size_t slotbytes = (size_t)(bf ? 1 : 2) * (8 * a.Qfp + 32);
+    const size_t fixed = (size_t)2 * 32 * 65 * 4 + (size_t)LS * slotbytes + (size_t)(2 * 4 + 6 + 2 * LS) * 8;
     const size_t avail = (size_t)maxsmem - 1024;                // static shared memory and slack
     // stages: a multiple of the issuers (each owns S / nis of them)
     int S = 4;
@@ -686,20 +686,17 @@ cudaError_t launch_final_tc(const FinalLaunch &F, int mode, cudaStream_t s, cons
     auto run = [&](auto kern) -> cudaError_t {
         cudaError_t r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (r != cudaSuccess) return r;
-        kern<<<grid, (NEPI + NISS + npw) * 32, smem, s>>>(a);
+        kern<<<grid, NTHREADS, smem, s>>>(a);
         return cudaGetLastError();
     };
 #define FFBP_TC_RUN(MW)                                                                                    \
-    (npw == 10 ? FFBP_TC_RUN_NPW(MW, 10) : FFBP_TC_RUN_NPW(MW, 12))
-#define FFBP_TC_RUN_NPW(MW, N)                                                                                \
-    (bf ? (a.w ? run(final_tc_kernel<true, true, MW, N>) : run(final_tc_kernel<true, false, MW, N>))       \
-        : (a.w ? run(final_tc_kernel<false, true, MW, N>) : run(final_tc_kernel<false, false, MW, N>)))
+    (bf ? (a.w ? run(final_tc_kernel<true, true, MW>) : run(final_tc_kernel<true, false, MW>))             \
+        : (a.w ? run(final_tc_kernel<false, true, MW>) : run(final_tc_kernel<false, false, MW>)))
     cudaError_t e;
     if (mw == 1) e = FFBP_TC_RUN(1);
     else if (mw == 2) e = FFBP_TC_RUN(2);
     else e = FFBP_TC_RUN(4);
 #undef FFBP_TC_RUN
-#undef FFBP_TC_RUN_NPW
     return e;
 }
 
