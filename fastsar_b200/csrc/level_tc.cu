@@ -12,15 +12,20 @@
 //
 // Pass 1 (level_tc_gemm): per parent and pulse the product on the tensor cores, three bfloat16 products (x = hi + lo:
 // hi hi + hi lo + lo hi) accumulated in float32; then the ramp, a power-of-two scale into float16's range, and the
-// intermediate y [Np, C, P, Kop] as float16 pairs. Real form: A' = [Mr_0; Mi_0; Mr_1; Mi_1; ...] (128 rows, two per
-// child, K = the taps padded to Lkp), B' = [Xr_j; Xi_j] (2 Nt rows: the real and imaginary Hankel rows of the tile's
-// Nt columns), D = A' B'^T: re = MrXr - MiXi, im = MrXi + MiXr.
+// intermediate y [Np, C, P, Kop] as float16 pairs. Real form: A' (128 rows, two per child: Mr, Mi; K = the taps
+// padded to Lkp), B' = [Xr_j; Xi_j] (2 Nt rows: the real and imaginary Hankel rows of the tile's Nt columns),
+// D = A' B'^T: re = MrXr - MiXi, im = MrXi + MiXr.
 // Block roles: warps 8..23 produce, per pulse, the modulated taps (once per pulse, for all column tiles) and per
 // (pulse, tile) the bfloat16 hi/lo planes of the parent row's window and from them the Hankel rows; warp 24 issues the
 // MMAs (M = 128, N = 2 Nt, K = 16) into one of two TMEM accumulators; warps 0..7 read the accumulator (warp w reads
-// lane quarter w % 4, i.e. children 16 (w % 4) .. + 15, and half of the columns), exchange halves between the
-// two rows of a child, apply the ramp and store. The producers' phases bound a stage, so they get two warps of
-// every three (with 16 consumer and 8 producer warps a stage took 8-10 % longer at the second and third levels).
+// lane quarter w % 4, i.e. children 16 (w % 4) .. + 15, and half of the columns), combine re/im, apply the ramp and
+// store. Two read-outs, chosen by the tap count: with up to 32 taps (light producers, the consumers bound the stage)
+// A' holds in each group of 16 rows the Mr rows of 8 children and then their Mi rows, and 16-row accumulator loads
+// give each thread both rows of a child (no exchange between threads); with more taps A' = [Mr_0; Mi_0; Mr_1; ...]
+// and the two lanes of a child exchange halves (measured faster there: 11.7 against 12.4 ms at the 12,288 x 8,832
+// spotlight's third level, 8.2 against 7.1 ms the other way at its first). The producers' phases bound a stage at
+// more taps, so they get two warps of every three (with 16 consumer and 8 producer warps a stage took 8-10 % longer
+// at the second and third levels).
 //
 // Pass 2 (level_fir): the pulse FIR of the intermediate on the CUDA cores in float32 (a thread per two columns with
 // the ceil(Lp / Dp) outputs it feeds in registers), written as complex64 with the largest component recorded.
@@ -144,6 +149,17 @@ __device__ __forceinline__ uint32_t core_off(int row, int kchunk, int nkc)
     return (uint32_t)(((row >> 3) * nkc + kchunk) * 128 + (row & 7) * 16);
 }
 
+// 16 accumulator lanes x 8 columns from (lane, column) addr: thread l gets lane l / 4 at columns 2 (l % 4) and
+// 2 (l % 4) + 1 (v[0], v[1]) and lane l / 4 + 8 at the same columns (v[2], v[3]); without waiting
+__device__ __forceinline__ void tmem_ld16x256(uint32_t addr, float *v)
+{
+    uint32_t r[4];
+    asm volatile("tcgen05.ld.sync.aligned.16x256b.x1.b32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(addr));
+#pragma unroll
+    for (int i = 0; i < 4; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 struct GemmArgs {
     const float2 *__restrict__ x;     // [Np, P, K]
     const float2 *__restrict__ ph;    // [Np, C, P] (c0, sl)
@@ -265,7 +281,10 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                     split2(mr[2 * e], mr[2 * e + 1], rh[e], rl[e]);
                     split2(mi[2 * e], mi[2 * e + 1], ih[e], il[e]);
                 }
-                const uint32_t o0 = core_off(2 * c, u, nkc), o1 = core_off(2 * c + 1, u, nkc);
+                // the rows of child c's Mr and Mi: with up to 32 taps, in each group of 16 rows the Mr rows of 8
+                // children and then their Mi rows (the consumers' 16-row read-out); else rows 2 c and 2 c + 1
+                const int row = NKC <= 4 ? 16 * (c >> 3) + (c & 7) : 2 * c, row2 = NKC <= 4 ? row + 8 : row + 1;
+                const uint32_t o0 = core_off(row, u, nkc), o1 = core_off(row2, u, nkc);
                 *reinterpret_cast<uint4 *>(Ab + o0) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
                 *reinterpret_cast<uint4 *>(Ab + apart + o0) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
                 *reinterpret_cast<uint4 *>(Ab + o1) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
@@ -435,84 +454,174 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
         }
         __syncwarp();
     } else {
-        // ------------------------------------------------------------------ consumers (warps 0..7)
-        const int q = warp & 3, g = warp >> 2;
-        const int c = 16 * q + (lane >> 1);                   // this lane's child (row 2c: Mr, row 2c + 1: Mi)
-        const bool odd = lane & 1;
-        const bool live = c < a.C;
-        const int cw = a.Nt / (NCW / 4);                      // columns of this warp per tile
-        const float2 *__restrict__ phc = a.ph + ((size_t)n * a.C + (live ? c : 0)) * a.P;
-        __half2 *__restrict__ yc = a.y + ((size_t)n * a.C + (live ? c : 0)) * a.P * a.Kop;
-        // the child's phase (c0, sl) of the current pulse, and of the next one loaded a pulse ahead
-        float2 q0 = make_float2(0.f, 0.f), qn = (live && npl > 0) ? __ldg(&phc[p0]) : make_float2(0.f, 0.f);
-        for (int s = 0; s < nst; ++s) {
-            const int pl_i = s / a.ntile, tt = s - pl_i * a.ntile, p = p0 + pl_i;
-            const int db = s & 1;
-            if (tt == 0) {
-                q0 = qn;
-                if (live && pl_i + 1 < npl) qn = __ldg(&phc[p + 1]);
-            }
-            // warp-uniform: the accumulator loads below are warp-collective
-            if (!__all_sync(0xffffffffu, mbar_wait(&dfull[db], (uint32_t)((s >> 1) & 1), 200, &s_abort, a.err))) break;
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t base = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(db * 256);
-            const float2 st = cis_cycles(q0.y * (float)a.Dk), st8 = cis_cycles(q0.y * (float)(8 * a.Dk));
-            // this lane's ramp at its first column of the chunk: seeded at the first chunk, then 8 columns on
-            float2 wc = cis_cycles(fmaf(q0.y, (float)(a.Dk * (tt * a.Nt + g * cw + (odd ? 4 : 0)) - a.plk) - a.kc, q0.x));
-            wc.x *= scale;
-            wc.y *= scale;
-            // chunks of 8 columns; the next chunk's accumulator loads are in flight while one is processed
-            float vr[8], vi[8], nr[8], ni[8];
-            tmem_ld8(base + (uint32_t)(g * cw), vr);
-            tmem_ld8(base + (uint32_t)(a.Nt + g * cw), vi);
-            tmem_wait_ld();
-            // the accumulator is released as soon as its last chunk is in registers
-            auto release = [&]() {
-                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&dempty[db]);
+        if constexpr (NKC <= 4) {
+            // ------------------------------------------------------------------ consumers (warps 0..7), up to 32 taps
+            // Warp w reads TMEM lane quarter q = w % 4 (A' rows 32 q .. 32 q + 31: children 16 q .. 16 q + 15) and
+            // column half g = w / 4 of the tile. A 16x256b load of row group h (rows 32 q + 16 h ..) gives thread l the
+            // Mr and Mi rows of child cc + 8 h (cc = 16 q + l / 4) at columns jl, jl + 1 (jl = 2 (l % 4)) of an 8-column
+            // chunk: each thread forms re/im of its two children at two columns with no exchange between threads, the
+            // two columns as packed float32 pairs.
+            const int q = warp & 3, g = warp >> 2;
+            const int cc = 16 * q + (lane >> 2), jl = 2 * (lane & 3);
+            const int cw = a.Nt / (NCW / 4);                      // columns of this warp per tile
+            // child cc + 8 h's phases and intermediate rows (child 0's for a child past the last, whose results are
+            // not stored)
+            auto phc = [&](int h) {
+                const int c = cc + 8 * h;
+                return a.ph + ((size_t)n * a.C + (c < a.C ? c : 0)) * a.P;
             };
-            if (cw == 8) release();
-            for (int k8 = 0; k8 < cw; k8 += 8) {
-                const int cb = g * cw + k8;                   // first column of the chunk within the tile
-                const bool more = k8 + 8 < cw;
-                if (more) {
-                    tmem_ld8(base + (uint32_t)(cb + 8), nr);
-                    tmem_ld8(base + (uint32_t)(a.Nt + cb + 8), ni);
-                }
-                // even lane (Mr row) keeps columns 0..3 of the chunk, odd lane (Mi row) columns 4..7
-                float mr_r[4], mr_i[4], mi_r[4], mi_i[4];
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const float sr = odd ? vr[i] : vr[4 + i], si = odd ? vi[i] : vi[4 + i];
-                    const float rr = __shfl_xor_sync(0xffffffffu, sr, 1), ri = __shfl_xor_sync(0xffffffffu, si, 1);
-                    const float orr = odd ? vr[4 + i] : vr[i], ori = odd ? vi[4 + i] : vi[i];
-                    mr_r[i] = odd ? rr : orr;
-                    mr_i[i] = odd ? ri : ori;
-                    mi_r[i] = odd ? orr : rr;
-                    mi_i[i] = odd ? ori : ri;
-                }
-                const int j0 = tt * a.Nt + cb + (odd ? 4 : 0);
-                float2 w = wc;
-                wc = cmul(wc, st8);
-                if (live && j0 < a.Ko) {
-                    uint32_t outw[4];
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        const float re = mr_r[i] - mi_i[i], im = mr_i[i] + mi_r[i];
-                        const float2 o = cmul(w, make_float2(re, im));
-                        const __half2 hv = __floats2half2_rn(o.x, o.y);
-                        outw[i] = *reinterpret_cast<const uint32_t *>(&hv);
-                        w = cmul(w, st);
+            float2 q0[2], qn[2];                                  // the children's (c0, sl): this pulse, the next
+    #pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                q0[h] = make_float2(0.f, 0.f);
+                qn[h] = (cc + 8 * h < a.C && npl > 0) ? __ldg(phc(h) + p0) : make_float2(0.f, 0.f);
+            }
+            for (int s = 0; s < nst; ++s) {
+                const int pl_i = s / a.ntile, tt = s - pl_i * a.ntile, p = p0 + pl_i;
+                const int db = s & 1;
+                if (tt == 0) {
+    #pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        q0[h] = qn[h];
+                        if (cc + 8 * h < a.C && pl_i + 1 < npl) qn[h] = __ldg(phc(h) + p + 1);
                     }
-                    *reinterpret_cast<uint4 *>(yc + (size_t)p * a.Kop + j0) = make_uint4(outw[0], outw[1], outw[2], outw[3]);
                 }
+                // warp-uniform: the accumulator loads below are warp-collective
+                if (!__all_sync(0xffffffffu, mbar_wait(&dfull[db], (uint32_t)((s >> 1) & 1), 200, &s_abort, a.err))) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t base = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(db * 256);
+                // per child: the ramp at this thread's two columns of the first chunk (x parts, y parts), and the
+                // step of 8 columns
+                float2 wv[2], st1[2], st8[2];
+    #pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    st1[h] = cis_cycles(q0[h].y * (float)a.Dk);
+                    st8[h] = cis_cycles(q0[h].y * (float)(8 * a.Dk));
+                    float2 w0 = cis_cycles(fmaf(q0[h].y, (float)(a.Dk * (tt * a.Nt + g * cw + jl) - a.plk) - a.kc, q0[h].x));
+                    w0.x *= scale;
+                    w0.y *= scale;
+                    wv[h] = w0;
+                }
+                // units (chunk of 8 columns, row group h) in order, the next unit's accumulator loads in flight while
+                // one is processed; a unit's registers: (Mr, Mr, Mi, Mi) x (column jl, jl + 1) of the Xr and the Xi
+                // columns
+                float ua[8], ub[8];
+                auto load = [&](int k8, int h, float *v) {
+                    const uint32_t bh = base + ((uint32_t)(16 * h) << 16) + (uint32_t)(g * cw + k8);
+                    tmem_ld16x256(bh, v);
+                    tmem_ld16x256(bh + (uint32_t)a.Nt, v + 4);
+                };
+                auto unit = [&](int k8, int h, const float *v) {
+                    // re = Mr Xr - Mi Xi, im = Mr Xi + Mi Xr at the two columns; times the ramp; the ramp 8 columns on
+                    const float2 w0 = wv[h], w1 = cmul(w0, st1[h]);
+                    const float2 o0 = cmul(w0, make_float2(v[0] - v[6], v[4] + v[2]));
+                    const float2 o1 = cmul(w1, make_float2(v[1] - v[7], v[5] + v[3]));
+                    const int c = cc + 8 * h, j = tt * a.Nt + g * cw + k8 + jl;
+                    if (c < a.C && j < a.Ko) {
+                        const __half2 h0 = __floats2half2_rn(o0.x, o0.y), h1 = __floats2half2_rn(o1.x, o1.y);
+                        *reinterpret_cast<uint2 *>(a.y + (((size_t)n * a.C + c) * a.P + p) * a.Kop + j) =
+                            make_uint2(*reinterpret_cast<const uint32_t *>(&h0), *reinterpret_cast<const uint32_t *>(&h1));
+                    }
+                    wv[h] = cmul(w0, st8[h]);
+                };
+                load(0, 0, ua);
                 tmem_wait_ld();
-                if (more && k8 + 16 >= cw) release();
-#pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    vr[i] = nr[i];
-                    vi[i] = ni[i];
+                for (int k8 = 0; k8 < cw; k8 += 8) {
+                    load(k8, 1, ub);
+                    unit(k8, 0, ua);
+                    tmem_wait_ld();
+                    if (k8 + 8 == cw) {
+                        // the accumulator's last unit is in registers: release it to the MMA issuer
+                        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(&dempty[db]);
+                    } else {
+                        load(k8 + 8, 0, ua);
+                    }
+                    unit(k8, 1, ub);
+                    tmem_wait_ld();
+                }
+            }
+        } else {
+            // ------------------------------------------------------------------ consumers (warps 0..7), more taps
+            const int q = warp & 3, g = warp >> 2;
+            const int c = 16 * q + (lane >> 1);                   // this lane's child (row 2c: Mr, row 2c + 1: Mi)
+            const bool odd = lane & 1;
+            const bool live = c < a.C;
+            const int cw = a.Nt / (NCW / 4);                      // columns of this warp per tile
+            const float2 *__restrict__ phc = a.ph + ((size_t)n * a.C + (live ? c : 0)) * a.P;
+            __half2 *__restrict__ yc = a.y + ((size_t)n * a.C + (live ? c : 0)) * a.P * a.Kop;
+            // the child's phase (c0, sl) of the current pulse, and of the next one loaded a pulse ahead
+            float2 q0 = make_float2(0.f, 0.f), qn = (live && npl > 0) ? __ldg(&phc[p0]) : make_float2(0.f, 0.f);
+            for (int s = 0; s < nst; ++s) {
+                const int pl_i = s / a.ntile, tt = s - pl_i * a.ntile, p = p0 + pl_i;
+                const int db = s & 1;
+                if (tt == 0) {
+                    q0 = qn;
+                    if (live && pl_i + 1 < npl) qn = __ldg(&phc[p + 1]);
+                }
+                // warp-uniform: the accumulator loads below are warp-collective
+                if (!__all_sync(0xffffffffu, mbar_wait(&dfull[db], (uint32_t)((s >> 1) & 1), 200, &s_abort, a.err))) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t base = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(db * 256);
+                const float2 st = cis_cycles(q0.y * (float)a.Dk), st8 = cis_cycles(q0.y * (float)(8 * a.Dk));
+                // this lane's ramp at its first column of the chunk: seeded at the first chunk, then 8 columns on
+                float2 wc = cis_cycles(fmaf(q0.y, (float)(a.Dk * (tt * a.Nt + g * cw + (odd ? 4 : 0)) - a.plk) - a.kc, q0.x));
+                wc.x *= scale;
+                wc.y *= scale;
+                // chunks of 8 columns; the next chunk's accumulator loads are in flight while one is processed
+                float vr[8], vi[8], nr[8], ni[8];
+                tmem_ld8(base + (uint32_t)(g * cw), vr);
+                tmem_ld8(base + (uint32_t)(a.Nt + g * cw), vi);
+                tmem_wait_ld();
+                // the accumulator is released as soon as its last chunk is in registers
+                auto release = [&]() {
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&dempty[db]);
+                };
+                if (cw == 8) release();
+                for (int k8 = 0; k8 < cw; k8 += 8) {
+                    const int cb = g * cw + k8;                   // first column of the chunk within the tile
+                    const bool more = k8 + 8 < cw;
+                    if (more) {
+                        tmem_ld8(base + (uint32_t)(cb + 8), nr);
+                        tmem_ld8(base + (uint32_t)(a.Nt + cb + 8), ni);
+                    }
+                    // even lane (Mr row) keeps columns 0..3 of the chunk, odd lane (Mi row) columns 4..7
+                    float mr_r[4], mr_i[4], mi_r[4], mi_i[4];
+    #pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        const float sr = odd ? vr[i] : vr[4 + i], si = odd ? vi[i] : vi[4 + i];
+                        const float rr = __shfl_xor_sync(0xffffffffu, sr, 1), ri = __shfl_xor_sync(0xffffffffu, si, 1);
+                        const float orr = odd ? vr[4 + i] : vr[i], ori = odd ? vi[4 + i] : vi[i];
+                        mr_r[i] = odd ? rr : orr;
+                        mr_i[i] = odd ? ri : ori;
+                        mi_r[i] = odd ? orr : rr;
+                        mi_i[i] = odd ? ori : ri;
+                    }
+                    const int j0 = tt * a.Nt + cb + (odd ? 4 : 0);
+                    float2 w = wc;
+                    wc = cmul(wc, st8);
+                    if (live && j0 < a.Ko) {
+                        uint32_t outw[4];
+    #pragma unroll
+                        for (int i = 0; i < 4; ++i) {
+                            const float re = mr_r[i] - mi_i[i], im = mr_i[i] + mi_r[i];
+                            const float2 o = cmul(w, make_float2(re, im));
+                            const __half2 hv = __floats2half2_rn(o.x, o.y);
+                            outw[i] = *reinterpret_cast<const uint32_t *>(&hv);
+                            w = cmul(w, st);
+                        }
+                        *reinterpret_cast<uint4 *>(yc + (size_t)p * a.Kop + j0) = make_uint4(outw[0], outw[1], outw[2], outw[3]);
+                    }
+                    tmem_wait_ld();
+                    if (more && k8 + 16 >= cw) release();
+    #pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        vr[i] = nr[i];
+                        vi[i] = ni[i];
+                    }
                 }
             }
         }
