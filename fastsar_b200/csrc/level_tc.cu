@@ -289,6 +289,15 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                 *reinterpret_cast<uint4 *>(Ab + apart + o0) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
                 *reinterpret_cast<uint4 *>(Ab + o1) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
                 *reinterpret_cast<uint4 *>(Ab + apart + o1) = make_uint4(il[0], il[1], il[2], il[3]);
+                if (NKC > 4 && a.C <= 32) {
+                    // at most 32 children: rows 64 .. 127 repeat rows 0 .. 63, so that all four lane quarters of the
+                    // accumulator hold children and the consumers split the columns four ways
+                    const uint32_t d0 = core_off(row + 64, u, nkc), d1 = core_off(row2 + 64, u, nkc);
+                    *reinterpret_cast<uint4 *>(Ab + d0) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+                    *reinterpret_cast<uint4 *>(Ab + apart + d0) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+                    *reinterpret_cast<uint4 *>(Ab + d1) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+                    *reinterpret_cast<uint4 *>(Ab + apart + d1) = make_uint4(il[0], il[1], il[2], il[3]);
+                }
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
@@ -544,11 +553,15 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             }
         } else {
             // ------------------------------------------------------------------ consumers (warps 0..7), more taps
+            // with at most 32 children lane quarters 2, 3 repeat quarters 0, 1 (A' rows 64 .. 127), and warp w takes
+            // the column quarter w / 4 + 2 (w % 4 / 2) of the tile instead of the column half w / 4
+            const int rp = a.C <= 32 ? 2 : 1;
             const int q = warp & 3, g = warp >> 2;
-            const int c = 16 * q + (lane >> 1);                   // this lane's child (row 2c: Mr, row 2c + 1: Mi)
+            const int c = 16 * (rp == 2 ? (q & 1) : q) + (lane >> 1);   // this lane's child (rows 2c: Mr, 2c + 1: Mi)
             const bool odd = lane & 1;
             const bool live = c < a.C;
-            const int cw = a.Nt / (NCW / 4);                      // columns of this warp per tile
+            const int cw = a.Nt / (NCW / 4) / rp;                 // columns of this warp per tile (a multiple of 8)
+            const int cofs = (rp == 2 ? g + 2 * (q >> 1) : g) * cw;   // this warp's first column within the tile
             const float2 *__restrict__ phc = a.ph + ((size_t)n * a.C + (live ? c : 0)) * a.P;
             __half2 *__restrict__ yc = a.y + ((size_t)n * a.C + (live ? c : 0)) * a.P * a.Kop;
             // the child's phase (c0, sl) of the current pulse, and of the next one loaded a pulse ahead
@@ -566,13 +579,13 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                 const uint32_t base = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(db * 256);
                 const float2 st = cis_cycles(q0.y * (float)a.Dk), st8 = cis_cycles(q0.y * (float)(8 * a.Dk));
                 // this lane's ramp at its first column of the chunk: seeded at the first chunk, then 8 columns on
-                float2 wc = cis_cycles(fmaf(q0.y, (float)(a.Dk * (tt * a.Nt + g * cw + (odd ? 4 : 0)) - a.plk) - a.kc, q0.x));
+                float2 wc = cis_cycles(fmaf(q0.y, (float)(a.Dk * (tt * a.Nt + cofs + (odd ? 4 : 0)) - a.plk) - a.kc, q0.x));
                 wc.x *= scale;
                 wc.y *= scale;
                 // chunks of 8 columns; the next chunk's accumulator loads are in flight while one is processed
                 float vr[8], vi[8], nr[8], ni[8];
-                tmem_ld8(base + (uint32_t)(g * cw), vr);
-                tmem_ld8(base + (uint32_t)(a.Nt + g * cw), vi);
+                tmem_ld8(base + (uint32_t)cofs, vr);
+                tmem_ld8(base + (uint32_t)(a.Nt + cofs), vi);
                 tmem_wait_ld();
                 // the accumulator is released as soon as its last chunk is in registers
                 auto release = [&]() {
@@ -582,7 +595,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                 };
                 if (cw == 8) release();
                 for (int k8 = 0; k8 < cw; k8 += 8) {
-                    const int cb = g * cw + k8;                   // first column of the chunk within the tile
+                    const int cb = cofs + k8;                     // first column of the chunk within the tile
                     const bool more = k8 + 8 < cw;
                     if (more) {
                         tmem_ld8(base + (uint32_t)(cb + 8), nr);
