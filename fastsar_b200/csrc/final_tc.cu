@@ -19,10 +19,9 @@
 // Block roles (persistent over units; one block per SM):
 //   warp 6       loader: stages each final subaperture's samples and geometry by cp.async into a ring of LS
 //                slots, LS - 1 subapertures ahead (its copies' completion arrives on the slot's barrier);
-//   warps 7..18  producers: per final subaperture they build A' and B' (128 rows x Qfp
-//                each) in shared memory from the staged slot, a row's ramp by a complex recurrence along q seeded in
-//                float64, converted to the operand type, into a ring of S stages (K-major, no swizzle: core
-//                matrices of 8 rows x 16 bytes);
+//   warps 7..18  producers: per final subaperture they build A' and B' (128 rows x Qfp each) in shared memory from
+//                the staged slot, a row's ramp by a complex recurrence along q seeded in float64, converted to the
+//                operand type, into a ring of S stages (K-major, no swizzle: core matrices of 8 rows x 16 bytes);
 //   warps 4, 5   one thread each issues tcgen05.mma: warp 4 + k takes the final subapertures p = k mod 2 of every
 //                unit into its own accumulator (two 128-column accumulators per issuer, 512 TMEM columns), from its
 //                own stages k, k + 2, ... of the ring (a stage with one consumer, so that no parity wait can run two

@@ -468,8 +468,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             // Warp w reads TMEM lane quarter q = w % 4 (A' rows 32 q .. 32 q + 31: children 16 q .. 16 q + 15) and
             // column half g = w / 4 of the tile. A 16x256b load of row group h (rows 32 q + 16 h ..) gives thread l the
             // Mr and Mi rows of child cc + 8 h (cc = 16 q + l / 4) at columns jl, jl + 1 (jl = 2 (l % 4)) of an 8-column
-            // chunk: each thread forms re/im of its two children at two columns with no exchange between threads, the
-            // two columns as packed float32 pairs.
+            // chunk: each thread forms re/im of its two children at two columns with no exchange between threads.
             const int q = warp & 3, g = warp >> 2;
             const int cc = 16 * q + (lane >> 2), jl = 2 * (lane & 3);
             const int cw = a.Nt / (NCW / 4);                      // columns of this warp per tile
@@ -480,7 +479,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                 return a.ph + ((size_t)n * a.C + (c < a.C ? c : 0)) * a.P;
             };
             float2 q0[2], qn[2];                                  // the children's (c0, sl): this pulse, the next
-    #pragma unroll
+#pragma unroll
             for (int h = 0; h < 2; ++h) {
                 q0[h] = make_float2(0.f, 0.f);
                 qn[h] = (cc + 8 * h < a.C && npl > 0) ? __ldg(phc(h) + p0) : make_float2(0.f, 0.f);
@@ -489,7 +488,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                 const int pl_i = s / a.ntile, tt = s - pl_i * a.ntile, p = p0 + pl_i;
                 const int db = s & 1;
                 if (tt == 0) {
-    #pragma unroll
+#pragma unroll
                     for (int h = 0; h < 2; ++h) {
                         q0[h] = qn[h];
                         if (cc + 8 * h < a.C && pl_i + 1 < npl) qn[h] = __ldg(phc(h) + p + 1);
@@ -499,10 +498,10 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                 if (!__all_sync(0xffffffffu, mbar_wait(&dfull[db], (uint32_t)((s >> 1) & 1), 200, &s_abort, a.err))) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t base = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(db * 256);
-                // per child: the ramp at this thread's two columns of the first chunk (x parts, y parts), and the
-                // step of 8 columns
+                // per child: the ramp at this thread's first column of the first chunk, its step of one column and of
+                // 8 columns
                 float2 wv[2], st1[2], st8[2];
-    #pragma unroll
+#pragma unroll
                 for (int h = 0; h < 2; ++h) {
                     st1[h] = cis_cycles(q0[h].y * (float)a.Dk);
                     st8[h] = cis_cycles(q0[h].y * (float)(8 * a.Dk));
@@ -603,7 +602,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                     }
                     // even lane (Mr row) keeps columns 0..3 of the chunk, odd lane (Mi row) columns 4..7
                     float mr_r[4], mr_i[4], mi_r[4], mi_i[4];
-    #pragma unroll
+#pragma unroll
                     for (int i = 0; i < 4; ++i) {
                         const float sr = odd ? vr[i] : vr[4 + i], si = odd ? vi[i] : vi[4 + i];
                         const float rr = __shfl_xor_sync(0xffffffffu, sr, 1), ri = __shfl_xor_sync(0xffffffffu, si, 1);
@@ -618,7 +617,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                     wc = cmul(wc, st8);
                     if (live && j0 < a.Ko) {
                         uint32_t outw[4];
-    #pragma unroll
+#pragma unroll
                         for (int i = 0; i < 4; ++i) {
                             const float re = mr_r[i] - mi_i[i], im = mr_i[i] + mi_r[i];
                             const float2 o = cmul(w, make_float2(re, im));
@@ -630,7 +629,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                     }
                     tmem_wait_ld();
                     if (more && k8 + 16 >= cw) release();
-    #pragma unroll
+#pragma unroll
                     for (int i = 0; i < 8; ++i) {
                         vr[i] = nr[i];
                         vi[i] = ni[i];
