@@ -158,6 +158,8 @@ TC_LEVEL_CASES = [
     (1, 200, 900, 64, 3, 10, 0.6),    # 64 children (every accumulator row), several column tiles
     (2, 120, 700, 56, 7, 8, 0.45),    # 56 children, 57 frequency taps
     (8, 90, 160, 30, 5, 6, 0.6),      # many parents, 30 children
+    (3, 70, 700, 12, 9, 4, 0.45),     # 12 children, 73 taps (accumulator rows repeated: lane quarters 1, 3 idle)
+    (2, 60, 500, 32, 6, 5, 0.45),     # 32 children, the most with the rows repeated
     (2, 100, 800, 56, 9, 8, 0.45),    # 73 frequency taps (K padded to 80)
     (1, 90, 1200, 40, 10, 6, 0.5),    # 90 frequency taps (K padded to 96)
 ]
