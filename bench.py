@@ -33,8 +33,10 @@ one CUDA graph, with per-pass errors and pairwise coherence against float64.
 
 --impl reference: the reference's own CPU implementation (its fastsar/ffbp_cpu.cpp kernels, compiled from its
 sources by oracle/Makefile, driven by the oracle's restatement of its host orchestration) on this host's cores, on
-a bounded sample of the same workload: a fixed subset of the first level's children, whose work is a fixed
-fraction of the image's; rank 0 alone runs and prints.
+the same workload and config: per step one group of 4 first-level children (1/16 of the image's work), the groups
+in turn, so that 16 steps form the whole image; its history (the same geometry, targets and corner reflectors) is
+synthesized on the host by the oracle, so that the arm loads no library of the product; rank 0 alone runs and
+prints. The GPU arm's `parity` compares its images with the reference former's pixels of one group (no gain).
 """
 import argparse
 import json
@@ -148,31 +150,57 @@ def launch_work(plan, launches):
     return out
 
 
-def cpu_sample(w, S_host, steps, warmup, kind):
-    """The reference CPU former on a bounded sample of the workload: the first-level children of `children`.
-    -> (GBP/s of the sample, threads, description)."""
+def child_groups(plan, per=4):
+    """The first level's children in groups of `per`, each group spread over the image (group g: children g, g + n,
+    g + 2 n, ... with n = G / per): a bounded sample of the image's work per group, all groups together the image."""
+    G = plan['levels'][0]['C']
+    per = max(1, min(per, G))
+    n = (G + per - 1) // per
+    return [[g + n * j for j in range(per) if g + n * j < G] for g in range(n)]
+
+
+def cpu_sample(w, S_host, steps, warmup, kind, rotate=False):
+    """The reference CPU former (the oracle's driver over the reference's kernels, or its port) on a bounded sample
+    of the workload: per call the first-level children of one group (child_groups), the first group each call, or
+    with rotate the groups in turn. -> dict(gbps, threads, desc, seconds per call, image of the first group's call,
+    plan, children of that group)."""
     sys.path.insert(0, os.path.join(ROOT, 'oracle'))
     import oracle as O
     col = w['col']
     form, plan = O.image_former(col.ant, col.fmin, col.df, col.K, w['nx'], w['ny'], w['spx'], w['spy'], w['e1'],
                                 w['e2'], kind=kind)
-    G = plan['levels'][0]['C']
-    nch = max(1, G // 16)
-    children = list(range(0, G, G // nch))[:nch]
-    pix = O.children_pixels(plan, children)
-    times = []
+    groups = child_groups(plan)
+    times, pix, first = [], 0, None
     for i in range(warmup + steps):
+        ch = groups[i % len(groups)] if rotate else groups[0]
         t0 = time.perf_counter()
-        form(S_host, ng=8, children=children)
+        img = form(S_host, ng=8, children=ch)
         dt = time.perf_counter() - t0
+        if first is None and ch == groups[0]:
+            first = img
         if i >= warmup:
             times.append(dt)
-    t = float(np.median(times))
+            pix += O.children_pixels(plan, ch)
+    t = float(np.sum(times))
     gbps = pix * col.Np / t / 1e9
     threads = O.lib(kind).ffbp_cpu_threads()
-    desc = (f'{len(children)} of the {G} first-level children ({pix} of {w["nx"] * w["ny"]} pixels, all '
-            f'{col.Np} pulses), median of {len(times)} warm calls of {t:.2f} s')
-    return gbps, threads, desc, t
+    G = plan['levels'][0]['C']
+    desc = (f'{len(groups[0])} of the {G} first-level children per call (1/{len(groups)} of the image; '
+            + ('the groups in turn, ' if rotate else 'the first group, ')
+            + f'{len(times)} timed calls after {warmup}: {pix} pixels x {col.Np} pulses in {t:.2f} s)')
+    return dict(gbps=gbps, threads=threads, desc=desc, seconds=t / max(1, len(times)), image=first, plan=plan,
+                children=groups[0])
+
+
+def bench_config(args, w, world):
+    """The `config` of the JSON line, the same in both arms: the workload and the form it is measured on."""
+    col = w['col']
+    return dict(workload=f'{args.workload}: {col.Np} pulses x {col.K} samples -> {w["nx"]} x {w["ny"]} px at '
+                         f'{w["spx"]} m',
+                form=f"chosen form precision='float16', taps='learned', pmax={CHOSEN_PMAX}, against plain float32 "
+                     "FFBP",
+                l2=f'inputs larger than L2 ({col.Np * col.K * 8 / 1e9:.2f} GB history per step), no flush',
+                parallelism=f'replicas x{world}' if world > 1 else 'single GPU')
 
 
 def main():
@@ -248,6 +276,7 @@ def main():
         e1.record()
         torch.cuda.synchronize()
         c = clk.stop() if clk else None
+        former.check()                    # a run whose tensor-core pipeline aborted is not a timing
         barrier()
         return max_over_ranks(e0.elapsed_time(e1) / steps), c
 
@@ -320,18 +349,36 @@ def main():
                 ms=kms, algorithmic_bytes=work[k]['bytes'], algorithmic_flops=work[k]['flops'],
                 hbm_frac=gbs / hbm, compute_frac=(fl / fpk) if work[k]['units'] else None)
 
-    # the reference CPU former on this host, bounded sample
-    cpu = None
+    # the reference CPU former on this host, bounded sample; its pixels are also the parity check of both forms
+    # against the reference's own kernels at this size (no gain fitted, the bar of fastsar tests/test_ffbp_cpu.py)
+    cpu, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             sys.path.insert(0, os.path.join(ROOT, 'oracle'))
             import oracle as O
             kind = 'reference' if O.available('reference') else 'port'
-            Sh = S_host.numpy()
-            gbps_c, thr, desc, _ = cpu_sample(w, Sh, 1, 1, kind)
-            cpu = dict(value=gbps_c, unit='GBP/s', cores=thr, kind=kind, sample=desc)
+            r = cpu_sample(w, S_host.numpy(), 1, 1, kind)
+            cpu = dict(value=r['gbps'], unit='GBP/s', cores=r['threads'], kind=kind, sample=r['desc'])
+            m = O.children_mask(r['plan'], r['children'])
+            ref_px = r['image'][m]
+            a_plain, a_chosen = out_plain.cpu().numpy()[m], out.cpu().numpy()[m]
+            parity = dict(plain_vs_reference=O.err_db(a_plain, ref_px), chosen_vs_reference=O.err_db(a_chosen, ref_px),
+                          plain_peak_ratio=float(np.abs(a_plain).max() / np.abs(ref_px).max()),
+                          reference=f'the reference CPU former ({kind} kernels) on the pixels of first-level children '
+                                    f'{r["children"]} ({int(m.sum())} pixels), no gain fitted')
+            log(f'[bench] parity on {int(m.sum())} pixels: plain {parity["plain_vs_reference"]:.1f} dB, chosen '
+                f'{parity["chosen_vs_reference"]:.1f} dB vs the reference former')
         except Exception as e:  # the baseline is reported, never required
             log(f'[bench] cpu baseline failed: {type(e).__name__}: {e}')
+
+    # one image host to host, nothing in flight before or after it (the reference's protocol, docs/performance.md:
+    # 5-9): upload, formation, download
+    ts = []
+    for _ in range(max(2, min(args.steps, 5))):
+        t0 = time.perf_counter()
+        chosen.form_many([S_host], [img_host])
+        ts.append(time.perf_counter() - t0)
+    ms_single = 1e3 * float(np.median(ts))
 
     value = world * npix * P / (ms * 1e-3) / 1e9
     nlaunch = chosen._dev.launches()
@@ -340,13 +387,10 @@ def main():
         ms_per_step=ms, higher_is_better=True, scaling='weak', vs_baseline=None,
         dtype='mixed: bf16x3 and f16 tensor products, f16 intermediate, f32 accumulation',
         data=f'synthetic: {w["n_scatterers"]} seeded scatterers simulated on the GPU in float64, noise -40 dB',
-        config=dict(workload=f'{args.workload}: {P} pulses x {col.K} samples -> {w["nx"]} x {w["ny"]} px at '
-                             f'{w["spx"]} m', form=f"precision='float16', taps='learned', pmax={CHOSEN_PMAX}",
-                    T=chosen.T,
-                    taps=[(l['kind_k'], l['kind_p']) for l in plan['levels']], atten_db_fallback=chosen.atten,
-                    levels=[(l['C'], l['Dk'], l['Dp']) for l in plan['levels']],
-                    l2='inputs larger than L2 (1.07 GB history per step), no flush',
-                    parallelism=f'replicas x{world}' if world > 1 else 'single GPU'),
+        config=bench_config(args, w, world),
+        form_plan=dict(T=chosen.T, taps=[(l['kind_k'], l['kind_p']) for l in plan['levels']],
+                       atten_db_fallback=chosen.atten, levels=[(l['C'], l['Dk'], l['Dp']) for l in plan['levels']]),
+        parity=parity,
         err_db=dict(chosen=err_chosen, plain=err_plain, reference='float64 exact backprojection, 64x, linear, '
                     f'{len(idx)} random pixels, one complex gain fitted', no_gain_fitted=err_nofit),
         plain_fp32=dict(value=world * npix * P / (ms_plain * 1e-3) / 1e9, ms_per_step=ms_plain, stages_ms=stages_plain,
@@ -357,7 +401,11 @@ def main():
         roofline=roof,
         cpu_baseline=cpu,
         e2e=dict(value=world * npix * P / (ms_e2e * 1e-3) / 1e9, unit='GBP/s', ms_per_step=ms_e2e,
-                 h2d_bytes_per_step=int(S.numel() * 8), d2h_bytes_per_step=int(npix * 8)),
+                 h2d_bytes_per_step=int(S.numel() * 8), d2h_bytes_per_step=int(npix * 8),
+                 how='ImageFormer.form_many over the steps: each history up and each image back, two images in flight',
+                 single_image_ms=ms_single,
+                 single_image=dict(value=npix * P / (ms_single * 1e-3) / 1e9,
+                                   how='one form_many call of one image, wall clock: upload, formation, download')),
         gpu_launches=nlaunch * args.steps,
         clocks=clocks)
     if rank == 0:
@@ -440,14 +488,18 @@ def run_patches(args):
         return run
     ms_plain = timed(seq(plain, outs_p), args.steps, args.warmup)
     for f in plain:
+        f.check()
         f.release()
     del outs_p
     torch.cuda.empty_cache()
     ms_seq = timed(seq(chosen, outs_c), args.steps, args.warmup)
+    for f in chosen:
+        f.check()
     batch = BatchFormer(chosen, sources=[sp['ci'] for sp in specs])
     for k, S in enumerate(hist):
         batch.histories[k].copy_(S)
     ms_batch = timed(lambda: batch.form_device(check=False), args.steps, args.warmup)
+    batch.check()
     imgs = batch.form_device()
     # errors against float64 64x on random pixels of every patch
     errs = []
@@ -533,6 +585,7 @@ def run_stack(args):
     for col, S in zip(passes, hist):
         f = mk(col)
         ms_plain += timed(lambda: f.form_device(S, out, check=False), max(1, args.steps // 2), 1)
+        f.check()
         f.release()
         del f
         torch.cuda.empty_cache()
@@ -554,6 +607,8 @@ def run_stack(args):
         for buf, S in zip(b.histories, hist[i:i + group]):
             buf.copy_(S)
     ms_batch = timed(lambda: [b.form_device(check=False) for b in batches], args.steps, args.warmup)
+    for b in batches:
+        b.check()
     imgs = [m for b in batches for m in b.form_device()]
     # errors and coherence against float64 64x on random pixels
     n_pix = min(args.err_pixels, nx * ny)
@@ -593,9 +648,41 @@ def run_stack(args):
     print(json.dumps(line), flush=True)
 
 
+def reference_history(w, seed):
+    """The reference arm's input: the workload's geometry and seeded scene (the same targets and corner reflectors as
+    the GPU arm's, whose clutter adds about 10^5 scatterers more and is left out here: the CPU former's time does not
+    depend on the sample values), synthesized on the host cores by the oracle's float64 direct sum, plus the same
+    level of complex Gaussian noise. No code of the product runs (its GPU library is not loaded). -> (S, description)."""
+    import oracle as O
+    from fastsar_b200 import sim
+    col, sc = w['col'], w['scene']
+    rng = np.random.default_rng(seed)
+    ex, ey = sc['extent']
+    pos, amp = sim.scene(rng, ex / w['spx'], ey / w['spy'], w['spx'], w['spy'], w['e1'], w['e2'],
+                         n_points=sc['n_points'], rcs_sigma_db=sc.get('rcs_sigma_db', 0.0),
+                         n_corners=sc.get('n_corners', 0), clutter_db=None, col=col, fill=1.0)
+    t0 = time.time()
+    S = O.simulate(col, pos, amp)
+    sigma = 10.0 ** (sc['noise_db'] / 20.0) / np.sqrt(2.0)
+    nrng = np.random.default_rng(seed + 1)
+    for p0 in range(0, col.Np, 1024):                       # in blocks: the float64 draws of the whole history are 2 GB
+        blk = S[p0:p0 + 1024]
+        blk += (nrng.standard_normal(blk.shape, np.float32) + 1j * nrng.standard_normal(blk.shape, np.float32)) * sigma
+    log(f'[bench] reference arm: {len(amp)} scatterers synthesized on the host in {time.time() - t0:.1f} s')
+    return S, (f'synthetic: the same geometry and {len(amp)} seeded targets and corner reflectors as the GPU arm, '
+               f'synthesized on the host in float64 (clutter left out: the CPU time does not depend on the values), '
+               f'noise {sc["noise_db"]:.0f} dB')
+
+
 def run_reference(args, world, rank):
-    """The reference arm: its CPU former on this host's cores, rank 0 only."""
+    """The reference arm: the reference's own CPU former (its ffbp_cpu.cpp kernels from oracle/_ref, driven by the
+    oracle's restatement of its host orchestration) on this host's cores, rank 0 only; the groups of first-level
+    children in turn, one group per step, so that 16 steps form the whole image. The GPU library is never loaded."""
     if rank != 0:
+        return
+    if not args.workload.startswith('spotlight'):
+        print(json.dumps(dict(impl='reference', unavailable=f'the reference arm runs the spotlight workloads, not '
+                                                            f'{args.workload}')), flush=True)
         return
     sys.path.insert(0, os.path.join(ROOT, 'oracle'))
     ncpu = len(os.sched_getaffinity(0)) if hasattr(os, 'sched_getaffinity') else os.cpu_count()
@@ -603,21 +690,16 @@ def run_reference(args, world, rank):
     os.environ.setdefault('OMP_PROC_BIND', 'close')
     os.environ.setdefault('OMP_PLACES', 'cores')
     import oracle as O
-    kind = 'reference' if O.available('reference') else 'port'
-    import torch
     from fastsar_b200 import sim
-    torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', '0')))
-    w, S = sim.synthetic_history(args.workload, seed=args.seed)
-    Sh = S.cpu().numpy()
-    del S
-    gbps, thr, desc, t = cpu_sample(w, Sh, args.steps, args.warmup, kind)
-    line = dict(metric=METRIC, value=gbps, unit='GBP/s', n_gpus=world, steps=args.steps, warmup=args.warmup,
-                ms_per_step=t * 1e3, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32',
-                data='synthetic (the same seeded history as the GPU arm)', impl='reference',
-                config=dict(workload=f'{args.workload}: {w["col"].Np} pulses x {w["col"].K} samples -> '
-                                     f'{w["nx"]} x {w["ny"]} px at {w["spx"]} m'),
-                cpu_baseline=dict(value=gbps, unit='GBP/s', cores=thr, kind=kind, sample=desc),
-                e2e=dict(value=gbps, unit='GBP/s', h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    kind = 'reference' if O.available('reference') else 'port'
+    w = sim.workload(args.workload)
+    Sh, data = reference_history(w, args.seed)
+    r = cpu_sample(w, Sh, args.steps, args.warmup, kind, rotate=True)
+    line = dict(metric=METRIC, value=r['gbps'], unit='GBP/s', n_gpus=world, steps=args.steps, warmup=args.warmup,
+                ms_per_step=r['seconds'] * 1e3, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32',
+                data=data, impl='reference', config=bench_config(args, w, world),
+                cpu_baseline=dict(value=r['gbps'], unit='GBP/s', cores=r['threads'], kind=kind, sample=r['desc']),
+                e2e=dict(value=r['gbps'], unit='GBP/s', h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     print(json.dumps(line), flush=True)
 
 

@@ -212,7 +212,9 @@ class DevicePlan:
 
     def form(self, S_dev, img_dev, stream=None, check=True):
         """S_dev [P, K] complex64 torch tensor on the device -> img_dev [nx, ny] complex64 (written). check: read back
-        the first non-finite pulse (a wait for the stream) and raise ValueError naming it."""
+        the first non-finite pulse (a wait for the stream) and raise ValueError naming it, and RuntimeError when a
+        tensor-core kernel of this call aborted. Without check nothing waits: an abort is raised by the next call
+        or by check()."""
         import torch
         L = _lib.load()
         stream = torch.cuda.current_stream(self.device) if stream is None else stream
@@ -224,6 +226,23 @@ class DevicePlan:
             raise ValueError(f'phase history has non-finite samples (NaN or inf), the first in pulse {bad.value}; '
                              'zero them (S[~np.isfinite(S)] = 0) or drop the pulses')
         return img_dev
+
+    def check(self, stream=None):
+        """Wait for the stream and raise RuntimeError if a tensor-core kernel of an earlier form call (one made with
+        check=False) aborted because a bounded wait of its pipeline ran out; its image is then incomplete. Each
+        failure is raised once: here, or by the next form call."""
+        import torch
+        L = _lib.load()
+        stream = torch.cuda.current_stream(self.device) if stream is None else stream
+        _lib.check(L.ffbp_plan_check(self.handle, ctypes.c_void_p(stream.cuda_stream)), 'ffbp_plan_check')
+
+    def test_wait(self, kind, limit_us=1000):
+        """Test hook of the failure report: the MMA issuers of this plan's launches of `kind` ('level_tc_gemm',
+        'final_tc', or None to turn it off) first wait limit_us microseconds on a barrier nothing completes, as a
+        stuck pipeline's would, so that the kernel aborts and the failure is reported."""
+        L = _lib.load()
+        k = {None: 0, 'level_tc_gemm': _lib.FFBP_KIND_LEVEL_TC_GEMM, 'final_tc': _lib.FFBP_KIND_FINAL_TC}[kind]
+        _lib.check(L.ffbp_plan_test_wait(self.handle, k, int(limit_us) if k else 0), 'ffbp_plan_test_wait')
 
     def form_timed(self, S_dev, img_dev, stream=None):
         """form with the device time (ms) of each launch: [level 0, ..., level nlev-1, final] (waits for the stream)."""
@@ -277,7 +296,9 @@ class ImageFormer:
     precision='float32' runs the float32 kernels with the reference's filters (70 dB stop band); 'float16' is the
     mixed-precision form: the levels and the final stage on the tensor cores (split bfloat16 products, a float16
     intermediate, float16 final operands, float32 accumulation) with 80 dB filters, whose smaller error leaves room
-    for the reduced-precision arithmetic. atten (an extension of this package) sets the filters' stop band in dB.
+    for the reduced-precision arithmetic. Unlike the reference's precision='float16' (float16 storage on its own
+    plan), this changes the plan: 80 dB filters instead of 70 dB (unless atten is given) and T = 32 always (the
+    tensor-core final stage's tile; a warning when its predicted error misses target_db). atten (an extension of this package) sets the filters' stop band in dB.
     taps (an extension too): 'kaiser' (default, the reference's Kaiser-sinc decimators), 'learned' (the packaged
     learned decimation taps, fastsar_b200.learned: 8-output-sample filters where the network covers a level's
     decimation and pass fraction, Kaiser-sinc ones elsewhere) or a LearnedTaps instance."""
@@ -495,6 +516,12 @@ class ImageFormer:
             S_dev = self._gate(S_dev)
         return self._dev.form(S_dev, out, check=check)
 
+    def check(self):
+        """Wait for the device and raise RuntimeError if a tensor-core kernel of an earlier form_device(check=False)
+        call aborted (a bounded wait of its pipeline ran out, leaving that image incomplete); the next form call
+        raises it otherwise. Each failure is raised once."""
+        self._dev.check()
+
     def form_many(self, histories, images=None):
         """Form a sequence of images from host memory: histories [P, K] complex64 (torch CPU tensors or numpy
         arrays; page-locked torch tensors, `pin_memory=True`, let the copies overlap the formation) -> images
@@ -635,6 +662,15 @@ class BatchFormer:
                                      f'inf), the first in pulse {b}; zero them (S[~np.isfinite(S)] = 0) or drop the '
                                      'pulses')
         return self.images
+
+    def check(self):
+        """Wait for the device and raise RuntimeError if a tensor-core kernel of an earlier form_device(check=False)
+        launch aborted (a bounded wait ran out), naming the image."""
+        for i, f in enumerate(self.formers):
+            try:
+                f.check()
+            except RuntimeError as e:
+                raise RuntimeError(f'image {i}: {e}') from None
 
     def __call__(self, histories):
         """Host histories (one per source) -> numpy images."""

@@ -1,4 +1,5 @@
-"""Single-stage cases of a workload's plan, for timing one kernel at a time and for small profiler captures:
+"""A profiling harness, not part of the former's API: single-stage cases of a workload's plan, for timing one kernel
+at a time and for small profiler captures (the commands of profiles/*.md run it):
 
     python -m fastsar_b200.cases level L1 [--parents 8] [--pulses 2048] [--form tc|fp32] [--taps learned|80|70]
     python -m fastsar_b200.cases final [--tiles 20000] [--mode f16|bf16x3|fp32] [--taps learned|80|70]

@@ -68,6 +68,18 @@ struct ffbp_plan {
     cudaEvent_t ev_up[2] = {}, ev_formed[2] = {}, ev_down[2] = {};
     int *h_status = nullptr;
     int n_status = 0;
+    // the device the plan lives on, and the abort count of its tensor-core kernels: d_aborts (device memory) is
+    // raised by every bounded wait that runs out and is never reset; each form call copies it into h_aborts
+    // (page-locked) at its end, so that the host sees earlier calls' aborts without waiting; `reported` is the count
+    // already returned as an error
+    int device = -1;
+    int *d_aborts = nullptr;
+    int *h_aborts = nullptr;
+    int reported = 0;
+    // test hook (ffbp_plan_test_wait): the kind of launch whose pipeline waits on a barrier nothing completes, and
+    // that wait's limit
+    int test_kind = 0;
+    unsigned test_ns = 0;
 
     template <class T_>
     cudaError_t alloc(T_ **p, size_t count)
@@ -91,8 +103,25 @@ struct ffbp_plan {
         if (up) cudaStreamDestroy(up);
         if (down) cudaStreamDestroy(down);
         if (h_status) cudaFreeHost(h_status);
+        if (h_aborts) cudaFreeHost(h_aborts);
     }
 };
+
+namespace {
+
+const char *const WAIT_MSG = "a tensor-core kernel stopped waiting on its pipeline (a bounded wait ran out) and "
+                             "left its output incomplete";
+
+// FFBP_E_CUDA when the plan's tensor-core kernels aborted since the last report (h_aborts as last copied back).
+int aborted(ffbp_plan *p, const char *when)
+{
+    const int n = *reinterpret_cast<volatile int *>(p->h_aborts);
+    if (n == p->reported) return FFBP_OK;
+    p->reported = n;
+    return fail(FFBP_E_CUDA, "%s: %s", when, WAIT_MSG);
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -130,6 +159,7 @@ int ffbp_plan_create(const ffbp_plan_desc *d, void *stream_, ffbp_plan **out)
         return fail(FFBP_E_ARG, "bad grid: nx %d ny %d Nx %d Ny %d ox %d oy %d", d->nx, d->ny, d->Nx, d->Ny, d->ox, d->oy);
     if (!d->h_ant_f || !d->h_cen_f || !d->h_first_f) return fail(FFBP_E_ARG, "final-stage geometry missing");
     ffbp_plan *p = new ffbp_plan();
+    cudaGetDevice(&p->device);
     p->nlev = d->nlev; p->T = d->T; p->nx = d->nx; p->ny = d->ny; p->Nx = d->Nx; p->Ny = d->Ny;
     p->ox = d->ox; p->oy = d->oy; p->Pf = d->Pf; p->Qf = d->Qf; p->final_mode = d->final_mode;
     p->spx = d->spx; p->spy = d->spy;
@@ -240,6 +270,11 @@ int ffbp_plan_create(const ffbp_plan_desc *d, void *stream_, ffbp_plan **out)
     e = ffbp::launch_final_geom((const double *)dantf, d->Pf, (const double *)dcenf, B, d->e1, d->e2, p->ux, p->uy,
                                 p->ucx, p->ucy, p->rc, s);
     if (e != cudaSuccess) return cleanup(cuda_fail(e, "final geometry kernel"));
+    if ((e = p->alloc(&p->d_aborts, 1)) != cudaSuccess || (e = cudaMemsetAsync(p->d_aborts, 0, sizeof(int), s)) != cudaSuccess)
+        return cleanup(cuda_fail(e, "allocate the abort count"));
+    if ((e = cudaHostAlloc(reinterpret_cast<void **>(&p->h_aborts), sizeof(int), cudaHostAllocDefault)) != cudaSuccess)
+        return cleanup(cuda_fail(e, "allocate the abort count"));
+    *p->h_aborts = 0;
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cleanup(cuda_fail(e, "plan set-up"));
     *out = p;
     return cleanup(FFBP_OK);
@@ -283,6 +318,13 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
                      FormProfile *prof)
 {
     if (!p || !d_S || !d_img || !d_ws) return fail(FFBP_E_ARG, "ffbp_form: null argument");
+    {
+        int dev = -1;
+        cudaGetDevice(&dev);
+        if (dev != p->device) return fail(FFBP_E_ARG, "the plan lives on device %d, but device %d is current", p->device, dev);
+    }
+    // an abort of an earlier call that the host has not been told of yet (no wait: the count as last copied back)
+    if (int rc = aborted(p, "an earlier form call on this plan")) return rc;
     size_t need;
     ffbp_plan_workspace_bytes(p, &need);
     if (ws_bytes < need) return fail(FFBP_E_WORKSPACE, "workspace of %zu bytes, %zu needed", ws_bytes, need);
@@ -293,8 +335,9 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
     float2 *bufA = reinterpret_cast<float2 *>(ws + 256);
     float2 *bufB = reinterpret_cast<float2 *>(ws + 256 + align256(p->bufA * sizeof(float2)));
     void *scratch = ws + 256 + align256(p->bufA * sizeof(float2)) + align256(p->bufB * sizeof(float2));
-    // status words: bad[0] the first non-finite pulse (0x7f7f7f7f: none), bad[1] the tensor-core kernels' wait
-    // status, bad[2 + l] the largest |component| of level l's input (float bits; l = nlev: the final stage's)
+    // status words: bad[0] the first non-finite pulse (0x7f7f7f7f: none), bad[1] unused, bad[2 + l] the largest
+    // |component| of level l's input (float bits; l = nlev: the final stage's). The tensor-core kernels count the
+    // bounded waits that ran out in the plan's d_aborts.
     int *amax = bad + 2;
     cudaError_t e = cudaMemsetAsync(bad, 0x7f, sizeof(int), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(bad + 1, 0, (size_t)(p->nlev + 2) * sizeof(int), s);
@@ -323,9 +366,10 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
         L.Np = v.Np; L.C = v.C; L.P = v.P; L.K = v.K; L.Ko = v.Ko; L.Po = v.Po; L.Dk = v.Dk; L.Lk = v.Lk; L.plk = v.plk;
         L.Dp = v.Dp; L.Lp = v.Lp; L.plp = v.plp; L.kc = v.kc;
         L.amax = amax + l + 1;
+        L.test_wait_ns = p->test_kind == FFBP_KIND_LEVEL_TC_GEMM ? p->test_ns : 0u;
         const char *why = nullptr;
         if (level_on_tc(p, l)) {
-            e = ffbp::launch_level_tc_gemm(L, amax + l, scratch, bad + 1, s, &why);
+            e = ffbp::launch_level_tc_gemm(L, amax + l, scratch, p->d_aborts, s, &why);
             if (!why && e == cudaSuccess) {
                 mark(FFBP_KIND_LEVEL_TC_GEMM << 8 | l);
                 e = ffbp::launch_level_tc_fir(L, amax + l, scratch, s, &why);
@@ -343,26 +387,28 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
     F.d = in; F.B = p->ntiles; F.Pf = p->Pf; F.Qf = p->Qf; F.T = p->T; F.ux = p->ux; F.uy = p->uy;
     F.spx = p->spx; F.spy = p->spy; F.a0 = p->a0; F.a1 = p->a1; F.fc2 = p->fc2; F.ucx = p->ucx; F.ucy = p->ucy;
     F.rc = p->rc; F.w = p->wf; F.tiles = nullptr; F.img = static_cast<float2 *>(d_img); F.first = p->first;
-    F.nx = p->nx; F.ny = p->ny; F.ox = p->ox; F.oy = p->oy; F.scale = 1.f; F.err = bad + 1;
+    F.nx = p->nx; F.ny = p->ny; F.ox = p->ox; F.oy = p->oy; F.scale = 1.f; F.err = p->d_aborts;
     F.amax = amax + p->nlev;
+    F.test_wait_ns = p->test_kind == FFBP_KIND_FINAL_TC ? p->test_ns : 0u;
     const int fm = p->final_mode & 0xff;
     const char *why = nullptr;
     e = fm == FFBP_FINAL_FP32 ? ffbp::launch_final_fp32(F, s, &why) : ffbp::launch_final_tc(F, fm, s, &why);
     if (why) return fail(FFBP_E_UNSUPPORTED, "final stage: %s", why);
     if (e != cudaSuccess) return cuda_fail(e, "final kernel");
     mark((fm == FFBP_FINAL_FP32 ? FFBP_KIND_FINAL : FFBP_KIND_FINAL_TC) << 8 | p->nlev);
+    // the abort count back to the host once this call's kernels are done (read by the next call, or below)
+    if ((e = cudaMemcpyAsync(p->h_aborts, p->d_aborts, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+        return cuda_fail(e, "status read");
     if (prof) {
-        if ((e = cudaEventSynchronize(prof->ev.back())) != cudaSuccess) return cuda_fail(e, "form");
-        int st = 0;
-        if ((e = cudaMemcpy(&st, bad + 1, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess) return cuda_fail(e, "status read");
-        if (st) return fail(FFBP_E_CUDA, "a tensor-core kernel stopped waiting on its pipeline (a bounded wait ran out)");
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "form");
+        if (int rc = aborted(p, "ffbp_form")) return rc;
     }
     if (h_bad) {
-        int v[2] = {0, 0};
-        if ((e = cudaMemcpyAsync(v, bad, 2 * sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return cuda_fail(e, "status read");
+        int v = 0;
+        if ((e = cudaMemcpyAsync(&v, bad, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return cuda_fail(e, "status read");
         if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "form");
-        *h_bad = (v[0] == 0x7f7f7f7f) ? -1 : v[0];
-        if (v[1]) return fail(FFBP_E_CUDA, "a tensor-core kernel stopped waiting on its pipeline (a bounded wait ran out)");
+        *h_bad = (v == 0x7f7f7f7f) ? -1 : v;
+        if (int rc = aborted(p, "ffbp_form")) return rc;
     }
     return FFBP_OK;
 }
@@ -422,7 +468,7 @@ int ffbp_form_host(ffbp_plan *p, const void *const *h_S, void *const *h_img, int
             (e = cudaStreamWaitEvent(s, p->ev_up[b], 0)) != cudaSuccess ||
             (i >= 2 && (e = cudaStreamWaitEvent(s, p->ev_down[b], 0)) != cudaSuccess)) { rc = cuda_fail(e, "ffbp_form_host"); break; }
         if ((rc = form_impl(p, dS[b], dI[b], d_ws, ws_bytes, stream, nullptr, nullptr)) != FFBP_OK) break;
-        if ((e = cudaMemcpyAsync(p->h_status + 2 * i, bad, 2 * sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        if ((e = cudaMemcpyAsync(p->h_status + 2 * i, bad, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
             (e = cudaEventRecord(p->ev_formed[b], s)) != cudaSuccess ||
             (e = cudaStreamWaitEvent(p->down, p->ev_formed[b], 0)) != cudaSuccess ||
             (e = cudaMemcpyAsync(h_img[i], dI[b], ib, cudaMemcpyDeviceToHost, p->down)) != cudaSuccess ||
@@ -433,12 +479,8 @@ int ffbp_form_host(ffbp_plan *p, const void *const *h_S, void *const *h_img, int
     if (rc != FFBP_OK) return rc;
     if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
         return cuda_fail(e1 != cudaSuccess ? e1 : e2 != cudaSuccess ? e2 : e3, "ffbp_form_host");
-    for (int i = 0; i < n; ++i) {
-        h_bad[i] = p->h_status[2 * i] == 0x7f7f7f7f ? -1 : p->h_status[2 * i];
-        if (p->h_status[2 * i + 1])
-            return fail(FFBP_E_CUDA, "image %d: a tensor-core kernel stopped waiting on its pipeline (a bounded wait ran out)", i);
-    }
-    return FFBP_OK;
+    for (int i = 0; i < n; ++i) h_bad[i] = p->h_status[2 * i] == 0x7f7f7f7f ? -1 : p->h_status[2 * i];
+    return aborted(p, "ffbp_form_host");
 }
 
 }  // extern "C"
@@ -448,7 +490,8 @@ int ffbp_form_host(ffbp_plan *p, const void *const *h_S, void *const *h_img, int
 // graph launch replaces them all.
 struct ffbp_batch {
     int n = 0;
-    std::vector<const int *> status;     // each plan's workspace status words (first non-finite pulse, wait status)
+    std::vector<const int *> status;     // each plan's workspace status word (first non-finite pulse)
+    std::vector<ffbp_plan *> plans;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int *h_status = nullptr;             // page-locked, 2 n ints
@@ -514,7 +557,10 @@ int ffbp_batch_create(ffbp_plan *const *plans, int n, const void *const *d_S, vo
     cleanup();
     if (rc != FFBP_OK) { delete b; return rc; }
     if (e != cudaSuccess || e2 != cudaSuccess) { delete b; return cuda_fail(e != cudaSuccess ? e : e2, "ffbp_batch_create: graph"); }
-    for (int i = 0; i < n; ++i) b->status.push_back(static_cast<const int *>(d_ws[i]));
+    for (int i = 0; i < n; ++i) {
+        b->status.push_back(static_cast<const int *>(d_ws[i]));
+        b->plans.push_back(plans[i]);
+    }
     if ((e = cudaHostAlloc(reinterpret_cast<void **>(&b->h_status), 2 * (size_t)n * sizeof(int), cudaHostAllocDefault)) != cudaSuccess) {
         delete b;
         return cuda_fail(e, "ffbp_batch_create: status array");
@@ -527,18 +573,19 @@ int ffbp_batch_form(ffbp_batch *b, void *stream, int *h_bad)
 {
     if (!b) return fail(FFBP_E_ARG, "ffbp_batch_form: null batch");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // aborts of earlier launches that the host has not been told of (the counts as last copied back)
+    for (int i = 0; i < b->n; ++i)
+        if (aborted(b->plans[i], "an earlier batch launch") != FFBP_OK) return fail(FFBP_E_CUDA, "image %d: %s", i, WAIT_MSG);
     cudaError_t e = cudaGraphLaunch(b->exec, s);
     if (e != cudaSuccess) return cuda_fail(e, "ffbp_batch_form");
     if (!h_bad) return FFBP_OK;
     for (int i = 0; i < b->n && e == cudaSuccess; ++i)
-        e = cudaMemcpyAsync(b->h_status + 2 * i, b->status[i], 2 * sizeof(int), cudaMemcpyDeviceToHost, s);
+        e = cudaMemcpyAsync(b->h_status + 2 * i, b->status[i], sizeof(int), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_fail(e, "ffbp_batch_form");
-    for (int i = 0; i < b->n; ++i) {
-        h_bad[i] = b->h_status[2 * i] == 0x7f7f7f7f ? -1 : b->h_status[2 * i];
-        if (b->h_status[2 * i + 1])
-            return fail(FFBP_E_CUDA, "image %d: a tensor-core kernel stopped waiting on its pipeline (a bounded wait ran out)", i);
-    }
+    for (int i = 0; i < b->n; ++i) h_bad[i] = b->h_status[2 * i] == 0x7f7f7f7f ? -1 : b->h_status[2 * i];
+    for (int i = 0; i < b->n; ++i)
+        if (aborted(b->plans[i], "ffbp_batch_form") != FFBP_OK) return fail(FFBP_E_CUDA, "image %d: %s", i, WAIT_MSG);
     return FFBP_OK;
 }
 
@@ -551,6 +598,26 @@ int ffbp_batch_destroy(ffbp_batch *b)
 int ffbp_form(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, size_t ws_bytes, void *stream, int *h_bad)
 {
     return form_impl(p, d_S, d_img, d_ws, ws_bytes, stream, h_bad, nullptr);
+}
+
+int ffbp_plan_check(ffbp_plan *p, void *stream)
+{
+    if (!p) return fail(FFBP_E_ARG, "ffbp_plan_check: null plan");
+    cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "ffbp_plan_check");
+    return aborted(p, "a form call on this plan");
+}
+
+int ffbp_plan_test_wait(ffbp_plan *p, int kind, unsigned limit_us)
+{
+    if (!p) return fail(FFBP_E_ARG, "ffbp_plan_test_wait: null plan");
+    if (kind != 0 && kind != FFBP_KIND_LEVEL_TC_GEMM && kind != FFBP_KIND_FINAL_TC)
+        return fail(FFBP_E_ARG, "ffbp_plan_test_wait: kind %d is neither 0, FFBP_KIND_LEVEL_TC_GEMM nor FFBP_KIND_FINAL_TC", kind);
+    if (kind != 0 && (limit_us < 1 || limit_us > 1000000))
+        return fail(FFBP_E_ARG, "ffbp_plan_test_wait: limit of %u us outside 1 .. 1000000", limit_us);
+    p->test_kind = kind;
+    p->test_ns = kind ? limit_us * 1000u : 0u;
+    return FFBP_OK;
 }
 
 int ffbp_form_timed(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, size_t ws_bytes, void *stream,

@@ -94,10 +94,11 @@ __device__ __forceinline__ uint64_t global_ns()
 }
 
 // Bounded wait for the phase of parity `parity` of *bar: false (and the block's abort flag and *err set) when it
-// has not completed after WAIT_NS of wall time, or when another thread of the block has aborted. HINT_NS is the
+// has not completed after limit_ns of wall time, or when another thread of the block has aborted. HINT_NS is the
 // suspend-time hint of each poll (0: poll without one).
 template <uint32_t HINT_NS>
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort, int *err)
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort, int *err,
+                                          uint64_t limit_ns = WAIT_NS)
 {
     if (mbar_test(bar, parity)) return true;
     const uint64_t t0 = global_ns();
@@ -105,11 +106,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volati
         if (HINT_NS ? mbar_test_sleep(bar, parity, HINT_NS) : mbar_test(bar, parity)) return true;
         if ((it & 255u) == 0) {
             if (*abort) return false;
-            if (global_ns() - t0 > WAIT_NS) break;
+            if (global_ns() - t0 > limit_ns) break;
         }
     }
     *abort = 1;
-    if (err) atomicExch(err, 1);
+    if (err) atomicAdd(err, 1);
     return false;
 }
 
@@ -172,6 +173,7 @@ struct TcArgs {
     int *err;
     const int *amax;
     int interleave;                        // the order of the producer warps' items (final_tc_kernel)
+    unsigned test_wait_ns;                 // tests only: the issuers' wait on a barrier nothing completes (0: none)
 };
 
 // The power of two s that brings samples whose components are at most *amax (a float's bits; null: unknown) to
@@ -279,6 +281,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
     uint64_t *lfull = drain + 2, *lempty = lfull + LS;
     __shared__ uint32_t s_tmem;
     __shared__ volatile int s_abort;
+    __shared__ uint64_t s_never;                                // a barrier nothing arrives on (the tests' stuck wait)
 
     const int t = threadIdx.x, warp = t / 32, lane = t % 32;
     const int nis = a.nis;
@@ -299,6 +302,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
             mbar_init(&lfull[k], 32);                      // the loader's 32 threads, once their copies have landed
             mbar_init(&lempty[k], NPW);
         }
+        mbar_init(&s_never, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == NEPI) {
@@ -518,7 +522,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
             const int rs = a.S / nis;
             int slot = 0;                                       // this issuer's stages: k + nis slot
             uint32_t par = 0;
-            for (int ul = 0; ul < nul; ++ul) {
+            // tests of the failure report: a wait that runs out before any MMA, as a stuck pipeline's would
+            const bool stuck = a.test_wait_ns &&
+                               !mbar_wait<ISSUER_HINT_NS>(&s_never, 0, &s_abort, a.err, a.test_wait_ns);
+            for (int ul = stuck ? nul : 0; ul < nul; ++ul) {
                 const int ab = ul & 1;
                 if (!mbar_wait<ISSUER_HINT_NS>(&acce[ab], (uint32_t)(((ul >> 1) & 1) ^ 1), &s_abort, a.err)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -655,6 +662,7 @@ cudaError_t launch_final_tc(const FinalLaunch &F, int mode, cudaStream_t s, cons
     a.ux = F.ux; a.uy = F.uy; a.spx = F.spx; a.spy = F.spy; a.a0 = F.a0; a.a1 = F.a1; a.fc2 = F.fc2;
     a.ucx = F.ucx; a.ucy = F.ucy; a.rc = F.rc; a.w = F.w; a.tiles = F.tiles; a.img = F.img; a.first = F.first;
     a.nx = F.nx; a.ny = F.ny; a.ox = F.ox; a.oy = F.oy; a.scale = F.scale; a.err = F.err; a.amax = F.amax;
+    a.test_wait_ns = F.test_wait_ns;
     int dev = 0, nsm = 148, maxsmem = 227 * 1024;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);

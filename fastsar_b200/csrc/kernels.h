@@ -18,6 +18,8 @@ struct LevelLaunch {
     int Np, C, P, K, Ko, Po, Dk, Lk, plk, Dp, Lp, plp;
     double kc;
     int *amax = nullptr;  // or the largest |component| of the output, as float bits (atomicMax; start at 0)
+    unsigned test_wait_ns = 0;   // tensor-core pass 1 only, for tests of the failure report: when nonzero the MMA
+                                 // issuer first waits this long on a barrier nothing completes, as a stuck pipeline
 };
 
 // Returns cudaSuccess, or an error with *why set to a static message for shapes the kernels do not cover.
@@ -26,7 +28,7 @@ cudaError_t launch_level(const LevelLaunch &L, cudaStream_t s, const char **why)
 // A level on the tensor cores (level_tc.cu): the frequency FIR of every child as one product per pulse (bfloat16
 // x 3, float32 accumulation) into a float16 intermediate in `scratch` (level_tc_scratch_bytes), then the pulse FIR
 // in float32. amax_in: the largest |component| of L.x (float bits), which sets the intermediate's scale; L.amax
-// receives the output's. err: set when a bounded wait runs out.
+// receives the output's. err: raised (atomicAdd) when a bounded wait runs out.
 bool level_tc_supported(int C, int Lk, int Dk);
 size_t level_tc_scratch_bytes(int Np, int C, int P, int Ko);
 cudaError_t launch_level_tc(const LevelLaunch &L, const int *amax_in, void *scratch, int *err, cudaStream_t s,
@@ -63,8 +65,9 @@ struct FinalLaunch {
     const int2 *first;    // [B] first pixel of each tile on the padded grid
     int nx, ny, ox, oy;
     float scale;
-    int *err = nullptr;   // set to 1 by a kernel whose bounded wait ran out (tensor-core stage), or null
+    int *err = nullptr;   // raised (atomicAdd) by a kernel whose bounded wait ran out (tensor-core stage), or null
     const int *amax = nullptr;   // the largest |component| of d (float bits), for the float16 operands' scale
+    unsigned test_wait_ns = 0;   // tensor-core stage only, for tests of the failure report (as in LevelLaunch)
 };
 cudaError_t launch_final_fp32(const FinalLaunch &F, cudaStream_t s, const char **why);
 cudaError_t launch_final_tc(const FinalLaunch &F, int mode, cudaStream_t s, const char **why);

@@ -83,9 +83,10 @@ __device__ __forceinline__ uint64_t global_ns()
     return t;
 }
 
-// Bounded wait for the phase of parity `parity`: false (the block's abort flag and *err set) after WAIT_NS, or when
-// another thread of the block has aborted.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t hint_ns, volatile int *abort, int *err)
+// Bounded wait for the phase of parity `parity`: false (the block's abort flag set and *err raised) after limit_ns,
+// or when another thread of the block has aborted.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t hint_ns, volatile int *abort, int *err,
+                                          uint64_t limit_ns = WAIT_NS)
 {
     if (mbar_test(bar, parity, 0)) return true;
     const uint64_t t0 = global_ns();
@@ -93,11 +94,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32
         if (mbar_test(bar, parity, hint_ns)) return true;
         if ((it & 255u) == 0) {
             if (*abort) return false;
-            if (global_ns() - t0 > WAIT_NS) break;
+            if (global_ns() - t0 > limit_ns) break;
         }
     }
     *abort = 1;
-    if (err) atomicExch(err, 1);
+    if (err) atomicAdd(err, 1);
     return false;
 }
 
@@ -172,6 +173,7 @@ struct GemmArgs {
     int *err;
     int Np, C, P, K, Ko, Kop, Dk, Lk, plk, Lkp, Nt, ntile, W, pseg, nseg, SB;
     float kc;
+    unsigned test_wait_ns;            // tests only: the MMA issuer's wait on a barrier nothing completes (0: none)
 };
 
 // The power of two that brings values up to 4 amax (the taps' absolute sum is below 4 for the decimators of any
@@ -207,6 +209,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
     __shared__ uint32_t s_tmem;
     __shared__ volatile int s_abort;
     __shared__ float s_scale;
+    __shared__ uint64_t s_never;                             // a barrier nothing arrives on (the tests' stuck wait)
 
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int n = blockIdx.x / a.nseg, seg = blockIdx.x % a.nseg;
@@ -232,6 +235,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             mbar_init(&pfull[i], NLT);
             mbar_init(&pempty[i], NHT);
         }
+        mbar_init(&s_never, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int i = t; i < a.Lkp; i += NTHR) s_tk[i] = i < a.Lk ? (a.tk ? a.tk[i] : 1.f) : 0.f;   // Dk = 1: one tap 1
@@ -439,7 +443,9 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             const uint32_t sA0 = smem_u32(sA), sB0 = smem_u32(sB);
             int sb = 0;
             uint32_t sbpar = 0;
-            for (int s = 0; s < nst; ++s) {
+            // tests of the failure report: a wait that runs out before any MMA, as a stuck pipeline's would
+            const bool stuck = a.test_wait_ns && !mbar_wait(&s_never, 0, 0, &s_abort, a.err, a.test_wait_ns);
+            for (int s = stuck ? nst : 0; s < nst; ++s) {
                 const int pl_i = s / a.ntile, tt = s - pl_i * a.ntile;
                 const int ab = pl_i & 1, db = s & 1;
                 if (tt == 0 && !mbar_wait(&afull[ab], (uint32_t)((pl_i >> 1) & 1), 0, &s_abort, a.err)) break;
@@ -836,7 +842,7 @@ cudaError_t launch_level_tc_gemm(const LevelLaunch &L, const int *amax_in, void 
     a.x = L.x; a.ph = L.phase; a.tk = L.tk; a.wp = L.wp; a.wk = L.wk; a.bad = L.bad; a.amax_in = amax_in;
     a.y = static_cast<__half2 *>(scratch); a.err = err;
     a.Np = L.Np; a.C = L.C; a.P = L.P; a.K = L.K; a.Ko = L.Ko; a.Kop = (L.Ko + 3) & ~3; a.Dk = L.Dk; a.Lk = Lk;
-    a.plk = plk; a.Lkp = ((Lk + 15) / 16) * 16; a.kc = (float)L.kc;
+    a.plk = plk; a.Lkp = ((Lk + 15) / 16) * 16; a.kc = (float)L.kc; a.test_wait_ns = L.test_wait_ns;
     int dev = 0, maxsmem = 227 * 1024;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);

@@ -36,6 +36,7 @@ def time_former(f, S_dev, reps=3):
         e1.record()
         torch.cuda.synchronize()
         ts.append(e0.elapsed_time(e1))
+    f.check()                                        # a candidate whose pipeline aborted is not timed as a success
     return float(np.median(ts))
 
 
@@ -60,7 +61,7 @@ def tune_former(make, candidates, S_dev, target_db=-60.0, reps=3):
             continue
         try:
             ms = time_former(f, S_dev, reps)
-        except ValueError as e:                      # a shape a kernel refuses (FFBP_E_UNSUPPORTED)
+        except (ValueError, RuntimeError) as e:      # a shape a kernel refuses (FFBP_E_UNSUPPORTED), or an abort
             table.append((kw, err, f'not formed: {str(e)[:60]}'))
             f.release()
             del f

@@ -112,11 +112,28 @@ int ffbp_plan_destroy(ffbp_plan *plan);
 int ffbp_plan_workspace_bytes(const ffbp_plan *plan, size_t *bytes);
 
 /* Form the image: d_S [P0, K0] complex64 phase history (unwindowed; the plan's window is applied here) ->
- * d_img [nx, ny] complex64. d_ws: the workspace (ffbp_plan_workspace_bytes, 256-byte aligned). Asynchronous on
- * `stream`. The first non-finite sample's pulse index (or -1) is written to h_bad_pulse when it is not NULL,
- * which makes the call wait for the stream. Replaces form(S) of fastsar/ffbp_cuda.py:1084-1211.                */
+ * d_img [nx, ny] complex64. d_ws: the workspace (ffbp_plan_workspace_bytes, 256-byte aligned). The device the plan
+ * was created on must be current (FFBP_E_ARG otherwise). Asynchronous on `stream`. The first non-finite sample's
+ * pulse index (or -1) is written to h_bad_pulse when it is not NULL, which makes the call wait for the stream.
+ * Failure reports of the tensor-core kernels: every bounded wait of theirs that runs out (a pipeline that stopped
+ * making progress, which leaves that call's image incomplete) is counted in the plan. With h_bad_pulse the call
+ * waits and returns FFBP_E_CUDA when its own kernels aborted; without it, the failure is returned by the plan's
+ * next form call (FFBP_E_CUDA, before it launches anything) or by ffbp_plan_check. Each failure is reported once.
+ * Replaces form(S) of fastsar/ffbp_cuda.py:1084-1211.                                                            */
 int ffbp_form(ffbp_plan *plan, const void *d_S, void *d_img, void *d_ws, size_t ws_bytes, void *stream,
               int *h_bad_pulse);
+
+/* Wait for `stream` and return FFBP_E_CUDA if a tensor-core kernel of an earlier form call on this plan aborted
+ * (a bounded wait ran out) and that has not been reported yet. For callers of ffbp_form without h_bad_pulse, after
+ * a batch of calls (the reference raises from inside form(), fastsar/ffbp_cuda.py:1084-1211).                    */
+int ffbp_plan_check(ffbp_plan *plan, void *stream);
+
+/* Test hook of the failure report above (no counterpart in the reference): from the next form call on, the MMA
+ * issuers of the plan's launches of `kind` (FFBP_KIND_LEVEL_TC_GEMM or FFBP_KIND_FINAL_TC) first wait on a barrier
+ * that nothing completes, with a limit of limit_us microseconds (1 .. 10^6), so that the wait runs out as a stuck
+ * pipeline's would and the kernel winds down without its MMAs; kind 0 turns it off. The kernels stay well-formed:
+ * every wait is bounded and the block frees its tensor memory before it exits.                                 */
+int ffbp_plan_test_wait(ffbp_plan *plan, int kind, unsigned limit_us);
 
 /* Form n images from host memory, overlapping each history's upload and each image's download with the
  * formation of its neighbours (the reference's pinned double-buffered upload, fastsar/ffbp_cuda.py:692-765,
@@ -124,7 +141,8 @@ int ffbp_form(ffbp_plan *plan, const void *d_S, void *d_img, void *d_ws, size_t 
  * (pageable memory works, without the overlap). d_stage: two device histories and two device images,
  * ffbp_plan_host_bytes bytes, 256-byte aligned; d_ws: the form workspace. The formation runs on `stream`, the copies
  * on two streams of the plan. Returns when every image is in host memory; h_bad[i] is image i's first non-finite
- * pulse (or -1). No counterpart in the reference's API.                                                         */
+ * pulse (or -1); FFBP_E_CUDA when a tensor-core kernel of one of the calls aborted. No counterpart in the
+ * reference's API.                                                         */
 int ffbp_plan_host_bytes(const ffbp_plan *plan, size_t *bytes);
 int ffbp_form_host(ffbp_plan *plan, const void *const *h_S, void *const *h_img, int n, void *d_stage,
                    size_t stage_bytes, void *d_ws, size_t ws_bytes, void *stream, int *h_bad);
@@ -133,8 +151,10 @@ int ffbp_form_host(ffbp_plan *plan, const void *const *h_S, void *const *h_img, 
  * captures the n form calls once into a CUDA graph, each plan's launches on a branch of its own so that the kernels
  * of different plans run side by side, on the buffers given here: d_S[i] (plan i's history), d_img[i] (its image),
  * d_ws[i] (its workspace of ws_bytes[i], 256-byte aligned; one per plan, they run at once). The call runs no
- * kernel (it captures on a stream of its own; `stream` is unused). ffbp_batch_form launches the graph on `stream` (the buffers' current contents are formed); with h_bad
- * (n ints) it waits and writes each image's first non-finite pulse (or -1). No counterpart in the reference,
+ * kernel (it captures on a stream of its own; `stream` is unused). ffbp_batch_form launches the graph on `stream`
+ * (the buffers' current contents are formed); with h_bad (n ints) it waits, writes each image's first non-finite
+ * pulse (or -1) and returns FFBP_E_CUDA when a tensor-core kernel aborted (without h_bad: at the next launch, or by
+ * ffbp_plan_check on the plan). No counterpart in the reference,
  * which forms patches one after the other (fastsar/patches.py:619-972).                                      */
 typedef struct ffbp_batch ffbp_batch;
 int ffbp_batch_create(ffbp_plan *const *plans, int n, const void *const *d_S, void *const *d_img, void *const *d_ws,
@@ -193,7 +213,7 @@ int ffbp_level(const void *d_x, int Np, int P, int K, const void *d_phase, int C
  * accumulated in float32; the ramp exp(2 pi i (c0 + sl (Dk j - plk - kc))); a float16 intermediate in d_scratch
  * (ffbp_level_tc_scratch_bytes, 16-byte aligned), scaled by a power of two from the input's largest component;
  * the pulse FIR in float32. C <= 64 and Lk <= 96 (FFBP_E_UNSUPPORTED otherwise). d_status: 3 ints, zeroed by the
- * caller: [0] set when a bounded wait of the kernel ran out, [1] the input's largest |component| (float bits,
+ * caller: [0] nonzero when a bounded wait of the kernel ran out, [1] the input's largest |component| (float bits,
  * filled here), [2] the output's. No counterpart in the reference (its levels run in float32 only).            */
 size_t ffbp_level_tc_scratch_bytes(int Np, int C, int P, int Ko);
 int ffbp_level_tc(const void *d_x, int Np, int P, int K, const void *d_phase, int C, const float *d_tk, int Lk, int plk,

@@ -11,6 +11,9 @@
  *   final_tiles                 fastsar/ffbp_cpu.cpp:302-469  the separable T x T tile sum and the quadratic phase
  *   bp_points_f64               fastsar/bp.py:99-137          exact backprojection at points (here with float64
  *                                                            profiles as well: the FP64 oracle)
+ *   simulate_points             fastsar/sim.py:69-90          phase history of point scatterers (the benchmark's
+ *                                                            reference arm synthesizes its input with it, so that
+ *                                                            arm runs no code of the product)
  *
  * The entry points keep the reference's C names and signatures (float32 inputs and outputs), so that one driver
  * (oracle/oracle.py) runs either this port or the reference's own compiled kernels. The arithmetic differs on
@@ -243,5 +246,77 @@ void bp_points_f64(const double* prof, int P, int nfft, const double* tx, const 
         }
         out[2 * n] += ar;
         out[2 * n + 1] += ai;
+    }
+}
+
+/* Phase history of point scatterers for the reference arm of the benchmark (fastsar/sim.py:69-90 computes the same
+   sum): S[p, k] += sum_n amp[n] exp(-4 pi i (fmin + k df) dR_pn / c), dR_pn = |pos[n] - ant[p]| - |ant[p]|, float64
+   throughout; along k each scatterer's term is a geometric sequence, stepped by a complex product and re-seeded from
+   the exact phase every 256 samples. S [P, K] complex64 interleaved (added to); amp [N] complex128 interleaved.
+   Pulses in parallel. */
+/* built for the host's widest vectors at run time (AVX-512, AVX2 or the x86-64 baseline) */
+__attribute__((target_clones("avx512f", "avx2", "default")))
+void simulate_points(const double* ant, int P, int K, double fmin, double df, const double* pos, const double* amp,
+                     int N, float* S)
+{
+    const double C = 299792458.0;
+    enum { SEG = 256, VB = 8 };
+    const int NP = (N + VB - 1) / VB * VB;
+#pragma omp parallel
+    {
+        double* dr = (double*)malloc(sizeof(double) * (size_t)NP);
+        double* am = (double*)malloc(sizeof(double) * 2 * (size_t)NP);
+#pragma omp for schedule(dynamic, 4)
+        for (int p = 0; p < P; ++p) {
+            const double* a = ant + 3 * p;
+            const double ra = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+            for (int n = 0; n < NP; ++n) {
+                if (n < N) {
+                    const double* q = pos + 3 * (size_t)n;
+                    const double dx = q[0] - a[0], dy = q[1] - a[1], dz = q[2] - a[2];
+                    dr[n] = sqrt(dx * dx + dy * dy + dz * dz) - ra;
+                    am[2 * n] = amp[2 * (size_t)n];
+                    am[2 * n + 1] = amp[2 * (size_t)n + 1];
+                } else {
+                    dr[n] = am[2 * n] = am[2 * n + 1] = 0.0;
+                }
+            }
+            float* out = S + 2 * (size_t)p * K;
+            for (int k0 = 0; k0 < K; k0 += SEG) {
+                const int k1 = k0 + SEG < K ? k0 + SEG : K;
+                double ar[SEG], ai[SEG];
+                for (int k = 0; k < k1 - k0; ++k) ar[k] = ai[k] = 0.0;
+                for (int n0 = 0; n0 < NP; n0 += VB) {
+                    double zr[VB], zi[VB], wr[VB], wi[VB];
+                    for (int j = 0; j < VB; ++j) {
+                        double c, s;
+                        /* the phase in cycles, -2 (fmin + k df) dR / c, at k0; the step of one sample */
+                        cis_cycles(-2.0 * (fmin + k0 * df) * dr[n0 + j] / C, &c, &s);
+                        zr[j] = am[2 * (n0 + j)] * c - am[2 * (n0 + j) + 1] * s;
+                        zi[j] = am[2 * (n0 + j)] * s + am[2 * (n0 + j) + 1] * c;
+                        cis_cycles(-2.0 * df * dr[n0 + j] / C, &wr[j], &wi[j]);
+                    }
+                    for (int k = 0; k < k1 - k0; ++k) {
+                        double sr = 0.0, si = 0.0;
+#pragma omp simd reduction(+ : sr, si)
+                        for (int j = 0; j < VB; ++j) {
+                            sr += zr[j];
+                            si += zi[j];
+                            const double tr = zr[j] * wr[j] - zi[j] * wi[j];
+                            zi[j] = zr[j] * wi[j] + zi[j] * wr[j];
+                            zr[j] = tr;
+                        }
+                        ar[k] += sr;
+                        ai[k] += si;
+                    }
+                }
+                for (int k = k0; k < k1; ++k) {
+                    out[2 * k] += (float)ar[k - k0];
+                    out[2 * k + 1] += (float)ai[k - k0];
+                }
+            }
+        }
+        free(dr);
+        free(am);
     }
 }

@@ -5,10 +5,11 @@ product (fastsar_b200) never imports it.
 Parity is pinned: tests/test_oracle.py checks this module's kernels and images against the reference's own outputs
 (tests/golden, written by tests/golden/make_golden.py from saulpingerman/FastSAR 0.3.1).
 
-Two CPU implementations of the reference's factorized backprojection run through one driver (`make_ffbp`), which
-restates the reference's host orchestration fastsar/ffbp_cpu.py:158-293 (level-0 children in groups, each carried
-through the later levels, the float64 child phases of the deeper levels, the final-stage geometry, the tile
-assembly and the crop):
+`simulate` synthesizes point-scatterer histories on the host cores (the benchmark's reference arm, which must run no
+code of the product). Two CPU implementations of the reference's factorized backprojection run through one driver
+(`make_ffbp`), which restates the reference's host orchestration fastsar/ffbp_cpu.py:158-293 (level-0 children in
+groups, each carried through the later levels, the float64 child phases of the deeper levels, the final-stage
+geometry, the tile assembly and the crop):
 
   kind='port'       oracle/liboracle.so, the float64 restatement of the kernels in oracle/ffbp_oracle.c
   kind='reference'  oracle/_ref/libffbp_cpu_ref_*.so, the reference's fastsar/ffbp_cpu.cpp compiled from its own
@@ -73,6 +74,8 @@ def lib(kind='port'):
     L.ffbp_cpu_threads.restype = i
     if kind == 'port':
         L.bp_points_f64.argtypes = [f64, i, i, f64, vp, f64, f64, ctypes.c_long, dbl, dbl, f64]
+        L.simulate_points.argtypes = [f64, i, i, dbl, dbl, f64, f64, i, f32]
+        L.simulate_points.restype = None
     _LIBS[kind] = L
     return L
 
@@ -282,6 +285,27 @@ def image_former(ant, fmin, df, K, nx, ny, spx, spy, e1=(1.0, 0.0, 0.0), e2=(0.0
             S = S.astype(np.complex64)
         return inner(np.ascontiguousarray(S), ng, children)
     return form, plan
+
+
+def children_mask(plan, children):
+    """[nx, ny] bool: the pixels of the cropped image that the given level-0 children form."""
+    sx0, sy0 = plan['levels'][0]['sx'], plan['levels'][0]['sy']
+    mx, my = plan['Nx'] // sx0, plan['Ny'] // sy0
+    full = np.zeros((plan['Nx'], plan['Ny']), bool)
+    for g in children:
+        x, y = g // sy0, g % sy0
+        full[x * mx:(x + 1) * mx, y * my:(y + 1) * my] = True
+    return full[plan['ox']:plan['ox'] + plan['nx'], plan['oy']:plan['oy'] + plan['ny']]
+
+
+def simulate(col, pos, amp):
+    """Phase history [P, K] complex64 of point scatterers on the host cores (the port's simulate_points, float64)."""
+    S = np.zeros((col.Np, col.K), np.complex64)
+    amp = np.ascontiguousarray(amp, np.complex128)
+    lib('port').simulate_points(np.ascontiguousarray(col.ant, np.float64), col.Np, col.K, float(col.fmin),
+                                float(col.df), np.ascontiguousarray(pos, np.float64), amp.view(np.float64), len(amp),
+                                S.view(np.float32))
+    return S
 
 
 def children_pixels(plan, children):

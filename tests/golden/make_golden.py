@@ -1,8 +1,9 @@
 """Generate the golden fixtures under tests/golden from the reference implementation (saulpingerman/FastSAR 0.3.1).
 
-Run in a container where the reference's sources are present (default /root/reference, or --ref PATH):
+Run where the reference's sources are present, naming their directory by --ref or the FASTSAR_REFERENCE environment
+variable:
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    FASTSAR_REFERENCE=<reference checkout> python tests/golden/make_golden.py [--only exact|gate|weights]
 
 The reference's modules fastsar/ffbp.py and fastsar/ffbp2.py import JAX at module level but its planner and CPU paths
 use only NumPy, so a stub `jax` package is inserted before the import; its C++ kernels are compiled by its own
@@ -19,6 +20,9 @@ Fixtures:
   gate.npz            the range gate: _gate_plan on wide-band and spotlight geometries, the gated history of a seeded
                       random history (first pulses), and ImageFormer(backend='cpu', range_gate=True)'s image of a
                       simulated wide-band scene (python tests/golden/make_golden.py --only gate writes this file alone)
+  weights.npz         aperture weights: api.final_weights (plain and with gradients) of the test scene's 2-level plan
+                      for a pixel- and pulse-dependent weight (WEIGHT below), and ImageFormer(backend='cpu',
+                      aperture_weight=WEIGHT)'s image (--only weights writes this file alone)
 """
 import argparse
 import os
@@ -180,12 +184,51 @@ def gate(fastsar):
     np.savez_compressed(os.path.join(HERE, 'gate.npz'), **rec)
 
 
+def weight_fn(P):
+    """The aperture weight of the weights fixture: weight(points [m, 3], pulses [n]) -> [n, m], a raised cosine over
+    the pulses times a gentle linear ramp over the scene (pixel-dependent, so the gradient terms matter).
+    tests/test_plan.py and tests/test_gpu_weights.py build the same function."""
+    def w(q, p):
+        q, p = np.asarray(q, np.float64), np.asarray(p, np.float64)
+        over_p = 0.55 + 0.45 * np.cos(np.pi * (p - 0.5 * (P - 1)) / P)
+        over_q = 1.0 + 0.006 * q[:, 0] - 0.004 * q[:, 1]
+        return over_p[:, None] * over_q[None, :]
+    return w
+
+
+def weights(fastsar):
+    """weights.npz: the reference's final_weights and its CPU former's image with an aperture weight."""
+    from fastsar import sim, ffbp2, api
+    c_small = sim.make_collect(res=0.5, scene=60.0, r0=5e3)
+    rng = np.random.default_rng(1)                                 # the scene of fastsar tests/test_ffbp_cpu.py
+    pos = np.stack([rng.uniform(-25, 25, 40), rng.uniform(-25, 25, 40), np.zeros(40)], 1)
+    amp = rng.standard_normal(40) + 1j * rng.standard_normal(40)
+    S = sim.simulate_brute(c_small, pos, amp).astype(np.complex64)
+    P = S.shape[0]
+    wfun = weight_fn(P)
+    plan = ffbp2.make_plan(c_small, 128, 128, 0.5, 0.5, T=16, nlev=2, pmax=0.4, e1=(1.0, 0.0, 0.0), e2=(0.0, 1.0, 0.0))
+    # the history is image_small.npz's (the same seeded scene), so it is not stored again
+    rec = dict(w_plain=api.final_weights(plan, wfun, P), w_grad=api.final_weights(plan, wfun, P, grad=True),
+               w_centre=api.final_weights(plan, wfun, P, nodes=1))
+    for nlev in (2, 3):
+        f = api.ImageFormer(c_small.ant, c_small.fmin, c_small.df, c_small.K, 128, 128, 0.5, 0.5, backend='cpu', T=16,
+                            levels=nlev, window=False, aperture_weight=wfun)
+        rec[f'img_l{nlev}'] = f(S)
+    np.savez_compressed(os.path.join(HERE, 'weights.npz'), **rec)
+    print('weights done', rec['w_grad'].shape)
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('--ref', default='/root/reference')
-    ap.add_argument('--only', choices=('exact', 'gate'), default=None)
+    ap.add_argument('--ref', default=os.environ.get('FASTSAR_REFERENCE'))
+    ap.add_argument('--only', choices=('exact', 'gate', 'weights'), default=None)
     args = ap.parse_args()
+    if not args.ref:
+        sys.exit('make_golden: name the reference checkout by --ref PATH or FASTSAR_REFERENCE')
     fs = import_reference(args.ref)
+    if args.only == 'weights':
+        weights(fs)
+        return
     if args.only == 'exact':
         from fastsar import sim
         from fastsar.exact import ExactFormer

@@ -1,0 +1,80 @@
+"""Failure reports of the tensor-core kernels, on a B200, without a GPU fault.
+
+Every wait of the tensor-core pipelines (level pass 1, final stage) is bounded; one that runs out sets the block's
+abort flag, the block winds down (no MMA left in flight, its tensor memory freed) and the plan's abort count rises.
+The test hook ffbp_plan_test_wait makes the MMA issuers first wait, with a limit of a few milliseconds, on a barrier
+that nothing completes: the wait runs out exactly as a stuck pipeline's would. The tests check that the failure is
+reported whichever way the caller forms (check=False: by check() or by the next call; check=True: by the call
+itself), that it is reported once, and that the plan then forms correct images again."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip('torch')
+if not torch.cuda.is_available():
+    pytest.skip('no CUDA device', allow_module_level=True)
+
+
+def _former(golden):
+    from fastsar_b200 import ImageFormer, sim
+    g = golden('image_spot512')
+    w = sim.workload('spotlight_512')
+    col = w['col']
+    f = ImageFormer(col.ant, col.fmin, col.df, col.K, 512, 512, 0.25, 0.25, w['e1'], w['e2'], precision='float16')
+    return f, torch.from_numpy(g['S']).cuda()
+
+
+@pytest.mark.parametrize('kind', ['level_tc_gemm', 'final_tc'])
+def test_bounded_wait_that_runs_out_is_reported(golden, kind):
+    f, S = _former(golden)
+    want = f.form_device(S).cpu().numpy()
+    out = torch.empty((512, 512), dtype=torch.complex64, device='cuda')
+    f._dev.test_wait(kind, 2000)
+    # without check the call returns at once; the abort is raised by check(), once
+    f.form_device(S, out, check=False)
+    with pytest.raises(RuntimeError, match='bounded wait ran out'):
+        f.check()
+    f.check()
+    # with check the call waits and raises its own abort
+    with pytest.raises(RuntimeError, match='bounded wait ran out'):
+        f.form_device(S, out)
+    # an abort of a check=False call is raised by the plan's next call, before it launches anything
+    f.form_device(S, out, check=False)
+    torch.cuda.synchronize()
+    with pytest.raises(RuntimeError, match='earlier form call'):
+        f.form_device(S, out, check=False)
+    f.check()
+    # the hook off: the same plan forms the same image as before, bit for bit
+    f._dev.test_wait(None)
+    got = f.form_device(S).cpu().numpy()
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_batch_reports_an_abort(golden):
+    """A batch's graph holds the launches as captured: captured with the hook on, every launch of it aborts, and
+    each abort is reported (by the launch that waits, or by the next launch)."""
+    from fastsar_b200 import BatchFormer
+    f, S = _former(golden)
+    f._dev.test_wait('final_tc', 2000)
+    batch = BatchFormer([f])
+    batch.histories[0].copy_(S)
+    with pytest.raises(RuntimeError, match='image 0'):
+        batch.form_device()
+    batch.form_device(check=False)
+    torch.cuda.synchronize()
+    with pytest.raises(RuntimeError, match='image 0'):
+        batch.form_device(check=False)
+    batch.check()
+    del batch
+    f._dev.test_wait(None)
+
+
+def test_test_hook_rejects_bad_arguments(golden):
+    from fastsar_b200 import _lib
+    f, _ = _former(golden)
+    L = _lib.load()
+    with pytest.raises(ValueError, match='kind'):
+        _lib.check(L.ffbp_plan_test_wait(f._dev.handle, 5, 100), 'ffbp_plan_test_wait')
+    with pytest.raises(ValueError, match='limit'):
+        _lib.check(L.ffbp_plan_test_wait(f._dev.handle, _lib.FFBP_KIND_FINAL_TC, 0), 'ffbp_plan_test_wait')

@@ -151,3 +151,27 @@ def test_metrics_detect_a_planted_error(golden, oracle_lib):
     e = oracle_lib.err_db(bad, ref)
     assert -60 < e < -30, e
     assert oracle_lib.rel_db(2j * ref, ref) < -150
+
+
+@pytest.mark.parametrize('nlev', [2, 3])
+def test_oracle_aperture_weight_image(golden, oracle_lib, nlev):
+    """The oracle's weighted final stage (w0, gx, gyr per tile and subaperture, fastsar/ffbp_cpu.cpp:302-469) with the
+    weights of plan.final_weights against the reference CPU former's image with the same aperture_weight
+    (tests/golden/weights.npz): the float64 port within -90 dB, the reference's own kernels within -110 dB."""
+    from fastsar_b200 import plan as P_
+    from fastsar_b200.sim import Collect
+    from test_plan import weight_fn
+    img, g = golden('image_small'), golden('weights')
+    fmin, df, K = img['scal']
+    ant = img['ant']
+    col = Collect(fmin=float(fmin), df=float(df), K=int(K), ant=ant, res=0.5)
+    plan = P_.make_plan(col, 128, 128, 0.5, 0.5, T=16, nlev=nlev, pmax=0.4, e1=(1.0, 0.0, 0.0), e2=(0.0, 1.0, 0.0))
+    coll = P_.collection_arrays(plan, ant)
+    wf = P_.final_weights(plan, weight_fn(ant.shape[0]), ant.shape[0], grad=True)
+    O = oracle_lib
+    got = O.make_ffbp(plan, coll, 'port', wf=wf)(img['S'])
+    assert O.err_db(got, g[f'img_l{nlev}']) < -90.0
+    if O.available('reference'):
+        got = O.make_ffbp(plan, coll, 'reference', wf=wf)(img['S'])
+        d = np.abs(got - g[f'img_l{nlev}']) ** 2
+        assert d.sum() <= 10 ** -11 * np.sum(np.abs(g[f'img_l{nlev}']) ** 2)

@@ -141,3 +141,28 @@ def test_decimator_rows_sum_to_one():
                 F[i, j] = fr['kern'][r]
     interior = slice(fr['L'], 300 - fr['L'])
     np.testing.assert_allclose(F.sum(1)[interior], 1.0, atol=1e-12)
+
+
+def weight_fn(P):
+    """The aperture weight of tests/golden/weights.npz (tests/golden/make_golden.py weight_fn): a raised cosine over
+    the pulses times a linear ramp over the scene."""
+    def w(q, p):
+        q, p = np.asarray(q, np.float64), np.asarray(p, np.float64)
+        over_p = 0.55 + 0.45 * np.cos(np.pi * (p - 0.5 * (P - 1)) / P)
+        over_q = 1.0 + 0.006 * q[:, 0] - 0.004 * q[:, 1]
+        return over_p[:, None] * over_q[None, :]
+    return w
+
+
+def test_final_weights_match_reference(golden):
+    """plan.final_weights against the reference's api.final_weights (fastsar/api.py:203-244) on the test scene's
+    2-level plan: the Gauss-Legendre mean, the centre-pulse form and the gradient form, to float32 rounding."""
+    g, img = golden('weights'), golden('image_small')
+    fmin, df, K = img['scal']
+    col = Collect(fmin=float(fmin), df=float(df), K=int(K), ant=img['ant'], res=0.5)
+    plan = P_.make_plan(col, 128, 128, 0.5, 0.5, T=16, nlev=2, pmax=0.4, e1=(1.0, 0.0, 0.0), e2=(0.0, 1.0, 0.0))
+    P = img['ant'].shape[0]
+    w = weight_fn(P)
+    np.testing.assert_allclose(P_.final_weights(plan, w, P), g['w_plain'], rtol=1e-6, atol=1e-7)
+    np.testing.assert_allclose(P_.final_weights(plan, w, P, nodes=1), g['w_centre'], rtol=1e-6, atol=1e-7)
+    np.testing.assert_allclose(P_.final_weights(plan, w, P, grad=True), g['w_grad'], rtol=1e-5, atol=1e-7)
