@@ -31,6 +31,9 @@ collections formed by one CUDA graph, against the same formers one after another
 --workload stack_8: a repeat-pass stack (run_stack): 8 passes of one scene formed to a common 8,192 x 8,192 grid by
 one CUDA graph, with per-pass errors and pairwise coherence against float64.
 
+--workload learned_4k: the learned decimation taps against the Kaiser-sinc decimators at oversamplings of the child
+data from 4x to about 1x (run_learned): error against float64 and time per image, the float32 former throughout.
+
 --impl reference: the reference's own CPU implementation (its fastsar/ffbp_cpu.cpp kernels, compiled from its
 sources by oracle/Makefile, driven by the oracle's restatement of its host orchestration) on this host's cores, on
 the same workload and config: per step one group of 4 first-level children (1/16 of the image's work), the groups
@@ -111,6 +114,8 @@ def launch_work(plan, launches):
     [(kind, level, ms)]:
       level_fp32     bytes: the input samples, the child phases, the output samples; flops: the rotation (8 per
                      input sample and child) and the two FIRs (4 per tap and output sample, complex by real);
+      level_tc       (one pass) bytes: the input samples, the phases, the output samples; flops: the children's
+                     frequency FIR as a complex product, 8 C Lk Ko per parent and pulse, and the pulse FIR;
       level_tc_gemm  bytes: the input samples, the phases, the float16 intermediate written (4 per sample); flops:
                      the children's frequency FIR as a complex product, 8 C Lk Ko per parent and pulse;
       level_tc_fir   bytes: the intermediate read and the output written; flops: 4 Lp per output sample;
@@ -141,6 +146,9 @@ def launch_work(plan, launches):
         if kind == 'level_fp32':
             out.append(dict(bytes=float(8 * (Np * P * K + N * P + N * Po * Ko)),
                             flops=float(N * P * (8.0 * K + 4.0 * Lk * Ko) + N * Po * Ko * 4.0 * Lp), units='fp32'))
+        elif kind == 'level_tc':
+            out.append(dict(bytes=float(8 * (Np * P * K + N * P + N * Po * Ko)),
+                            flops=float(8.0 * N * P * Lk * Ko + 4.0 * N * Po * Ko * Lp), units='tensor'))
         elif kind == 'level_tc_gemm':
             out.append(dict(bytes=float(8 * (Np * P * K + N * P) + 4 * N * P * Ko),
                             flops=float(8.0 * N * P * Lk * Ko), units='tensor'))
@@ -224,6 +232,8 @@ def main():
         return run_patches(args)
     if args.workload.startswith('stack'):
         return run_stack(args)
+    if args.workload.startswith('learned'):
+        return run_learned(args)
 
     import torch
     import torch.distributed as dist
@@ -645,6 +655,67 @@ def run_stack(args):
                     reference=f'float64 exact backprojection, 64x, {n_pix} random pixels, no gain fitted'),
         coherence=dict(max_abs_diff_vs_float64=max(dcoh), float64_range=[round(min(cref), 4), round(max(cref), 4)],
                        pairs=len(pairs)))
+    print(json.dumps(line), flush=True)
+
+
+def run_learned(args):
+    """--workload learned_4k: the learned decimation taps against the reference's Kaiser-sinc decimators on the
+    4,096-pulse x 4,096-sample spotlight (the 512-pulse spotlight's geometry: 9.6 GHz, 300 MHz, 600 km, 45 deg,
+    1.5 deg) formed to 2,048 x 2,048 pixels at 0.25 m, the float32 former (levels and final stage) throughout so that
+    the filters alone differ. The oversampling of the child data is 1 / pmax: pmax 0.95, 0.5 and 0.25 are the "1x",
+    "2x" and "4x" of a child's extent. Per row: the error against the float64 exact backprojection at 64x on 4,096
+    random pixels (no gain fitted), the device time per image, the filters each level got. One GPU; one JSON line."""
+    import torch
+    from fastsar_b200 import sim, ImageFormer
+    from fastsar_b200.exact import backproject_device, plane_points
+    torch.cuda.set_device(0)
+    w, S = sim.synthetic_history('spotlight_4k', seed=args.seed, n_clutter=20000)
+    col = w['col']
+    nx, ny = w['nx'], w['ny']
+    idx = np.random.default_rng(9).choice(nx * ny, 4096, replace=False)
+    pts = plane_points(nx, ny, w['spx'], w['spy'], w['e1'], w['e2']).reshape(-1, 3)[idx]
+    ref = backproject_device(S, col.ant, col.fmin, col.df, pts, upsample=64).cpu().numpy()
+    it = torch.from_numpy(idx).cuda()
+    rows = []
+    cases = [('kaiser', 70.0, 0.25), ('kaiser', 70.0, 0.4), ('kaiser', 70.0, 0.5), ('kaiser', 80.0, 0.25),
+             ('kaiser', 80.0, 0.5), ('learned', 80.0, 0.5), ('learned', 80.0, 0.55), ('learned', 80.0, 0.65),
+             ('learned', 80.0, 0.75), ('learned', 80.0, 0.95)]
+    out = torch.empty((nx, ny), dtype=torch.complex64, device='cuda')
+    for taps, atten, pmax in cases:
+        try:
+            f = ImageFormer(col.ant, col.fmin, col.df, col.K, nx, ny, w['spx'], w['spy'], w['e1'], w['e2'],
+                            taps=taps, atten=atten, pmax=pmax)
+        except ValueError as e:
+            rows.append(dict(taps=taps, atten=atten, pmax=pmax, error=str(e)[:80]))
+            continue
+        f.form_device(S, out)
+        ts = []
+        for _ in range(max(3, args.steps)):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            f.form_device(S, out, check=False)
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        f.check()
+        a = out.reshape(-1)[it].cpu().numpy().astype(np.complex128)
+        db = float(10 * np.log10(np.sum(np.abs(a - ref) ** 2) / np.sum(np.abs(ref) ** 2)))
+        lv = f._plan['levels']
+        rows.append(dict(taps=taps, atten=atten, pmax=pmax, oversampling=round(1.0 / pmax, 2), err_db=round(db, 2),
+                         ms=round(float(np.median(ts)), 3),
+                         kinds=[(l['kind_k'], l['kind_p']) for l in lv],
+                         taps_per_level=[((l['fir_k'] or {}).get('L', 1), (l['fir_p'] or {}).get('L', 1)) for l in lv],
+                         final=(f._plan['final']['P'], f._plan['final']['K'])))
+        log(f'[bench] {taps} {atten:.0f} dB pmax {pmax}: {db:.1f} dB, {np.median(ts):.2f} ms')
+        f.release()
+        del f
+        torch.cuda.empty_cache()
+    line = dict(metric='error (dB vs float64 64x) and time per image of the decimation filters, learned against '
+                       'Kaiser-sinc, by oversampling', unit='dB / ms', n_gpus=1, steps=args.steps,
+                data='synthetic: spotlight_4k, seeded targets, clutter -30 dB, noise -40 dB, simulated in float64',
+                config=dict(workload='learned_4k: 4096 pulses x 4096 samples -> 2048 x 2048 px at 0.25 m, float32 '
+                                     'former', oversampling='1 / pmax of the child extent'),
+                rows=rows)
     print(json.dumps(line), flush=True)
 
 

@@ -12,8 +12,10 @@ LIB_PATH = os.path.join(HERE, 'libffbp_b200.so')
 FFBP_OK, FFBP_E_ARG, FFBP_E_CUDA, FFBP_E_NOMEM, FFBP_E_WORKSPACE, FFBP_E_UNSUPPORTED = 0, -1, -2, -3, -4, -5
 FFBP_FINAL_FP32, FFBP_FINAL_TC_F16, FFBP_FINAL_TC_BF16X3 = 0, 1, 2
 FFBP_LEVELS_TC = 0x100
-KIND_NAMES = {1: 'amax', 2: 'level_fp32', 3: 'level_tc_gemm', 4: 'level_tc_fir', 5: 'final_fp32', 6: 'final_tc'}
-FFBP_KIND_LEVEL_TC_GEMM, FFBP_KIND_FINAL_TC = 3, 6
+KIND_NAMES = {1: 'amax', 2: 'level_fp32', 3: 'level_tc_gemm', 4: 'level_tc_fir', 5: 'final_fp32', 6: 'final_tc',
+              7: 'level_tc'}
+FFBP_KIND_LEVEL_TC_GEMM, FFBP_KIND_FINAL_TC, FFBP_KIND_LEVEL_TC = 3, 6, 7
+FFBP_LEVELS_TC2 = 0x200
 
 # every symbol include/ffbp_b200.h declares
 EXPORTS = ('ffbp_last_error', 'ffbp_abi_version', 'ffbp_plan_create', 'ffbp_plan_destroy', 'ffbp_plan_workspace_bytes',
@@ -22,7 +24,7 @@ EXPORTS = ('ffbp_last_error', 'ffbp_abi_version', 'ffbp_plan_create', 'ffbp_plan
            'ffbp_form_profile', 'ffbp_exact_pad', 'ffbp_exact_backproject', 'ffbp_mlp_param_count',
            'ffbp_mlp_max_decimation', 'ffbp_mlp_work_bytes', 'ffbp_plan_host_bytes', 'ffbp_form_host', 'ffbp_gate_pad',
            'ffbp_gate_fold', 'ffbp_gate_taper', 'ffbp_batch_create', 'ffbp_batch_form', 'ffbp_batch_destroy', 'ffbp_mlp_taps', 'ffbp_mlp_grad', 'ffbp_mlp_train_step',
-           'ffbp_plan_check', 'ffbp_plan_test_wait')
+           'ffbp_plan_check', 'ffbp_plan_test_wait', 'ffbp_level_fused')
 
 _c_int, _c_double, _vp = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
 
@@ -42,7 +44,7 @@ class PlanDesc(ctypes.Structure):
                 ('e1', _c_double * 3), ('e2', _c_double * 3), ('Pf', _c_int), ('Qf', _c_int),
                 ('f0f', _c_double), ('dff', _c_double), ('fcf', _c_double),
                 ('h_ant_f', _vp), ('h_cen_f', _vp), ('h_first_f', _vp), ('h_wp', _vp), ('h_wk', _vp),
-                ('h_wf', _vp), ('wf_ndim', _c_int), ('final_mode', _c_int)]
+                ('h_wf', _vp), ('wf_ndim', _c_int), ('final_mode', _c_int), ('partial', _c_int)]
 
 
 _LIB = None
@@ -91,6 +93,8 @@ def load():
                                 _c_double, _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t,
                                 _vp, _vp]
     L.ffbp_level_tc_scratch_bytes.argtypes = [_c_int, _c_int, _c_int, _c_int]
+    L.ffbp_level_fused.argtypes = [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_int,
+                                   _c_double, _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp, _vp]
     L.ffbp_mlp_param_count.argtypes = []
     L.ffbp_mlp_work_bytes.argtypes = [_c_int]
     L.ffbp_mlp_taps.argtypes = [_vp, _vp, _c_int, _vp, _vp, _vp]
@@ -100,9 +104,9 @@ def load():
     L.ffbp_mlp_train_step.argtypes = [_vp, _vp, _vp, _c_int, _vp, ctypes.c_float, _vp, _vp, _c_int, _vp, _vp, _c_int,
                                       ctypes.c_float, _c_int, _vp, _vp, _vp]
     L.ffbp_exact_pad.argtypes = [_vp, _c_int, _c_int, _vp, _vp, _c_int, _vp, _vp, _c_int, _vp]
-    L.ffbp_exact_backproject.argtypes = [_vp, _c_int, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp, _c_int, _c_int, _c_int,
-                                         _c_int, _c_int, _c_int, _c_double, _c_double, _vp, _vp, _c_double, _c_double,
-                                         _c_int, _c_int, _vp, _vp, _vp]
+    L.ffbp_exact_backproject.argtypes = [_vp, _c_int, _c_int, _vp, _vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_int,
+                                         _c_int, _c_double, _c_double, _vp, _vp, _c_double, _c_double, _c_int, _c_int,
+                                         _vp, _vp, _vp]
     L.ffbp_phases.argtypes = [_vp, _c_int, _vp, _c_int, _vp, _c_int, _vp, _c_double, _c_double, _c_int, _vp, _vp]
     L.ffbp_final.argtypes = [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _c_double, _c_double, _c_double,
                              _c_double, _vp, _vp, _vp, _c_double, _vp, _c_int, _vp, _vp]

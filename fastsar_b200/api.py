@@ -101,13 +101,15 @@ def _check_grid(nx, ny, spx, spy, e1, e2):
 
 def _final_mode(precision):
     """The formation mode of a precision: 'float32' the float32 kernels (FASTSAR_FINAL=tc3 puts the final stage on
-    the tensor cores in split bfloat16); 'float16' the levels and the final stage on the tensor cores (FASTSAR_LEVELS=
-    fp32 keeps the levels on the float32 kernel)."""
+    the tensor cores in split bfloat16); 'float16' the levels and the final stage on the tensor cores, the levels in
+    one pass (FASTSAR_LEVELS=tc2: in two passes through a float16 intermediate; fp32: on the float32 kernel)."""
     if precision == 'float16':
         lv = os.environ.get('FASTSAR_LEVELS', 'tc').strip().lower() or 'tc'
-        if lv not in ('tc', 'fp32'):
-            raise ValueError(f"FASTSAR_LEVELS must be 'tc' or 'fp32', got {lv!r}")
-        return _lib.FFBP_FINAL_TC_F16 | (_lib.FFBP_LEVELS_TC if lv == 'tc' else 0)
+        if lv not in ('tc', 'tc1', 'tc2', 'fp32'):
+            raise ValueError(f"FASTSAR_LEVELS must be 'tc', 'tc1', 'tc2' or 'fp32', got {lv!r}")
+        flags = {'tc': _lib.FFBP_LEVELS_TC | _lib.FFBP_LEVELS_TC2, 'tc1': _lib.FFBP_LEVELS_TC,
+                 'tc2': _lib.FFBP_LEVELS_TC | _lib.FFBP_LEVELS_TC2, 'fp32': 0}[lv]
+        return _lib.FFBP_FINAL_TC_F16 | flags
     choice = os.environ.get('FASTSAR_FINAL', 'fp32').strip().lower() or 'fp32'
     if choice not in ('fp32', 'tc3'):
         raise ValueError(f"FASTSAR_FINAL must be 'fp32' or 'tc3', got {choice!r}")
@@ -118,7 +120,8 @@ class DevicePlan:
     """A plan of fastsar_b200.plan uploaded through ffbp_plan_create: the device-resident filters, windows, child
     phases and final-stage geometry, and the workspace of a form call. Owns the library's plan handle."""
 
-    def __init__(self, plan, wp=None, wk=None, wf=None, ref=None, final_mode=_lib.FFBP_FINAL_FP32, device=None):
+    def __init__(self, plan, wp=None, wk=None, wf=None, ref=None, final_mode=_lib.FFBP_FINAL_FP32, device=None,
+                 partial=False):
         import torch
         L = _lib.load()
         self.plan = plan
@@ -165,6 +168,7 @@ class DevicePlan:
         if wf is not None:
             pd.h_wf, pd.wf_ndim = k32(wf), int(wf.ndim)
         pd.final_mode = final_mode
+        pd.partial = 1 if partial or plan.get('partial') else 0
         h = ctypes.c_void_p()
         with torch.cuda.device(self.device):
             stream = torch.cuda.current_stream(self.device)
@@ -237,11 +241,12 @@ class DevicePlan:
         _lib.check(L.ffbp_plan_check(self.handle, ctypes.c_void_p(stream.cuda_stream)), 'ffbp_plan_check')
 
     def test_wait(self, kind, limit_us=1000):
-        """Test hook of the failure report: the MMA issuers of this plan's launches of `kind` ('level_tc_gemm',
-        'final_tc', or None to turn it off) first wait limit_us microseconds on a barrier nothing completes, as a
+        """Test hook of the failure report: the MMA issuers of this plan's launches of `kind` ('level_tc' or
+        'level_tc_gemm': the tensor-core levels in either form; 'final_tc'; None to turn it off) first wait limit_us microseconds on a barrier nothing completes, as a
         stuck pipeline's would, so that the kernel aborts and the failure is reported."""
         L = _lib.load()
-        k = {None: 0, 'level_tc_gemm': _lib.FFBP_KIND_LEVEL_TC_GEMM, 'final_tc': _lib.FFBP_KIND_FINAL_TC}[kind]
+        k = {None: 0, 'level_tc': _lib.FFBP_KIND_LEVEL_TC, 'level_tc_gemm': _lib.FFBP_KIND_LEVEL_TC_GEMM,
+             'final_tc': _lib.FFBP_KIND_FINAL_TC}[kind]
         _lib.check(L.ffbp_plan_test_wait(self.handle, k, int(limit_us) if k else 0), 'ffbp_plan_test_wait')
 
     def form_timed(self, S_dev, img_dev, stream=None):

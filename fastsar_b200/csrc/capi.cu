@@ -151,7 +151,8 @@ int ffbp_plan_create(const ffbp_plan_desc *d, void *stream_, ffbp_plan **out)
     if (d->T != 16 && d->T != 32) return fail(FFBP_E_ARG, "final tile size T must be 16 or 32, got %d", d->T);
     {
         const int fm = d->final_mode & 0xff, flags = d->final_mode & ~0xff;
-        if ((fm != FFBP_FINAL_FP32 && fm != FFBP_FINAL_TC_F16 && fm != FFBP_FINAL_TC_BF16X3) || (flags & ~FFBP_LEVELS_TC))
+        if ((fm != FFBP_FINAL_FP32 && fm != FFBP_FINAL_TC_F16 && fm != FFBP_FINAL_TC_BF16X3) ||
+            (flags & ~(FFBP_LEVELS_TC | FFBP_LEVELS_TC2)))
             return fail(FFBP_E_ARG, "unknown final_mode %d", d->final_mode);
     }
     if (d->nlev > 8) return fail(FFBP_E_ARG, "%d levels, at most 8", d->nlev);
@@ -243,7 +244,8 @@ int ffbp_plan_create(const ffbp_plan_desc *d, void *stream_, ffbp_plan **out)
     p->ntiles = B;
     const ffbp_level_desc &last = d->levels[d->nlev - 1];
     if (p->Pf != last.Po || p->Qf != last.Ko) return cleanup(fail(FFBP_E_ARG, "final stage %dx%d != last level output %dx%d", p->Pf, p->Qf, last.Po, last.Ko));
-    if ((long)B * d->T * d->T != (long)d->Nx * d->Ny) return cleanup(fail(FFBP_E_ARG, "tiles %d of %d^2 do not cover %dx%d", B, d->T, d->Nx, d->Ny));
+    if (d->partial ? (long)B * d->T * d->T > (long)d->Nx * d->Ny : (long)B * d->T * d->T != (long)d->Nx * d->Ny)
+        return cleanup(fail(FFBP_E_ARG, "tiles %d of %d^2 do not %s %dx%d", B, d->T, d->partial ? "fit" : "cover", d->Nx, d->Ny));
     void *q;
     if (d->h_wp) {
         if ((e = upload(d->h_wp, sizeof(float) * d->levels[0].P, &q, true)) != cudaSuccess) return cleanup(cuda_fail(e, "upload window"));
@@ -280,23 +282,36 @@ int ffbp_plan_create(const ffbp_plan_desc *d, void *stream_, ffbp_plan **out)
     return cleanup(FFBP_OK);
 }
 
-// Whether level l runs on the tensor cores (FFBP_LEVELS_TC and a shape the kernel covers).
-static bool level_on_tc(const ffbp_plan *p, int l)
+// How level l runs: 0 the float32 kernel; 1 the one-pass tensor-core kernel (FFBP_LEVELS_TC, a shape it covers,
+// FFBP_LEVELS_TC2 not set); 2 the two-pass tensor-core kernels (FFBP_LEVELS_TC2, or a shape only they cover).
+static int level_form(const ffbp_plan *p, int l)
 {
+    if (!(p->final_mode & FFBP_LEVELS_TC)) return 0;
     const DevLevel &v = p->lv[l];
-    return (p->final_mode & FFBP_LEVELS_TC) && ffbp::level_tc_supported(v.C, v.Dk > 1 ? v.Lk : 1, v.Dk);
+    const int Lk = v.Dk > 1 ? v.Lk : 1, Lp = v.Dp > 1 ? v.Lp : 1;
+    if (!(p->final_mode & FFBP_LEVELS_TC2) && ffbp::level_fused_supported(v.C, Lk, v.Dk, Lp, v.Dp)) return 1;
+    return ffbp::level_tc_supported(v.C, Lk, v.Dk) ? 2 : 0;
 }
 
-// The float16 intermediate of the tensor-core levels: the largest any of them needs.
+// The float16 intermediate of the two-pass tensor-core levels: the largest any of them needs.
 static size_t tc_scratch(const ffbp_plan *p)
 {
     size_t m = 0;
     for (int l = 0; l < p->nlev; ++l) {
-        if (!level_on_tc(p, l)) continue;
+        if (level_form(p, l) != 2) continue;
         const DevLevel &v = p->lv[l];
         m = std::max(m, ffbp::level_tc_scratch_bytes(v.Np, v.C, v.P, v.Ko));
     }
     return m;
+}
+
+// Whether any level runs the two-pass kernels, whose intermediate is scaled from the input's largest component
+// (the history's is found by a scan ahead of the first level).
+static bool any_two_pass(const ffbp_plan *p)
+{
+    for (int l = 0; l < p->nlev; ++l)
+        if (level_form(p, l) == 2) return true;
+    return false;
 }
 
 int ffbp_plan_workspace_bytes(const ffbp_plan *p, size_t *bytes)
@@ -352,7 +367,7 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
     };
     mark(0);
     const float2 *in = static_cast<const float2 *>(d_S);
-    if (level_on_tc(p, 0)) {
+    if (level_form(p, 0) == 2) {
         if ((e = ffbp::launch_amax(in, (size_t)p->lv[0].P * p->lv[0].K, amax, s)) != cudaSuccess) return cuda_fail(e, "history scan");
         mark(FFBP_KIND_AMAX << 8);
     }
@@ -366,9 +381,13 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
         L.Np = v.Np; L.C = v.C; L.P = v.P; L.K = v.K; L.Ko = v.Ko; L.Po = v.Po; L.Dk = v.Dk; L.Lk = v.Lk; L.plk = v.plk;
         L.Dp = v.Dp; L.Lp = v.Lp; L.plp = v.plp; L.kc = v.kc;
         L.amax = amax + l + 1;
-        L.test_wait_ns = p->test_kind == FFBP_KIND_LEVEL_TC_GEMM ? p->test_ns : 0u;
+        L.test_wait_ns = p->test_kind == FFBP_KIND_LEVEL_TC ? p->test_ns : 0u;
         const char *why = nullptr;
-        if (level_on_tc(p, l)) {
+        const int form = level_form(p, l);
+        if (form == 1) {
+            e = ffbp::launch_level_fused(L, p->d_aborts, s, &why);
+            if (!why && e == cudaSuccess) mark(FFBP_KIND_LEVEL_TC << 8 | l);
+        } else if (form == 2) {
             e = ffbp::launch_level_tc_gemm(L, amax + l, scratch, p->d_aborts, s, &why);
             if (!why && e == cudaSuccess) {
                 mark(FFBP_KIND_LEVEL_TC_GEMM << 8 | l);
@@ -611,8 +630,10 @@ int ffbp_plan_check(ffbp_plan *p, void *stream)
 int ffbp_plan_test_wait(ffbp_plan *p, int kind, unsigned limit_us)
 {
     if (!p) return fail(FFBP_E_ARG, "ffbp_plan_test_wait: null plan");
-    if (kind != 0 && kind != FFBP_KIND_LEVEL_TC_GEMM && kind != FFBP_KIND_FINAL_TC)
-        return fail(FFBP_E_ARG, "ffbp_plan_test_wait: kind %d is neither 0, FFBP_KIND_LEVEL_TC_GEMM nor FFBP_KIND_FINAL_TC", kind);
+    if (kind != 0 && kind != FFBP_KIND_LEVEL_TC_GEMM && kind != FFBP_KIND_LEVEL_TC && kind != FFBP_KIND_FINAL_TC)
+        return fail(FFBP_E_ARG, "ffbp_plan_test_wait: kind %d is neither 0, FFBP_KIND_LEVEL_TC, FFBP_KIND_LEVEL_TC_GEMM "
+                    "nor FFBP_KIND_FINAL_TC", kind);
+    if (kind == FFBP_KIND_LEVEL_TC_GEMM) kind = FFBP_KIND_LEVEL_TC;              // both tensor-core level forms
     if (kind != 0 && (limit_us < 1 || limit_us > 1000000))
         return fail(FFBP_E_ARG, "ffbp_plan_test_wait: limit of %u us outside 1 .. 1000000", limit_us);
     p->test_kind = kind;
@@ -671,7 +692,8 @@ int ffbp_plan_info(const ffbp_plan *p, int *nlev, int *launches)
     if (nlev) *nlev = p->nlev;
     if (launches) {
         int n = 1;
-        for (int l = 0; l < p->nlev; ++l) n += level_on_tc(p, l) ? 2 + (l == 0) : 1;
+        for (int l = 0; l < p->nlev; ++l) n += level_form(p, l) == 2 ? 2 : 1;
+        if (any_two_pass(p) && level_form(p, 0) == 2) n += 1;      // the history scan
         *launches = n;
     }
     return FFBP_OK;
@@ -728,6 +750,25 @@ int ffbp_level_tc(const void *d_x, int Np, int P, int K, const void *d_phase, in
     return FFBP_OK;
 }
 
+int ffbp_level_fused(const void *d_x, int Np, int P, int K, const void *d_phase, int C, const float *d_tk, int Lk,
+                     int plk, int Dk, int Ko, double kc, const float *d_tp, int Lp, int plp, int Dp, int Po,
+                     const float *d_wp, const float *d_wk, void *d_out, int *d_bad, int *d_status, void *stream)
+{
+    if (!d_x || !d_phase || !d_out || !d_status) return fail(FFBP_E_ARG, "ffbp_level_fused: null buffer");
+    if (Np < 1 || P < 1 || K < 1 || C < 1 || Dk < 1 || Dp < 1 || Ko < 1 || Po < 1) return fail(FFBP_E_ARG, "ffbp_level_fused: non-positive size");
+    if ((Dk > 1 && (!d_tk || Lk < 1)) || (Dp > 1 && (!d_tp || Lp < 1))) return fail(FFBP_E_ARG, "ffbp_level_fused: taps missing");
+    ffbp::LevelLaunch L;
+    L.x = static_cast<const float2 *>(d_x); L.phase = static_cast<const float2 *>(d_phase); L.tk = d_tk; L.tp = d_tp;
+    L.wp = d_wp; L.wk = d_wk; L.out = static_cast<float2 *>(d_out); L.bad = d_bad;
+    L.Np = Np; L.C = C; L.P = P; L.K = K; L.Ko = Ko; L.Po = Po; L.Dk = Dk; L.Lk = Lk; L.plk = plk; L.Dp = Dp;
+    L.Lp = Lp; L.plp = plp; L.kc = kc; L.amax = d_status + 2;
+    const char *why = nullptr;
+    cudaError_t e = ffbp::launch_level_fused(L, d_status, static_cast<cudaStream_t>(stream), &why);
+    if (why) return fail(FFBP_E_UNSUPPORTED, "ffbp_level_fused: %s", why);
+    if (e != cudaSuccess) return cuda_fail(e, "ffbp_level_fused");
+    return FFBP_OK;
+}
+
 int ffbp_exact_pad(const void *d_S, int n, int K, const float *d_wp, const float *d_wk, int nfft, void *d_pad,
                    int *d_bad, int p_off, void *stream)
 {
@@ -739,20 +780,21 @@ int ffbp_exact_pad(const void *d_S, int n, int K, const float *d_wp, const float
     return FFBP_OK;
 }
 
-int ffbp_exact_backproject(const void *d_prof, int n, int nfft, int W, const long long *d_blo, const int *d_lo,
-                           const double *d_ant, const double *d_ref, const double *d_cen, int ntx, int nty, int tx,
-                           int ty, int nx, int ny, double spx, double spy, const double *e1, const double *e2,
-                           double inv_dr, double kcyc, int cubic, int along1, void *d_win, void *d_out, void *stream)
+int ffbp_exact_backproject(const void *d_prof, int n, int nfft, const double *d_ant, const double *d_ref,
+                           const double *d_cen, int ntx, int nty, int tx, int ty, int nx, int ny, double spx, double spy,
+                           const double *e1, const double *e2, double inv_dr, double kcyc, int cubic, int along1,
+                           int *d_err, void *d_out, void *stream)
 {
-    if (!d_prof || !d_blo || !d_lo || !d_ant || !d_ref || !d_cen || !e1 || !e2 || !d_win || !d_out)
+    if (!d_prof || !d_ant || !d_ref || !d_cen || !e1 || !e2 || !d_out)
         return fail(FFBP_E_ARG, "ffbp_exact_backproject: null buffer");
-    if (n < 0 || W > nfft || ntx < 1 || nty < 1 || nx < 1 || ny < 1 || ntx * tx < nx || nty * ty < ny)
+    if (n < 0 || ntx < 1 || nty < 1 || nx < 1 || ny < 1 || (long)ntx * tx < nx || (long)nty * ty < ny ||
+        !(inv_dr > 0.0) || !std::isfinite(kcyc))
         return fail(FFBP_E_ARG, "ffbp_exact_backproject: bad sizes");
     const char *why = nullptr;
-    cudaError_t e = ffbp::launch_exact_tiles(static_cast<const float2 *>(d_prof), n, nfft, W, d_blo, d_lo, d_ant, d_ref,
-                                             d_cen, ntx, nty, tx, ty, nx, ny, spx, spy, e1, e2, inv_dr, kcyc, cubic,
-                                             along1, static_cast<float2 *>(d_win), static_cast<float2 *>(d_out),
-                                             static_cast<cudaStream_t>(stream), &why);
+    cudaError_t e = ffbp::launch_exact_tiles(static_cast<const float2 *>(d_prof), n, nfft, d_ant, d_ref, d_cen, ntx, nty,
+                                             tx, ty, nx, ny, spx, spy, e1, e2, inv_dr, kcyc, cubic, along1,
+                                             static_cast<float2 *>(d_out), d_err, static_cast<cudaStream_t>(stream),
+                                             &why);
     if (why) return fail(FFBP_E_ARG, "ffbp_exact_backproject: %s", why);
     if (e != cudaSuccess) return cuda_fail(e, "ffbp_exact_backproject");
     return FFBP_OK;

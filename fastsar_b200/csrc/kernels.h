@@ -33,6 +33,11 @@ bool level_tc_supported(int C, int Lk, int Dk);
 size_t level_tc_scratch_bytes(int Np, int C, int P, int Ko);
 cudaError_t launch_level_tc(const LevelLaunch &L, const int *amax_in, void *scratch, int *err, cudaStream_t s,
                             const char **why);
+// The same level in one pass (level_fused.cu): the pulse FIR's running sums held in tensor memory, the output
+// written once as complex64 with its largest component recorded in L.amax; no intermediate. Levels of at most 64
+// children, 96 frequency taps and 8 output pulses per input pulse.
+bool level_fused_supported(int C, int Lk, int Dk, int Lp, int Dp);
+cudaError_t launch_level_fused(const LevelLaunch &L, int *err, cudaStream_t s, const char **why);
 // its two passes, for callers that time them apart
 cudaError_t launch_level_tc_gemm(const LevelLaunch &L, const int *amax_in, void *scratch, int *err, cudaStream_t s,
                                  const char **why);
@@ -80,14 +85,14 @@ cudaError_t launch_simulate(const double *ant, int P, int K, double fmin, double
                             const double2 *amp, int N, float2 *S, cudaStream_t s);
 
 // Exact backprojection onto a grid's tiles (exact_tiles.cu): the windowed, zero-padded history of a chunk of pulses
-// (its fftshift folded in), and the crop plus tiled backprojection of its inverse-FFT profiles.
+// (its fftshift folded in), and the tiled backprojection of its inverse-FFT profiles, each tile's range band of every
+// profile staged by bulk copies. err: raised when a bounded wait ran out (or null).
 cudaError_t launch_exact_pad(const float2 *s, int n, int K, const float *wp, const float *wk, int nfft, float2 *pad,
                              int *bad, int p_off, cudaStream_t st);
-cudaError_t launch_exact_tiles(const float2 *prof, int n, int nfft, int W, const long long *blo, const int *lo,
-                               const double *ant, const double *ref, const double *cen, int ntx, int nty, int tx,
-                               int ty, int nx, int ny, double spx, double spy, const double *e1, const double *e2,
-                               double inv_dr, double kcyc, int cubic, int along1, float2 *win, float2 *out,
-                               cudaStream_t st, const char **why);
+cudaError_t launch_exact_tiles(const float2 *prof, int n, int nfft, const double *ant, const double *ref,
+                               const double *cen, int ntx, int nty, int tx, int ty, int nx, int ny, double spx,
+                               double spy, const double *e1, const double *e2, double inv_dr, double kcyc, int cubic,
+                               int along1, float2 *out, int *err, cudaStream_t st, const char **why);
 
 // The range gate (gate.cu): pad and window a block of pulses, gather the bins about bin 0, taper the kept samples.
 cudaError_t launch_gate_pad(const float2 *S, int n, int K, const float *wp, const float *wk, int npl, int Kp,

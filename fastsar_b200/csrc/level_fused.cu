@@ -1,0 +1,589 @@
+// A level on the tcgen05 tensor cores in one pass (sm_100a): the rotation, the frequency FIR and the pulse FIR of one
+// merge stage of the FFBP (the reference's rot_fir_k + fir_p: fastsar/ffbp_cpu.cpp:146-293, fastsar/ffbp_cuda.py:
+// 48-256), with nothing at the input pulse rate leaving the multiprocessor.
+//
+// The frequency FIR of child c at input pulse p factors as
+//     y_c[p, j] = R_c,p[j] sum_r m_c,p[r] x[p, Dk j + r - plk],   m_c,p[r] = hk[r] exp(2 pi i sl r),
+//     R_c,p[j] = exp(2 pi i (c0 + sl (Dk j - plk - kc))),
+// a dense product per pulse (children x taps times taps x columns: the children's modulated taps times the Hankel
+// windows of the parent's row) followed by a ramp; the pulse FIR then sums, for output pulse i,
+//     out_c[i, j] = sum_r hp[r] y_c[Dp i + r - plp, j].
+//
+// A block owns one parent, one tile of Nt output columns (32; 64 when the level has at most 32 children) and a
+// segment of output pulses, and sweeps the input pulses those outputs need, in order. Per pulse:
+//   warps 16..19  the modulated taps of every child (A': rows 2c and 2c + 1 the real and imaginary parts of child c,
+//                 K = taps padded to 16; rows 64..127 repeat rows 0..63 when there are at most 32 children), split
+//                 into bfloat16 hi + lo, into the A' buffer of the pulse's issuer;
+//   warps 20, 21  the window of the parent's row the tile reads (cp.async, a ring XS pulses deep), windowed at the
+//                 first level, as bfloat16 hi/lo planes with even- and odd-shifted copies;
+//   warps 22..25  the Hankel rows from the planes (B': 2 Nt rows, the real and imaginary windows of each column);
+//   warps 26, 27  one thread each issues the pulse's tcgen05.mma (M = 128, N = 2 Nt, K = 16; hi hi + hi lo + lo hi)
+//                 into its own tensor-memory accumulator: warp 26 the even pulses, warp 27 the odd ones;
+//   warps 0..15   read the accumulator (warp w: lane quarter w % 4, one chunk of 8 columns), exchange halves between
+//                 a child's two rows, apply the ramp, and add the pulse into the pulse FIR's running sums: per
+//                 (child, column) the ceil(Lp / Dp) <= 8 output pulses the input pulse feeds, held in tensor memory
+//                 (16 columns of the thread's own lane: a ring of 8 complex slots, output i in slot i mod 8). When an
+//                 output pulse has had its last input the slot is written out (complex64) and cleared.
+// The running sums need C x Nt x 8 complex values per block (256 tensor-memory columns), which is what bounds the
+// tile to 32 columns (64 with the repeated rows).
+//
+// Every wait on a barrier is bounded in time; a wait that runs out sets the block's abort flag and raises *err, and
+// every role winds down without touching a barrier again.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "kernels.h"
+#include "tc_common.cuh"
+
+namespace ffbp {
+
+namespace {
+
+using namespace tc;
+
+constexpr int F_NCW = 16;                        // consumer warps 0..15
+constexpr int F_NAW = 4;                         // A' producers 16..19
+constexpr int F_NLW = 1;                         // planes 20
+constexpr int F_NHW = 2;                         // Hankel rows 22..23
+constexpr int F_AW0 = F_NCW, F_LW0 = F_AW0 + F_NAW, F_HW0 = F_LW0 + F_NLW, F_IW0 = F_HW0 + F_NHW;
+constexpr int F_NWARPS = F_IW0 + 2;              // + the two MMA issuers
+constexpr int F_NTHR = F_NWARPS * 32;
+constexpr int F_NAT = F_NAW * 32, F_NLT = F_NLW * 32, F_NHT = F_NHW * 32;
+constexpr int F_XS = 4;                          // the planes warps' ring of staged windows
+constexpr int F_AP = 8;                          // running sums per (child, column): output pulses an input feeds
+constexpr uint64_t F_WAIT_NS = 2000000000ull;
+
+struct FusedArgs {
+    const float2 *__restrict__ x;     // [Np, P, K]
+    const float2 *__restrict__ ph;    // [Np, C, P] (c0, sl)
+    const float *__restrict__ tk;     // [Lk] (null: Dk = 1, one tap 1)
+    const float *__restrict__ tp;     // [Lp] (null: Dp = 1, one tap 1)
+    const float *__restrict__ wp;     // [P] or null
+    const float *__restrict__ wk;     // [K] or null
+    int *bad;                         // first non-finite pulse (first level) or null
+    float2 *out;                      // [Np C, Po, Ko]
+    int *amax;                        // largest |component| of the output (float bits) or null
+    int *err;
+    int Np, C, P, K, Ko, Po, Dk, Lk, plk, Lkp, Dp, Lp, plp, Nt, ntile, W, oseg, nseg, SB;
+    float kc;
+    unsigned test_wait_ns;            // tests only: the issuers' wait on a barrier nothing completes (0: none)
+};
+
+// The taps of the pulse FIR by (input phase r0 = (p + plp) mod Dp, newest output qn = (p + plp) / Dp modulo 8,
+// ring slot s): the input pulse feeds output qn - a with tap hp[r0 + a Dp] (a < 8, r0 + a Dp < Lp), and output
+// qn - a sits in slot (qn - a) mod 8. Each tap twice, for the packed multiply-adds of a complex value.
+__device__ __forceinline__ void fill_tap_table(const FusedArgs &a, float2 *s_tap, int t)
+{
+    for (int e = t; e < a.Dp * F_AP * F_AP; e += F_NTHR) {
+        const int r0 = e / (F_AP * F_AP), m = (e / F_AP) % F_AP, s = e % F_AP;
+        const int ao = ((m - s) % F_AP + F_AP) % F_AP;
+        const int r = r0 + ao * a.Dp;
+        const float v = r < a.Lp ? (a.tp ? a.tp[r] : 1.f) : 0.f;      // Dp = 1: the one tap 1
+        s_tap[e] = make_float2(v, v);
+    }
+}
+
+// Slot s of a ring of 8 complex values held as 16 floats: read, or clear (a warp-uniform switch, no local memory)
+__device__ __forceinline__ float2 ring_get(const float *v, int s)
+{
+    switch (s) {
+        case 0: return make_float2(v[0], v[1]);
+        case 1: return make_float2(v[2], v[3]);
+        case 2: return make_float2(v[4], v[5]);
+        case 3: return make_float2(v[6], v[7]);
+        case 4: return make_float2(v[8], v[9]);
+        case 5: return make_float2(v[10], v[11]);
+        case 6: return make_float2(v[12], v[13]);
+        default: return make_float2(v[14], v[15]);
+    }
+}
+
+__device__ __forceinline__ void ring_clear(float *v, int s)
+{
+    switch (s) {
+        case 0: v[0] = v[1] = 0.f; break;
+        case 1: v[2] = v[3] = 0.f; break;
+        case 2: v[4] = v[5] = 0.f; break;
+        case 3: v[6] = v[7] = 0.f; break;
+        case 4: v[8] = v[9] = 0.f; break;
+        case 5: v[10] = v[11] = 0.f; break;
+        case 6: v[12] = v[13] = 0.f; break;
+        default: v[14] = v[15] = 0.f; break;
+    }
+}
+
+__device__ __forceinline__ int floor_div(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+
+template <int NKC>
+__global__ void __maxnreg__(80) level_fused_kernel(const FusedArgs a)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    constexpr int nkc = NKC;                                 // core matrices along K (Lkp = 8 NKC)
+    const uint32_t apart = 128u * a.Lkp * 2u;                // one part (hi or lo) of A'
+    const uint32_t bpart = 2u * a.Nt * a.Lkp * 2u;           // one part of B'
+    unsigned char *sA = smem;                                // [issuer][hi, lo]
+    unsigned char *sB = sA + 4 * apart;                      // [SB stages][hi, lo]
+    const int Wp = (a.W + 9) & ~1;
+    uint32_t *pl = reinterpret_cast<uint32_t *>(sB + (size_t)a.SB * 2 * bpart);     // two stages' planes
+    float *s_tk = reinterpret_cast<float *>(pl + 16 * (Wp / 2));                     // [Lkp]
+    float2 *s_x = reinterpret_cast<float2 *>(s_tk + a.Lkp);                           // [XS][Wp]
+    float2 *s_tap = s_x + (size_t)F_XS * Wp;                                          // [Dp][8][8]
+    uint64_t *bars = reinterpret_cast<uint64_t *>(s_tap + (size_t)a.Dp * F_AP * F_AP);
+    uint64_t *afull = bars, *aempty = bars + 2, *bfull = bars + 4, *bempty = bfull + a.SB, *dfull = bempty + a.SB,
+             *dempty = dfull + 2, *pfull = dempty + 2, *pempty = pfull + 2, *drain = pempty + 2;
+    __shared__ uint32_t s_tmem;
+    __shared__ volatile int s_abort;
+    __shared__ uint64_t s_never;                             // a barrier nothing arrives on (the tests' stuck wait)
+
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int tt = blockIdx.x % a.ntile, seg = (blockIdx.x / a.ntile) % a.nseg, n = blockIdx.x / (a.ntile * a.nseg);
+    const int i_s = seg * a.oseg, i_e = min(a.Po, i_s + a.oseg);           // this block's output pulses
+    const int pa = max(0, a.Dp * i_s - a.plp), pb = min(a.P, a.Dp * (i_e - 1) - a.plp + a.Lp);
+    const int nst = max(0, pb - pa);                          // input pulses swept (one stage each)
+    const int kb = a.Dk * a.Nt * tt - a.plk;                  // first input sample of the tile's window
+
+    if (t == 0) {
+        s_abort = 0;
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&afull[i], F_NAW);
+            mbar_init(&aempty[i], 1);
+            mbar_init(&dfull[i], 1);
+            mbar_init(&dempty[i], F_NCW);
+            mbar_init(&pfull[i], F_NLT);
+            mbar_init(&pempty[i], F_NHT);
+            mbar_init(&drain[i], 1);
+        }
+        for (int i = 0; i < a.SB; ++i) {
+            mbar_init(&bfull[i], F_NHW);
+            mbar_init(&bempty[i], 1);
+        }
+        mbar_init(&s_never, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int i = t; i < a.Lkp; i += F_NTHR) s_tk[i] = i < a.Lk ? (a.tk ? a.tk[i] : 1.f) : 0.f;   // Dk = 1: one tap 1
+    fill_tap_table(a, s_tap, t);
+    // A' rows of no child stay zero: clear both buffers once
+    for (int i = t; i < (int)(4 * apart / 16); i += F_NTHR) reinterpret_cast<uint4 *>(sA)[i] = make_uint4(0, 0, 0, 0);
+    if (warp == F_IW0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" :: "r"(smem_u32(&s_tmem)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+
+    if (warp >= F_AW0 && warp < F_LW0) {
+        // ------------------------------------------------------------------ A' producers
+        // the modulated taps of pulse s into the A' buffer of its issuer (s & 1), once that issuer's MMAs of pulse
+        // s - 2 have completed
+        const int at = t - F_AW0 * 32;
+        const float2 *__restrict__ phn = a.ph + (size_t)n * a.C * a.P;
+        for (int s = 0; s < nst; ++s) {
+            const int ab = s & 1, p = pa + s;
+            if (!mbar_wait(&aempty[ab], (uint32_t)(((s >> 1) & 1) ^ 1), 1000, &s_abort, a.err, F_WAIT_NS)) break;
+            unsigned char *Ab = sA + ab * 2 * apart;
+            for (int item = at; item < a.C * nkc; item += F_NAT) {
+                const int u = item / a.C, c = item - u * a.C;    // consecutive threads: consecutive children
+                const float sl = __ldg(&phn[(size_t)c * a.P + p]).y;
+                // exp(2 pi i sl r) for r = 8u .. 8u + 7: two independent recurrences (even and odd r)
+                const float2 st = cis_cycles(sl), st2 = cmul(st, st);
+                float2 ze = cis_cycles(sl * (float)(8 * u)), zo = cmul(ze, st);
+                float mr[8], mi[8];
+#pragma unroll
+                for (int e = 0; e < 8; e += 2) {
+                    const float h0 = s_tk[8 * u + e], h1 = s_tk[8 * u + e + 1];
+                    mr[e] = h0 * ze.x;
+                    mi[e] = h0 * ze.y;
+                    mr[e + 1] = h1 * zo.x;
+                    mi[e + 1] = h1 * zo.y;
+                    ze = cmul(ze, st2);
+                    zo = cmul(zo, st2);
+                }
+                uint32_t rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    split2(mr[2 * e], mr[2 * e + 1], rh[e], rl[e]);
+                    split2(mi[2 * e], mi[2 * e + 1], ih[e], il[e]);
+                }
+                // rows 2c (the real parts) and 2c + 1 (the imaginary parts); with at most 32 children rows 64..127
+                // repeat rows 0..63, so that all four lane quarters of the accumulator hold children
+                const int reps = a.C <= 32 ? 2 : 1;
+                for (int rr = 0; rr < reps; ++rr) {
+                    const uint32_t o0 = core_off(2 * c + 64 * rr, u, nkc), o1 = core_off(2 * c + 1 + 64 * rr, u, nkc);
+                    *reinterpret_cast<uint4 *>(Ab + o0) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+                    *reinterpret_cast<uint4 *>(Ab + apart + o0) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+                    *reinterpret_cast<uint4 *>(Ab + o1) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+                    *reinterpret_cast<uint4 *>(Ab + apart + o1) = make_uint4(il[0], il[1], il[2], il[3]);
+                }
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&afull[ab]);
+        }
+    } else if (warp >= F_LW0 && warp < F_HW0) {
+        // ------------------------------------------------------------------ B' producers: planes
+        const int pt = t - F_LW0 * 32;
+        const float2 *__restrict__ xn = a.x + (size_t)n * a.P * a.K;
+        const int npair = (a.W + 1) / 2;                      // window samples in pairs (2i, 2i + 1)
+        // the window of pulse pa + st: samples kb + i, i < W, copied XS - 1 stages ahead into ring slot st % XS
+        // (zero outside [0, K)); one cp.async group per stage
+        auto stage_x = [&](int st) {
+            if (st < nst) {
+                const int p = pa + st;
+                float2 *dst = s_x + (size_t)(st % F_XS) * Wp;
+                for (int i = pt; i < a.W; i += F_NLT) {
+                    const int k = kb + i;
+                    const bool v = k >= 0 && k < a.K;
+                    const float2 *src = v ? xn + (size_t)p * a.K + k : xn;
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;"
+                                 :: "r"(smem_u32(dst + i)), "l"(src), "r"(v ? 8 : 0) : "memory");
+                }
+            }
+            asm volatile("cp.async.commit_group;" ::: "memory");
+        };
+#pragma unroll
+        for (int d = 0; d < F_XS - 1; ++d) stage_x(d);
+        // after a failed wait the warps keep stepping through the stages (and the named barrier, which both planes
+        // warps must reach) without waiting or working
+        bool ok = true;
+        for (int s = 0; s < nst; ++s) {
+            const int p = pa + s;
+            asm volatile("cp.async.wait_group %0;" :: "n"(F_XS - 2) : "memory");   // this thread's copies of stage s
+            // every planes thread's copies of stage s are in, and its reads of stage s - 1's window done
+            asm volatile("bar.sync 1, %0;" :: "n"(F_NLT) : "memory");
+            stage_x(s + F_XS - 1);
+            if (ok) ok = mbar_wait(&pempty[s & 1], (uint32_t)(((s >> 1) & 1) ^ 1), 1000, &s_abort, a.err, F_WAIT_NS);
+            if (ok) {
+                uint32_t *plb = pl + (s & 1) * 8 * (Wp / 2);
+                const float2 *xs = s_x + (size_t)(s % F_XS) * Wp;
+                const float wpp = a.wp ? a.wp[p] : 1.f;
+                for (int i = pt; i < npair; i += F_NLT) {
+                    float2 v[3];                              // samples 2i, 2i + 1, 2i + 2 (windowed)
+#pragma unroll
+                    for (int h = 0; h < 3; ++h) {
+                        const int e = 2 * i + h, k = kb + e;
+                        v[h] = e < a.W ? xs[e] : make_float2(0.f, 0.f);
+                        if (a.wp && k >= 0 && k < a.K && e < a.W) {
+                            const float w = wpp * a.wk[k];
+                            v[h].x *= w;
+                            v[h].y *= w;
+                        }
+                        if (h < 2 && a.bad && !(isfinite(v[h].x) && isfinite(v[h].y))) atomicMin(a.bad, p);
+                    }
+                    uint32_t rh, rl, ih, il, orh, orl, oih, oil;
+                    split2(v[0].x, v[1].x, rh, rl);
+                    split2(v[0].y, v[1].y, ih, il);
+                    split2(v[1].x, v[2].x, orh, orl);
+                    split2(v[1].y, v[2].y, oih, oil);
+                    const int hw = Wp / 2;
+                    plb[i] = rh;
+                    plb[hw + i] = orh;
+                    plb[2 * hw + i] = rl;
+                    plb[3 * hw + i] = orl;
+                    plb[4 * hw + i] = ih;
+                    plb[5 * hw + i] = oih;
+                    plb[6 * hw + i] = il;
+                    plb[7 * hw + i] = oil;
+                }
+                mbar_arrive(&pfull[s & 1]);
+            }
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+    } else if (warp >= F_HW0 && warp < F_IW0) {
+        // ------------------------------------------------------------------ B' producers: Hankel rows
+        // row j < Nt: the real window from Dk j; row Nt + j: the imaginary one; 8 elements (16 bytes) per chunk. A
+        // warp takes 8 rows (lane % 8) x 4 K chunks (lane / 8) at a time, the 8 rows' stores filling one 128-byte
+        // core matrix; warp pw the row blocks pw, pw + NHW, ...
+        constexpr int UB = (NKC + 3) / 4;
+        const int r8 = lane & 7, uq = lane >> 3, pw = warp - F_HW0;
+        const int nrb = a.Nt / 8;
+        const int nmine = nrb > pw ? (nrb - 1 - pw) / F_NHW + 1 : 0;
+        const int ostep = 8 * F_NHW * a.Dk, wstep = ostep >> 1;             // ostep is even
+        const uint32_t bstep = (uint32_t)(F_NHW * nkc * 128);
+        for (int s = 0; s < nst; ++s) {
+            const int sb = s % a.SB;
+            const uint32_t sbpar = (uint32_t)((s / a.SB) & 1);
+            if (!mbar_wait(&pfull[s & 1], (uint32_t)((s >> 1) & 1), 1000, &s_abort, a.err, F_WAIT_NS)) break;
+            if (!mbar_wait(&bempty[sb], sbpar ^ 1u, 1000, &s_abort, a.err, F_WAIT_NS)) break;
+            unsigned char *Bb = sB + sb * 2 * bpart;
+            const uint32_t *plb = pl + (s & 1) * 8 * (Wp / 2);
+#pragma unroll
+            for (int ub = 0; ub < UB; ++ub) {
+                const int u = ub * 4 + uq;
+                if (u >= NKC) continue;
+                const int o0 = a.Dk * (8 * pw + r8) + 8 * u;                    // first element, first block
+                const int cp = o0 & 1;
+#pragma unroll
+                for (int pi = 0; pi < 4; ++pi) {                              // (part, re/im)
+                    const int part = pi & 1, im = pi >> 1;
+                    const uint32_t *src = plb + (2 * (2 * im + part) + cp) * (Wp / 2) + (o0 >> 1);
+                    unsigned char *dst = Bb + part * bpart + core_off(im * a.Nt + 8 * pw + r8, u, nkc);
+                    for (int m = 0; m < nmine; ++m) {
+                        const uint32_t *s0 = src + m * wstep;
+                        *reinterpret_cast<uint4 *>(dst + m * bstep) = make_uint4(s0[0], s0[1], s0[2], s0[3]);
+                    }
+                }
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            mbar_arrive(&pempty[s & 1]);                      // this thread's reads of the planes are done
+            if (lane == 0) mbar_arrive(&bfull[sb]);
+        }
+    } else if (warp >= F_IW0) {
+        // ------------------------------------------------------------------ MMA issue
+        // issuer k = warp - F_IW0 takes the pulses s = k mod 2 into its accumulator (columns 2 Nt k ..), from A'
+        // buffer k and the B' stages s mod SB (SB even: each stage has one issuer)
+        const int k = warp - F_IW0;
+        if (lane == 0) {
+            const int ncol = 2 * a.Nt;
+            const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(ncol >> 3) << 17) | ((128u >> 4) << 24);
+            const uint32_t sbo = (uint32_t)nkc * 128;
+            const uint32_t ah = smem_u32(sA) + (uint32_t)k * 2 * apart, al = ah + apart;
+            const uint32_t dt = tmem + (uint32_t)(k * ncol);
+            // tests of the failure report: a wait that runs out before any MMA, as a stuck pipeline's would
+            const bool stuck = a.test_wait_ns && !mbar_wait(&s_never, 0, 0, &s_abort, a.err, a.test_wait_ns);
+            for (int s = stuck ? nst : k; s < nst; s += 2) {
+                const int sb = s % a.SB;
+                if (!mbar_wait(&afull[k], (uint32_t)((s >> 1) & 1), 0, &s_abort, a.err, F_WAIT_NS)) break;
+                if (!mbar_wait(&bfull[sb], (uint32_t)((s / a.SB) & 1), 0, &s_abort, a.err, F_WAIT_NS)) break;
+                if (!mbar_wait(&dempty[k], (uint32_t)(((s >> 1) & 1) ^ 1), 0, &s_abort, a.err, F_WAIT_NS)) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t bh = smem_u32(sB) + (uint32_t)sb * 2 * bpart, bl = bh + bpart;
+                for (int ks = 0; ks < a.Lkp / 16; ++ks) {
+                    const uint32_t ko = 256u * ks;
+                    mma_bf16(dt, smem_desc(ah + ko, 128, sbo), smem_desc(bh + ko, 128, sbo), idesc, ks > 0 ? 1u : 0u);
+                    mma_bf16(dt, smem_desc(ah + ko, 128, sbo), smem_desc(bl + ko, 128, sbo), idesc, 1u);
+                    mma_bf16(dt, smem_desc(al + ko, 128, sbo), smem_desc(bh + ko, 128, sbo), idesc, 1u);
+                }
+                mma_commit(&bempty[sb]);
+                mma_commit(&dfull[k]);
+                mma_commit(&aempty[k]);
+            }
+        }
+        __syncwarp();
+    } else {
+        // ------------------------------------------------------------------ consumers (warps 0..15)
+        // Warp w reads lane quarter q = w % 4: rows 2c, 2c + 1 for the children c = 16 q + lane / 2 (with at most 32
+        // children quarters 2, 3 repeat 0, 1 and take other columns), at one chunk of 8 columns; lanes 2c and 2c + 1
+        // exchange halves so that each forms its child's outputs at 4 of the 8 columns.
+        const int rp = a.C <= 32 ? 2 : 1;
+        const int q = warp & 3, g = warp >> 2;
+        const int c = 16 * (rp == 2 ? (q & 1) : q) + (lane >> 1);
+        const bool odd = lane & 1, live = c < a.C;
+        const int chunk = rp == 2 ? g + 4 * (q >> 1) : g;           // 8-column chunk of the tile
+        const int j0 = tt * a.Nt + chunk * 8 + (odd ? 4 : 0);         // this thread's first output column
+        const uint32_t lanes = (uint32_t)(32 * q) << 16;
+        const uint32_t fir = tmem + lanes + (uint32_t)(4 * a.Nt + 64 * g);   // this thread's running sums, 4 x 16 cols
+        const float2 *__restrict__ phc = a.ph + ((size_t)n * a.C + (live ? c : 0)) * a.P;
+        float2 *__restrict__ outc = a.out + ((size_t)n * a.C + (live ? c : 0)) * a.Po * a.Ko;
+        {
+            float z[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) z[i] = 0.f;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) tmem_st16(fir + 16u * e, z);
+            tmem_wait_st();
+        }
+        float vmax = 0.f;
+        float2 qn = nst > 0 ? __ldg(&phc[pa]) : make_float2(0.f, 0.f);   // the next pulse's (c0, sl)
+        int s = 0;
+        for (; s < nst; ++s) {
+            const int p = pa + s, k = s & 1;
+            const float2 q0 = qn;
+            if (s + 1 < nst) qn = __ldg(&phc[p + 1]);
+            // warp-uniform: the accumulator loads below are warp-collective
+            if (!__all_sync(0xffffffffu, mbar_wait(&dfull[k], (uint32_t)((s >> 1) & 1), 200, &s_abort, a.err, F_WAIT_NS)))
+                break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            float vr[8], vi[8];
+            const uint32_t acc = tmem + lanes + (uint32_t)(k * 2 * a.Nt + chunk * 8);
+            tmem_ld8(acc, vr);
+            tmem_ld8(acc + (uint32_t)a.Nt, vi);
+            tmem_wait_ld();
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&dempty[k]);          // the accumulator is free for the issuer's next pulse
+            // the child's outputs at columns j0 .. j0 + 3 of this pulse: re = Mr Xr - Mi Xi, im = Mr Xi + Mi Xr, times
+            // the ramp exp(2 pi i (c0 + sl (Dk j - plk - kc))) (seeded at j0, stepped by exp(2 pi i sl Dk))
+            float yr[4], yi[4];
+            {
+                const float2 st = cis_cycles(q0.y * (float)a.Dk);
+                float2 w = cis_cycles(fmaf(q0.y, (float)(a.Dk * j0 - a.plk) - a.kc, q0.x));
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const float sr = odd ? vr[i] : vr[4 + i], si = odd ? vi[i] : vi[4 + i];
+                    const float rr = __shfl_xor_sync(0xffffffffu, sr, 1), ri = __shfl_xor_sync(0xffffffffu, si, 1);
+                    const float orr = odd ? vr[4 + i] : vr[i], ori = odd ? vi[4 + i] : vi[i];
+                    const float mr_r = odd ? rr : orr, mr_i = odd ? ri : ori;
+                    const float mi_r = odd ? orr : rr, mi_i = odd ? ori : ri;
+                    const float2 y = cmul(w, make_float2(mr_r - mi_i, mr_i + mi_r));
+                    yr[i] = y.x;
+                    yi[i] = y.y;
+                    w = cmul(w, st);
+                }
+            }
+            // the pulse FIR: this input pulse's taps in ring-slot order, and the output it completes (if any)
+            const int pp = p + a.plp;                         // >= 0
+            const int r0 = pp % a.Dp, qq = pp / a.Dp;
+            const float4 *tq = reinterpret_cast<const float4 *>(s_tap + ((size_t)r0 * F_AP + (qq & 7)) * F_AP);
+            float2 tp8[8];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const float4 v = tq[i];
+                tp8[2 * i] = make_float2(v.x, v.y);
+                tp8[2 * i + 1] = make_float2(v.z, v.w);
+            }
+            const int cn = pp - a.Lp + 1;
+            const int ic = floor_div(cn, a.Dp);
+            const bool done = cn == ic * a.Dp;                // output ic has had its last input (block-uniform)
+            const int cslot = ic & 7;                         // two's complement: ic mod 8, also for ic < 0
+            const bool store = done && live && ic >= i_s && ic < i_e;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                float v[16];
+                tmem_ld16(fir + 16u * e, v);
+                tmem_wait_ld();
+                const float2 y = make_float2(yr[e], yi[e]);
+#pragma unroll
+                for (int sl = 0; sl < 8; ++sl) {
+                    const float2 r = ffma2(tp8[sl], y, make_float2(v[2 * sl], v[2 * sl + 1]));
+                    v[2 * sl] = r.x;
+                    v[2 * sl + 1] = r.y;
+                }
+                if (done) {
+                    const float2 o = ring_get(v, cslot);
+                    ring_clear(v, cslot);
+                    const int j = j0 + e;
+                    if (store && j < a.Ko) {
+                        outc[(size_t)ic * a.Ko + j] = o;
+                        vmax = fmaxf(vmax, fmaxf(fabsf(o.x), fabsf(o.y)));
+                    }
+                }
+                tmem_st16(fir + 16u * e, v);
+            }
+            tmem_wait_st();
+        }
+        // outputs whose last input lies past the end of the input (or of the sweep) are complete now: those fed by
+        // the sweep's last pulse are in the ring (at most 8, in distinct slots), those past it had no input at all;
+        // after an abort nothing more is written
+        if (s == nst && !s_abort) {
+            const int ic_last = floor_div(pa + nst - 1 + a.plp - a.Lp + 1, a.Dp);   // the last output completed
+            const int qn_last = floor_div(pa + nst - 1 + a.plp, a.Dp);              // the newest output fed
+            for (int i = max(i_s, ic_last + 1); i < i_e; ++i) {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    float v[16];
+                    tmem_ld16(fir + 16u * e, v);
+                    tmem_wait_ld();
+                    const float2 o = i <= qn_last ? ring_get(v, i & 7) : make_float2(0.f, 0.f);
+                    const int j = j0 + e;
+                    if (live && j < a.Ko) {
+                        outc[(size_t)i * a.Ko + j] = o;
+                        vmax = fmaxf(vmax, fmaxf(fabsf(o.x), fabsf(o.y)));
+                    }
+                }
+            }
+        }
+        if (a.amax) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+            if (lane == 0 && vmax > 0.f) atomicMax(a.amax, __float_as_int(vmax));
+        }
+    }
+
+    // teardown: every role is done (or aborted); each issuer drains its MMAs before the tensor memory is freed
+    __syncthreads();
+    if (warp >= F_IW0 && lane == 0) {
+        uint64_t *dr = &drain[warp - F_IW0];
+        mma_commit(dr);
+        const uint64_t t0 = global_ns();
+        while (!mbar_test(dr, 0, 0) && global_ns() - t0 < F_WAIT_NS) {
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (warp == F_IW0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" :: "r"(tmem));
+}
+
+// Dynamic shared memory: both issuers' A' (hi, lo), sb stages of B' (hi, lo), two stages' window planes, the taps,
+// the staged windows, the pulse taps' table and the barriers (afull, aempty, dfull, dempty, pfull, pempty, drain:
+// two each; bfull, bempty: sb each).
+size_t fused_smem(int Lkp, int Dk, int Nt, int sb, int Dp)
+{
+    const size_t apart = (size_t)128 * Lkp * 2, bpart = (size_t)2 * Nt * Lkp * 2;
+    const int W = Dk * (Nt - 1) + Lkp, Wp = (W + 9) & ~1;
+    return 4 * apart + (size_t)sb * 2 * bpart + (size_t)16 * (Wp / 2) * 4 + (size_t)Lkp * 4 + (size_t)F_XS * Wp * 8 +
+           (size_t)Dp * F_AP * F_AP * 8 + (size_t)(14 + 2 * sb) * 8;
+}
+
+constexpr size_t FUSED_SMEM_MAX = 226 * 1024;             // the opt-in limit less static shared memory and slack
+
+}  // namespace
+
+bool level_fused_supported(int C, int Lk, int Dk, int Lp, int Dp)
+{
+    const int Lkp = ((Lk + 15) / 16) * 16;
+    const int AP = (Lp + Dp - 1) / Dp;
+    const int Nt = C <= 32 ? 64 : 32;
+    return C >= 1 && C <= 64 && Lkp <= 96 && Dk >= 1 && Dp >= 1 && Dp <= 32 && AP <= F_AP &&
+           fused_smem(Lkp, Dk, Nt, 2, Dp) <= FUSED_SMEM_MAX;
+}
+
+cudaError_t launch_level_fused(const LevelLaunch &L, int *err, cudaStream_t s, const char **why)
+{
+    *why = nullptr;
+    const int Lk = L.Dk > 1 ? L.Lk : 1, plk = L.Dk > 1 ? L.plk : 0;
+    const int Lp = L.Dp > 1 ? L.Lp : 1, plp = L.Dp > 1 ? L.plp : 0;
+    if (!level_fused_supported(L.C, Lk, L.Dk, Lp, L.Dp)) {
+        *why = "the one-pass tensor-core level takes C <= 64 children, Lk <= 96 taps and pulse FIRs of at most 8 "
+               "outputs per input";
+        return cudaErrorNotSupported;
+    }
+    if (plp < 0 || plk < 0) { *why = "negative filter offsets"; return cudaErrorNotSupported; }
+    FusedArgs a;
+    a.x = L.x; a.ph = L.phase; a.tk = L.tk; a.tp = L.tp; a.wp = L.wp; a.wk = L.wk; a.bad = L.bad; a.out = L.out;
+    a.amax = L.amax; a.err = err;
+    a.Np = L.Np; a.C = L.C; a.P = L.P; a.K = L.K; a.Ko = L.Ko; a.Po = L.Po; a.Dk = L.Dk; a.Lk = Lk; a.plk = plk;
+    a.Lkp = ((Lk + 15) / 16) * 16; a.Dp = L.Dp; a.Lp = Lp; a.plp = plp; a.kc = (float)L.kc;
+    a.test_wait_ns = L.test_wait_ns;
+    a.Nt = L.C <= 32 ? 64 : 32;
+    a.ntile = (L.Ko + a.Nt - 1) / a.Nt;
+    a.W = a.Dk * (a.Nt - 1) + a.Lkp;
+    // output segments: enough blocks for the device several times over, each segment at least 4 filter lengths long
+    int nseg = 1;
+    while ((long)L.Np * a.ntile * nseg < 148L * 6 && L.Po / (nseg * 2) >= 4 * ((Lp + L.Dp - 1) / L.Dp)) nseg *= 2;
+    a.oseg = (L.Po + nseg - 1) / nseg;
+    a.nseg = (L.Po + a.oseg - 1) / a.oseg;
+    int dev = 0, maxsmem = 227 * 1024;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const size_t avail = std::min((size_t)maxsmem - 1024, FUSED_SMEM_MAX);
+    int SB = 4;
+    if (fused_smem(a.Lkp, a.Dk, a.Nt, SB, a.Dp) > avail) SB = 2;
+    a.SB = SB;
+    const size_t smem = fused_smem(a.Lkp, a.Dk, a.Nt, SB, a.Dp);
+    if (smem > avail) { *why = "the one-pass level's operands do not fit shared memory"; return cudaErrorNotSupported; }
+    const long nb = (long)L.Np * a.ntile * a.nseg;
+    if (nb > 0x7fffffffL) return cudaErrorInvalidValue;
+    auto run = [&](auto kern) -> cudaError_t {
+        cudaError_t r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (r != cudaSuccess) return r;
+        kern<<<(unsigned)nb, F_NTHR, smem, s>>>(a);
+        return cudaGetLastError();
+    };
+    switch (a.Lkp / 8) {
+        case 2: return run(level_fused_kernel<2>);
+        case 4: return run(level_fused_kernel<4>);
+        case 6: return run(level_fused_kernel<6>);
+        case 8: return run(level_fused_kernel<8>);
+        case 10: return run(level_fused_kernel<10>);
+        default: return run(level_fused_kernel<12>);
+    }
+}
+
+}  // namespace ffbp

@@ -117,8 +117,9 @@ class ExactFormer:
     error from the third-order range expansion, 4 pi f_max / c h^4 / (2 r^3), stays below 3e-4 rad; former.tile,
     former.predicted_error_db), the tile centres, and per pulse the window of range bins the grid can reach (with a
     tile of margin). A call, per chunk of pulses: the windowed history zero-padded to nfft = 2^ceil(log2(upsample
-    K)) samples, its inverse FFT (cuFFT), the crop of each profile's window, and the tiled backprojection (CUDA,
-    fastsar_b200/csrc/exact_tiles.cu). backend accepts the reference's values; only 'auto' and 'cuda' run. profiles
+    K)) samples, its inverse FFT (cuFFT), and the tiled backprojection (CUDA, fastsar_b200/csrc/exact_tiles.cu),
+    which stages each tile's band of every profile by bulk copies (the reachable window blo / W below stays part of
+    the set-up: it decides whether the grid fits the profiles without ambiguity). backend accepts the reference's values; only 'auto' and 'cuda' run. profiles
     is accepted for compatibility; the profiles stay float32. One former must not be called from two threads at
     once."""
 
@@ -238,8 +239,7 @@ class ExactFormer:
         """What a call needs on the device: dict(backend, needed, available, full_speed, parts)."""
         import torch
         ch = min(self.chunk, self.P)
-        parts = dict(history=self.P * self.K * 8, padded=ch * self.nfft * 8 * 2, window=ch * self.W * 8,
-                     image=self.nx * self.ny * 8)
+        parts = dict(history=self.P * self.K * 8, padded=ch * self.nfft * 8 * 2, image=self.nx * self.ny * 8)
         free, _ = torch.cuda.mem_get_info()
         need = float(sum(parts.values()))
         return dict(backend=self.backend, needed=need, available=float(free), full_speed=need <= free, parts=parts)
@@ -249,8 +249,8 @@ class ExactFormer:
         if self._dev is None:
             dev = torch.device('cuda', torch.cuda.current_device())
             t = lambda a, dt=None: torch.from_numpy(np.ascontiguousarray(a if dt is None else a.astype(dt))).to(dev)
-            self._dev = dict(ant=t(self.ant), ref=t(self.ref), cen=t(self.cen), blo=t(self.blo, np.int64),
-                             lo=t(self.lo, np.int32), wp=t(self.wp, np.float32), wk=t(self.wk, np.float32))
+            self._dev = dict(ant=t(self.ant), ref=t(self.ref), cen=t(self.cen), wp=t(self.wp, np.float32),
+                             wk=t(self.wk, np.float32))
         return self._dev
 
     def form_device(self, S_dev, check=True):
@@ -262,12 +262,12 @@ class ExactFormer:
         d = self._upload()
         dev = S_dev.device
         S_dev = S_dev.to(torch.complex64).contiguous()
-        P, K, nfft, W = self.P, self.K, self.nfft, self.W
+        P, K, nfft = self.P, self.K, self.nfft
         ch = min(self.chunk, P)
         out = torch.zeros((self.nx, self.ny), dtype=torch.complex64, device=dev)
         pad = torch.zeros((ch, nfft), dtype=torch.complex64, device=dev)
-        win = torch.empty((ch, W), dtype=torch.complex64, device=dev)
         bad = torch.full((1,), 2 ** 31 - 1, dtype=torch.int32, device=dev)
+        err = torch.zeros((1,), dtype=torch.int32, device=dev)
         s = torch.cuda.current_stream(dev).cuda_stream
         e1 = (ctypes.c_double * 3)(*self.e1)
         e2 = (ctypes.c_double * 3)(*self.e2)
@@ -277,13 +277,14 @@ class ExactFormer:
             _lib.check(L.ffbp_exact_pad(S_dev[p0:p1].data_ptr(), n, K, d['wp'].data_ptr(), d['wk'].data_ptr(), nfft,
                                         pad.data_ptr(), bad.data_ptr() if check else None, p0, s), 'ffbp_exact_pad')
             prof = torch.fft.ifft(pad[:n], dim=1)
-            _lib.check(L.ffbp_exact_backproject(prof.data_ptr(), n, nfft, W, d['blo'][p0:p1].data_ptr(),
-                                                d['lo'][p0:p1].data_ptr(), d['ant'][p0:p1].data_ptr(),
+            _lib.check(L.ffbp_exact_backproject(prof.data_ptr(), n, nfft, d['ant'][p0:p1].data_ptr(),
                                                 d['ref'][p0:p1].data_ptr(), d['cen'].data_ptr(), self.ntx, self.nty,
                                                 self.tx, self.ty, self.nx, self.ny, self.spx, self.spy, e1, e2,
-                                                self.inv_dr, self.kcyc, int(self.cubic), self.along1, win.data_ptr(),
+                                                self.inv_dr, self.kcyc, int(self.cubic), self.along1, err.data_ptr(),
                                                 out.data_ptr(), s), 'ffbp_exact_backproject')
             del prof
+        if int(err.item()):
+            raise RuntimeError('ffbp_exact_backproject: a bounded wait for the profiles ran out; the image is incomplete')
         if check:
             b = int(bad.item())
             if b != 2 ** 31 - 1:

@@ -46,11 +46,16 @@ enum {
                             /* given (each component below 2^14 in magnitude)                                   */
     FFBP_FINAL_TC_BF16X3 = 2, /* tcgen05 tensor cores, operands split x = hi + lo in bfloat16, the hi*hi, hi*lo, */
                               /* lo*hi and lo*lo products accumulated in float32                               */
-    FFBP_LEVELS_TC = 0x100    /* flag, or-ed into ffbp_plan_desc.final_mode: the levels on the tensor cores     */
+    FFBP_LEVELS_TC = 0x100,   /* flag, or-ed into ffbp_plan_desc.final_mode: the levels on the tensor cores     */
                               /* (per pulse the children's modulated frequency taps times the parent row's      */
-                              /* Hankel windows, three bfloat16 products; a float16 intermediate; the pulse FIR */
-                              /* in float32). Levels of more than 64 children or 64 frequency taps stay on the  */
-                              /* float32 kernel. The workspace grows by the intermediate of the largest level.  */
+                              /* Hankel windows, three bfloat16 products accumulated in float32), in one pass:  */
+                              /* the ramp and the pulse FIR follow each pulse's product on the multiprocessor,  */
+                              /* the FIR's running sums in tensor memory. Levels the one-pass kernel does not   */
+                              /* cover (more than 8 output pulses per input pulse) take the two-pass form below; */
+                              /* levels of more than 64 children or 96 frequency taps stay on the float32 kernel */
+    FFBP_LEVELS_TC2 = 0x200   /* flag, with FFBP_LEVELS_TC: every tensor-core level in two passes (the product   */
+                              /* and ramp into a float16 intermediate in the workspace, then the pulse FIR in   */
+                              /* float32), the form before the one-pass kernel                                    */
 };
 
 /* One level of the plan (fastsar/ffbp2.py:192-250, make_plan's per-level record). All pointers are host memory. */
@@ -90,6 +95,8 @@ typedef struct {
     const float *h_wf;      /* aperture weights per (tile, final subaperture): [ntiles, Pf] (wf_ndim 2) or       */
     int wf_ndim;            /* [3, ntiles, Pf] weight and its gradients along e1, e2 (wf_ndim 3); NULL / 0 none  */
     int final_mode;         /* FFBP_FINAL_*, or-ed with FFBP_LEVELS_TC for the tensor-core levels                 */
+    int partial;            /* 0: the final tiles cover the padded grid; 1: a part of it (a shard of the first     */
+                            /* level's children: their descendants' tiles only; the image's other pixels untouched)*/
 } ffbp_plan_desc;
 
 typedef struct ffbp_plan ffbp_plan;
@@ -129,7 +136,8 @@ int ffbp_form(ffbp_plan *plan, const void *d_S, void *d_img, void *d_ws, size_t 
 int ffbp_plan_check(ffbp_plan *plan, void *stream);
 
 /* Test hook of the failure report above (no counterpart in the reference): from the next form call on, the MMA
- * issuers of the plan's launches of `kind` (FFBP_KIND_LEVEL_TC_GEMM or FFBP_KIND_FINAL_TC) first wait on a barrier
+ * issuers of the plan's launches of `kind` (FFBP_KIND_LEVEL_TC or FFBP_KIND_LEVEL_TC_GEMM: the tensor-core levels in
+ * either form; FFBP_KIND_FINAL_TC: the tensor-core final stage) first wait on a barrier
  * that nothing completes, with a limit of limit_us microseconds (1 .. 10^6), so that the wait runs out as a stuck
  * pipeline's would and the kernel winds down without its MMAs; kind 0 turns it off. The kernels stay well-formed:
  * every wait is bounded and the block frees its tensor memory before it exits.                                 */
@@ -187,7 +195,8 @@ enum {
     FFBP_KIND_LEVEL_TC_GEMM = 3,   /* a tensor-core level's first pass (products, ramp, float16 intermediate)     */
     FFBP_KIND_LEVEL_TC_FIR = 4,    /* a tensor-core level's pulse FIR                                              */
     FFBP_KIND_FINAL = 5,           /* the float32 final stage                                                      */
-    FFBP_KIND_FINAL_TC = 6         /* the tensor-core final stage                                                  */
+    FFBP_KIND_FINAL_TC = 6,        /* the tensor-core final stage                                                  */
+    FFBP_KIND_LEVEL_TC = 7         /* a one-pass tensor-core level                                                 */
 };
 int ffbp_form_profile(ffbp_plan *plan, const void *d_S, void *d_img, void *d_ws, size_t ws_bytes, void *stream,
                       float *h_ms, int *h_kind, int n);
@@ -216,6 +225,15 @@ int ffbp_level(const void *d_x, int Np, int P, int K, const void *d_phase, int C
  * caller: [0] nonzero when a bounded wait of the kernel ran out, [1] the input's largest |component| (float bits,
  * filled here), [2] the output's. No counterpart in the reference (its levels run in float32 only).            */
 size_t ffbp_level_tc_scratch_bytes(int Np, int C, int P, int Ko);
+
+/* The same level in one pass (the arithmetic of FFBP_LEVELS_TC without FFBP_LEVELS_TC2): the three bfloat16 products,
+ * the ramp and the pulse FIR's running sums (tensor memory) in one kernel; the output written once as complex64. No
+ * scratch. C <= 64, Lk <= 96 and ceil(Lp / Dp) <= 8 (FFBP_E_UNSUPPORTED otherwise). d_status: 3 ints, zeroed by the
+ * caller: [0] nonzero when a bounded wait of the kernel ran out, [2] the output's largest |component| (float bits).
+ * No counterpart in the reference (its levels run in float32 only).                                               */
+int ffbp_level_fused(const void *d_x, int Np, int P, int K, const void *d_phase, int C, const float *d_tk, int Lk,
+                     int plk, int Dk, int Ko, double kc, const float *d_tp, int Lp, int plp, int Dp, int Po,
+                     const float *d_wp, const float *d_wk, void *d_out, int *d_bad, int *d_status, void *stream);
 int ffbp_level_tc(const void *d_x, int Np, int P, int K, const void *d_phase, int C, const float *d_tk, int Lk, int plk,
                   int Dk, int Ko, double kc, const float *d_tp, int Lp, int plp, int Dp, int Po, const float *d_wp,
                   const float *d_wk, void *d_out, int *d_bad, void *d_scratch, size_t scratch_bytes, int *d_status,
@@ -225,18 +243,21 @@ int ffbp_level_tc(const void *d_x, int Np, int P, int K, const void *d_phase, in
  * ffbp_exact_pad writes the windowed samples S[p, k] wp[p_off + p] wk[k] of d_S [n, K] complex64 into d_pad [n, nfft]
  * at bin k - K/2 (mod nfft) (fastsar/exact.py:186-194 pad_window; the other bins are the caller's, zeroed once)
  * and records in d_bad (optional, atomic min) the first pulse p_off + p with a non-finite sample; after the caller's
- * inverse FFT of length nfft (cuFFT, normalised by 1/nfft), ffbp_exact_backproject crops each profile's W reachable
- * bins from blo[p] (circularly, scaled by nfft: fastsar/exact.py:196-205 crop) into d_win [n, W] and adds the tiled
- * backprojection (fastsar/exact.py:58-162 bp_tiles) onto d_out [nx, ny] complex64. Tiles tx x ty in {32 x 32,
- * 16 x 16, 8 x 16, 8 x 8}; d_cen [ntx nty, 3] their centres (float64), tile (bx, by) at index bx nty + by; lo[p] =
- * blo[p] - nfft/2; e1, e2 host pointers to 3 doubles; cubic 1 (Lagrange, 4 samples) or 0 (linear); along1 1 to run
- * consecutive blocks along e1.                                                                                    */
+ * inverse FFT of length nfft (cuFFT, normalised by 1/nfft: bin 0 is zero delay), ffbp_exact_backproject adds the
+ * tiled backprojection (the mathematics of fastsar/exact.py:58-162 bp_tiles) of the profiles d_prof [n, nfft]
+ * complex64 (16-byte aligned, nfft even) onto d_out [nx, ny] complex64: per tile its centre's range in float64, per
+ * pixel the range to third order about it, a cubic Lagrange (cubic 1, 4 samples) or linear (0) read of the profile at
+ * dR inv_dr (circularly), times exp(2 pi i kcyc dR), the sum times nfft. The profiles are read in place (each tile's
+ * band of bins, no cropped copy; fastsar/exact.py:196-205 crops them first). Tiles tx x ty in {32 x 32, 16 x 16,
+ * 8 x 16, 8 x 8}; d_cen [ntx nty, 3] their centres (float64), tile (bx, by) at index bx nty + by; d_ant [n, 3],
+ * d_ref [n] the pulses' antenna positions and reference ranges; e1, e2 host pointers to 3 doubles; along1 1 to run
+ * consecutive blocks along e1. d_err (optional) is raised when a bounded wait of the kernel ran out.             */
 int ffbp_exact_pad(const void *d_S, int n, int K, const float *d_wp, const float *d_wk, int nfft, void *d_pad,
                    int *d_bad, int p_off, void *stream);
-int ffbp_exact_backproject(const void *d_prof, int n, int nfft, int W, const long long *d_blo, const int *d_lo,
-                           const double *d_ant, const double *d_ref, const double *d_cen, int ntx, int nty, int tx,
-                           int ty, int nx, int ny, double spx, double spy, const double *e1, const double *e2,
-                           double inv_dr, double kcyc, int cubic, int along1, void *d_win, void *d_out, void *stream);
+int ffbp_exact_backproject(const void *d_prof, int n, int nfft, const double *d_ant, const double *d_ref,
+                           const double *d_cen, int ntx, int nty, int tx, int ty, int nx, int ny, double spx, double spy,
+                           const double *e1, const double *e2, double inv_dr, double kcyc, int cubic, int along1,
+                           int *d_err, void *d_out, void *stream);
 
 /* The range gate (fastsar/ffbp_cuda.py:767-864 and ImageFormer._gate fastsar/api.py:525-564), three steps around the
  * caller's two FFTs (cuFFT) per block of n pulses: ffbp_gate_pad writes d_z [n, Kp] complex64: zeros, and at
