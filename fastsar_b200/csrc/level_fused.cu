@@ -11,15 +11,15 @@
 //
 // A block owns one parent, one tile of Nt output columns (32; 64 when the level has at most 32 children) and a
 // segment of output pulses, and sweeps the input pulses those outputs need, in order. Per pulse:
-//   warps 16..19  the modulated taps of every child (A': rows 2c and 2c + 1 the real and imaginary parts of child c,
+//   warps 8..12   the modulated taps of every child (A': rows 2c and 2c + 1 the real and imaginary parts of child c,
 //                 K = taps padded to 16; rows 64..127 repeat rows 0..63 when there are at most 32 children), split
 //                 into bfloat16 hi + lo, into the A' buffer of the pulse's issuer;
-//   warps 20, 21  the window of the parent's row the tile reads (cp.async, a ring XS pulses deep), windowed at the
+//   warp 13       the window of the parent's row the tile reads (cp.async, a ring XS pulses deep), windowed at the
 //                 first level, as bfloat16 hi/lo planes with even- and odd-shifted copies;
-//   warps 22..25  the Hankel rows from the planes (B': 2 Nt rows, the real and imaginary windows of each column);
-//   warps 26, 27  one thread each issues the pulse's tcgen05.mma (M = 128, N = 2 Nt, K = 16; hi hi + hi lo + lo hi)
-//                 into its own tensor-memory accumulator: warp 26 the even pulses, warp 27 the odd ones;
-//   warps 0..15   read the accumulator (warp w: lane quarter w % 4, one chunk of 8 columns), exchange halves between
+//   warps 14, 15  the Hankel rows from the planes (B': 2 Nt rows, the real and imaginary windows of each column);
+//   warps 16, 17  one thread each issues the pulse's tcgen05.mma (M = 128, N = 2 Nt, K = 16; hi hi + hi lo + lo hi)
+//                 into its own tensor-memory accumulator: warp 16 the even pulses, warp 17 the odd ones;
+//   warps 0..7    read the accumulator (warp w: lane quarter w % 4, two chunks of 8 columns), exchange halves between
 //                 a child's two rows, apply the ramp, and add the pulse into the pulse FIR's running sums: per
 //                 (child, column) the ceil(Lp / Dp) <= 8 output pulses the input pulse feeds, held in tensor memory
 //                 (16 columns of the thread's own lane: a ring of 8 complex slots, output i in slot i mod 8). When an
@@ -43,10 +43,10 @@ namespace {
 
 using namespace tc;
 
-constexpr int F_NCW = 16;                        // consumer warps 0..15
-constexpr int F_NAW = 4;                         // A' producers 16..19
-constexpr int F_NLW = 1;                         // planes 20
-constexpr int F_NHW = 2;                         // Hankel rows 22..23
+constexpr int F_NCW = 8;                         // consumer warps 0..7
+constexpr int F_NAW = 5;                         // A' producers 8..12
+constexpr int F_NLW = 1;                         // planes 13
+constexpr int F_NHW = 2;                         // Hankel rows 14..15
 constexpr int F_AW0 = F_NCW, F_LW0 = F_AW0 + F_NAW, F_HW0 = F_LW0 + F_NLW, F_IW0 = F_HW0 + F_NHW;
 constexpr int F_NWARPS = F_IW0 + 2;              // + the two MMA issuers
 constexpr int F_NTHR = F_NWARPS * 32;
@@ -85,39 +85,38 @@ __device__ __forceinline__ void fill_tap_table(const FusedArgs &a, float2 *s_tap
     }
 }
 
-// Slot s of a ring of 8 complex values held as 16 floats: read, or clear (a warp-uniform switch, no local memory)
-__device__ __forceinline__ float2 ring_get(const float *v, int s)
+// Slot s of a ring of 8 complex values held as 16 floats: read it and clear it (selects on static indices, so that
+// the ring stays in registers)
+__device__ __forceinline__ float2 ring_take(float *v, int s)
 {
-    switch (s) {
-        case 0: return make_float2(v[0], v[1]);
-        case 1: return make_float2(v[2], v[3]);
-        case 2: return make_float2(v[4], v[5]);
-        case 3: return make_float2(v[6], v[7]);
-        case 4: return make_float2(v[8], v[9]);
-        case 5: return make_float2(v[10], v[11]);
-        case 6: return make_float2(v[12], v[13]);
-        default: return make_float2(v[14], v[15]);
+    float ox = 0.f, oy = 0.f;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        const bool m = t == s;
+        ox = m ? v[2 * t] : ox;
+        oy = m ? v[2 * t + 1] : oy;
+        v[2 * t] = m ? 0.f : v[2 * t];
+        v[2 * t + 1] = m ? 0.f : v[2 * t + 1];
     }
+    return make_float2(ox, oy);
 }
 
-__device__ __forceinline__ void ring_clear(float *v, int s)
+// Slot s of a ring, read only
+__device__ __forceinline__ float2 ring_get(const float *v, int s)
 {
-    switch (s) {
-        case 0: v[0] = v[1] = 0.f; break;
-        case 1: v[2] = v[3] = 0.f; break;
-        case 2: v[4] = v[5] = 0.f; break;
-        case 3: v[6] = v[7] = 0.f; break;
-        case 4: v[8] = v[9] = 0.f; break;
-        case 5: v[10] = v[11] = 0.f; break;
-        case 6: v[12] = v[13] = 0.f; break;
-        default: v[14] = v[15] = 0.f; break;
+    float ox = 0.f, oy = 0.f;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        ox = t == s ? v[2 * t] : ox;
+        oy = t == s ? v[2 * t + 1] : oy;
     }
+    return make_float2(ox, oy);
 }
 
 __device__ __forceinline__ int floor_div(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
 
 template <int NKC>
-__global__ void __maxnreg__(80) level_fused_kernel(const FusedArgs a)
+__global__ void __maxnreg__(112) level_fused_kernel(const FusedArgs a)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
     constexpr int nkc = NKC;                                 // core matrices along K (Lkp = 8 NKC)
@@ -366,26 +365,29 @@ __global__ void __maxnreg__(80) level_fused_kernel(const FusedArgs a)
         }
         __syncwarp();
     } else {
-        // ------------------------------------------------------------------ consumers (warps 0..15)
+        // ------------------------------------------------------------------ consumers (warps 0..7)
         // Warp w reads lane quarter q = w % 4: rows 2c, 2c + 1 for the children c = 16 q + lane / 2 (with at most 32
-        // children quarters 2, 3 repeat 0, 1 and take other columns), at one chunk of 8 columns; lanes 2c and 2c + 1
-        // exchange halves so that each forms its child's outputs at 4 of the 8 columns.
+        // children quarters 2, 3 repeat 0, 1 and take other columns), at two chunks of 8 columns; lanes 2c and 2c + 1
+        // exchange halves so that each forms its child's outputs at 4 of a chunk's 8 columns: 8 (child, column)
+        // elements per thread, each with its ring of 8 running sums (16 tensor-memory columns of the thread's lane).
         const int rp = a.C <= 32 ? 2 : 1;
         const int q = warp & 3, g = warp >> 2;
         const int c = 16 * (rp == 2 ? (q & 1) : q) + (lane >> 1);
         const bool odd = lane & 1, live = c < a.C;
-        const int chunk = rp == 2 ? g + 4 * (q >> 1) : g;           // 8-column chunk of the tile
-        const int j0 = tt * a.Nt + chunk * 8 + (odd ? 4 : 0);         // this thread's first output column
+        const int chunk0 = (rp == 2 ? 4 * (q >> 1) : 0) + 2 * g;     // this warp's chunks chunk0, chunk0 + 1
+        const int jb = tt * a.Nt + chunk0 * 8 + (odd ? 4 : 0);       // this thread's first output column
         const uint32_t lanes = (uint32_t)(32 * q) << 16;
-        const uint32_t fir = tmem + lanes + (uint32_t)(4 * a.Nt + 64 * g);   // this thread's running sums, 4 x 16 cols
+        const uint32_t fir = tmem + lanes + (uint32_t)(4 * a.Nt + 128 * g);  // running sums: element e at 16 e
         const float2 *__restrict__ phc = a.ph + ((size_t)n * a.C + (live ? c : 0)) * a.P;
         float2 *__restrict__ outc = a.out + ((size_t)n * a.C + (live ? c : 0)) * a.Po * a.Ko;
+        // element e (0..7): chunk chunk0 + e / 4, column jb + 8 (e / 4) + e % 4
+        auto col = [&](int e) { return jb + 8 * (e >> 2) + (e & 3); };
         {
             float z[16];
 #pragma unroll
             for (int i = 0; i < 16; ++i) z[i] = 0.f;
 #pragma unroll
-            for (int e = 0; e < 4; ++e) tmem_st16(fir + 16u * e, z);
+            for (int e = 0; e < 8; ++e) tmem_st16(fir + 16u * e, z);
             tmem_wait_st();
         }
         float vmax = 0.f;
@@ -399,71 +401,73 @@ __global__ void __maxnreg__(80) level_fused_kernel(const FusedArgs a)
             if (!__all_sync(0xffffffffu, mbar_wait(&dfull[k], (uint32_t)((s >> 1) & 1), 200, &s_abort, a.err, F_WAIT_NS)))
                 break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            float vr[8], vi[8];
-            const uint32_t acc = tmem + lanes + (uint32_t)(k * 2 * a.Nt + chunk * 8);
-            tmem_ld8(acc, vr);
-            tmem_ld8(acc + (uint32_t)a.Nt, vi);
-            tmem_wait_ld();
-            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&dempty[k]);          // the accumulator is free for the issuer's next pulse
-            // the child's outputs at columns j0 .. j0 + 3 of this pulse: re = Mr Xr - Mi Xi, im = Mr Xi + Mi Xr, times
-            // the ramp exp(2 pi i (c0 + sl (Dk j - plk - kc))) (seeded at j0, stepped by exp(2 pi i sl Dk))
-            float yr[4], yi[4];
-            {
-                const float2 st = cis_cycles(q0.y * (float)a.Dk);
-                float2 w = cis_cycles(fmaf(q0.y, (float)(a.Dk * j0 - a.plk) - a.kc, q0.x));
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const float sr = odd ? vr[i] : vr[4 + i], si = odd ? vi[i] : vi[4 + i];
-                    const float rr = __shfl_xor_sync(0xffffffffu, sr, 1), ri = __shfl_xor_sync(0xffffffffu, si, 1);
-                    const float orr = odd ? vr[4 + i] : vr[i], ori = odd ? vi[4 + i] : vi[i];
-                    const float mr_r = odd ? rr : orr, mr_i = odd ? ri : ori;
-                    const float mi_r = odd ? orr : rr, mi_i = odd ? ori : ri;
-                    const float2 y = cmul(w, make_float2(mr_r - mi_i, mr_i + mi_r));
-                    yr[i] = y.x;
-                    yi[i] = y.y;
-                    w = cmul(w, st);
-                }
-            }
             // the pulse FIR: this input pulse's taps in ring-slot order, and the output it completes (if any)
             const int pp = p + a.plp;                         // >= 0
             const int r0 = pp % a.Dp, qq = pp / a.Dp;
             const float4 *tq = reinterpret_cast<const float4 *>(s_tap + ((size_t)r0 * F_AP + (qq & 7)) * F_AP);
-            float2 tp8[8];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const float4 v = tq[i];
-                tp8[2 * i] = make_float2(v.x, v.y);
-                tp8[2 * i + 1] = make_float2(v.z, v.w);
-            }
             const int cn = pp - a.Lp + 1;
             const int ic = floor_div(cn, a.Dp);
             const bool done = cn == ic * a.Dp;                // output ic has had its last input (block-uniform)
             const int cslot = ic & 7;                         // two's complement: ic mod 8, also for ic < 0
             const bool store = done && live && ic >= i_s && ic < i_e;
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                float v[16];
-                tmem_ld16(fir + 16u * e, v);
+            const float2 st = cis_cycles(q0.y * (float)a.Dk), st8 = cis_cycles(q0.y * (float)(8 * a.Dk));
+            float2 w = cis_cycles(fmaf(q0.y, (float)(a.Dk * jb - a.plk) - a.kc, q0.x));
+            const uint32_t acc = tmem + lanes + (uint32_t)(k * 2 * a.Nt + chunk0 * 8);
+#pragma unroll 1
+            for (int h = 0; h < 2; ++h) {
+                // chunk h: the Xr and Xi columns of the accumulator
+                float xr[8], xi[8];
+                tmem_ld8(acc + 8u * h, xr);
+                tmem_ld8(acc + (uint32_t)a.Nt + 8u * h, xi);
                 tmem_wait_ld();
-                const float2 y = make_float2(yr[e], yi[e]);
+                if (h == 1) {
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&dempty[k]);  // the accumulator is free for the issuer's next pulse
+                }
+                // the child's outputs at the chunk's 4 columns: re = Mr Xr - Mi Xi, im = Mr Xi + Mi Xr, times the
+                // ramp exp(2 pi i (c0 + sl (Dk j - plk - kc))) (seeded at the chunk's first column, stepped by
+                // exp(2 pi i sl Dk))
+                float2 y[4];
+                float2 wc = w;
 #pragma unroll
-                for (int sl = 0; sl < 8; ++sl) {
-                    const float2 r = ffma2(tp8[sl], y, make_float2(v[2 * sl], v[2 * sl + 1]));
-                    v[2 * sl] = r.x;
-                    v[2 * sl + 1] = r.y;
+                for (int i = 0; i < 4; ++i) {
+                    const float sr = odd ? xr[i] : xr[4 + i], si = odd ? xi[i] : xi[4 + i];
+                    const float rr = __shfl_xor_sync(0xffffffffu, sr, 1), ri = __shfl_xor_sync(0xffffffffu, si, 1);
+                    const float orr = odd ? xr[4 + i] : xr[i], ori = odd ? xi[4 + i] : xi[i];
+                    const float mr_r = odd ? rr : orr, mr_i = odd ? ri : ori;
+                    const float mi_r = odd ? orr : rr, mi_i = odd ? ori : ri;
+                    y[i] = cmul(wc, make_float2(mr_r - mi_i, mr_i + mi_r));
+                    wc = cmul(wc, st);
                 }
-                if (done) {
-                    const float2 o = ring_get(v, cslot);
-                    ring_clear(v, cslot);
-                    const int j = j0 + e;
-                    if (store && j < a.Ko) {
-                        outc[(size_t)ic * a.Ko + j] = o;
-                        vmax = fmaxf(vmax, fmaxf(fabsf(o.x), fabsf(o.y)));
+                w = cmul(w, st8);
+                // the elements' rings: load, update, store (the next element's load issued before this one's stores)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int ee = 4 * h + e;
+                    float v[16];
+                    tmem_ld16(fir + 16u * ee, v);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int sl = 0; sl < 8; sl += 2) {
+                        const float4 tv = tq[sl / 2];         // the taps of slots sl, sl + 1, each twice
+                        float2 r = ffma2(make_float2(tv.x, tv.y), y[e], make_float2(v[2 * sl], v[2 * sl + 1]));
+                        v[2 * sl] = r.x;
+                        v[2 * sl + 1] = r.y;
+                        r = ffma2(make_float2(tv.z, tv.w), y[e], make_float2(v[2 * sl + 2], v[2 * sl + 3]));
+                        v[2 * sl + 2] = r.x;
+                        v[2 * sl + 3] = r.y;
                     }
+                    if (done) {
+                        const float2 o = ring_take(v, cslot);
+                        const int j = col(ee);
+                        if (store && j < a.Ko) {
+                            outc[(size_t)ic * a.Ko + j] = o;
+                            vmax = fmaxf(vmax, fmaxf(fabsf(o.x), fabsf(o.y)));
+                        }
+                    }
+                    tmem_st16(fir + 16u * ee, v);
                 }
-                tmem_st16(fir + 16u * e, v);
             }
             tmem_wait_st();
         }
@@ -474,13 +478,13 @@ __global__ void __maxnreg__(80) level_fused_kernel(const FusedArgs a)
             const int ic_last = floor_div(pa + nst - 1 + a.plp - a.Lp + 1, a.Dp);   // the last output completed
             const int qn_last = floor_div(pa + nst - 1 + a.plp, a.Dp);              // the newest output fed
             for (int i = max(i_s, ic_last + 1); i < i_e; ++i) {
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
+#pragma unroll 1
+                for (int e = 0; e < 8; ++e) {
                     float v[16];
                     tmem_ld16(fir + 16u * e, v);
                     tmem_wait_ld();
                     const float2 o = i <= qn_last ? ring_get(v, i & 7) : make_float2(0.f, 0.f);
-                    const int j = j0 + e;
+                    const int j = col(e);
                     if (live && j < a.Ko) {
                         outc[(size_t)i * a.Ko + j] = o;
                         vmax = fmaxf(vmax, fmaxf(fabsf(o.x), fabsf(o.y)));
