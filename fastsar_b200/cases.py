@@ -3,6 +3,7 @@ at a time and for small profiler captures (the commands of profiles/*.md run it)
 
     python -m fastsar_b200.cases level L1 [--parents 8] [--pulses 2048] [--form tc|fp32] [--taps learned|80|70]
     python -m fastsar_b200.cases final [--tiles 20000] [--mode f16|bf16x3|fp32] [--taps learned|80|70]
+    python -m fastsar_b200.cases exact [--workload spotlight_4k] [--interp cubic|linear] [--pulses 1024]
 
 `level`: one merge stage of the plan (its children, decimations and filters) on `--parents` parents of random
 samples and random child phases, through ffbp_level_tc (tensor cores: its two launches, level_tc_gemm and
@@ -112,9 +113,44 @@ def final_case(tiles, mode='f16', taps='learned', reps=2, seed=2, pmax=0.5):
               flush=True)
 
 
+def exact_case(workload='spotlight_4k', interp='cubic', pulses=1024, reps=5):
+    """ExactFormer's tiled backprojection alone (ffbp_exact_backproject) on one chunk of a workload's pulses: the
+    seeded synthetic history padded, windowed and inverse-transformed once, then the kernel timed."""
+    import ctypes
+    import torch
+    from .exact import ExactFormer
+    L = _lib.load()
+    w, S = sim.synthetic_history(workload, seed=1, n_clutter=20000)
+    col = w['col']
+    f = ExactFormer(col.ant, col.fmin, col.df, col.K, w['nx'], w['ny'], w['spx'], w['spy'], w['e1'], w['e2'],
+                    interp=interp, chunk=pulses)
+    d = f._upload()
+    n = min(f.chunk, f.P)
+    st = torch.cuda.current_stream().cuda_stream
+    pad = torch.zeros((n, f.nfft), dtype=torch.complex64, device='cuda')
+    _lib.check(L.ffbp_exact_pad(S[:n].data_ptr(), n, f.K, d['wp'].data_ptr(), d['wk'].data_ptr(), f.nfft,
+                                pad.data_ptr(), None, 0, st), 'ffbp_exact_pad')
+    prof = torch.fft.ifft(pad, dim=1).contiguous()
+    e1, e2 = (ctypes.c_double * 3)(*f.e1), (ctypes.c_double * 3)(*f.e2)
+    out = torch.zeros((f.nx, f.ny), dtype=torch.complex64, device='cuda')
+    for r in range(reps + 1):
+        e0, e1_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _lib.check(L.ffbp_exact_backproject(prof.data_ptr(), n, f.nfft, d['ant'].data_ptr(), d['ref'].data_ptr(),
+                                            d['cen'].data_ptr(), f.ntx, f.nty, f.tx, f.ty, f.nx, f.ny, f.spx, f.spy,
+                                            e1, e2, f.inv_dr, f.kcyc, int(f.cubic), f.along1, None, out.data_ptr(),
+                                            st), 'ffbp_exact_backproject')
+        e1_.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1_)
+        if r:
+            print(f'exact {workload} {interp} tile {f.tile}, {n} pulses: {ms:.3f} ms, '
+                  f'{f.nx * f.ny * n / (ms * 1e-3) / 1e9:.0f} GBP/s', flush=True)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description='time one stage of a workload plan')
-    ap.add_argument('stage', choices=('level', 'final'))
+    ap.add_argument('stage', choices=('level', 'final', 'exact'))
     ap.add_argument('level', nargs='?', default='L1', choices=('L0', 'L1', 'L2'))
     ap.add_argument('--parents', type=int, default=8)
     ap.add_argument('--pulses', type=int, default=0)
@@ -124,8 +160,12 @@ def main(argv=None):
     ap.add_argument('--taps', default='learned', help="'learned' or a Kaiser-sinc attenuation in dB (70, 80)")
     ap.add_argument('--reps', type=int, default=3)
     ap.add_argument('--pmax', type=float, default=0.5)
+    ap.add_argument('--workload', default='spotlight_4k', help='exact: the workload')
+    ap.add_argument('--interp', choices=('cubic', 'linear'), default='cubic', help='exact: the interpolation')
     a = ap.parse_args(argv)
-    if a.stage == 'level':
+    if a.stage == 'exact':
+        exact_case(a.workload, a.interp, a.pulses or 1024, a.reps)
+    elif a.stage == 'level':
         level_case(int(a.level[1]), a.parents, a.pulses, a.form, a.taps, a.reps, pmax=a.pmax)
     else:
         final_case(a.tiles, a.mode, a.taps, a.reps, pmax=a.pmax)

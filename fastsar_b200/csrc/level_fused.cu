@@ -11,14 +11,14 @@
 //
 // A block owns one parent, one tile of Nt output columns (32; 64 when the level has at most 32 children) and a
 // segment of output pulses, and sweeps the input pulses those outputs need, in order. Per pulse:
-//   warps 8..12   the modulated taps of every child (A': rows 2c and 2c + 1 the real and imaginary parts of child c,
+//   warps 8..11   the modulated taps of every child (A': rows 2c and 2c + 1 the real and imaginary parts of child c,
 //                 K = taps padded to 16; rows 64..127 repeat rows 0..63 when there are at most 32 children), split
 //                 into bfloat16 hi + lo, into the A' buffer of the pulse's issuer;
-//   warp 13       the window of the parent's row the tile reads (cp.async, a ring XS pulses deep), windowed at the
+//   warp 12       the window of the parent's row the tile reads (cp.async, a ring XS pulses deep), windowed at the
 //                 first level, as bfloat16 hi/lo planes with even- and odd-shifted copies;
-//   warps 14, 15  the Hankel rows from the planes (B': 2 Nt rows, the real and imaginary windows of each column);
-//   warps 16, 17  one thread each issues the pulse's tcgen05.mma (M = 128, N = 2 Nt, K = 16; hi hi + hi lo + lo hi)
-//                 into its own tensor-memory accumulator: warp 16 the even pulses, warp 17 the odd ones;
+//   warp 13       the Hankel rows from the planes (B': 2 Nt rows, the real and imaginary windows of each column);
+//   warps 14, 15  one thread each issues the pulse's tcgen05.mma (M = 128, N = 2 Nt, K = 16; hi hi + hi lo + lo hi)
+//                 into its own tensor-memory accumulator: warp 14 the even pulses, warp 15 the odd ones;
 //   warps 0..7    read the accumulator (warp w: lane quarter w % 4, two chunks of 8 columns), exchange halves between
 //                 a child's two rows, apply the ramp, and add the pulse into the pulse FIR's running sums: per
 //                 (child, column) the ceil(Lp / Dp) <= 8 output pulses the input pulse feeds, held in tensor memory
@@ -44,9 +44,9 @@ namespace {
 using namespace tc;
 
 constexpr int F_NCW = 8;                         // consumer warps 0..7
-constexpr int F_NAW = 5;                         // A' producers 8..12
-constexpr int F_NLW = 1;                         // planes 13
-constexpr int F_NHW = 2;                         // Hankel rows 14..15
+constexpr int F_NAW = 4;                         // A' producers 8..11
+constexpr int F_NLW = 1;                         // planes 12
+constexpr int F_NHW = 1;                         // Hankel rows 13
 constexpr int F_AW0 = F_NCW, F_LW0 = F_AW0 + F_NAW, F_HW0 = F_LW0 + F_NLW, F_IW0 = F_HW0 + F_NHW;
 constexpr int F_NWARPS = F_IW0 + 2;              // + the two MMA issuers
 constexpr int F_NTHR = F_NWARPS * 32;
@@ -116,7 +116,7 @@ __device__ __forceinline__ float2 ring_get(const float *v, int s)
 __device__ __forceinline__ int floor_div(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
 
 template <int NKC>
-__global__ void __maxnreg__(112) level_fused_kernel(const FusedArgs a)
+__global__ void __launch_bounds__(F_NTHR, 1) level_fused_kernel(const FusedArgs a)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
     constexpr int nkc = NKC;                                 // core matrices along K (Lkp = 8 NKC)
