@@ -391,6 +391,17 @@ __global__ void __launch_bounds__(F_NTHR, 1) level_fused_kernel(const FusedArgs 
             tmem_wait_st();
         }
         float vmax = 0.f;
+        // outputs whose window ends before the first input pulse (the leading margin of the decimator's layout) have
+        // no input: zero
+        {
+            const int i_first = floor_div(pa + a.plp - a.Lp + a.Dp, a.Dp);     // the first output fed by the sweep
+            for (int i = i_s; i < min(i_e, i_first); ++i)
+#pragma unroll 1
+                for (int e = 0; e < 8; ++e) {
+                    const int j = col(e);
+                    if (live && j < a.Ko) outc[(size_t)i * a.Ko + j] = make_float2(0.f, 0.f);
+                }
+        }
         float2 qn = nst > 0 ? __ldg(&phc[pa]) : make_float2(0.f, 0.f);   // the next pulse's (c0, sl)
         int s = 0;
         for (; s < nst; ++s) {
