@@ -1,13 +1,14 @@
 """A profiling harness, not part of the former's API: single-stage cases of a workload's plan, for timing one kernel
 at a time and for small profiler captures (the commands of profiles/*.md run it):
 
-    python -m fastsar_b200.cases level L1 [--parents 8] [--pulses 2048] [--form tc|fp32] [--taps learned|80|70]
+    python -m fastsar_b200.cases level L1 [--parents 8] [--pulses 2048] [--form tc|fused|fp32] [--taps learned|80|70]
     python -m fastsar_b200.cases final [--tiles 20000] [--mode f16|bf16x3|fp32] [--taps learned|80|70]
     python -m fastsar_b200.cases exact [--workload spotlight_4k] [--interp cubic|linear] [--pulses 1024]
 
 `level`: one merge stage of the plan (its children, decimations and filters) on `--parents` parents of random
-samples and random child phases, through ffbp_level_tc (tensor cores: its two launches, level_tc_gemm and
-level_fir) or ffbp_level (float32: level_kernel); `--pulses` shortens the pulse axis (the pulse filter is then
+samples and random child phases, through ffbp_level_tc (tensor cores in two passes: level_tc_gemm and level_fir),
+ffbp_level_fused (tensor cores in one pass) or ffbp_level (float32: level_kernel); `--pulses` shortens the pulse
+axis (the pulse filter is then
 designed for the shorter axis by the same rule). `final`: the final stage through ffbp_final on `--tiles` tiles of
 the plan's final shape with random samples and geometry. Each prints the event-timed duration of every repetition.
 The defaults are the 16,384 x 8,192 -> 12,288 x 8,832 spotlight (workload spotlight_12k) planned as the chosen form
@@ -67,7 +68,11 @@ def level_case(level, parents, pulses=0, form='tc', taps='learned', reps=3, seed
     scr = torch.empty(nb // 4 + 4, dtype=torch.int32, device='cuda') if form == 'tc' else None
 
     def run():
-        if form == 'tc':
+        if form == 'fused':
+            _lib.check(L.ffbp_level_fused(x.data_ptr(), parents, P, K, ph.data_ptr(), C, tk.data_ptr(), fk['L'],
+                                          fk['pl'], Dk, Ko, (K - 1) / 2.0, tp.data_ptr(), fp['L'], fp['pl'], Dp, Po,
+                                          None, None, out.data_ptr(), None, st.data_ptr(), s), 'ffbp_level_fused')
+        elif form == 'tc':
             _lib.check(L.ffbp_level_tc(x.data_ptr(), parents, P, K, ph.data_ptr(), C, tk.data_ptr(), fk['L'], fk['pl'],
                                        Dk, Ko, (K - 1) / 2.0, tp.data_ptr(), fp['L'], fp['pl'], Dp, Po, None, None,
                                        out.data_ptr(), None, scr.data_ptr(), nb, st.data_ptr(), s), 'ffbp_level_tc')
@@ -154,7 +159,7 @@ def main(argv=None):
     ap.add_argument('level', nargs='?', default='L1', choices=('L0', 'L1', 'L2'))
     ap.add_argument('--parents', type=int, default=8)
     ap.add_argument('--pulses', type=int, default=0)
-    ap.add_argument('--form', choices=('tc', 'fp32'), default='tc')
+    ap.add_argument('--form', choices=('tc', 'fused', 'fp32'), default='tc')
     ap.add_argument('--tiles', type=int, default=20000)
     ap.add_argument('--mode', choices=('f16', 'bf16x3', 'fp32'), default='f16')
     ap.add_argument('--taps', default='learned', help="'learned' or a Kaiser-sinc attenuation in dB (70, 80)")

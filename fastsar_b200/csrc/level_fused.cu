@@ -45,8 +45,8 @@ using namespace tc;
 
 constexpr int F_NCW = 8;                         // consumer warps 0..7
 constexpr int F_NAW = 4;                         // A' producers 8..11
-constexpr int F_NLW = 1;                         // planes 12
-constexpr int F_NHW = 1;                         // Hankel rows 13
+constexpr int F_NLW = 2;                         // planes 12..13
+constexpr int F_NHW = 4;                         // Hankel rows 14..17
 constexpr int F_AW0 = F_NCW, F_LW0 = F_AW0 + F_NAW, F_HW0 = F_LW0 + F_NLW, F_IW0 = F_HW0 + F_NHW;
 constexpr int F_NWARPS = F_IW0 + 2;              // + the two MMA issuers
 constexpr int F_NTHR = F_NWARPS * 32;
@@ -421,8 +421,6 @@ __global__ void __launch_bounds__(F_NTHR, 1) level_fused_kernel(const FusedArgs 
             const bool done = cn == ic * a.Dp;                // output ic has had its last input (block-uniform)
             const int cslot = ic & 7;                         // two's complement: ic mod 8, also for ic < 0
             const bool store = done && live && ic >= i_s && ic < i_e;
-            const float2 st = cis_cycles(q0.y * (float)a.Dk), st8 = cis_cycles(q0.y * (float)(8 * a.Dk));
-            float2 w = cis_cycles(fmaf(q0.y, (float)(a.Dk * jb - a.plk) - a.kc, q0.x));
             const uint32_t acc = tmem + lanes + (uint32_t)(k * 2 * a.Nt + chunk0 * 8);
 #pragma unroll 1
             for (int h = 0; h < 2; ++h) {
@@ -440,7 +438,8 @@ __global__ void __launch_bounds__(F_NTHR, 1) level_fused_kernel(const FusedArgs 
                 // ramp exp(2 pi i (c0 + sl (Dk j - plk - kc))) (seeded at the chunk's first column, stepped by
                 // exp(2 pi i sl Dk))
                 float2 y[4];
-                float2 wc = w;
+                const float2 st = cis_cycles(q0.y * (float)a.Dk);
+                float2 wc = cis_cycles(fmaf(q0.y, (float)(a.Dk * (jb + 8 * h) - a.plk) - a.kc, q0.x));
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
                     const float sr = odd ? xr[i] : xr[4 + i], si = odd ? xi[i] : xi[4 + i];
@@ -451,7 +450,6 @@ __global__ void __launch_bounds__(F_NTHR, 1) level_fused_kernel(const FusedArgs 
                     y[i] = cmul(wc, make_float2(mr_r - mi_i, mr_i + mi_r));
                     wc = cmul(wc, st);
                 }
-                w = cmul(w, st8);
                 // the elements' rings: load, update, store (the next element's load issued before this one's stores)
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
