@@ -17,7 +17,7 @@ ValueError, as the reference does for a backend its machine lacks.
 Precision: 'float32' (default): float32 arithmetic everywhere, the final stage on the CUDA cores or, where built,
 as three bfloat16 products on the tensor cores (the reference's float32 CUDA default, fastsar/ffbp_cuda.py:949-953);
 FASTSAR_FINAL=fp32 keeps the CUDA cores. 'float16': the final stage's operands in float16 on the tensor cores with
-float32 accumulation (T = 32).
+float32 accumulation (T = 16 or 32).
 """
 import ctypes
 import os
@@ -102,7 +102,7 @@ def _check_grid(nx, ny, spx, spy, e1, e2):
 def _final_mode(precision):
     """The formation mode of a precision: 'float32' the float32 kernels (FASTSAR_FINAL=tc3 puts the final stage on
     the tensor cores in split bfloat16); 'float16' the levels and the final stage on the tensor cores, the levels in
-    one pass (FASTSAR_LEVELS=tc2: in two passes through a float16 intermediate; fp32: on the float32 kernel)."""
+    two passes through a float16 intermediate (FASTSAR_LEVELS=tc1: in one pass; fp32: on the float32 kernel)."""
     if precision == 'float16':
         lv = os.environ.get('FASTSAR_LEVELS', 'tc').strip().lower() or 'tc'
         if lv not in ('tc', 'tc1', 'tc2', 'fp32'):
@@ -302,8 +302,9 @@ class ImageFormer:
     mixed-precision form: the levels and the final stage on the tensor cores (split bfloat16 products, a float16
     intermediate, float16 final operands, float32 accumulation) with 80 dB filters, whose smaller error leaves room
     for the reduced-precision arithmetic. Unlike the reference's precision='float16' (float16 storage on its own
-    plan), this changes the plan: 80 dB filters instead of 70 dB (unless atten is given) and T = 32 always (the
-    tensor-core final stage's tile; a warning when its predicted error misses target_db). atten (an extension of this package) sets the filters' stop band in dB.
+    plan), this changes the plan's filters: 80 dB instead of 70 dB (unless atten is given); T is chosen as for
+    'float32' (choose_T: 32 where its predicted error meets target_db, else 16; the tensor-core final stage takes
+    both). atten (an extension of this package) sets the filters' stop band in dB.
     taps (an extension too): 'kaiser' (default, the reference's Kaiser-sinc decimators), 'learned' (the packaged
     learned decimation taps, fastsar_b200.learned: 8-output-sample filters where the network covers a level's
     decimation and pass fraction, Kaiser-sinc ones elsewhere) or a LearnedTaps instance."""
@@ -343,21 +344,13 @@ class ImageFormer:
         self.predicted_error_db = None
         fmax = float(fmin) + self.K * float(df)
         if T == 'auto':
-            if precision == 'float16':
-                T, err = 32, _plan.final_phase_error(self.ant, fmax, nx, ny, spx, spy, e1, e2, 32)
-                if err > target_db:
-                    warnings.warn(f'cuda float16 needs T=32, predicted error {err:.1f} dB misses target {target_db:.1f} dB; '
-                                  "use precision='float32' for this geometry")
-            else:
-                T, err = _plan.choose_T(self.ant, fmax, nx, ny, spx, spy, e1, e2, target_db)
-                if err > target_db:
-                    warnings.warn(f'predicted error {err:.1f} dB at T={T} misses target {target_db:.1f} dB '
-                                  '(short range for this pixel size)')
+            T, err = _plan.choose_T(self.ant, fmax, nx, ny, spx, spy, e1, e2, target_db)
+            if err > target_db:
+                warnings.warn(f'predicted error {err:.1f} dB at T={T} misses target {target_db:.1f} dB '
+                              '(short range for this pixel size)')
             self.predicted_error_db = float(err)
         if T not in (16, 32):
             raise ValueError(f'the final stage supports T=16 or T=32, not {T}')
-        if precision == 'float16' and T != 32:
-            raise ValueError('cuda float16 uses the tensor-core final stage, which is built for T=32')
         self.T = T
         if ref is not None and np.shape(ref) != (self.P,):
             raise ValueError(f'ref must hold one range per pulse ({self.P}), got shape {np.shape(ref)}')

@@ -9,10 +9,11 @@
 // One MMA is M = 128, N = 128, K = 16, and a "unit" is what one accumulator holds:
 //   FFBP_FINAL_TC_BF16X3  one tile, operands split x = hi + lo in bfloat16: A' = [A_hi; A_lo], B' = [B_hi; B_lo], so
 //                         one product gives hi hi, hi lo, lo hi and lo lo of the tile, summed in the epilogue;
-//   FFBP_FINAL_TC_F16     two tiles in float16, A' = [A_1; A_2], B' = [B_1; B_2]: the two diagonal 64 x 64 blocks
-//                         of the product are the tiles. The samples are scaled by a power of two (from the largest
-//                         sample component, which the last level kernel records) into float16's range, and the
-//                         pixels by its inverse.
+//   FFBP_FINAL_TC_F16     two T = 32 tiles in float16, A' = [A_1; A_2], B' = [B_1; B_2]: the two diagonal 64 x 64
+//                         blocks of the product are the tiles; or four T = 16 tiles, whose 32 x 32 diagonal blocks
+//                         are, each epilogue warp reading one of them from its own lane quarter. The samples are
+//                         scaled by a power of two (from the largest sample component, which the last level kernel
+//                         records) into float16's range, and the pixels by its inverse.
 // The per-instruction issue cost of tcgen05.mma is the same for a 64 x 64 and a 128 x 128 product, so the larger
 // shape does two or four times the work per instruction; two issuing warps double the rate again.
 //
@@ -42,7 +43,6 @@ namespace ffbp {
 
 namespace {
 
-constexpr int TT = 32;                     // tile side
 constexpr int NEPI = 4;                    // epilogue warps 0..3 (TMEM lane quarters 0..3)
 constexpr int NISS = 2;                    // MMA issuing warps 4, 5
 constexpr int NLD = 1;                     // loader warp 6
@@ -218,19 +218,21 @@ __device__ __forceinline__ uint4 flip_sign(uint4 v)
     return make_uint4(v.x ^ sg, v.y ^ sg, v.z ^ sg, v.w ^ sg);
 }
 
-// The tile of slot ts (0, or 1 for the second float16 tile) of this block's local unit ul (>= B when none).
-template <bool BF>
+// The tile of slot ts (float16: 128 / (2 TT) tiles per unit, split bfloat16: one) of this block's local unit ul
+// (>= B when none).
+template <bool BF, int TT>
 __device__ __forceinline__ int unit_tile(int ul, int ts)
 {
     const int u = (int)blockIdx.x + ul * (int)gridDim.x;
-    return BF ? u : 2 * u + ts;
+    return BF ? u : (64 / TT) * u + ts;
 }
 
-// The pixels of one tile from P0 = D'[0:32, :] and P1 = D'[32:64, :] (rows of 64 + 1 floats in shared memory):
-// thread t of the 128 epilogue threads takes row i = t / 4 and eight consecutive columns.
+// The pixels of one T = 32 tile from P0 = D'[0:32, :] and P1 = D'[32:64, :] (rows of 64 + 1 floats in shared
+// memory): thread t of the 128 epilogue threads takes row i = t / 4 and eight consecutive columns.
 __device__ __forceinline__ void tile_pixels(const TcArgs &a, int tile, const float *P0, const float *P1, int t,
                                             float scale)
 {
+    constexpr int TT = 32;
     const int i = t >> 2, jb = (t & 3) * 8;
     const double cx = a.ucx[tile], cy = a.ucy[tile];
     const float f = (float)(a.fc2 / (2.0 * a.rc[tile]));
@@ -264,18 +266,57 @@ __device__ __forceinline__ void tile_pixels(const TcArgs &a, int tile, const flo
     }
 }
 
-template <bool BF, bool WEIGHTED, int MAXWI>
+// The pixels of one T = 16 tile: lane l < 16 of the warp holds accumulator row l (Ar row i = l) at the tile's 32
+// columns (Br then Bi: v0 = D[i][j], v1 = D[i][j + 16]), lane l + 16 row Ai (v0 = D[i + 16][j], v1 = D[i + 16][j + 16]);
+// re = D[i][j] - D[i + 16][j + 16], im = D[i][j + 16] + D[i + 16][j]. Lanes 0..15 write row i's 16 pixels.
+__device__ __forceinline__ void tile16_pixels(const TcArgs &a, int tile, const float *v0, const float *v1, int lane,
+                                              float scale)
+{
+    constexpr int TT = 16;
+    float re[16], im[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const float d11 = __shfl_down_sync(0xffffffffu, v1[j], 16), d10 = __shfl_down_sync(0xffffffffu, v0[j], 16);
+        re[j] = v0[j] - d11;
+        im[j] = v1[j] + d10;
+    }
+    if (lane >= 16 || tile >= a.B) return;
+    const int i = lane;
+    const double cx = a.ucx[tile], cy = a.ucy[tile];
+    const float f = (float)(a.fc2 / (2.0 * a.rc[tile]));
+    const float dx = ((float)i - 0.5f * (TT - 1)) * (float)a.spx;
+    const int2 f0 = a.img ? a.first[tile] : make_int2(0, 0);
+    const int x = f0.x + i - a.ox;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const float dy = ((float)j - 0.5f * (TT - 1)) * (float)a.spy;
+        const float los = (float)cx * dx + (float)cy * dy;
+        const float qc = (dx * dx + dy * dy - los * los) * f;
+        const float2 o = cmul(make_float2(re[j], im[j]), cis_cycles(qc));
+        const float2 ov = make_float2(o.x * scale, o.y * scale);
+        if (a.img) {
+            const int y = f0.y + j - a.oy;
+            if (x >= 0 && x < a.nx && y >= 0 && y < a.ny) a.img[(size_t)x * a.ny + y] = ov;
+        } else {
+            a.tiles[((size_t)tile * TT + i) * TT + j] = ov;
+        }
+    }
+}
+
+template <bool BF, bool WEIGHTED, int MAXWI, int TT>
 __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
 {
+    constexpr int NTS = BF ? 1 : 64 / TT;                       // tiles per unit
     extern __shared__ __align__(1024) unsigned char smem[];
     const int ng = a.Qfp / 8;                                   // core matrices along K per operand
     const uint32_t H = 64u * a.Qfp * 2u;                        // 64 operand rows
+    const uint32_t HS = 2u * TT * a.Qfp * 2u;                   // one tile's operand rows (float16), 2 TT rows
     const uint32_t stagebytes = 4u * H;                         // A' (128 rows), B' (128 rows)
     float *sP = reinterpret_cast<float *>(smem + (size_t)a.S * stagebytes);             // [2][32][65]
     // the loader's ring: per slot and tile slot, the subaperture's Qfp samples (zero past Qf), ux, uy and the
     // three weights (tsb bytes)
     unsigned char *ring = reinterpret_cast<unsigned char *>(sP + 2 * 32 * 65);
-    const uint32_t tsb = 8u * a.Qfp + 32u, slotbytes = (BF ? 1u : 2u) * tsb;
+    const uint32_t tsb = 8u * a.Qfp + 32u, slotbytes = (uint32_t)NTS * tsb;
     uint64_t *bars = reinterpret_cast<uint64_t *>(ring + (size_t)LS * slotbytes);
     uint64_t *full = bars, *empty = bars + a.S, *accf = bars + 2 * a.S, *acce = accf + 2, *drain = acce + 2;
     uint64_t *lfull = drain + 2, *lempty = lfull + LS;
@@ -322,13 +363,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
         // Qfp samples (8 bytes each, zero past Qf and for a tile past the last), ux, uy and the weights, by cp.async
         // into ring slot it % LS; the copies' completion arrives on lfull (each thread's, .noinc), the producers'
         // reads of the slot on lempty. The next unit's samples and geometry are prefetched into L2 a unit ahead.
-        const int nts = BF ? 1 : 2;
+        const int nts = NTS;
         const int ntot = nul * a.Pf;
         const size_t nbp = (size_t)a.B * a.Pf;
         auto prefetch_unit = [&](int ul) {
             if (ul >= nul) return;
             for (int ts = 0; ts < nts; ++ts) {
-                const int tile = unit_tile<BF>(ul, ts);
+                const int tile = unit_tile<BF, TT>(ul, ts);
                 if (tile >= a.B) break;
                 const char *dbeg = reinterpret_cast<const char *>(a.d + (size_t)tile * a.Pf * a.Qf);
                 const int dbytes = a.Pf * a.Qf * (int)sizeof(float2);
@@ -348,7 +389,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
             if (p == 0) prefetch_unit(ul + 1);
             const uint32_t sl = smem_u32(ring) + (uint32_t)ls * slotbytes;
             for (int ts = 0; ts < nts; ++ts) {
-                const int tile = unit_tile<BF>(ul, ts);
+                const int tile = unit_tile<BF, TT>(ul, ts);
                 const bool tv = tile < a.B;
                 const size_t bp = tv ? (size_t)tile * a.Pf + p : 0;
                 const float2 *src = a.d + bp * a.Qf;
@@ -374,15 +415,16 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
         // r and 31 - r (d times the ramp and d times its conjugate); a B item writes Br, Bi of row r and, without
         // weights, row 31 - r from row r's words (the same real part, the imaginary part's sign flipped).
         const int pw = warp - PW0;
-        const int hg = (ng + 1) / 2;
-        const int nts = BF ? 1 : 2;
+        constexpr int GPI = 64 / TT;                            // 8-sample groups per item: a lane per row pair
+        const int hg = (ng + GPI - 1) / GPI;
+        const int nts = NTS;
         const int nwi = nts * 2 * hg;
         const int ntot = nul * a.Pf;
-        const int r = lane & 15, sub = lane >> 4;
-        // byte offsets (without the group) of rows r, r + 32, 31 - r, 63 - r within a 64-row half operand
+        const int r = lane % (TT / 2), sub = lane / (TT / 2);
+        // byte offsets (without the group) of rows r, r + TT, TT - 1 - r, 2 TT - 1 - r within a tile's 2 TT rows
         uint32_t roff[4];
         {
-            const int rows[4] = {r, r + 32, 31 - r, 63 - r};
+            const int rows[4] = {r, r + TT, TT - 1 - r, 2 * TT - 1 - r};
 #pragma unroll
             for (int k = 0; k < 4; ++k) roff[k] = (uint32_t)(((rows[k] >> 3) * ng) * 128 + (rows[k] & 7) * 16);
         }
@@ -426,13 +468,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
             for (int k = 0; k < MAXWI; ++k) {
                 if (it_ts[k] < 0) break;
                 const int ts = it_ts[k], op = it_op[k];
-                const int g = 2 * it_gp[k] + sub;
+                const int g = GPI * it_gp[k] + sub;
                 if (g >= ng) continue;
                 const unsigned char *tsp = slotb + (uint32_t)ts * tsb;
                 const float *gw = reinterpret_cast<const float *>(tsp + 8 * a.Qfp + 16);   // the weights
                 const bool isA = op == 0;
                 const double u = *reinterpret_cast<const double *>(tsp + 8 * a.Qfp + (isA ? 0 : 8));
-                const float dlf = ((float)r - 0.5f * (TT - 1)) * (isA ? sp32x : sp32y);      // r < 16: dl < 0
+                const float dlf = ((float)r - 0.5f * (TT - 1)) * (isA ? sp32x : sp32y);      // r < TT / 2: dl < 0
                 const double dl = ((double)r - 0.5 * (TT - 1)) * (isA ? a.spx : a.spy);
                 const double ud = -(u * dl);
                 float2 wv = cis_cycles_d(ud * fma(a.a1, 8.0 * g, a.a0));
@@ -444,7 +486,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
                     else { w1 = 1.f + gw[2] * dlf; w2 = 1.f - gw[2] * dlf; }
                 }
                 // operand base: A' or B'; half: bfloat16 hi (lo one half further), float16 the tile slot's; group g
-                unsigned char *ob = sbase + (isA ? 0u : 2u * H) + (BF ? 0u : (uint32_t)ts * H) + (uint32_t)g * 128u;
+                unsigned char *ob = sbase + (isA ? 0u : 2u * H) + (BF ? 0u : (uint32_t)ts * HS) + (uint32_t)g * 128u;
                 float r1[8], i1[8], r2[8], i2[8];
                 if (isA) {
                     const float4 *dq = reinterpret_cast<const float4 *>(tsp + 64 * g);
@@ -604,8 +646,20 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
                     if (lane == 0) mbar_arrive(&acce[ab]);
                 }
                 asm volatile("bar.sync 1, 128;" ::: "memory");
-                if (live) tile_pixels(a, unit_tile<BF>(ul, 0), P0, P1, t, oscale);
+                if (live) tile_pixels(a, unit_tile<BF, TT>(ul, 0), P0, P1, t, oscale);
                 asm volatile("bar.sync 1, 128;" ::: "memory");
+            } else if (TT == 16) {
+                // tile slot ts = warp: accumulator rows [32 ts, 32 ts + 32) (this warp's lane quarter) at columns
+                // [32 ts, 32 ts + 32)
+                if (live) {
+                    float v0[16], v1[16];
+                    gather(32 * warp, 0, v0);
+                    gather(32 * warp + 16, 0, v1);
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&acce[ab]);
+                    tile16_pixels(a, unit_tile<BF, TT>(ul, warp), v0, v1, lane, oscale);
+                }
             } else {
                 // tile slot ts: accumulator rows and columns [64 ts, 64 ts + 64), read by warps 2 ts and 2 ts + 1
                 for (int ts = 0; ts < 2; ++ts) {
@@ -622,7 +676,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
                         if (lane == 0) mbar_arrive(&acce[ab]);
                     }
                     asm volatile("bar.sync 1, 128;" ::: "memory");
-                    const int tile = unit_tile<BF>(ul, ts);
+                    const int tile = unit_tile<BF, TT>(ul, ts);
                     if (live && tile < a.B) tile_pixels(a, tile, P0, P1, t, oscale);
                     asm volatile("bar.sync 1, 128;" ::: "memory");
                 }
@@ -651,13 +705,17 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
 cudaError_t launch_final_tc(const FinalLaunch &F, int mode, cudaStream_t s, const char **why)
 {
     *why = nullptr;
-    if (F.T != 32) { *why = "the tensor-core final stage is built for T = 32"; return cudaErrorNotSupported; }
+    const bool bf = mode == 2;
+    if (F.T != 32 && (F.T != 16 || bf)) {
+        *why = "the tensor-core final stage takes T = 32 (split bfloat16 or float16) or T = 16 (float16)";
+        return cudaErrorNotSupported;
+    }
     if (F.B <= 0) return cudaSuccess;
     if ((long long)F.B * F.Pf >= (1LL << 31)) { *why = "more than 2^31 final tile subapertures"; return cudaErrorNotSupported; }
-    const bool bf = mode == 2;
+    const int nts = bf ? 1 : 64 / F.T;                          // tiles per unit
     TcArgs a;
     a.d = F.d; a.B = F.B; a.Pf = F.Pf; a.Qf = F.Qf; a.Qfp = (F.Qf + 15) & ~15;
-    a.nunits = bf ? F.B : (F.B + 1) / 2;
+    a.nunits = (F.B + nts - 1) / nts;
     a.nis = F.Pf >= NISS ? NISS : 1;
     a.ux = F.ux; a.uy = F.uy; a.spx = F.spx; a.spy = F.spy; a.a0 = F.a0; a.a1 = F.a1; a.fc2 = F.fc2;
     a.ucx = F.ucx; a.ucy = F.ucy; a.rc = F.rc; a.w = F.w; a.tiles = F.tiles; a.img = F.img; a.first = F.first;
@@ -670,14 +728,14 @@ cudaError_t launch_final_tc(const FinalLaunch &F, int mode, cudaStream_t s, cons
     // warp items per stage: (tile slots) x (A, B) x (pairs of 8-sample groups) over the NPW producer warps; when
     // every warp gets the same even number of items they are interleaved (as many A items, the heavier, as B
     // items on each warp: 3 % faster at 47 x 91 in float16; 1 % slower at 38 x 71, whose count is uneven)
-    const int ng = a.Qfp / 8, hg = (ng + 1) / 2;
-    const int nwi = (bf ? 1 : 2) * 2 * hg;
+    const int ng = a.Qfp / 8, gpi = 64 / F.T, hg = (ng + gpi - 1) / gpi;
+    const int nwi = nts * 2 * hg;
     a.interleave = nwi % (2 * NPW) == 0 ? 1 : 0;
     const int maxwi = (nwi + NPW - 1) / NPW;
     if (maxwi > 4) { *why = "more than 256 frequency samples per final tile"; return cudaErrorNotSupported; }
     const int mw = maxwi <= 1 ? 1 : (maxwi <= 2 ? 2 : 4);
     const size_t stage = (size_t)4 * 64 * a.Qfp * 2;
-    const size_t slotbytes = (size_t)(bf ? 1 : 2) * (8 * a.Qfp + 32);
+    const size_t slotbytes = (size_t)nts * (8 * a.Qfp + 32);
     const size_t fixed = (size_t)2 * 32 * 65 * 4 + (size_t)LS * slotbytes + (size_t)(2 * 4 + 6 + 2 * LS) * 8;
     const size_t avail = (size_t)maxsmem - 1024;                // static shared memory and slack
     // stages: a multiple of the issuers (each owns S / nis of them)
@@ -696,9 +754,10 @@ cudaError_t launch_final_tc(const FinalLaunch &F, int mode, cudaStream_t s, cons
         kern<<<grid, NTHREADS, smem, s>>>(a);
         return cudaGetLastError();
     };
-#define FFBP_TC_RUN(MW)                                                                                    \
-    (bf ? (a.w ? run(final_tc_kernel<true, true, MW>) : run(final_tc_kernel<true, false, MW>))             \
-        : (a.w ? run(final_tc_kernel<false, true, MW>) : run(final_tc_kernel<false, false, MW>)))
+#define FFBP_TC_RUN(MW)                                                                                       \
+    (bf ? (a.w ? run(final_tc_kernel<true, true, MW, 32>) : run(final_tc_kernel<true, false, MW, 32>))        \
+        : F.T == 16 ? (a.w ? run(final_tc_kernel<false, true, MW, 16>) : run(final_tc_kernel<false, false, MW, 16>)) \
+                    : (a.w ? run(final_tc_kernel<false, true, MW, 32>) : run(final_tc_kernel<false, false, MW, 32>)))
     cudaError_t e;
     if (mw == 1) e = FFBP_TC_RUN(1);
     else if (mw == 2) e = FFBP_TC_RUN(2);

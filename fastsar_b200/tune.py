@@ -11,7 +11,7 @@ import numpy as np
 
 from . import plan as _plan
 
-CHOSEN = [dict(precision='float16', taps='learned', pmax=0.5, T=32, levels=lv) for lv in (2, 3, 4)]
+CHOSEN = [dict(precision='float16', taps='learned', pmax=0.5, T=t, levels=lv) for t in (16, 32) for lv in (2, 3, 4)]
 FLOAT32 = [dict(precision='float32', taps='learned', T=t, levels=lv) for t in (16, 32) for lv in (2, 3, 4)]
 
 

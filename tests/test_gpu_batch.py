@@ -1,5 +1,5 @@
 """BatchFormer on a B200: patches of uneven sizes from two collections (the 512-pulse spotlight and the reference's
-small CPU test case), float32 and the tensor-core form, captured into one CUDA graph (ffbp_batch_create) and formed
+small CPU test case), float32 and the tensor-core form (T = 32 and 16), captured into one CUDA graph (ffbp_batch_create) and formed
 by one launch, give bit for bit the images each former forms alone; a non-finite sample is reported with its
 history's index; a range-gated former is refused."""
 import numpy as np
@@ -26,11 +26,12 @@ def _patches(golden):
                                      ((-10.0, -20.0), (160, 160), 'float16')]:
         c = np.array([cy, cx, 0.0])
         f = ImageFormer(col.ant - c, col.fmin, col.df, col.K, nx, ny, 0.25, 0.25, w['e1'], w['e2'], ref=r0,
-                        precision=prec, T=32 if prec == 'float16' else 'auto')
+                        precision=prec)
         out.append((f, g['S']))
     s = golden('image_small')
     fmin, df, K = s['scal']
     out.append((ImageFormer(s['ant'], fmin, df, int(K), 128, 128, 0.5, 0.5, T=16, levels=3), s['S']))
+    out.append((ImageFormer(s['ant'], fmin, df, int(K), 128, 128, 0.5, 0.5, T=16, levels=3, precision='float16'), s['S']))
     return out
 
 
@@ -50,11 +51,11 @@ def test_batch_matches_formers_alone(golden):
     with pytest.raises(ValueError, match='phase history 3 .*pulse 11'):
         batch(hs)
     # the spotlight's patches sharing one device history
-    shared = BatchFormer([f for f, _ in pairs], sources=[0, 0, 0, 0, 0, 1])
+    shared = BatchFormer([f for f, _ in pairs], sources=[0, 0, 0, 0, 0, 1, 1])
     got = shared([pairs[0][1], pairs[-1][1]])
     assert all(np.array_equal(a, b) for a, b in zip(got, want))
     with pytest.raises(ValueError, match='differ'):
-        BatchFormer([f for f, _ in pairs], sources=[0, 0, 0, 0, 0, 0])
+        BatchFormer([f for f, _ in pairs], sources=[0, 0, 0, 0, 0, 0, 0])
 
 
 def test_batch_refuses_gated_formers():

@@ -335,17 +335,17 @@ def test_torch_input_matches_numpy(golden):
 
 # ------------------------------------------------------------------------------------------------ tensor-core final
 
-@pytest.mark.parametrize('mode,tol', [(2, 2e-4), (1, 3e-3)], ids=['bf16x3', 'f16'])
+@pytest.mark.parametrize('mode,tol,T', [(2, 2e-4, 32), (1, 3e-3, 32), (1, 3e-3, 16)], ids=['bf16x3', 'f16', 'f16-t16'])
 @pytest.mark.parametrize('weighted', [False, True])
 @pytest.mark.parametrize('shape', [(5, 13, 57), (300, 7, 96), (3, 40, 130), (4, 1, 40), (301, 38, 71), (400, 59, 113)],
                          ids=['small', 'many-tiles', 'long-q', 'one-subaperture', 'spotlight-12k-final', 'two-stages'])
-def test_final_tensor_cores_match_oracle(lib, oracle_lib, mode, tol, weighted, shape):
-    """The tcgen05 final stage (T = 32) against the float64 oracle: split bfloat16 products within 2e-4, one
-    float16 product within 3e-3 (its operands carry 11 bits); units beyond one per multiprocessor, an odd tile count
-    (the float16 form pairs tiles), one final subaperture (one MMA issuer), padding of Qf to a multiple of 16,
-    aperture weights, the chosen form's final stage shape at the 12,288 x 8,832 spotlight (Pf 38, Qf 71), and a shape whose
-    operands leave room for two pipeline stages only, with an odd subaperture count and several units per block."""
-    T = 32
+def test_final_tensor_cores_match_oracle(lib, oracle_lib, mode, tol, T, weighted, shape):
+    """The tcgen05 final stage against the float64 oracle: split bfloat16 products within 2e-4, one float16 product
+    within 3e-3 (its operands carry 11 bits), T = 32 and (float16) T = 16; units beyond one per multiprocessor, tile
+    counts that leave a float16 unit part-filled (two T = 32 or four T = 16 tiles a unit), one final subaperture (one
+    MMA issuer), padding of Qf to a multiple of 16, aperture weights, the chosen form's final stage shape at the
+    12,288 x 8,832 spotlight (Pf 38, Qf 71), and a shape whose operands leave room for two pipeline stages only, with
+    an odd subaperture count and several units per block."""
     rng = np.random.default_rng(7 * mode + weighted + shape[0])
     B, Pf, Qf = shape
     d = (rng.standard_normal((B, Pf, Qf)) + 1j * rng.standard_normal((B, Pf, Qf))).astype(np.complex64)
@@ -393,21 +393,23 @@ def test_image_tensor_cores_match_reference(golden, oracle_lib, monkeypatch):
     assert e < -70.0
 
 
-def test_image_mixed_precision_against_float64(golden, oracle_lib):
-    """precision='float16' (tensor-core levels and final stage, 80 dB filters) on the 512-pulse spotlight: its error
-    against the float64 exact backprojection (64x) is below -60 dB and no worse than the reference former's own
-    (its 70 dB filters put it -66.8 dB from the float64 image); against the reference former's image the two
-    formers' filter errors add."""
+@pytest.mark.parametrize('T', ['auto', 16])
+def test_image_mixed_precision_against_float64(golden, oracle_lib, T):
+    """precision='float16' (tensor-core levels and final stage, 80 dB filters) on the 512-pulse spotlight, with the
+    chosen tile size (32 here) and with T = 16 (four tiles per tensor-core unit): its error against the float64 exact
+    backprojection (64x) is below -60 dB and no worse than the reference former's own (its 70 dB filters put it
+    -66.8 dB from the float64 image); against the reference former's image the two formers' filter errors add."""
     from fastsar_b200 import ImageFormer, sim
     g = golden('image_spot512')
     w = sim.workload('spotlight_512')
     col = w['col']
-    f = ImageFormer(col.ant, col.fmin, col.df, col.K, 512, 512, 0.25, 0.25, w['e1'], w['e2'], precision='float16')
+    f = ImageFormer(col.ant, col.fmin, col.df, col.K, 512, 512, 0.25, 0.25, w['e1'], w['e2'], precision='float16', T=T)
+    assert f.T == (32 if T == 'auto' else T)
     img = f(g['S'])
     e = oracle_lib.err_db(img, g['ffbp'])
     e64 = oracle_lib.rel_db(img.ravel()[g['bp64_idx']], g['bp64'])
     eref = oracle_lib.rel_db(g['ffbp'].ravel()[g['bp64_idx']], g['bp64'])
-    print(f'float16: {e64:.1f} dB vs float64 BP 64x (reference former {eref:.1f} dB); {e:.1f} dB vs reference former')
+    print(f'float16 T={f.T}: {e64:.1f} dB vs float64 BP 64x (reference former {eref:.1f} dB); {e:.1f} dB vs reference former')
     assert e64 < -60.0
     assert e64 < eref + 0.5
     assert e < -50.0
