@@ -265,7 +265,10 @@ def main():
     # plain float32 FFBP (the reference's arithmetic and filters)
     mk = lambda prec, **kw: ImageFormer(col.ant, col.fmin, col.df, col.K, w['nx'], w['ny'], w['spx'], w['spy'],
                                         w['e1'], w['e2'], precision=prec, **kw)
-    chosen = mk('float16', taps='learned', pmax=CHOSEN_PMAX)
+    # the tensor-core levels' launch options are timed per level shape when the former is built (before any timing)
+    t1 = time.time()
+    chosen = mk('float16', taps='learned', pmax=CHOSEN_PMAX, tune_levels=True)
+    log(f'[bench] chosen form built, level launch options tuned in {time.time() - t1:.1f} s: {chosen.level_opts}')
     plain = mk('float32')
     plan = chosen._plan
     npix, P = w['nx'] * w['ny'], col.Np
@@ -399,7 +402,8 @@ def main():
         data=f'synthetic: {w["n_scatterers"]} seeded scatterers simulated on the GPU in float64, noise -40 dB',
         config=bench_config(args, w, world),
         form_plan=dict(T=chosen.T, taps=[(l['kind_k'], l['kind_p']) for l in plan['levels']],
-                       atten_db_fallback=chosen.atten, levels=[(l['C'], l['Dk'], l['Dp']) for l in plan['levels']]),
+                       atten_db_fallback=chosen.atten, levels=[(l['C'], l['Dk'], l['Dp']) for l in plan['levels']],
+                       level_launch_options=chosen.level_opts),
         parity=parity,
         err_db=dict(chosen=err_chosen, plain=err_plain, reference='float64 exact backprojection, 64x, linear, '
                     f'{len(idx)} random pixels, one complex gain fitted', no_gain_fitted=err_nofit),
@@ -604,7 +608,7 @@ def run_stack(args):
         del f
         torch.cuda.empty_cache()
     del out
-    chosen = [mk(col, precision='float16', taps='learned', pmax=0.5) for col in passes]
+    chosen = [mk(col, precision='float16', taps='learned', pmax=0.5, tune_levels=True) for col in passes]
     # one graph over all passes; where the device cannot hold every pass's buffers at once, graphs of fewer
     group = len(chosen)
     while True:
@@ -693,9 +697,9 @@ def run_learned(args):
             f = ImageFormer(col.ant, col.fmin, col.df, col.K, nx, ny, w['spx'], w['spy'], w['e1'], w['e2'],
                             taps=taps, atten=atten, pmax=pmax)
             f.form_device(S, out)
-        except ValueError as e:
+        except (ValueError, RuntimeError) as e:
             # a plan the float32 former cannot form (the level kernel's limits: 256 frequency taps, a pulse filter
-            # spanning 16 output pulses)
+            # spanning 16 output pulses) or whose workspace does not fit the device
             rows.append(dict(taps=taps, atten=atten, pmax=pmax, oversampling=round(1.0 / pmax, 2), error=str(e)[:100]))
             log(f'[bench] {taps} {atten:.0f} dB pmax {pmax}: not formed: {str(e)[:100]}')
             continue

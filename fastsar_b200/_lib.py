@@ -24,9 +24,14 @@ EXPORTS = ('ffbp_last_error', 'ffbp_abi_version', 'ffbp_plan_create', 'ffbp_plan
            'ffbp_form_profile', 'ffbp_exact_pad', 'ffbp_exact_backproject', 'ffbp_mlp_param_count',
            'ffbp_mlp_max_decimation', 'ffbp_mlp_work_bytes', 'ffbp_plan_host_bytes', 'ffbp_form_host', 'ffbp_gate_pad',
            'ffbp_gate_fold', 'ffbp_gate_taper', 'ffbp_batch_create', 'ffbp_batch_form', 'ffbp_batch_destroy', 'ffbp_mlp_taps', 'ffbp_mlp_grad', 'ffbp_mlp_train_step',
-           'ffbp_plan_check', 'ffbp_plan_test_wait', 'ffbp_level_fused')
+           'ffbp_plan_check', 'ffbp_plan_test_wait', 'ffbp_level_fused', 'ffbp_level_tc_ex')
 
 _c_int, _c_double, _vp = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+
+
+class TcOpts(ctypes.Structure):
+    """ffbp_tc_opts: launch options of a tensor-core level's first pass (0 keeps a field's default)."""
+    _fields_ = [('nt', _c_int), ('sb', _c_int), ('copies', _c_int), ('repeat', _c_int)]
 
 
 class LevelDesc(ctypes.Structure):
@@ -35,7 +40,7 @@ class LevelDesc(ctypes.Structure):
                 ('h_taps_k', _vp), ('Lk', _c_int), ('plk', _c_int),
                 ('h_taps_p', _vp), ('Lp', _c_int), ('plp', _c_int),
                 ('f0', _c_double), ('df', _c_double),
-                ('h_ant', _vp), ('h_ref', _vp), ('h_cen', _vp), ('h_range', _vp)]
+                ('h_ant', _vp), ('h_ref', _vp), ('h_cen', _vp), ('h_range', _vp), ('tc', TcOpts)]
 
 
 class PlanDesc(ctypes.Structure):
@@ -92,6 +97,7 @@ def load():
     L.ffbp_level_tc.argtypes = [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_int,
                                 _c_double, _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t,
                                 _vp, _vp]
+    L.ffbp_level_tc_ex.argtypes = L.ffbp_level_tc.argtypes[:-1] + [ctypes.POINTER(TcOpts), _vp]
     L.ffbp_level_tc_scratch_bytes.argtypes = [_c_int, _c_int, _c_int, _c_int]
     L.ffbp_level_fused.argtypes = [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_int,
                                    _c_double, _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp, _vp]

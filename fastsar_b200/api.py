@@ -151,6 +151,8 @@ class DevicePlan:
             d.h_ant, d.h_ref, d.h_cen = k64(lv['ant']), k64(lv['ref']), k64(lv['cen'])
             if i == 0 and ref is not None:
                 d.h_range = k64(ref)
+            tc = lv.get('tc') or {}
+            d.tc.nt, d.tc.sb, d.tc.copies, d.tc.repeat = (int(tc.get(k, 0)) for k in ('nt', 'sb', 'copies', 'repeat'))
         fin = plan['final']
         pd = _lib.PlanDesc()
         pd.nlev, pd.levels = len(plan['levels']), ctypes.cast(lvs, ctypes.POINTER(_lib.LevelDesc))
@@ -307,11 +309,15 @@ class ImageFormer:
     both). atten (an extension of this package) sets the filters' stop band in dB.
     taps (an extension too): 'kaiser' (default, the reference's Kaiser-sinc decimators), 'learned' (the packaged
     learned decimation taps, fastsar_b200.learned: 8-output-sample filters where the network covers a level's
-    decimation and pass fraction, Kaiser-sinc ones elsewhere) or a LearnedTaps instance."""
+    decimation and pass fraction, Kaiser-sinc ones elsewhere) or a LearnedTaps instance. tune_levels (an extension):
+    with precision='float16', time the tensor-core levels' launch options (columns per tile, operand stages, plane
+    copies, row repeat) per level shape on the GPU when the former is built (fastsar_b200.tune.tune_levels; cached
+    per shape in the process); the choice changes the image at the rounding level only (about 1e-5 relative: a
+    float16 rounding of the intermediate flipped here and there)."""
 
     def __init__(self, ant, fmin, df, K, nx, ny, spx, spy, e1=(1.0, 0.0, 0.0), e2=(0.0, 1.0, 0.0), *, backend='auto',
                  precision='float32', window=True, T='auto', levels=None, pmax=0.4, target_db=-40.0, aperture_weight=None,
-                 ref=None, range_gate='auto', padded=None, atten=None, taps='kaiser'):
+                 ref=None, range_gate='auto', padded=None, atten=None, taps='kaiser', tune_levels=False):
         self.ant = _check_positions(ant)
         self.P, self.K = self.ant.shape[0], int(K)
         if self.K < 2:
@@ -413,9 +419,15 @@ class ImageFormer:
         wp = wk = None
         if window:
             self.wp, self.wk = wp, wk = _window(self.P, self.K)
+        mode = _final_mode(precision)
+        # the tensor-core levels' launch options, timed per level shape (fastsar_b200.tune.tune_levels; cached)
+        self.level_opts = None
+        if tune_levels and mode & _lib.FFBP_LEVELS_TC and mode & _lib.FFBP_LEVELS_TC2:
+            from . import tune as _tune
+            self.level_opts = _tune.tune_levels(plan)
         # a gated history is windowed in the gate, before its transforms; the former then takes it as it is
         self._dev = DevicePlan(plan, None if self.range_gate else wp, None if self.range_gate else wk, wf,
-                               None if ref is None else np.asarray(ref, np.float64), _final_mode(precision))
+                               None if ref is None else np.asarray(ref, np.float64), mode)
         self._S = None
         self._img = None
         self._gate_dev = None

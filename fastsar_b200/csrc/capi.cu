@@ -43,6 +43,7 @@ int cuda_fail(cudaError_t e, const char *what)
 
 struct DevLevel {
     int C, Dk, Dp, K, P, Ko, Po, Lk, plk, Lp, plp, Np;
+    ffbp_tc_opts tc{};
     float *tk = nullptr, *tp = nullptr;
     float2 *phase = nullptr;
     double kc;
@@ -203,6 +204,7 @@ int ffbp_plan_create(const ffbp_plan_desc *d, void *stream_, ffbp_plan **out)
         v.Lp = L.Dp > 1 ? L.Lp : 1; v.plp = L.Dp > 1 ? L.plp : 0;
         v.Np = B;
         v.kc = (L.K - 1) / 2.0;
+        v.tc = L.tc;
         void *q;
         if (L.Dk > 1) {
             if ((e = upload(L.h_taps_k, sizeof(float) * L.Lk, &q, true)) != cudaSuccess) return cleanup(cuda_fail(e, "upload taps"));
@@ -382,6 +384,7 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
         L.Dp = v.Dp; L.Lp = v.Lp; L.plp = v.plp; L.kc = v.kc;
         L.amax = amax + l + 1;
         L.test_wait_ns = p->test_kind == FFBP_KIND_LEVEL_TC ? p->test_ns : 0u;
+        L.tc_nt = v.tc.nt; L.tc_sb = v.tc.sb; L.tc_pc = v.tc.copies; L.tc_rp = v.tc.repeat;
         const char *why = nullptr;
         const int form = level_form(p, l);
         if (form == 1) {
@@ -729,6 +732,15 @@ int ffbp_level_tc(const void *d_x, int Np, int P, int K, const void *d_phase, in
                   const float *d_wk, void *d_out, int *d_bad, void *d_scratch, size_t scratch_bytes, int *d_status,
                   void *stream)
 {
+    return ffbp_level_tc_ex(d_x, Np, P, K, d_phase, C, d_tk, Lk, plk, Dk, Ko, kc, d_tp, Lp, plp, Dp, Po, d_wp, d_wk,
+                            d_out, d_bad, d_scratch, scratch_bytes, d_status, nullptr, stream);
+}
+
+int ffbp_level_tc_ex(const void *d_x, int Np, int P, int K, const void *d_phase, int C, const float *d_tk, int Lk,
+                     int plk, int Dk, int Ko, double kc, const float *d_tp, int Lp, int plp, int Dp, int Po,
+                     const float *d_wp, const float *d_wk, void *d_out, int *d_bad, void *d_scratch,
+                     size_t scratch_bytes, int *d_status, const ffbp_tc_opts *opts, void *stream)
+{
     if (!d_x || !d_phase || !d_out || !d_scratch || !d_status) return fail(FFBP_E_ARG, "ffbp_level_tc: null buffer");
     if (Np < 1 || P < 1 || K < 1 || C < 1 || Dk < 1 || Dp < 1 || Ko < 1 || Po < 1) return fail(FFBP_E_ARG, "ffbp_level_tc: non-positive size");
     if ((Dk > 1 && (!d_tk || Lk < 1)) || (Dp > 1 && (!d_tp || Lp < 1))) return fail(FFBP_E_ARG, "ffbp_level_tc: taps missing");
@@ -740,6 +752,7 @@ int ffbp_level_tc(const void *d_x, int Np, int P, int K, const void *d_phase, in
     L.wp = d_wp; L.wk = d_wk; L.out = static_cast<float2 *>(d_out); L.bad = d_bad;
     L.Np = Np; L.C = C; L.P = P; L.K = K; L.Ko = Ko; L.Po = Po; L.Dk = Dk; L.Lk = Lk; L.plk = plk; L.Dp = Dp;
     L.Lp = Lp; L.plp = plp; L.kc = kc; L.amax = d_status + 2;
+    if (opts) { L.tc_nt = opts->nt; L.tc_sb = opts->sb; L.tc_pc = opts->copies; L.tc_rp = opts->repeat; }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaError_t e = ffbp::launch_amax(L.x, (size_t)Np * P * K, d_status + 1, s);
     if (e != cudaSuccess) return cuda_fail(e, "ffbp_level_tc");

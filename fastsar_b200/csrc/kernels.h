@@ -20,6 +20,9 @@ struct LevelLaunch {
     int *amax = nullptr;  // or the largest |component| of the output, as float bits (atomicMax; start at 0)
     unsigned test_wait_ns = 0;   // tensor-core pass 1 only, for tests of the failure report: when nonzero the MMA
                                  // issuer first waits this long on a barrier nothing completes, as a stuck pipeline
+    // tensor-core pass 1 launch options (0: the default): output columns per tile, B stages, plane copies (2 or 4),
+    // row repeat (1: off)
+    int tc_nt = 0, tc_sb = 0, tc_pc = 0, tc_rp = 0;
 };
 
 // Returns cudaSuccess, or an error with *why set to a static message for shapes the kernels do not cover.

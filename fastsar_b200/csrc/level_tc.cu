@@ -135,6 +135,25 @@ __device__ __forceinline__ void tmem_ld8(uint32_t addr, float *v)
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// 8 consecutive bfloat16 samples from a plane copy: four 4-byte loads (PC = 2) or two 8-byte loads (PC = 4)
+template <int PC>
+__device__ __forceinline__ uint4 ld_run(const uint32_t *s)
+{
+    if constexpr (PC == 4) {
+        const uint2 a = *reinterpret_cast<const uint2 *>(s), b = *reinterpret_cast<const uint2 *>(s + 2);
+        return make_uint4(a.x, a.y, b.x, b.y);
+    } else {
+        return make_uint4(s[0], s[1], s[2], s[3]);
+    }
+}
+
+// 8 bytes global -> shared by cp.async (zero-filled when !valid)
+__device__ __forceinline__ void cp_async8(void *dst, const void *src, bool valid)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;"
+                 :: "r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src), "r"(valid ? 8 : 0) : "memory");
+}
+
 // x = hi + lo with hi = bfloat16(x) and lo = bfloat16(x - hi), two values per 32-bit word (first value low)
 __device__ __forceinline__ void split2(float a, float b, uint32_t &hi, uint32_t &lo)
 {
@@ -172,9 +191,13 @@ struct GemmArgs {
     __half2 *y;                       // [Np, C, P, Kop]
     int *err;
     int Np, C, P, K, Ko, Kop, Dk, Lk, plk, Lkp, Nt, ntile, W, pseg, nseg, SB;
+    int rp;                           // 2: A' rows 64..127 repeat rows 0..63 (more than 32 taps, at most 32 children)
     float kc;
     unsigned test_wait_ns;            // tests only: the MMA issuer's wait on a barrier nothing completes (0: none)
 };
+
+// The plane length in elements of a window of W samples held in PC shifted copies: a multiple of 2 PC, with slack.
+__host__ __device__ constexpr int plane_len(int W, int PC) { return PC == 4 ? (W + 11) & ~3 : (W + 9) & ~1; }
 
 // The power of two that brings values up to 4 amax (the taps' absolute sum is below 4 for the decimators of any
 // plan) below 2^13: the float16 intermediate then stays in range and keeps 11 significant bits.
@@ -188,7 +211,7 @@ __device__ __forceinline__ float y_scale(const int *amax)
     return ldexpf(1.f, 13 - ex);
 }
 
-template <int NKC>
+template <int NKC, int PC>
 __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -197,11 +220,13 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
     const uint32_t bpart = 2u * a.Nt * a.Lkp * 2u;           // one part of B'
     unsigned char *sA = smem;                                // [2 pulses][hi, lo]
     unsigned char *sB = sA + 2 * 2 * apart;                  // [SB stages][hi, lo]
-    const int Wp = (a.W + 9) & ~1;                           // plane length in elements (even, with slack)
-    // planes: [xr hi, xr lo, xi hi, xi lo][even, odd copy][Wp / 2] words; the even copy's word w holds samples
-    // 2w, 2w + 1, the odd copy's 2w + 1, 2w + 2, so that any 8 consecutive samples are 4 aligned words of one copy
+    const int Wp = plane_len(a.W, PC);                       // plane length in elements
+    // planes: [xr hi, xr lo, xi hi, xi lo][copy c < PC][Wp / 2] words; copy c's word w holds samples 2w + c and
+    // 2w + c + 1. With PC = 2 any 8 consecutive samples o .. o + 7 are the 4 aligned words (o - c) / 2 .. + 3 of copy
+    // c = o mod 2; with PC = 4 they are the two 8-byte-aligned word pairs there of copy c = o mod 4 (copies 2 and 3
+    // are copies 0 and 1 a word on): half the shared loads, twice the plane stores and space
     uint32_t *pl = reinterpret_cast<uint32_t *>(sB + (size_t)a.SB * 2 * bpart);   // two stages' planes
-    float *s_tk = reinterpret_cast<float *>(pl + 16 * (Wp / 2));                  // [Lkp]
+    float *s_tk = reinterpret_cast<float *>(pl + 2 * 4 * PC * (Wp / 2));           // [Lkp]
     float2 *s_x = reinterpret_cast<float2 *>(s_tk + a.Lkp);                        // [XS][Wp] staged windows
     uint64_t *bars = reinterpret_cast<uint64_t *>(s_x + (size_t)XS * Wp);
     uint64_t *afull = bars, *aempty = bars + 2, *bfull = bars + 4, *bempty = bfull + a.SB, *dfull = bempty + a.SB,
@@ -210,6 +235,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
     __shared__ volatile int s_abort;
     __shared__ float s_scale;
     __shared__ uint64_t s_never;                             // a barrier nothing arrives on (the tests' stuck wait)
+    __shared__ float2 s_ph[2][64];                           // the children's (c0, sl) of a pulse and the next
 
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int n = blockIdx.x / a.nseg, seg = blockIdx.x % a.nseg;
@@ -258,13 +284,26 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
         // buffer is free once the MMAs of the pulse two back have completed); no named barrier
         const int at = t - NCW * 32;
         const float2 *__restrict__ phn = a.ph + (size_t)n * a.C * a.P;
+        // the children's phases of each pulse are copied into s_ph a pulse ahead (cp.async, thread c: child c), so
+        // that no item waits on a global load; after a failed wait a thread keeps stepping through the pulses (and
+        // the named barrier, which all A' threads must reach) without waiting or working
+        if (at < a.C && npl > 0) cp_async8(&s_ph[0][at], &phn[(size_t)at * a.P + p0], true);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        bool ok = true;
         for (int pl_i = 0; pl_i < npl; ++pl_i) {
             const int ab = pl_i & 1, p = p0 + pl_i;
-            if (!mbar_wait(&aempty[ab], (uint32_t)(((pl_i >> 1) & 1) ^ 1), 1000, &s_abort, a.err)) break;
+            asm volatile("cp.async.wait_all;" ::: "memory");
+            // every thread's phases of pulse p are in, and its reads of the other buffer (pulse p - 1) are done
+            asm volatile("bar.sync 2, %0;" :: "n"(NAT) : "memory");
+            if (at < a.C && pl_i + 1 < npl) cp_async8(&s_ph[(pl_i + 1) & 1][at], &phn[(size_t)at * a.P + p + 1], true);
+            asm volatile("cp.async.commit_group;" ::: "memory");
+            if (ok) ok = mbar_wait(&aempty[ab], (uint32_t)(((pl_i >> 1) & 1) ^ 1), 1000, &s_abort, a.err);
+            if (!ok) continue;
             unsigned char *Ab = sA + ab * 2 * apart;
+            const float2 *sph = s_ph[pl_i & 1];
             for (int item = at; item < a.C * nkc; item += NAT) {
                 const int u = item / a.C, c = item - u * a.C;   // consecutive threads: consecutive children
-                const float sl = __ldg(&phn[(size_t)c * a.P + p]).y;
+                const float sl = sph[c].y;
                 // exp(2 pi i sl r) for r = 8u .. 8u + 7: two independent recurrences (even and odd r)
                 const float2 st = cis_cycles(sl), st2 = cmul(st, st);
                 float2 ze = cis_cycles(sl * (float)(8 * u)), zo = cmul(ze, st);
@@ -293,7 +332,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                 *reinterpret_cast<uint4 *>(Ab + apart + o0) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
                 *reinterpret_cast<uint4 *>(Ab + o1) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
                 *reinterpret_cast<uint4 *>(Ab + apart + o1) = make_uint4(il[0], il[1], il[2], il[3]);
-                if (NKC > 4 && a.C <= 32) {
+                if (NKC > 4 && a.rp == 2) {
                     // at most 32 children: rows 64 .. 127 repeat rows 0 .. 63, so that all four lane quarters of the
                     // accumulator hold children and the consumers split the columns four ways
                     const uint32_t d0 = core_off(row + 64, u, nkc), d1 = core_off(row2 + 64, u, nkc);
@@ -307,6 +346,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             __syncwarp();
             if (lane == 0) mbar_arrive(&afull[ab]);
         }
+        asm volatile("cp.async.wait_all;" ::: "memory");
     } else if (warp >= NCW + NAW && warp < NCW + NAW + NLW) {
         // ------------------------------------------------------------------ B' producers: planes
         const int pt = t - (NCW + NAW) * 32;
@@ -342,10 +382,10 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             asm volatile("bar.sync 1, %0;" :: "n"(NLT) : "memory");
             stage_x(s + XS - 1);
             if (ok) ok = mbar_wait(&pempty[s & 1], (uint32_t)(((s >> 1) & 1) ^ 1), 1000, &s_abort, a.err);
-            // the window's planes: xr hi, xr lo, xi hi, xi lo as bfloat16 pairs (word i = samples 2i, 2i + 1), into
-            // plane buffer s & 1
+            // the window's planes: xr hi, xr lo, xi hi, xi lo as bfloat16 pairs (copy 0's word i = samples 2i,
+            // 2i + 1), into plane buffer s & 1
             if (ok) {
-                uint32_t *plb = pl + (s & 1) * 8 * (Wp / 2);
+                uint32_t *plb = pl + (s & 1) * 4 * PC * (Wp / 2);
                 const float2 *xs = s_x + (size_t)(s % XS) * Wp;
                 const int kb = a.Dk * a.Nt * tt - a.plk;
                 const float wpp = a.wp ? a.wp[p] : 1.f;
@@ -367,15 +407,19 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                     split2(v[0].y, v[1].y, ih, il);
                     split2(v[1].x, v[2].x, orh, orl);
                     split2(v[1].y, v[2].y, oih, oil);
+                    // copies 0, 1 at word i; copies 2, 3 (the same words) at word i - 1
                     const int hw = Wp / 2;
-                    plb[i] = rh;
-                    plb[hw + i] = orh;
-                    plb[2 * hw + i] = rl;
-                    plb[3 * hw + i] = orl;
-                    plb[4 * hw + i] = ih;
-                    plb[5 * hw + i] = oih;
-                    plb[6 * hw + i] = il;
-                    plb[7 * hw + i] = oil;
+                    const uint32_t w4[4][2] = {{rh, orh}, {rl, orl}, {ih, oih}, {il, oil}};
+#pragma unroll
+                    for (int pq = 0; pq < 4; ++pq) {
+                        uint32_t *q = plb + PC * pq * hw + i;
+                        q[0] = w4[pq][0];
+                        q[hw] = w4[pq][1];
+                        if (PC == 4 && i > 0) {
+                            q[2 * hw - 1] = w4[pq][0];
+                            q[3 * hw - 1] = w4[pq][1];
+                        }
+                    }
                 }
                 mbar_arrive(&pfull[s & 1]);
             }
@@ -392,7 +436,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             // A warp takes 8 rows (lane % 8) x 4 K chunks (lane / 8) at a time: the 8 rows' 16-byte stores fill one
             // 128-byte core matrix (no bank conflicts)
             unsigned char *Bb = sB + sb * 2 * bpart;
-            const uint32_t *plb = pl + (s & 1) * 8 * (Wp / 2);
+            const uint32_t *plb = pl + (s & 1) * 4 * PC * (Wp / 2);
             {
                 // lane (r8 = lane % 8, uq = lane / 8) keeps its row within a block of 8 and its K chunk within a
                 // group of 4; warp pw takes the row blocks pw, pw + NHW, ... of each (part, re/im, chunk group).
@@ -401,30 +445,29 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
                 const int r8 = lane & 7, uq = lane >> 3, pw = warp - NCW - NAW - NLW;
                 const int nrb = a.Nt / 8;
                 const int nmine = nrb > pw ? (nrb - 1 - pw) / NHW + 1 : 0;
-                const int ostep = 8 * NHW * a.Dk, wstep = ostep >> 1;               // ostep is even
+                const int ostep = 8 * NHW * a.Dk, wstep = ostep >> 1;               // ostep: a multiple of 8
                 const uint32_t bstep = (uint32_t)(NHW * nkc * 128);
 #pragma unroll
                 for (int ub = 0; ub < UB; ++ub) {
                     const int u = ub * 4 + uq;
                     if (u >= NKC) continue;
                     const int o0 = a.Dk * (8 * pw + r8) + 8 * u;                    // first element, first block
-                    const int cp = o0 & 1;
+                    const int cp = o0 & (PC - 1);                                   // the same in every block
 #pragma unroll
                     for (int pi = 0; pi < 4; ++pi) {                              // (part, re/im)
                         const int part = pi & 1, im = pi >> 1;
-                        const uint32_t *src = plb + (2 * (2 * im + part) + cp) * (Wp / 2) + (o0 >> 1);
+                        const uint32_t *src = plb + (PC * (2 * im + part) + cp) * (Wp / 2) + ((o0 - cp) >> 1);
                         unsigned char *dst = Bb + part * bpart + core_off(im * a.Nt + 8 * pw + r8, u, nkc);
                         int m = 0;
                         for (; m + 2 <= nmine; m += 2) {
                             const uint32_t *s0 = src + m * wstep, *s1 = s0 + wstep;
-                            const uint4 v0 = make_uint4(s0[0], s0[1], s0[2], s0[3]);
-                            const uint4 v1 = make_uint4(s1[0], s1[1], s1[2], s1[3]);
+                            const uint4 v0 = ld_run<PC>(s0), v1 = ld_run<PC>(s1);
                             *reinterpret_cast<uint4 *>(dst + m * bstep) = v0;
                             *reinterpret_cast<uint4 *>(dst + (m + 1) * bstep) = v1;
                         }
                         if (m < nmine) {
                             const uint32_t *s0 = src + m * wstep;
-                            *reinterpret_cast<uint4 *>(dst + m * bstep) = make_uint4(s0[0], s0[1], s0[2], s0[3]);
+                            *reinterpret_cast<uint4 *>(dst + m * bstep) = ld_run<PC>(s0);
                         }
                     }
                 }
@@ -560,7 +603,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             // ------------------------------------------------------------------ consumers (warps 0..7), more taps
             // with at most 32 children lane quarters 2, 3 repeat quarters 0, 1 (A' rows 64 .. 127), and warp w takes
             // the column quarter w / 4 + 2 (w % 4 / 2) of the tile instead of the column half w / 4
-            const int rp = a.C <= 32 ? 2 : 1;
+            const int rp = a.rp;
             const int q = warp & 3, g = warp >> 2;
             const int c = 16 * (rp == 2 ? (q & 1) : q) + (lane >> 1);   // this lane's child (rows 2c: Mr, 2c + 1: Mi)
             const bool odd = lane & 1;
@@ -808,22 +851,22 @@ size_t level_tc_scratch_bytes(int Np, int C, int P, int Ko)
 
 // Dynamic shared memory of level_tc_gemm: both pulses' A' (hi, lo), sb stages of B' (hi, lo), the window planes, the
 // taps, the staged windows and the barriers.
-static size_t gemm_smem(int Lkp, int Dk, int nt, int sb)
+static size_t gemm_smem(int Lkp, int Dk, int nt, int sb, int pc)
 {
     const size_t apart = (size_t)128 * Lkp * 2, bpart = (size_t)2 * nt * Lkp * 2;
-    const int W = Dk * (nt - 1) + Lkp, Wp = (W + 9) & ~1;
-    // two stages' planes; barriers: afull[2], aempty[2], bfull[sb], bempty[sb], dfull[2], dempty[2], pfull[2],
-    // pempty[2]
-    return 4 * apart + (size_t)sb * 2 * bpart + (size_t)16 * (Wp / 2) * 4 + (size_t)Lkp * 4 + (size_t)XS * Wp * 8 +
-           (size_t)(12 + 2 * sb) * 8;
+    const int W = Dk * (nt - 1) + Lkp, Wp = plane_len(W, pc);
+    // two stages' planes (4 planes x pc copies); barriers: afull[2], aempty[2], bfull[sb], bempty[sb], dfull[2],
+    // dempty[2], pfull[2], pempty[2]
+    return 4 * apart + (size_t)sb * 2 * bpart + (size_t)2 * 4 * pc * (Wp / 2) * 4 + (size_t)Lkp * 4 +
+           (size_t)XS * Wp * 8 + (size_t)(12 + 2 * sb) * 8;
 }
 
-constexpr size_t GEMM_SMEM_MAX = 226 * 1024;                 // the opt-in limit less static shared memory and slack
+constexpr size_t GEMM_SMEM_MAX = 225 * 1024;                 // the opt-in limit less static shared memory and slack
 
 bool level_tc_supported(int C, int Lk, int Dk)
 {
     const int Lkp = ((Lk + 15) / 16) * 16;
-    return C >= 1 && C <= 64 && Lkp <= 96 && Dk >= 1 && gemm_smem(Lkp, Dk, 32, 2) <= GEMM_SMEM_MAX;
+    return C >= 1 && C <= 64 && Lkp <= 96 && Dk >= 1 && gemm_smem(Lkp, Dk, 32, 2, 2) <= GEMM_SMEM_MAX;
 }
 
 cudaError_t launch_amax(const float2 *x, size_t n, int *amax, cudaStream_t s)
@@ -847,14 +890,28 @@ cudaError_t launch_level_tc_gemm(const LevelLaunch &L, const int *amax_in, void 
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&maxsmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     const size_t avail = std::min((size_t)maxsmem - 1024, GEMM_SMEM_MAX);
-    auto need = [&](int nt, int sb) { return gemm_smem(a.Lkp, a.Dk, nt, sb); };
-    // columns per tile: a multiple of 32 up to 128 whose operands fit shared memory with two B stages, the one that
-    // wastes the fewest columns on the last tile counting each tile as 32 columns of fixed cost
-    int best = 0, bestw = 1 << 30;
-    for (int nt = 128; nt >= 32; nt -= 32) {
-        if (need(nt, 2) > avail) continue;
-        const int nti = (L.Ko + nt - 1) / nt, waste = nti * nt - L.Ko + nti * 32;
-        if (waste < bestw) { bestw = waste; best = nt; }
+    // launch options (LevelLaunch::tc_*; 0 = the default): plane copies, row repeat, columns per tile, B stages
+    const int pc = L.tc_pc == 4 ? 4 : 2;
+    if (L.tc_pc != 0 && L.tc_pc != 2 && L.tc_pc != 4) { *why = "plane copies: 2 or 4"; return cudaErrorNotSupported; }
+    a.rp = (a.Lkp > 32 && L.C <= 32 && L.tc_rp != 1) ? 2 : 1;
+    const int unit = a.rp == 2 ? 32 : 16;                    // the consumers' column split: 8-column chunks per warp
+    auto need = [&](int nt, int sb) { return gemm_smem(a.Lkp, a.Dk, nt, sb, pc); };
+    int best = 0;
+    if (L.tc_nt) {
+        if (L.tc_nt % unit || L.tc_nt > 128 || need(L.tc_nt, 2) > avail) {
+            *why = "columns per tile: a multiple of 16 (32 with repeated rows) up to 128 whose operands fit shared memory";
+            return cudaErrorNotSupported;
+        }
+        best = L.tc_nt;
+    } else {
+        // a multiple of 32 up to 128 whose operands fit shared memory with two B stages, the one that wastes the
+        // fewest columns on the last tile counting each tile as 32 columns of fixed cost
+        int bestw = 1 << 30;
+        for (int nt = 128; nt >= 32; nt -= 32) {
+            if (need(nt, 2) > avail) continue;
+            const int nti = (L.Ko + nt - 1) / nt, waste = nti * nt - L.Ko + nti * 32;
+            if (waste < bestw) { bestw = waste; best = nt; }
+        }
     }
     if (!best) { *why = "the tensor-core level's operands do not fit shared memory"; return cudaErrorNotSupported; }
     a.Nt = best;
@@ -866,6 +923,13 @@ cudaError_t launch_level_tc_gemm(const LevelLaunch &L, const int *amax_in, void 
     a.pseg = (L.P + nseg - 1) / nseg;
     a.nseg = (L.P + a.pseg - 1) / a.pseg;
     int SB = 4;
+    if (L.tc_sb) {
+        if (L.tc_sb < 2 || L.tc_sb > 4 || need(a.Nt, L.tc_sb) > avail) {
+            *why = "B stages: 2 to 4 that fit shared memory";
+            return cudaErrorNotSupported;
+        }
+        SB = L.tc_sb;
+    }
     while (SB > 2 && need(a.Nt, SB) > avail) --SB;
     a.SB = SB;
     const size_t smem = need(a.Nt, SB);
@@ -878,14 +942,16 @@ cudaError_t launch_level_tc_gemm(const LevelLaunch &L, const int *amax_in, void 
         return cudaGetLastError();
     };
     cudaError_t e;
+#define FFBP_GEMM_RUN(N) (pc == 4 ? run(level_tc_gemm<N, 4>) : run(level_tc_gemm<N, 2>))
     switch (a.Lkp / 8) {
-        case 2: e = run(level_tc_gemm<2>); break;
-        case 4: e = run(level_tc_gemm<4>); break;
-        case 6: e = run(level_tc_gemm<6>); break;
-        case 8: e = run(level_tc_gemm<8>); break;
-        case 10: e = run(level_tc_gemm<10>); break;
-        default: e = run(level_tc_gemm<12>); break;
+        case 2: e = FFBP_GEMM_RUN(2); break;
+        case 4: e = FFBP_GEMM_RUN(4); break;
+        case 6: e = FFBP_GEMM_RUN(6); break;
+        case 8: e = FFBP_GEMM_RUN(8); break;
+        case 10: e = FFBP_GEMM_RUN(10); break;
+        default: e = FFBP_GEMM_RUN(12); break;
     }
+#undef FFBP_GEMM_RUN
     if (e != cudaSuccess) return e;
     return cudaSuccess;
 }

@@ -80,3 +80,130 @@ def tune_former(make, candidates, S_dev, target_db=-60.0, reps=3):
             raise ValueError('no candidate plan could be built for this patch')
         return make(**fallback[0]), fallback[0], table
     return best[0], best[1], table
+
+
+# ------------------------------------------------------------------------------------------- level launch options
+
+_LEVEL_CACHE = {}
+
+
+def level_signature(lv, Np):
+    """What the first pass of a tensor-core level's timing depends on: its shapes and filter lengths."""
+    Lk = lv['fir_k']['L'] if lv['fir_k'] is not None else 1
+    return (int(Np), int(lv['C']), int(lv['Dk']), int(Lk), int(lv['K']), int(lv['P']), int(lv['Ko']))
+
+
+def _level_candidates(C, Lk):
+    """Launch option sets of level_tc_gemm in the order a coordinate search visits them: plane copies, then columns
+    per tile (multiples of 32 with repeated A rows, of 16 without), then the row repeat off, then the B stages."""
+    Lkp = ((max(Lk, 1) + 15) // 16) * 16
+    rep_ok = Lkp > 32 and C <= 32
+    return dict(copies=[2, 4], nt=list(range(32, 129, 32)), nt16=list(range(16, 129, 16)), repeat_off=rep_ok,
+                sb=[2, 3, 4])
+
+
+def tune_level(lv, Np, reps=3, max_parents=1024, seed=0):
+    """The fastest launch options (ffbp_tc_opts as a dict) of one tensor-core level's first pass, timed with CUDA
+    events on random samples and child phases of the level's shapes and its own filters (at most max_parents
+    parents: the timing is linear in them beyond a few waves), by a coordinate search from the defaults. Results are
+    cached by level_signature. -> (opts, table [(opts, ms or reason)]); opts None when the level is not a
+    tensor-core level."""
+    import ctypes
+    import torch
+    from . import _lib
+    key = level_signature(lv, Np)
+    if key in _LEVEL_CACHE:
+        return _LEVEL_CACHE[key], []
+    L = _lib.load()
+    n = int(min(Np, max_parents))
+    C, P, K, Ko, Po, Dk, Dp = (int(lv[k]) for k in ('C', 'P', 'K', 'Ko', 'Po', 'Dk', 'Dp'))
+    fk, fp = lv['fir_k'], lv['fir_p']
+    Lk = fk['L'] if fk is not None else 1
+    g = torch.Generator(device='cuda')
+    g.manual_seed(seed)
+    x = torch.view_as_complex(torch.randn((n, P, K, 2), device='cuda', generator=g)).contiguous()
+    ph = torch.stack([torch.rand((n, C, P), device='cuda', generator=g) - 0.5,
+                      (torch.rand((n, C, P), device='cuda', generator=g) - 0.5) * 0.004], -1).contiguous()
+    tk = torch.tensor(np.asarray(fk['kern'], np.float32), device='cuda') if fk is not None else None
+    tp = torch.tensor(np.asarray(fp['kern'], np.float32), device='cuda') if fp is not None else None
+    out = torch.empty((n * C, Po, Ko), dtype=torch.complex64, device='cuda')
+    st = torch.zeros(3, dtype=torch.int32, device='cuda')
+    nb = int(L.ffbp_level_tc_scratch_bytes(n, C, P, Ko))
+    scr = torch.empty(nb // 4 + 4, dtype=torch.int32, device='cuda')
+    stream = torch.cuda.current_stream().cuda_stream
+    ptr = lambda t: None if t is None else t.data_ptr()
+
+    def run(o):
+        opts = _lib.TcOpts(o.get('nt', 0), o.get('sb', 0), o.get('copies', 0), o.get('repeat', 0))
+        _lib.check(L.ffbp_level_tc_ex(x.data_ptr(), n, P, K, ph.data_ptr(), C, ptr(tk), Lk,
+                                      fk['pl'] if fk is not None else 0, Dk, Ko, (K - 1) / 2.0, ptr(tp),
+                                      fp['L'] if fp is not None else 1, fp['pl'] if fp is not None else 0, Dp, Po,
+                                      None, None, out.data_ptr(), None, scr.data_ptr(), nb, st.data_ptr(),
+                                      ctypes.byref(opts), stream), 'ffbp_level_tc_ex')
+
+    table = []
+
+    def timed(o):
+        try:
+            run(o)
+            ts = []
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                run(o)
+                e1.record()
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1))
+        except ValueError as e:                       # an option set the launcher refuses (does not fit)
+            table.append((dict(o), f'refused: {str(e)[:60]}'))
+            return None
+        if int(st[0].item()):
+            raise RuntimeError('tensor-core level: a bounded wait ran out while tuning')
+        ms = float(np.median(ts))
+        table.append((dict(o), ms))
+        return ms
+
+    try:
+        best = {}
+        best_ms = timed(best)
+        if best_ms is None:
+            _LEVEL_CACHE[key] = None
+            return None, table
+        cand = _level_candidates(C, Lk)
+
+        def consider(o):
+            nonlocal best, best_ms
+            ms = timed(o)
+            if ms is not None and ms < best_ms:
+                best, best_ms = dict(o), ms
+        for c in cand['copies']:
+            consider(dict(best, copies=c))
+        for nt in cand['nt']:
+            consider(dict(best, nt=nt))
+        if cand['repeat_off']:
+            for nt in cand['nt16']:
+                consider(dict(best, repeat=1, nt=nt))
+        for sb in cand['sb']:
+            consider(dict(best, sb=sb))
+    finally:
+        del x, ph, out, scr
+        torch.cuda.empty_cache()
+    _LEVEL_CACHE[key] = best
+    return best, table
+
+
+def tune_levels(plan, reps=3):
+    """tune_level for every level of a plan whose first pass can run on the tensor cores; the chosen options are
+    stored in the plan's level records (key 'tc', read by DevicePlan) -> the list of per-level options (None for a
+    level left to the other kernels)."""
+    chosen = []
+    Np = 1
+    for lv in plan['levels']:
+        opts = None
+        if lv['C'] <= 64 and (lv['fir_k']['L'] if lv['fir_k'] is not None else 1) <= 96:
+            opts, _ = tune_level(lv, Np, reps=reps)
+        if opts is not None:
+            lv['tc'] = dict(opts)
+        chosen.append(opts)
+        Np *= int(lv['C'])
+    return chosen

@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define FFBP_B200_ABI_VERSION 1
+#define FFBP_B200_ABI_VERSION 2
 
 enum {
     FFBP_OK = 0,
@@ -58,6 +58,19 @@ enum {
                               /* float32), the form before the one-pass kernel                                    */
 };
 
+/* Launch options of a tensor-core level's first pass (level_tc_gemm; no counterpart in the reference, whose kernels
+ * take fixed shapes). 0 in a field keeps the default. They change the schedule, not the arithmetic: the plane copies
+ * and B stages leave every bit as it is; the columns per tile and the row repeat move the points where the output
+ * ramp's recurrence is seeded: a rounding-level change (about 1e-7 before the float16 intermediate, whose rounding
+ * it can flip by one unit: about 1e-5 relative in all). FFBP_E_UNSUPPORTED (at the form call) for a choice that
+ * does not fit.                                                                                                   */
+typedef struct {
+    int nt;                 /* output columns per tile: a multiple of 16 (32 with repeated rows), at most 128       */
+    int sb;                 /* stages of the B operand ring: 2 to 4                                                 */
+    int copies;             /* shifted copies of each bfloat16 plane: 2 (4-byte loads) or 4 (8-byte loads)         */
+    int repeat;             /* 1: no repeated A rows (default: repeated when more than 32 taps and at most 32 children) */
+} ffbp_tc_opts;
+
 /* One level of the plan (fastsar/ffbp2.py:192-250, make_plan's per-level record). All pointers are host memory. */
 typedef struct {
     int sx, sy;             /* children per parent along e1 and e2; C = sx * sy                                   */
@@ -74,6 +87,7 @@ typedef struct {
     const double *h_ref;    /* [B, 3] the parents' reference points (B = product of the earlier levels' C)        */
     const double *h_cen;    /* [B, C, 3] the children's centres                                                  */
     const double *h_range;  /* level 0 only, optional: [P] per-pulse one-way reference range (ImageFormer's ref=) */
+    ffbp_tc_opts tc;        /* launch options when the level runs on the tensor cores in two passes (zeros: defaults) */
 } ffbp_level_desc;
 
 /* The plan of one image (make_plan's record plus the final stage and the call options). Host memory.          */
@@ -238,6 +252,11 @@ int ffbp_level_tc(const void *d_x, int Np, int P, int K, const void *d_phase, in
                   int Dk, int Ko, double kc, const float *d_tp, int Lp, int plp, int Dp, int Po, const float *d_wp,
                   const float *d_wk, void *d_out, int *d_bad, void *d_scratch, size_t scratch_bytes, int *d_status,
                   void *stream);
+/* ffbp_level_tc with launch options for its first pass (NULL: the defaults), for tuning them per level shape.      */
+int ffbp_level_tc_ex(const void *d_x, int Np, int P, int K, const void *d_phase, int C, const float *d_tk, int Lk,
+                     int plk, int Dk, int Ko, double kc, const float *d_tp, int Lp, int plp, int Dp, int Po,
+                     const float *d_wp, const float *d_wk, void *d_out, int *d_bad, void *d_scratch,
+                     size_t scratch_bytes, int *d_status, const ffbp_tc_opts *opts, void *stream);
 
 /* Exact backprojection onto a grid (ExactFormer, fastsar/exact.py:404-801), in two calls per chunk of n pulses:
  * ffbp_exact_pad writes the windowed samples S[p, k] wp[p_off + p] wk[k] of d_S [n, K] complex64 into d_pad [n, nfft]

@@ -125,8 +125,9 @@ def test_level_kernel_window_and_nonfinite(lib, oracle_lib):
     assert int(bad.item()) == 77
 
 
-def _run_level_tc(lib, x, c0, sl, fk, fp, Ko, Po, Dk, Dp, window=None, bad=None):
-    """ffbp_level_tc on the device; -> (output, status [err, amax_in, amax_out] as ints)."""
+def _run_level_tc(lib, x, c0, sl, fk, fp, Ko, Po, Dk, Dp, window=None, bad=None, opts=None):
+    """ffbp_level_tc (ffbp_level_tc_ex with launch options opts: a dict of ffbp_tc_opts fields) on the device;
+    -> (output, status [err, amax_in, amax_out] as ints)."""
     L = lib.load()
     Np, P, K = x.shape
     C = c0.shape[1]
@@ -141,10 +142,14 @@ def _run_level_tc(lib, x, c0, sl, fk, fp, Ko, Po, Dk, Dp, window=None, bad=None)
     scratch = torch.empty(nbytes // 4 + 4, dtype=torch.int32, device='cuda')
     status = torch.zeros(3, dtype=torch.int32, device='cuda')
     s = torch.cuda.current_stream().cuda_stream
-    lib.check(L.ffbp_level_tc(dx.data_ptr(), Np, P, K, dph.data_ptr(), C, lib.tptr(tk), fk['L'] if fk else 1,
-                              fk['pl'] if fk else 0, Dk, Ko, (K - 1) / 2.0, lib.tptr(tp), fp['L'] if fp else 1,
-                              fp['pl'] if fp else 0, Dp, Po, lib.tptr(wp), lib.tptr(wk), out.data_ptr(), lib.tptr(bad),
-                              scratch.data_ptr(), nbytes, status.data_ptr(), s), 'ffbp_level_tc')
+    args = (dx.data_ptr(), Np, P, K, dph.data_ptr(), C, lib.tptr(tk), fk['L'] if fk else 1, fk['pl'] if fk else 0, Dk,
+            Ko, (K - 1) / 2.0, lib.tptr(tp), fp['L'] if fp else 1, fp['pl'] if fp else 0, Dp, Po, lib.tptr(wp),
+            lib.tptr(wk), out.data_ptr(), lib.tptr(bad), scratch.data_ptr(), nbytes, status.data_ptr())
+    if opts is None:
+        lib.check(L.ffbp_level_tc(*args, s), 'ffbp_level_tc')
+    else:
+        o = lib.TcOpts(*(int(opts.get(k, 0)) for k in ('nt', 'sb', 'copies', 'repeat')))
+        lib.check(L.ffbp_level_tc_ex(*args, ctypes.byref(o), s), 'ffbp_level_tc_ex')
     torch.cuda.synchronize()
     return out.cpu().numpy(), status.cpu().numpy()
 
@@ -184,6 +189,40 @@ def test_level_tensor_cores_match_oracle(lib, oracle_lib, case):
     assert amax_out == np.max(np.abs(got.view(np.float32)))
     amax_in = np.frombuffer(np.int32(st[1]).tobytes(), np.float32)[0]
     assert amax_in == np.max(np.abs(x.view(np.float32)))
+
+
+TC_OPTS_CASES = [TC_LEVEL_CASES[i] for i in (0, 4, 6, 7, 10)]
+
+
+@pytest.mark.parametrize('case', TC_OPTS_CASES,
+                         ids=[f'Np{c[0]}-P{c[1]}-K{c[2]}-C{c[3]}-Dk{c[4]}-Dp{c[5]}' for c in TC_OPTS_CASES])
+def test_level_tensor_cores_launch_options_same_bits(lib, case):
+    """The first pass's launch options (ffbp_tc_opts: columns per tile, B stages, plane copies, row repeat) change
+    the schedule, not the arithmetic: plane copies and B stages give the default's output bit for bit; columns per
+    tile and the row repeat move the points where the consumers seed the output ramp's recurrence (about 1e-7), which
+    can flip a rounding of the float16 intermediate (one unit: 5e-4 of that value): within 1e-4 of the default; a set
+    that does not fit is refused with FFBP_E_UNSUPPORTED (ValueError)."""
+    Np, P, K, C, Dk, Dp, pk = case
+    rng = np.random.default_rng(sum(case[:6]) + 11)
+    x, c0, sl, fk, fp, Ko, Po = _level_case(rng, Np, P, K, C, Dk, Dp, pk=pk)
+    want, _ = _run_level_tc(lib, x, c0, sl, fk, fp, Ko, Po, Dk, Dp)
+    sets = [dict(copies=4), dict(copies=2), dict(nt=32), dict(nt=64, copies=4), dict(nt=96), dict(nt=128, sb=2),
+            dict(sb=3), dict(repeat=1, nt=16), dict(repeat=1, nt=48, copies=4), dict(repeat=1, nt=80), dict(nt=48)]
+    ran = 0
+    for o in sets:
+        try:
+            got, st = _run_level_tc(lib, x, c0, sl, fk, fp, Ko, Po, Dk, Dp, opts=o)
+        except ValueError as e:
+            assert 'columns per tile' in str(e) or 'B stages' in str(e), (o, str(e))
+            continue
+        assert st[0] == 0
+        if set(o) <= {'copies', 'sb'}:
+            assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), o
+        else:
+            assert _rel(got, want) < 1e-4, (o, _rel(got, want))
+        ran += 1
+    print(f'{case}: {ran} of {len(sets)} option sets ran')
+    assert ran >= 5
 
 
 def test_level_tensor_cores_window_nonfinite_and_limits(lib, oracle_lib):
@@ -428,6 +467,30 @@ def test_image_tensor_cores_repeatable_bitwise(golden, monkeypatch, precision, f
     a = f(g['S'])
     b = f(g['S'])
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_image_tuned_levels_match_default(golden):
+    """ImageFormer(tune_levels=True) times the tensor-core levels' launch options per level shape when it is built
+    and plans with the fastest: every tuned level records its choice, and the image is the default's to within 1e-4
+    (the options move only the seeding of the output ramp's recurrence, and with it a float16 rounding here and
+    there)."""
+    from fastsar_b200 import ImageFormer, sim, tune
+    g = golden('image_spot512')
+    w = sim.workload('spotlight_512')
+    col = w['col']
+    args = (col.ant, col.fmin, col.df, col.K, 512, 512, 0.25, 0.25, w['e1'], w['e2'])
+    f = ImageFormer(*args, precision='float16', tune_levels=True)
+    assert f.level_opts is not None and len(f.level_opts) == f.levels
+    assert all(o is not None for o in f.level_opts)
+    print('tuned level options:', f.level_opts)
+    a = f(g['S'])
+    b = ImageFormer(*args, precision='float16')(g['S'])
+    print(f'tuned against default: {_rel(a, b):.1e}')
+    assert _rel(a, b) < 1e-4, _rel(a, b)
+    # a second former of the same shapes takes the options from the cache
+    n = len(tune._LEVEL_CACHE)
+    ImageFormer(*args, precision='float16', tune_levels=True).release()
+    assert len(tune._LEVEL_CACHE) == n
 
 
 def test_image_float16_large_amplitudes(golden, oracle_lib):
