@@ -10,6 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, 'libffbp_b200.so')
 
 FFBP_OK, FFBP_E_ARG, FFBP_E_CUDA, FFBP_E_NOMEM, FFBP_E_WORKSPACE, FFBP_E_UNSUPPORTED = 0, -1, -2, -3, -4, -5
+FFBP_E_TRANSFER = -6
 FFBP_FINAL_FP32, FFBP_FINAL_TC_F16, FFBP_FINAL_TC_BF16X3 = 0, 1, 2
 FFBP_LEVELS_TC = 0x100
 KIND_NAMES = {1: 'amax', 2: 'level_fp32', 3: 'level_tc_gemm', 4: 'level_tc_fir', 5: 'final_fp32', 6: 'final_tc',
@@ -24,7 +25,7 @@ EXPORTS = ('ffbp_last_error', 'ffbp_abi_version', 'ffbp_plan_create', 'ffbp_plan
            'ffbp_form_profile', 'ffbp_exact_pad', 'ffbp_exact_backproject', 'ffbp_mlp_param_count',
            'ffbp_mlp_max_decimation', 'ffbp_mlp_work_bytes', 'ffbp_plan_host_bytes', 'ffbp_form_host', 'ffbp_gate_pad',
            'ffbp_gate_fold', 'ffbp_gate_taper', 'ffbp_batch_create', 'ffbp_batch_form', 'ffbp_batch_destroy', 'ffbp_mlp_taps', 'ffbp_mlp_grad', 'ffbp_mlp_train_step',
-           'ffbp_plan_check', 'ffbp_plan_test_wait', 'ffbp_level_fused', 'ffbp_level_tc_ex')
+           'ffbp_plan_check', 'ffbp_plan_test_wait', 'ffbp_level_fused', 'ffbp_level_tc_ex', 'ffbp_plan_test_transfer')
 
 _c_int, _c_double, _vp = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
 
@@ -78,6 +79,7 @@ def load():
     L.ffbp_form_static.argtypes = [_vp, _vp, _vp, _vp, ctypes.POINTER(_c_int)]
     L.ffbp_plan_check.argtypes = [_vp, _vp]
     L.ffbp_plan_test_wait.argtypes = [_vp, _c_int, ctypes.c_uint]
+    L.ffbp_plan_test_transfer.argtypes = [_vp, _c_int]
     L.ffbp_plan_host_bytes.argtypes = [_vp, ctypes.POINTER(ctypes.c_size_t)]
     L.ffbp_batch_create.argtypes = [ctypes.POINTER(_vp), _c_int, ctypes.POINTER(_vp), ctypes.POINTER(_vp),
                                     ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_size_t), _vp, ctypes.POINTER(_vp)]

@@ -251,6 +251,11 @@ class DevicePlan:
              'final_tc': _lib.FFBP_KIND_FINAL_TC}[kind]
         _lib.check(L.ffbp_plan_test_wait(self.handle, k, int(limit_us) if k else 0), 'ffbp_plan_test_wait')
 
+    def test_transfer(self, image):
+        """Test hook of the transfer check: the next form_many call leaves out the upload of its image `image` (the
+        device buffer keeps what it held), as a transfer that did not deliver would; -1 turns it off."""
+        _lib.check(_lib.load().ffbp_plan_test_transfer(self.handle, int(image)), 'ffbp_plan_test_transfer')
+
     def form_timed(self, S_dev, img_dev, stream=None):
         """form with the device time (ms) of each launch: [level 0, ..., level nlev-1, final] (waits for the stream)."""
         import torch
@@ -537,7 +542,9 @@ class ImageFormer:
         arrays; page-locked torch tensors, `pin_memory=True`, let the copies overlap the formation) -> images
         [nx, ny] complex64 in host memory (the given `images`, or new page-locked tensors), returned as numpy
         arrays. Each history's upload and each image's download run on their own streams while the neighbouring
-        images form (ffbp_form_host). Raises ValueError naming the first image with non-finite samples."""
+        images form (ffbp_form_host). Every upload is checked by a sampled checksum on both sides of the transfer
+        (the reference's transfer check): RuntimeError naming the first history that did not arrive as it is in host
+        memory. Raises ValueError naming the first image with non-finite samples."""
         import torch
         hs = []
         for S in histories:

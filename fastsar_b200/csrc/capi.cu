@@ -51,6 +51,62 @@ struct DevLevel {
 
 size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
 
+// The transfer check of a history S [P, K] complex64 (the reference checks each uploaded block the same way,
+// fastsar/ffbp_cuda.py:759-764,826-863): sum over the sampled pulses r (every rs-th) of (r + 1) times the sum of the
+// sampled samples S[r, k] (every ks-th), in float64, on both sides of the transfer. A block that did not arrive
+// (a stale or half-written buffer) changes it by about the sum's own size. About 2,048 x 128 samples.
+void check_strides(int P, int K, int *rs, int *ks)
+{
+    *rs = P > 2048 ? P / 2048 : 1;
+    *ks = K > 128 ? K / 128 : 1;
+}
+
+// out[0], out[1] += the check of S (one warp per sampled pulse; atomics, so the last bits depend on the order)
+__global__ void transfer_check_kernel(const float2 *__restrict__ S, int P, int K, int rs, int ks, double *out)
+{
+    const int lane = threadIdx.x & 31;
+    const int r = ((int)blockIdx.x * (int)(blockDim.x >> 5) + (int)(threadIdx.x >> 5)) * rs;
+    if (r >= P) return;
+    double re = 0.0, im = 0.0;
+    for (int k = lane * ks; k < K; k += 32 * ks) {
+        const float2 v = S[(size_t)r * K + k];
+        re += v.x;
+        im += v.y;
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        re += __shfl_down_sync(0xffffffffu, re, o);
+        im += __shfl_down_sync(0xffffffffu, im, o);
+    }
+    if (lane == 0) {
+        atomicAdd(out, (r + 1.0) * re);
+        atomicAdd(out + 1, (r + 1.0) * im);
+    }
+}
+
+// The same check of a history in host memory, and its scale (the sum of (r + 1) (|re| + |im|) over the samples).
+void host_check(const float2 *S, int P, int K, double *re, double *im, double *scale)
+{
+    int rs, ks;
+    check_strides(P, K, &rs, &ks);
+    double a = 0.0, b = 0.0, m = 0.0;
+    for (int r = 0; r < P; r += rs) {
+        double x = 0.0, y = 0.0, z = 0.0;
+        for (int k = 0; k < K; k += ks) {
+            const float2 v = S[(size_t)r * K + k];
+            x += v.x;
+            y += v.y;
+            z += fabs((double)v.x) + fabs((double)v.y);
+        }
+        a += (r + 1.0) * x;
+        b += (r + 1.0) * y;
+        m += (r + 1.0) * z;
+    }
+    *re = a;
+    *im = b;
+    *scale = m;
+}
+
 }  // namespace
 
 struct ffbp_plan {
@@ -69,6 +125,13 @@ struct ffbp_plan {
     cudaEvent_t ev_up[2] = {}, ev_formed[2] = {}, ev_down[2] = {};
     int *h_status = nullptr;
     int n_status = 0;
+    // the transfer check of ffbp_form_host: per device history buffer a sampled checksum (two doubles) computed after
+    // its upload, copied into h_check (page-locked, two doubles per image); test_skip_upload: the index of the image
+    // whose upload the next ffbp_form_host call leaves out (ffbp_plan_test_transfer; -1 none)
+    double *d_check = nullptr;
+    double *h_check = nullptr;
+    int n_check = 0;
+    int test_skip_upload = -1;
     // the device the plan lives on, and the abort count of its tensor-core kernels: d_aborts (device memory) is
     // raised by every bounded wait that runs out and is never reset; each form call copies it into h_aborts
     // (page-locked) at its end, so that the host sees earlier calls' aborts without waiting; `reported` is the count
@@ -104,6 +167,7 @@ struct ffbp_plan {
         if (up) cudaStreamDestroy(up);
         if (down) cudaStreamDestroy(down);
         if (h_status) cudaFreeHost(h_status);
+        if (h_check) cudaFreeHost(h_check);
         if (h_aborts) cudaFreeHost(h_aborts);
     }
 };
@@ -472,6 +536,22 @@ int ffbp_form_host(ffbp_plan *p, const void *const *h_S, void *const *h_img, int
             return cuda_fail(e, "ffbp_form_host: status array");
         p->n_status = 2 * n;
     }
+    if (!p->d_check && (e = p->alloc(&p->d_check, 4)) != cudaSuccess) return cuda_fail(e, "ffbp_form_host: check sums");
+    if (p->n_check < 2 * n) {
+        if (p->h_check) cudaFreeHost(p->h_check);
+        p->h_check = nullptr;
+        p->n_check = 0;
+        if ((e = cudaHostAlloc(reinterpret_cast<void **>(&p->h_check), 2 * (size_t)n * sizeof(double), cudaHostAllocDefault)) != cudaSuccess)
+            return cuda_fail(e, "ffbp_form_host: check sums");
+        p->n_check = 2 * n;
+    }
+    const int skip = p->test_skip_upload;
+    p->test_skip_upload = -1;
+    const int P0 = p->lv[0].P, K0 = p->lv[0].K;
+    int crs, cks;
+    check_strides(P0, K0, &crs, &cks);
+    const int nrows = (P0 + crs - 1) / crs;
+    std::vector<double> sent(3 * (size_t)n, 0.0);           // per image: the host's check (re, im) and its scale
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const size_t sb = (size_t)p->lv[0].P * p->lv[0].K * sizeof(float2), ib = (size_t)p->nx * p->ny * sizeof(float2);
     char *st = static_cast<char *>(d_stage);
@@ -485,7 +565,13 @@ int ffbp_form_host(ffbp_plan *p, const void *const *h_S, void *const *h_img, int
     for (int i = 0; i < n && rc == FFBP_OK; ++i) {
         const int b = i & 1;
         if (i >= 2 && (e = cudaStreamWaitEvent(p->up, p->ev_formed[b], 0)) != cudaSuccess) { rc = cuda_fail(e, "ffbp_form_host"); break; }
-        if ((e = cudaMemcpyAsync(dS[b], h_S[i], sb, cudaMemcpyHostToDevice, p->up)) != cudaSuccess ||
+        // the upload, then the check of what arrived, computed on the upload stream and copied back
+        if ((i != skip && (e = cudaMemcpyAsync(dS[b], h_S[i], sb, cudaMemcpyHostToDevice, p->up)) != cudaSuccess) ||
+            (e = cudaMemsetAsync(p->d_check + 2 * b, 0, 2 * sizeof(double), p->up)) != cudaSuccess) { rc = cuda_fail(e, "ffbp_form_host"); break; }
+        transfer_check_kernel<<<(nrows + 7) / 8, 256, 0, p->up>>>(static_cast<const float2 *>(dS[b]), P0, K0, crs, cks,
+                                                                 p->d_check + 2 * b);
+        if ((e = cudaGetLastError()) != cudaSuccess ||
+            (e = cudaMemcpyAsync(p->h_check + 2 * i, p->d_check + 2 * b, 2 * sizeof(double), cudaMemcpyDeviceToHost, p->up)) != cudaSuccess ||
             (e = cudaEventRecord(p->ev_up[b], p->up)) != cudaSuccess ||
             (e = cudaStreamWaitEvent(s, p->ev_up[b], 0)) != cudaSuccess ||
             (i >= 2 && (e = cudaStreamWaitEvent(s, p->ev_down[b], 0)) != cudaSuccess)) { rc = cuda_fail(e, "ffbp_form_host"); break; }
@@ -495,6 +581,8 @@ int ffbp_form_host(ffbp_plan *p, const void *const *h_S, void *const *h_img, int
             (e = cudaStreamWaitEvent(p->down, p->ev_formed[b], 0)) != cudaSuccess ||
             (e = cudaMemcpyAsync(h_img[i], dI[b], ib, cudaMemcpyDeviceToHost, p->down)) != cudaSuccess ||
             (e = cudaEventRecord(p->ev_down[b], p->down)) != cudaSuccess) { rc = cuda_fail(e, "ffbp_form_host"); break; }
+        // the host side of image i's check, while the device works
+        host_check(static_cast<const float2 *>(h_S[i]), P0, K0, &sent[3 * i], &sent[3 * i + 1], &sent[3 * i + 2]);
     }
     // wait for everything queued (the host buffers are in use until then), also after an error
     const cudaError_t e1 = cudaStreamSynchronize(p->up), e2 = cudaStreamSynchronize(s), e3 = cudaStreamSynchronize(p->down);
@@ -502,6 +590,13 @@ int ffbp_form_host(ffbp_plan *p, const void *const *h_S, void *const *h_img, int
     if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
         return cuda_fail(e1 != cudaSuccess ? e1 : e2 != cudaSuccess ? e2 : e3, "ffbp_form_host");
     for (int i = 0; i < n; ++i) h_bad[i] = p->h_status[2 * i] == 0x7f7f7f7f ? -1 : p->h_status[2 * i];
+    for (int i = 0; i < n; ++i) {
+        const double dr = p->h_check[2 * i] - sent[3 * i], di = p->h_check[2 * i + 1] - sent[3 * i + 1];
+        if (!(fabs(dr) + fabs(di) <= 1e-9 * sent[3 * i + 2]))
+            return fail(FFBP_E_TRANSFER, "ffbp_form_host: history %d did not reach the device as it is in host memory "
+                        "(check sums %.9g%+.9gi sent, %.9g%+.9gi received): its image is not to be used", i, sent[3 * i],
+                        sent[3 * i + 1], p->h_check[2 * i], p->h_check[2 * i + 1]);
+    }
     return aborted(p, "ffbp_form_host");
 }
 
@@ -628,6 +723,14 @@ int ffbp_plan_check(ffbp_plan *p, void *stream)
     cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return cuda_fail(e, "ffbp_plan_check");
     return aborted(p, "a form call on this plan");
+}
+
+int ffbp_plan_test_transfer(ffbp_plan *p, int image)
+{
+    if (!p) return fail(FFBP_E_ARG, "ffbp_plan_test_transfer: null plan");
+    if (image < -1) return fail(FFBP_E_ARG, "ffbp_plan_test_transfer: image %d < -1", image);
+    p->test_skip_upload = image;
+    return FFBP_OK;
 }
 
 int ffbp_plan_test_wait(ffbp_plan *p, int kind, unsigned limit_us)

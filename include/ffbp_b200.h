@@ -35,7 +35,8 @@ enum {
     FFBP_E_CUDA = -2,       /* a CUDA call failed                                                           */
     FFBP_E_NOMEM = -3,      /* a device allocation of the plan failed                                       */
     FFBP_E_WORKSPACE = -4,  /* the workspace passed to ffbp_form is smaller than ffbp_plan_workspace_bytes   */
-    FFBP_E_UNSUPPORTED = -5 /* a shape the kernels do not cover (the message says which limit)              */
+    FFBP_E_UNSUPPORTED = -5,/* a shape the kernels do not cover (the message says which limit)              */
+    FFBP_E_TRANSFER = -6    /* a history did not reach the device as it is in host memory (ffbp_form_host)  */
 };
 
 /* Final-stage arithmetic (ImageFormer's precision=, fastsar/api.py:27-31).                                     */
@@ -157,14 +158,22 @@ int ffbp_plan_check(ffbp_plan *plan, void *stream);
  * every wait is bounded and the block frees its tensor memory before it exits.                                 */
 int ffbp_plan_test_wait(ffbp_plan *plan, int kind, unsigned limit_us);
 
+/* Test hook of the transfer check (no counterpart in the reference): the next ffbp_form_host call leaves out the
+ * upload of its image `image` (its device buffer keeps what it held), as a transfer that did not deliver would;
+ * -1 turns it off. One call only.                                                                                 */
+int ffbp_plan_test_transfer(ffbp_plan *plan, int image);
+
 /* Form n images from host memory, overlapping each history's upload and each image's download with the
  * formation of its neighbours (the reference's pinned double-buffered upload, fastsar/ffbp_cuda.py:692-765,
  * carried across images): h_S[i] [P0, K0] complex64 and h_img[i] [nx, ny] complex64 in page-locked host memory
  * (pageable memory works, without the overlap). d_stage: two device histories and two device images,
  * ffbp_plan_host_bytes bytes, 256-byte aligned; d_ws: the form workspace. The formation runs on `stream`, the copies
- * on two streams of the plan. Returns when every image is in host memory; h_bad[i] is image i's first non-finite
- * pulse (or -1); FFBP_E_CUDA when a tensor-core kernel of one of the calls aborted. No counterpart in the
- * reference's API.                                                         */
+ * on two streams of the plan. Every upload is checked (the reference's transfer check, fastsar/ffbp_cuda.py:759-764,
+ * 826-863): a position-weighted float64 sum of about 2,048 x 128 sampled samples, computed by a kernel on the upload
+ * stream and by the host while the device works, must agree to 1e-9 of its scale. Returns when every image is in
+ * host memory; h_bad[i] is image i's first non-finite pulse (or -1); FFBP_E_CUDA when a tensor-core kernel of one of
+ * the calls aborted; FFBP_E_TRANSFER, naming the first such history, when a check did not agree (that image is not
+ * to be used). No counterpart in the reference's API.                                                              */
 int ffbp_plan_host_bytes(const ffbp_plan *plan, size_t *bytes);
 int ffbp_form_host(ffbp_plan *plan, const void *const *h_S, void *const *h_img, int n, void *d_stage,
                    size_t stage_bytes, void *d_ws, size_t ws_bytes, void *stream, int *h_bad);

@@ -78,3 +78,21 @@ def test_test_hook_rejects_bad_arguments(golden):
         _lib.check(L.ffbp_plan_test_wait(f._dev.handle, 5, 100), 'ffbp_plan_test_wait')
     with pytest.raises(ValueError, match='limit'):
         _lib.check(L.ffbp_plan_test_wait(f._dev.handle, _lib.FFBP_KIND_FINAL_TC, 0), 'ffbp_plan_test_wait')
+
+
+def test_transfer_that_did_not_deliver_is_reported(golden):
+    """ffbp_form_host checks every upload with a sampled, position-weighted float64 sum computed on both sides of the
+    transfer. The test hook ffbp_plan_test_transfer leaves one upload out (its device buffer keeps the history of
+    two images before), as a transfer that did not deliver would: form_many raises naming that history; the hook is
+    one call only, and the next call's images equal form_device's."""
+    f, S = _former(golden)
+    rng = np.random.default_rng(4)
+    hs = [(golden('image_spot512')['S'] * (rng.standard_normal() + 1j * rng.standard_normal())).astype(np.complex64)
+          for _ in range(3)]
+    pinned = [torch.from_numpy(h).pin_memory() for h in hs]
+    want = [f.form_device(torch.from_numpy(h).cuda()).cpu().numpy() for h in hs]
+    f._dev.test_transfer(2)
+    with pytest.raises(RuntimeError, match='history 2 did not reach the device'):
+        f.form_many(pinned)
+    got = f.form_many(pinned)
+    assert all(np.array_equal(a, b) for a, b in zip(got, want))
