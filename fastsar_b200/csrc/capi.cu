@@ -448,7 +448,7 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
         L.Dp = v.Dp; L.Lp = v.Lp; L.plp = v.plp; L.kc = v.kc;
         L.amax = amax + l + 1;
         L.test_wait_ns = p->test_kind == FFBP_KIND_LEVEL_TC ? p->test_ns : 0u;
-        L.tc_nt = v.tc.nt; L.tc_sb = v.tc.sb; L.tc_pc = v.tc.copies; L.tc_rp = v.tc.repeat;
+        L.tc_nt = v.tc.nt; L.tc_sb = v.tc.sb; L.tc_pc = v.tc.copies; L.tc_rp = v.tc.repeat; L.tc_fir = v.tc.fir;
         const char *why = nullptr;
         const int form = level_form(p, l);
         if (form == 1) {
@@ -458,7 +458,7 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
             e = ffbp::launch_level_tc_gemm(L, amax + l, scratch, p->d_aborts, s, &why);
             if (!why && e == cudaSuccess) {
                 mark(FFBP_KIND_LEVEL_TC_GEMM << 8 | l);
-                e = ffbp::launch_level_tc_fir(L, amax + l, scratch, s, &why);
+                e = ffbp::launch_level_tc_fir(L, amax + l, scratch, p->d_aborts, s, &why);
                 if (!why && e == cudaSuccess) mark(FFBP_KIND_LEVEL_TC_FIR << 8 | l);
             }
         } else {
@@ -855,7 +855,7 @@ int ffbp_level_tc_ex(const void *d_x, int Np, int P, int K, const void *d_phase,
     L.wp = d_wp; L.wk = d_wk; L.out = static_cast<float2 *>(d_out); L.bad = d_bad;
     L.Np = Np; L.C = C; L.P = P; L.K = K; L.Ko = Ko; L.Po = Po; L.Dk = Dk; L.Lk = Lk; L.plk = plk; L.Dp = Dp;
     L.Lp = Lp; L.plp = plp; L.kc = kc; L.amax = d_status + 2;
-    if (opts) { L.tc_nt = opts->nt; L.tc_sb = opts->sb; L.tc_pc = opts->copies; L.tc_rp = opts->repeat; }
+    if (opts) { L.tc_nt = opts->nt; L.tc_sb = opts->sb; L.tc_pc = opts->copies; L.tc_rp = opts->repeat; L.tc_fir = opts->fir; }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaError_t e = ffbp::launch_amax(L.x, (size_t)Np * P * K, d_status + 1, s);
     if (e != cudaSuccess) return cuda_fail(e, "ffbp_level_tc");

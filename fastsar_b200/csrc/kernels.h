@@ -21,8 +21,8 @@ struct LevelLaunch {
     unsigned test_wait_ns = 0;   // tensor-core pass 1 only, for tests of the failure report: when nonzero the MMA
                                  // issuer first waits this long on a barrier nothing completes, as a stuck pipeline
     // tensor-core pass 1 launch options (0: the default): output columns per tile, B stages, plane copies (2 or 4),
-    // row repeat (1: off)
-    int tc_nt = 0, tc_sb = 0, tc_pc = 0, tc_rp = 0;
+    // row repeat (1: off); pass 2's kernel (1: CUDA cores, 2: tensor cores)
+    int tc_nt = 0, tc_sb = 0, tc_pc = 0, tc_rp = 0, tc_fir = 0;
 };
 
 // Returns cudaSuccess, or an error with *why set to a static message for shapes the kernels do not cover.
@@ -44,8 +44,12 @@ cudaError_t launch_level_fused(const LevelLaunch &L, int *err, cudaStream_t s, c
 // its two passes, for callers that time them apart
 cudaError_t launch_level_tc_gemm(const LevelLaunch &L, const int *amax_in, void *scratch, int *err, cudaStream_t s,
                                  const char **why);
-cudaError_t launch_level_tc_fir(const LevelLaunch &L, const int *amax_in, const void *scratch, cudaStream_t s,
-                                const char **why);
+// the second pass: the pulse FIR of the float16 intermediate, on the kernel LevelLaunch::tc_fir selects (the tensor
+// cores, level_fir_tc.cu, or the CUDA cores)
+cudaError_t launch_level_tc_fir(const LevelLaunch &L, const int *amax_in, const void *scratch, int *err,
+                                cudaStream_t s, const char **why);
+cudaError_t launch_level_fir_tc(const LevelLaunch &L, const int *amax_in, const void *scratch, int *err,
+                                cudaStream_t s, const char **why);
 // The largest |component| of n complex samples into *amax (float bits, atomicMax; start at 0).
 cudaError_t launch_amax(const float2 *x, size_t n, int *amax, cudaStream_t s);
 

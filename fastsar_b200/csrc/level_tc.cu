@@ -27,8 +27,10 @@
 // more taps, so they get two warps of every three (with 16 consumer and 8 producer warps a stage took 8-10 % longer
 // at the second and third levels).
 //
-// Pass 2 (level_fir): the pulse FIR of the intermediate on the CUDA cores in float32 (a thread per two columns with
-// the ceil(Lp / Dp) outputs it feeds in registers), written as complex64 with the largest component recorded.
+// Pass 2: the pulse FIR of the intermediate, written as complex64 with the largest component recorded: on the tensor
+// cores as a banded product per row (level_fir_tc.cu), or on the CUDA cores in float32 (level_fir: a thread per two
+// columns with the ceil(Lp / Dp) outputs it feeds in registers); a launch option, by default the tensor cores for
+// output pulse axes of 512 or more.
 //
 // Every wait on a barrier is bounded in time; a wait that runs out sets *err and the block winds down.
 #include <cuda_bf16.h>
@@ -956,7 +958,7 @@ cudaError_t launch_level_tc_gemm(const LevelLaunch &L, const int *amax_in, void 
     return cudaSuccess;
 }
 
-cudaError_t launch_level_tc_fir(const LevelLaunch &L, const int *amax_in, const void *scratch, cudaStream_t s,
+cudaError_t launch_level_fir_cc(const LevelLaunch &L, const int *amax_in, const void *scratch, cudaStream_t s,
                                 const char **why)
 {
     *why = nullptr;
@@ -991,7 +993,20 @@ cudaError_t launch_level_tc(const LevelLaunch &L, const int *amax_in, void *scra
 {
     cudaError_t e = launch_level_tc_gemm(L, amax_in, scratch, err, s, why);
     if (e != cudaSuccess || *why) return e;
-    return launch_level_tc_fir(L, amax_in, scratch, s, why);
+    return launch_level_tc_fir(L, amax_in, scratch, err, s, why);
+}
+
+cudaError_t launch_level_tc_fir(const LevelLaunch &L, const int *amax_in, const void *scratch, int *err,
+                                cudaStream_t s, const char **why)
+{
+    // the pulse FIR on the tensor cores (a banded product per row, level_fir_tc.cu) or on the CUDA cores (level_fir);
+    // by default the tensor cores where the output pulse axis fills several 128-row tiles (short axes leave most
+    // of a tile's rows and the chunks' pulses empty, where the CUDA-core kernel is faster)
+    const int Lp = L.Dp > 1 ? L.Lp : 1;
+    const int AP = (Lp + L.Dp - 1) / L.Dp;
+    const bool tc = L.tc_fir == 2 || (L.tc_fir == 0 && (L.Po >= 512 || AP > 12));
+    if (L.tc_fir != 0 && L.tc_fir != 1 && L.tc_fir != 2) { *why = "pulse FIR kernel: 1 (CUDA cores) or 2 (tensor cores)"; return cudaErrorNotSupported; }
+    return tc ? launch_level_fir_tc(L, amax_in, scratch, err, s, why) : launch_level_fir_cc(L, amax_in, scratch, s, why);
 }
 
 }  // namespace ffbp

@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define FFBP_B200_ABI_VERSION 2
+#define FFBP_B200_ABI_VERSION 3
 
 enum {
     FFBP_OK = 0,
@@ -59,8 +59,8 @@ enum {
                               /* float32), the form before the one-pass kernel                                    */
 };
 
-/* Launch options of a tensor-core level's first pass (level_tc_gemm; no counterpart in the reference, whose kernels
- * take fixed shapes). 0 in a field keeps the default. They change the schedule, not the arithmetic: the plane copies
+/* Launch options of a tensor-core level (level_tc_gemm, and the kernel of its pulse FIR; no counterpart in the
+ * reference, whose kernels take fixed shapes). 0 in a field keeps the default. They change the schedule, not the arithmetic: the plane copies
  * and B stages leave every bit as it is; the columns per tile and the row repeat move the points where the output
  * ramp's recurrence is seeded: a rounding-level change (about 1e-7 before the float16 intermediate, whose rounding
  * it can flip by one unit: about 1e-5 relative in all). FFBP_E_UNSUPPORTED (at the form call) for a choice that
@@ -70,6 +70,8 @@ typedef struct {
     int sb;                 /* stages of the B operand ring: 2 to 4                                                 */
     int copies;             /* shifted copies of each bfloat16 plane: 2 (4-byte loads) or 4 (8-byte loads)         */
     int repeat;             /* 1: no repeated A rows (default: repeated when more than 32 taps and at most 32 children) */
+    int fir;                /* the second pass's pulse FIR: 1 on the CUDA cores, 2 on the tensor cores (a banded    */
+                            /* product per row; default: the tensor cores for 512 or more output pulses)            */
 } ffbp_tc_opts;
 
 /* One level of the plan (fastsar/ffbp2.py:192-250, make_plan's per-level record). All pointers are host memory. */

@@ -148,7 +148,7 @@ def _run_level_tc(lib, x, c0, sl, fk, fp, Ko, Po, Dk, Dp, window=None, bad=None,
     if opts is None:
         lib.check(L.ffbp_level_tc(*args, s), 'ffbp_level_tc')
     else:
-        o = lib.TcOpts(*(int(opts.get(k, 0)) for k in ('nt', 'sb', 'copies', 'repeat')))
+        o = lib.TcOpts(*(int(opts.get(k, 0)) for k in ('nt', 'sb', 'copies', 'repeat', 'fir')))
         lib.check(L.ffbp_level_tc_ex(*args, ctypes.byref(o), s), 'ffbp_level_tc_ex')
     torch.cuda.synchronize()
     return out.cpu().numpy(), status.cpu().numpy()
@@ -170,19 +170,21 @@ TC_LEVEL_CASES = [
 ]
 
 
+@pytest.mark.parametrize('fir', [0, 2], ids=['fir-default', 'fir-tensor-cores'])
 @pytest.mark.parametrize('case', TC_LEVEL_CASES,
                          ids=[f'Np{c[0]}-P{c[1]}-K{c[2]}-C{c[3]}-Dk{c[4]}-Dp{c[5]}' for c in TC_LEVEL_CASES])
-def test_level_tensor_cores_match_oracle(lib, oracle_lib, case):
+def test_level_tensor_cores_match_oracle(lib, oracle_lib, case, fir):
     """The tensor-core level against the float64 oracle of the reference's rot_fir_k + fir_p: the products in split
     bfloat16 (about 2^-16) and the float16 intermediate (11 significant bits) leave a relative error near 2^-12;
-    the bar is 1e-3 (-60 dB). The output's largest component is recorded exactly."""
+    the bar is 1e-3 (-60 dB). The output's largest component is recorded exactly. The pulse FIR on its default
+    kernel (the CUDA cores at these sizes) and on the tensor cores (a banded product with float16 hi + lo taps)."""
     Np, P, K, C, Dk, Dp, pk = case
     rng = np.random.default_rng(sum(case[:6]) + 11)
     x, c0, sl, fk, fp, Ko, Po = _level_case(rng, Np, P, K, C, Dk, Dp, pk=pk)
-    got, st = _run_level_tc(lib, x, c0, sl, fk, fp, Ko, Po, Dk, Dp)
+    got, st = _run_level_tc(lib, x, c0, sl, fk, fp, Ko, Po, Dk, Dp, opts=dict(fir=fir) if fir else None)
     ref = _oracle_level_full(oracle_lib, x, c0, sl, fk, fp, Ko, Po, Dk, Dp)
     e = _rel(got, ref)
-    print(f'tensor-core level {case}: rel {e:.2e} ({20 * np.log10(e):.1f} dB)')
+    print(f'tensor-core level {case} fir {fir}: rel {e:.2e} ({20 * np.log10(e):.1f} dB)')
     assert st[0] == 0
     assert e < 1e-3, e
     amax_out = np.frombuffer(np.int32(st[2]).tobytes(), np.float32)[0]
@@ -197,17 +199,21 @@ TC_OPTS_CASES = [TC_LEVEL_CASES[i] for i in (0, 4, 6, 7, 10)]
 @pytest.mark.parametrize('case', TC_OPTS_CASES,
                          ids=[f'Np{c[0]}-P{c[1]}-K{c[2]}-C{c[3]}-Dk{c[4]}-Dp{c[5]}' for c in TC_OPTS_CASES])
 def test_level_tensor_cores_launch_options_same_bits(lib, case):
-    """The first pass's launch options (ffbp_tc_opts: columns per tile, B stages, plane copies, row repeat) change
-    the schedule, not the arithmetic: plane copies and B stages give the default's output bit for bit; columns per
-    tile and the row repeat move the points where the consumers seed the output ramp's recurrence (about 1e-7), which
-    can flip a rounding of the float16 intermediate (one unit: 5e-4 of that value): within 1e-4 of the default; a set
-    that does not fit is refused with FFBP_E_UNSUPPORTED (ValueError)."""
+    """The launch options (ffbp_tc_opts: columns per tile, B stages, plane copies, row repeat, the pulse FIR's
+    kernel) change the schedule, not the arithmetic: plane copies and B stages give the default's output bit for bit;
+    columns per tile and the row repeat move the points where the consumers seed the output ramp's recurrence (about
+    1e-7), which can flip a rounding of the float16 intermediate (one unit: 5e-4 of that value), and the two pulse
+    FIR kernels sum in different orders (the tensor cores with the taps as float16 hi + lo): within 1e-4 of the
+    default; a set that does not fit is refused with FFBP_E_UNSUPPORTED (ValueError)."""
     Np, P, K, C, Dk, Dp, pk = case
     rng = np.random.default_rng(sum(case[:6]) + 11)
     x, c0, sl, fk, fp, Ko, Po = _level_case(rng, Np, P, K, C, Dk, Dp, pk=pk)
     want, _ = _run_level_tc(lib, x, c0, sl, fk, fp, Ko, Po, Dk, Dp)
+    AP = -(-(fp['L'] if fp else 1) // Dp)
+    default_fir = 2 if (Po >= 512 or AP > 12) else 1            # the launcher's default for the pulse FIR's kernel
     sets = [dict(copies=4), dict(copies=2), dict(nt=32), dict(nt=64, copies=4), dict(nt=96), dict(nt=128, sb=2),
-            dict(sb=3), dict(repeat=1, nt=16), dict(repeat=1, nt=48, copies=4), dict(repeat=1, nt=80), dict(nt=48)]
+            dict(sb=3), dict(repeat=1, nt=16), dict(repeat=1, nt=48, copies=4), dict(repeat=1, nt=80), dict(nt=48),
+            dict(fir=1), dict(fir=2), dict(fir=1, copies=4)]
     ran = 0
     for o in sets:
         try:
@@ -216,13 +222,29 @@ def test_level_tensor_cores_launch_options_same_bits(lib, case):
             assert 'columns per tile' in str(e) or 'B stages' in str(e), (o, str(e))
             continue
         assert st[0] == 0
-        if set(o) <= {'copies', 'sb'}:
+        if set(o) <= {'copies', 'sb'} or (o == dict(fir=default_fir)):
             assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), o
         else:
             assert _rel(got, want) < 1e-4, (o, _rel(got, want))
         ran += 1
     print(f'{case}: {ran} of {len(sets)} option sets ran')
     assert ran >= 5
+
+
+def test_level_tensor_cores_long_pulse_filter(lib, oracle_lib):
+    """A pulse filter spanning more than 12 output pulses (Dp 2, pass fraction 0.9: 45 outputs per input pulse), which
+    only the tensor-core pulse FIR takes (the launcher's default there), against the float64 oracle; the CUDA-core
+    kernel refuses it with FFBP_E_UNSUPPORTED."""
+    rng = np.random.default_rng(21)
+    x, c0, sl, fk, fp, Ko, Po = _level_case(rng, 2, 120, 300, 8, 3, 2, pp=0.9)
+    assert -(-fp['L'] // 2) > 12
+    got, st = _run_level_tc(lib, x, c0, sl, fk, fp, Ko, Po, 3, 2)
+    ref = _oracle_level_full(oracle_lib, x, c0, sl, fk, fp, Ko, Po, 3, 2)
+    e = _rel(got, ref)
+    print(f'long pulse filter (Lp {fp["L"]}): rel {e:.2e}')
+    assert st[0] == 0 and e < 1e-3
+    with pytest.raises(ValueError, match='12 output pulses'):
+        _run_level_tc(lib, x, c0, sl, fk, fp, Ko, Po, 3, 2, opts=dict(fir=1))
 
 
 def test_level_tensor_cores_window_nonfinite_and_limits(lib, oracle_lib):
