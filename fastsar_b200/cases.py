@@ -1,7 +1,7 @@
 """A profiling harness, not part of the former's API: single-stage cases of a workload's plan, for timing one kernel
 at a time and for small profiler captures (the commands of profiles/*.md run it):
 
-    python -m fastsar_b200.cases level L1 [--parents 8] [--pulses 2048] [--form tc|fused|fp32] [--taps learned|80|70]
+    python -m fastsar_b200.cases level L1 [--parents 8] [--pulses 2048] [--form tc|fused|fp32] [--fir 0|1|2] [--taps learned|80|70]
     python -m fastsar_b200.cases final [--tiles 20000] [--mode f16|bf16x3|fp32] [--taps learned|80|70]
     python -m fastsar_b200.cases exact [--workload spotlight_4k] [--interp cubic|linear] [--pulses 1024]
 
@@ -15,6 +15,7 @@ The defaults are the 16,384 x 8,192 -> 12,288 x 8,832 spotlight (workload spotli
 (learned taps, pmax 0.5); --pmax 0.4 --taps 70 gives the reference's plan.
 """
 import argparse
+import ctypes
 
 import numpy as np
 
@@ -39,7 +40,7 @@ def workload_plan(name='spotlight_12k', taps='learned', pmax=0.5):
                               e1=w['e1'], e2=w['e2'], taps=model)
 
 
-def level_case(level, parents, pulses=0, form='tc', taps='learned', reps=3, seed=1, pmax=0.5):
+def level_case(level, parents, pulses=0, form='tc', taps='learned', reps=3, seed=1, pmax=0.5, fir=0):
     import torch
     L = _lib.load()
     w, pl = workload_plan(taps=taps, pmax=pmax)
@@ -73,9 +74,11 @@ def level_case(level, parents, pulses=0, form='tc', taps='learned', reps=3, seed
                                           fk['pl'], Dk, Ko, (K - 1) / 2.0, tp.data_ptr(), fp['L'], fp['pl'], Dp, Po,
                                           None, None, out.data_ptr(), None, st.data_ptr(), s), 'ffbp_level_fused')
         elif form == 'tc':
-            _lib.check(L.ffbp_level_tc(x.data_ptr(), parents, P, K, ph.data_ptr(), C, tk.data_ptr(), fk['L'], fk['pl'],
-                                       Dk, Ko, (K - 1) / 2.0, tp.data_ptr(), fp['L'], fp['pl'], Dp, Po, None, None,
-                                       out.data_ptr(), None, scr.data_ptr(), nb, st.data_ptr(), s), 'ffbp_level_tc')
+            o = _lib.TcOpts(0, 0, 0, 0, int(fir))
+            _lib.check(L.ffbp_level_tc_ex(x.data_ptr(), parents, P, K, ph.data_ptr(), C, tk.data_ptr(), fk['L'],
+                                          fk['pl'], Dk, Ko, (K - 1) / 2.0, tp.data_ptr(), fp['L'], fp['pl'], Dp, Po, None,
+                                          None, out.data_ptr(), None, scr.data_ptr(), nb, st.data_ptr(),
+                                          ctypes.byref(o), s), 'ffbp_level_tc_ex')
         else:
             _lib.check(L.ffbp_level(x.data_ptr(), parents, P, K, ph.data_ptr(), C, tk.data_ptr(), fk['L'], fk['pl'], Dk,
                                     Ko, (K - 1) / 2.0, tp.data_ptr(), fp['L'], fp['pl'], Dp, Po, None, None,
@@ -160,6 +163,8 @@ def main(argv=None):
     ap.add_argument('--parents', type=int, default=8)
     ap.add_argument('--pulses', type=int, default=0)
     ap.add_argument('--form', choices=('tc', 'fused', 'fp32'), default='tc')
+    ap.add_argument('--fir', type=int, choices=(0, 1, 2), default=0,
+                    help="tc: the pulse FIR's kernel (0 the launcher's default, 1 CUDA cores, 2 tensor cores)")
     ap.add_argument('--tiles', type=int, default=20000)
     ap.add_argument('--mode', choices=('f16', 'bf16x3', 'fp32'), default='f16')
     ap.add_argument('--taps', default='learned', help="'learned' or a Kaiser-sinc attenuation in dB (70, 80)")
@@ -171,7 +176,7 @@ def main(argv=None):
     if a.stage == 'exact':
         exact_case(a.workload, a.interp, a.pulses or 1024, a.reps)
     elif a.stage == 'level':
-        level_case(int(a.level[1]), a.parents, a.pulses, a.form, a.taps, a.reps, pmax=a.pmax)
+        level_case(int(a.level[1]), a.parents, a.pulses, a.form, a.taps, a.reps, pmax=a.pmax, fir=a.fir)
     else:
         final_case(a.tiles, a.mode, a.taps, a.reps, pmax=a.pmax)
 

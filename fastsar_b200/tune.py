@@ -7,6 +7,9 @@ with CUDA events and keep the fastest. No counterpart in the reference, which pl
 
 make(**kwargs) -> ImageFormer; candidates: a list of kwargs; S_dev: the patch's history on the device.
 """
+import json
+import os
+
 import numpy as np
 
 from . import plan as _plan
@@ -84,13 +87,51 @@ def tune_former(make, candidates, S_dev, target_db=-60.0, reps=3):
 
 # ------------------------------------------------------------------------------------------- level launch options
 
+# Tuned launch options by level signature. Seeded from the packaged file (fastsar_b200/data/level_opts.json, made by
+# `python -m fastsar_b200.tune --workload ...` on a B200) or from FASTSAR_TUNE_CACHE when set, which also receives
+# every new result; in-process otherwise.
 _LEVEL_CACHE = {}
+_CACHE_LOADED = False
+PACKAGED_CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'data', 'level_opts.json')
+
+
+def _cache_path():
+    return os.environ.get('FASTSAR_TUNE_CACHE') or None
+
+
+def _key(sig):
+    return ','.join(str(v) for v in sig)
+
+
+def _load_cache():
+    global _CACHE_LOADED
+    if _CACHE_LOADED:
+        return
+    _CACHE_LOADED = True
+    for path in (PACKAGED_CACHE, _cache_path()):
+        if path and os.path.exists(path):
+            with open(path) as f:
+                for k, v in json.load(f).get('levels', {}).items():
+                    _LEVEL_CACHE[tuple(int(x) for x in k.split(','))] = v
+
+
+def _save_cache(path):
+    doc = dict(device='B200 (sm_100a)', note='tensor-core level launch options by level signature: parents, children, '
+               'frequency decimation, frequency taps, input samples, input pulses, output samples, output pulses, '
+               'pulse decimation, pulse taps (fastsar_b200.tune.level_signature)',
+               levels={_key(k): v for k, v in sorted(_LEVEL_CACHE.items()) if v is not None})
+    tmp = path + '.tmp'
+    with open(tmp, 'w') as f:
+        json.dump(doc, f, indent=1, sort_keys=True)
+    os.replace(tmp, path)
 
 
 def level_signature(lv, Np):
-    """What the first pass of a tensor-core level's timing depends on: its shapes and filter lengths."""
+    """What a tensor-core level's timing depends on: its shapes and filter lengths."""
     Lk = lv['fir_k']['L'] if lv['fir_k'] is not None else 1
-    return (int(Np), int(lv['C']), int(lv['Dk']), int(Lk), int(lv['K']), int(lv['P']), int(lv['Ko']))
+    Lp = lv['fir_p']['L'] if lv['fir_p'] is not None else 1
+    return (int(Np), int(lv['C']), int(lv['Dk']), int(Lk), int(lv['K']), int(lv['P']), int(lv['Ko']), int(lv['Po']),
+            int(lv['Dp']), int(Lp))
 
 
 def _level_candidates(C, Lk):
@@ -112,6 +153,7 @@ def tune_level(lv, Np, reps=3, max_parents=1024, seed=0):
     import ctypes
     import torch
     from . import _lib
+    _load_cache()
     key = level_signature(lv, Np)
     if key in _LEVEL_CACHE:
         return _LEVEL_CACHE[key], []
@@ -192,6 +234,8 @@ def tune_level(lv, Np, reps=3, max_parents=1024, seed=0):
         del x, ph, out, scr
         torch.cuda.empty_cache()
     _LEVEL_CACHE[key] = best
+    if _cache_path():
+        _save_cache(_cache_path())
     return best, table
 
 
@@ -210,3 +254,41 @@ def tune_levels(plan, reps=3):
         chosen.append(opts)
         Np *= int(lv['C'])
     return chosen
+
+
+def main():
+    """python -m fastsar_b200.tune --workload spotlight_12k [--out path] [--reps 5]: time the launch options of the
+    chosen form's tensor-core levels (precision float16, learned taps, pmax 0.5) for a named workload's plan and
+    write them, with whatever the cache already held, to `out` (default: the packaged file)."""
+    import argparse
+    from . import sim, learned
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--workload', action='append', required=True)
+    ap.add_argument('--out', default=PACKAGED_CACHE)
+    ap.add_argument('--reps', type=int, default=5)
+    ap.add_argument('--max-parents', type=int, default=4096)
+    a = ap.parse_args()
+    _load_cache()
+    taps = learned.LearnedTaps.load()
+    for name in a.workload:
+        w = sim.workload(name)
+        col = w['col']
+        T, _ = _plan.choose_T(col.ant, col.fmin + col.K * col.df, w['nx'], w['ny'], w['spx'], w['spy'], w['e1'],
+                              w['e2'], -40.0)
+        pl = _plan.make_plan(col, w['nx'], w['ny'], w['spx'], w['spy'], T=T, nlev=3, pmax=0.5, atten=80.0,
+                             e1=w['e1'], e2=w['e2'], taps=taps)
+        Np = 1
+        for i, lv in enumerate(pl['levels']):
+            key = level_signature(lv, Np)
+            _LEVEL_CACHE.pop(key, None)
+            opts, table = tune_level(lv, Np, reps=a.reps, max_parents=a.max_parents)
+            print(f'{name} level {i} {key}: {opts}')
+            for o, ms in table:
+                print(f'    {o}: {ms if isinstance(ms, str) else f"{ms:.3f} ms"}')
+            Np *= int(lv['C'])
+    _save_cache(a.out)
+    print('wrote', a.out)
+
+
+if __name__ == '__main__':
+    main()

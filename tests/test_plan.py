@@ -166,3 +166,30 @@ def test_final_weights_match_reference(golden):
     np.testing.assert_allclose(P_.final_weights(plan, w, P), g['w_plain'], rtol=1e-6, atol=1e-7)
     np.testing.assert_allclose(P_.final_weights(plan, w, P, nodes=1), g['w_centre'], rtol=1e-6, atol=1e-7)
     np.testing.assert_allclose(P_.final_weights(plan, w, P, grad=True), g['w_grad'], rtol=1e-5, atol=1e-7)
+
+
+def test_packaged_level_options_cache_is_well_formed(tmp_path, monkeypatch):
+    """The packaged tuning cache (fastsar_b200/data/level_opts.json, written by python -m fastsar_b200.tune): every
+    key a level signature of 10 integers, every value a dict of ffbp_tc_opts fields with values the launcher takes;
+    and a cache written through FASTSAR_TUNE_CACHE reads back the same."""
+    import json
+    from fastsar_b200 import tune
+    doc = json.load(open(tune.PACKAGED_CACHE))
+    assert doc['levels']
+    for k, v in doc['levels'].items():
+        assert len([int(x) for x in k.split(',')]) == 10
+        assert set(v) <= {'nt', 'sb', 'copies', 'repeat', 'fir'}
+        assert v.get('copies', 2) in (2, 4) and v.get('fir', 1) in (1, 2) and v.get('repeat', 0) in (0, 1)
+        assert v.get('nt', 16) % 16 == 0 and 2 <= v.get('sb', 2) <= 4
+    monkeypatch.setattr(tune, '_LEVEL_CACHE', {})
+    monkeypatch.setattr(tune, '_CACHE_LOADED', False)
+    tune._load_cache()
+    assert len(tune._LEVEL_CACHE) == len(doc['levels'])
+    path = str(tmp_path / 'cache.json')
+    tune._LEVEL_CACHE[(1, 2, 3, 4, 5, 6, 7, 8, 9, 10)] = dict(nt=64, fir=2)
+    tune._save_cache(path)
+    monkeypatch.setenv('FASTSAR_TUNE_CACHE', path)
+    monkeypatch.setattr(tune, '_LEVEL_CACHE', {})
+    monkeypatch.setattr(tune, '_CACHE_LOADED', False)
+    tune._load_cache()
+    assert tune._LEVEL_CACHE[(1, 2, 3, 4, 5, 6, 7, 8, 9, 10)] == dict(nt=64, fir=2)
