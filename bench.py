@@ -697,7 +697,7 @@ def run_learned(args):
             f = ImageFormer(col.ant, col.fmin, col.df, col.K, nx, ny, w['spx'], w['spy'], w['e1'], w['e2'],
                             taps=taps, atten=atten, pmax=pmax)
             f.form_device(S, out)
-        except (ValueError, RuntimeError) as e:
+        except (ValueError, RuntimeError, MemoryError) as e:
             # a plan the float32 former cannot form (the level kernel's limits: 256 frequency taps, a pulse filter
             # spanning 16 output pulses) or whose workspace does not fit the device
             rows.append(dict(taps=taps, atten=atten, pmax=pmax, oversampling=round(1.0 / pmax, 2), error=str(e)[:100]))

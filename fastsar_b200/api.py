@@ -188,7 +188,19 @@ class DevicePlan:
     def workspace(self):
         import torch
         if self._ws is None:
-            self._ws = torch.empty(self.ws_bytes + 256, dtype=torch.uint8, device=self.device)
+            try:
+                self._ws = torch.empty(self.ws_bytes + 256, dtype=torch.uint8, device=self.device)
+            except torch.OutOfMemoryError:
+                free, total = torch.cuda.mem_get_info(self.device)
+                lv = self.plan['levels']
+                raise MemoryError(
+                    f'the plan needs {self.ws_bytes / 2**30:.1f} GiB of device workspace (the levels\' outputs and '
+                    f'the tensor-core levels\' float16 intermediate) and {free / 2**30:.1f} of {total / 2**30:.1f} GiB '
+                    f'are free on {self.device}; first-level children {lv[0]["C"]}, output samples per level '
+                    f'{[l["Ko"] for l in lv]}, pulses {[l["Po"] for l in lv]}. Remedies: a smaller pmax (less '
+                    'oversampling per level) or more levels, forming the image in parts (patches, or shard.ShardedFormer '
+                    'over several GPUs), the range gate for an image narrow in range (range_gate=True), or freeing '
+                    'other device memory') from None
         off = (-self._ws.data_ptr()) % 256
         return self._ws.data_ptr() + off
 

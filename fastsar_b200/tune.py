@@ -64,7 +64,7 @@ def tune_former(make, candidates, S_dev, target_db=-60.0, reps=3):
             continue
         try:
             ms = time_former(f, S_dev, reps)
-        except (ValueError, RuntimeError) as e:      # a shape a kernel refuses (FFBP_E_UNSUPPORTED), or an abort
+        except (ValueError, RuntimeError, MemoryError) as e:   # a shape a kernel refuses, an abort, no memory
             table.append((kw, err, f'not formed: {str(e)[:60]}'))
             f.release()
             del f

@@ -96,3 +96,18 @@ def test_transfer_that_did_not_deliver_is_reported(golden):
         f.form_many(pinned)
     got = f.form_many(pinned)
     assert all(np.array_equal(a, b) for a, b in zip(got, want))
+
+
+def test_workspace_that_does_not_fit_names_remedies():
+    """A plan whose workspace exceeds the device (learned taps at pmax 0.95 on the 4,096-pulse spotlight: the
+    Kaiser-sinc fallback's long filters and nearly no decimation ask for hundreds of GiB) raises MemoryError naming
+    the sizes and the remedies, before any kernel runs, and leaves the device usable."""
+    from fastsar_b200 import ImageFormer, sim
+    w = sim.workload('spotlight_4k')
+    col = w['col']
+    f = ImageFormer(col.ant, col.fmin, col.df, col.K, w['nx'], w['ny'], w['spx'], w['spy'], w['e1'], w['e2'],
+                    taps='learned', atten=80.0, pmax=0.95)
+    S = torch.zeros((col.Np, col.K), dtype=torch.complex64, device='cuda')
+    with pytest.raises(MemoryError, match='Remedies'):
+        f.form_device(S)
+    assert torch.zeros(4, device='cuda').sum().item() == 0.0
