@@ -32,7 +32,8 @@ _c_int, _c_double, _vp = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
 
 class TcOpts(ctypes.Structure):
     """ffbp_tc_opts: launch options of a tensor-core level's first pass (0 keeps a field's default)."""
-    _fields_ = [('nt', _c_int), ('sb', _c_int), ('copies', _c_int), ('repeat', _c_int), ('fir', _c_int)]
+    _fields_ = [('nt', _c_int), ('sb', _c_int), ('copies', _c_int), ('repeat', _c_int), ('fir', _c_int),
+                ('consumers', _c_int)]
 
 
 class LevelDesc(ctypes.Structure):

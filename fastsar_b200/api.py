@@ -152,8 +152,8 @@ class DevicePlan:
             if i == 0 and ref is not None:
                 d.h_range = k64(ref)
             tc = lv.get('tc') or {}
-            d.tc.nt, d.tc.sb, d.tc.copies, d.tc.repeat, d.tc.fir = (int(tc.get(k, 0))
-                                                                    for k in ('nt', 'sb', 'copies', 'repeat', 'fir'))
+            d.tc.nt, d.tc.sb, d.tc.copies, d.tc.repeat, d.tc.fir, d.tc.consumers = (
+                int(tc.get(k, 0)) for k in ('nt', 'sb', 'copies', 'repeat', 'fir', 'consumers'))
         fin = plan['final']
         pd = _lib.PlanDesc()
         pd.nlev, pd.levels = len(plan['levels']), ctypes.cast(lvs, ctypes.POINTER(_lib.LevelDesc))
@@ -329,7 +329,7 @@ class ImageFormer:
     learned decimation taps, fastsar_b200.learned: 8-output-sample filters where the network covers a level's
     decimation and pass fraction, Kaiser-sinc ones elsewhere) or a LearnedTaps instance. tune_levels (an extension):
     with precision='float16', time the tensor-core levels' launch options (columns per tile, operand stages, plane
-    copies, row repeat, the pulse FIR on the tensor or the CUDA cores) per level shape on the GPU when the former is
+    copies, row repeat, consumer warps, the pulse FIR on the tensor or the CUDA cores) per level shape on the GPU when the former is
     built (fastsar_b200.tune.tune_levels; cached
     per shape in the process); the choice changes the image at the rounding level only (about 1e-5 relative: a
     float16 rounding of the intermediate flipped here and there)."""

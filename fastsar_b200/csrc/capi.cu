@@ -449,6 +449,7 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
         L.amax = amax + l + 1;
         L.test_wait_ns = p->test_kind == FFBP_KIND_LEVEL_TC ? p->test_ns : 0u;
         L.tc_nt = v.tc.nt; L.tc_sb = v.tc.sb; L.tc_pc = v.tc.copies; L.tc_rp = v.tc.repeat; L.tc_fir = v.tc.fir;
+        L.tc_cw = v.tc.consumers;
         const char *why = nullptr;
         const int form = level_form(p, l);
         if (form == 1) {
@@ -855,7 +856,10 @@ int ffbp_level_tc_ex(const void *d_x, int Np, int P, int K, const void *d_phase,
     L.wp = d_wp; L.wk = d_wk; L.out = static_cast<float2 *>(d_out); L.bad = d_bad;
     L.Np = Np; L.C = C; L.P = P; L.K = K; L.Ko = Ko; L.Po = Po; L.Dk = Dk; L.Lk = Lk; L.plk = plk; L.Dp = Dp;
     L.Lp = Lp; L.plp = plp; L.kc = kc; L.amax = d_status + 2;
-    if (opts) { L.tc_nt = opts->nt; L.tc_sb = opts->sb; L.tc_pc = opts->copies; L.tc_rp = opts->repeat; L.tc_fir = opts->fir; }
+    if (opts) {
+        L.tc_nt = opts->nt; L.tc_sb = opts->sb; L.tc_pc = opts->copies; L.tc_rp = opts->repeat; L.tc_fir = opts->fir;
+        L.tc_cw = opts->consumers;
+    }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaError_t e = ffbp::launch_amax(L.x, (size_t)Np * P * K, d_status + 1, s);
     if (e != cudaSuccess) return cuda_fail(e, "ffbp_level_tc");

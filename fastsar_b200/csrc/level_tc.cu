@@ -213,9 +213,13 @@ __device__ __forceinline__ float y_scale(const int *amax)
     return ldexpf(1.f, 13 - ex);
 }
 
-template <int NKC, int PC>
+template <int NKC, int PC, int CW>
 __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
 {
+    // CW consumer warps (8, or 4 where the consumers idle and the Hankel copies bound the stage), the other warps'
+    // roles after them: 4 A', 4 planes, 16 - CW Hankel rows, the MMA issuer last (warp 24)
+    constexpr int NCW_ = CW, NHW_ = NBW + NCW - CW - NLW, NHT_ = NHW_ * 32;
+    static_assert(NCW_ + NAW + NLW + NHW_ == MMAW, "warp roles");
     extern __shared__ __align__(1024) unsigned char smem[];
     constexpr int nkc = NKC;                                 // core matrices along K (Lkp = 8 NKC)
     const uint32_t apart = 128u * a.Lkp * 2u;                // one part (hi or lo) of A'
@@ -253,15 +257,15 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             mbar_init(&afull[i], NAW);
             mbar_init(&aempty[i], 1);
             mbar_init(&dfull[i], 1);
-            mbar_init(&dempty[i], NCW);
+            mbar_init(&dempty[i], NCW_);
         }
         for (int i = 0; i < a.SB; ++i) {
-            mbar_init(&bfull[i], NHW);
+            mbar_init(&bfull[i], NHW_);
             mbar_init(&bempty[i], 1);
         }
         for (int i = 0; i < 2; ++i) {
             mbar_init(&pfull[i], NLT);
-            mbar_init(&pempty[i], NHT);
+            mbar_init(&pempty[i], NHT_);
         }
         mbar_init(&s_never, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -280,11 +284,11 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
     const uint32_t tmem = s_tmem;
     const float scale = s_scale;
 
-    if (warp >= NCW && warp < NCW + NAW) {
+    if (warp >= NCW_ && warp < NCW_ + NAW) {
         // ------------------------------------------------------------------ A' producers
         // the modulated taps of each pulse into A' buffer pulse & 1, a pulse ahead of the B' producers (the
         // buffer is free once the MMAs of the pulse two back have completed); no named barrier
-        const int at = t - NCW * 32;
+        const int at = t - NCW_ * 32;
         const float2 *__restrict__ phn = a.ph + (size_t)n * a.C * a.P;
         // the children's phases of each pulse are copied into s_ph a pulse ahead (cp.async, thread c: child c), so
         // that no item waits on a global load; after a failed wait a thread keeps stepping through the pulses (and
@@ -349,9 +353,9 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             if (lane == 0) mbar_arrive(&afull[ab]);
         }
         asm volatile("cp.async.wait_all;" ::: "memory");
-    } else if (warp >= NCW + NAW && warp < NCW + NAW + NLW) {
+    } else if (warp >= NCW_ + NAW && warp < NCW_ + NAW + NLW) {
         // ------------------------------------------------------------------ B' producers: planes
-        const int pt = t - (NCW + NAW) * 32;
+        const int pt = t - (NCW_ + NAW) * 32;
         const float2 *__restrict__ xn = a.x + (size_t)n * a.P * a.K;
         const int npair = (a.W + 1) / 2;                      // window samples in pairs (2i, 2i + 1)
         // the window of stage (pulse p, tile tt): samples k = kb + i, kb = Dk Nt tt - plk, i < W, copied XS - 1
@@ -427,7 +431,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             }
         }
         asm volatile("cp.async.wait_all;" ::: "memory");
-    } else if (warp >= NCW + NAW + NLW && warp < MMAW) {
+    } else if (warp >= NCW_ + NAW + NLW && warp < MMAW) {
         // ------------------------------------------------------------------ B' producers: Hankel rows
         int sb = 0;
         uint32_t sbpar = 0;
@@ -441,14 +445,14 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             const uint32_t *plb = pl + (s & 1) * 4 * PC * (Wp / 2);
             {
                 // lane (r8 = lane % 8, uq = lane / 8) keeps its row within a block of 8 and its K chunk within a
-                // group of 4; warp pw takes the row blocks pw, pw + NHW, ... of each (part, re/im, chunk group).
+                // group of 4; warp pw takes the row blocks pw, pw + NHW_, ... of each (part, re/im, chunk group).
                 // Along a warp's row blocks the window offset, the plane copy and the store move by constants.
                 constexpr int UB = (NKC + 3) / 4;
-                const int r8 = lane & 7, uq = lane >> 3, pw = warp - NCW - NAW - NLW;
+                const int r8 = lane & 7, uq = lane >> 3, pw = warp - NCW_ - NAW - NLW;
                 const int nrb = a.Nt / 8;
-                const int nmine = nrb > pw ? (nrb - 1 - pw) / NHW + 1 : 0;
-                const int ostep = 8 * NHW * a.Dk, wstep = ostep >> 1;               // ostep: a multiple of 8
-                const uint32_t bstep = (uint32_t)(NHW * nkc * 128);
+                const int nmine = nrb > pw ? (nrb - 1 - pw) / NHW_ + 1 : 0;
+                const int ostep = 8 * NHW_ * a.Dk, wstep = ostep >> 1;               // ostep: a multiple of 8
+                const uint32_t bstep = (uint32_t)(NHW_ * nkc * 128);
 #pragma unroll
                 for (int ub = 0; ub < UB; ++ub) {
                     const int u = ub * 4 + uq;
@@ -522,7 +526,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             // chunk: each thread forms re/im of its two children at two columns with no exchange between threads.
             const int q = warp & 3, g = warp >> 2;
             const int cc = 16 * q + (lane >> 2), jl = 2 * (lane & 3);
-            const int cw = a.Nt / (NCW / 4);                      // columns of this warp per tile
+            const int cw = a.Nt / (NCW_ / 4);                      // columns of this warp per tile
             // child cc + 8 h's phases and intermediate rows (child 0's for a child past the last, whose results are
             // not stored)
             auto phc = [&](int h) {
@@ -610,8 +614,8 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             const int c = 16 * (rp == 2 ? (q & 1) : q) + (lane >> 1);   // this lane's child (rows 2c: Mr, 2c + 1: Mi)
             const bool odd = lane & 1;
             const bool live = c < a.C;
-            const int cw = a.Nt / (NCW / 4) / rp;                 // columns of this warp per tile (a multiple of 8)
-            const int cofs = (rp == 2 ? g + 2 * (q >> 1) : g) * cw;   // this warp's first column within the tile
+            const int cw = a.Nt / (NCW_ / 4) / rp;                 // columns of this warp per tile (a multiple of 8)
+            const int cofs = (rp == 2 ? g + (NCW_ / 4) * (q >> 1) : g) * cw;   // this warp's first column in the tile
             const float2 *__restrict__ phc = a.ph + ((size_t)n * a.C + (live ? c : 0)) * a.P;
             __half2 *__restrict__ yc = a.y + ((size_t)n * a.C + (live ? c : 0)) * a.P * a.Kop;
             // the child's phase (c0, sl) of the current pulse, and of the next one loaded a pulse ahead
@@ -896,12 +900,14 @@ cudaError_t launch_level_tc_gemm(const LevelLaunch &L, const int *amax_in, void 
     const int pc = L.tc_pc == 4 ? 4 : 2;
     if (L.tc_pc != 0 && L.tc_pc != 2 && L.tc_pc != 4) { *why = "plane copies: 2 or 4"; return cudaErrorNotSupported; }
     a.rp = (a.Lkp > 32 && L.C <= 32 && L.tc_rp != 1) ? 2 : 1;
-    const int unit = a.rp == 2 ? 32 : 16;                    // the consumers' column split: 8-column chunks per warp
+    if (L.tc_cw != 0 && L.tc_cw != 4 && L.tc_cw != 8) { *why = "consumer warps: 4 or 8"; return cudaErrorNotSupported; }
+    const int cw = L.tc_cw == 4 ? 4 : 8;
+    const int unit = (cw == 8 && a.rp == 2) ? 32 : 16;       // the consumers' column split: 8-column chunks per warp
     auto need = [&](int nt, int sb) { return gemm_smem(a.Lkp, a.Dk, nt, sb, pc); };
     int best = 0;
     if (L.tc_nt) {
         if (L.tc_nt % unit || L.tc_nt > 128 || need(L.tc_nt, 2) > avail) {
-            *why = "columns per tile: a multiple of 16 (32 with repeated rows) up to 128 whose operands fit shared memory";
+            *why = "columns per tile: a multiple of 16 (32 with repeated rows and 8 consumer warps) up to 128 whose operands fit shared memory";
             return cudaErrorNotSupported;
         }
         best = L.tc_nt;
@@ -944,7 +950,9 @@ cudaError_t launch_level_tc_gemm(const LevelLaunch &L, const int *amax_in, void 
         return cudaGetLastError();
     };
     cudaError_t e;
-#define FFBP_GEMM_RUN(N) (pc == 4 ? run(level_tc_gemm<N, 4>) : run(level_tc_gemm<N, 2>))
+#define FFBP_GEMM_RUN(N)                                                                                     \
+    (cw == 4 ? (pc == 4 ? run(level_tc_gemm<N, 4, 4>) : run(level_tc_gemm<N, 2, 4>))                         \
+             : (pc == 4 ? run(level_tc_gemm<N, 4, 8>) : run(level_tc_gemm<N, 2, 8>)))
     switch (a.Lkp / 8) {
         case 2: e = FFBP_GEMM_RUN(2); break;
         case 4: e = FFBP_GEMM_RUN(4); break;

@@ -136,12 +136,13 @@ def level_signature(lv, Np):
 
 def _level_candidates(C, Lk):
     """Launch option sets of a tensor-core level in the order a coordinate search visits them: the pulse FIR's kernel
-    (CUDA or tensor cores), plane copies, then columns per tile (multiples of 32 with repeated A rows, of 16 without),
-    then the row repeat off, then the B stages."""
+    (CUDA or tensor cores), plane copies, consumer warps (8, or 4 with 12 Hankel-row warps), then columns per tile
+    (multiples of 32 with repeated A rows and 8 consumer warps, of 16 otherwise), then the row repeat off, then the B
+    stages."""
     Lkp = ((max(Lk, 1) + 15) // 16) * 16
     rep_ok = Lkp > 32 and C <= 32
-    return dict(fir=[1, 2], copies=[2, 4], nt=list(range(32, 129, 32)), nt16=list(range(16, 129, 16)),
-                repeat_off=rep_ok, sb=[2, 3, 4])
+    return dict(fir=[1, 2], copies=[2, 4], consumers=[8, 4], nt=list(range(32, 129, 32)),
+                nt16=list(range(16, 129, 16)), repeat_off=rep_ok, sb=[2, 3, 4])
 
 
 def tune_level(lv, Np, reps=3, max_parents=1024, seed=0):
@@ -177,7 +178,7 @@ def tune_level(lv, Np, reps=3, max_parents=1024, seed=0):
     ptr = lambda t: None if t is None else t.data_ptr()
 
     def run(o):
-        opts = _lib.TcOpts(o.get('nt', 0), o.get('sb', 0), o.get('copies', 0), o.get('repeat', 0), o.get('fir', 0))
+        opts = _lib.TcOpts(*(int(o.get(k, 0)) for k in ('nt', 'sb', 'copies', 'repeat', 'fir', 'consumers')))
         _lib.check(L.ffbp_level_tc_ex(x.data_ptr(), n, P, K, ph.data_ptr(), C, ptr(tk), Lk,
                                       fk['pl'] if fk is not None else 0, Dk, Ko, (K - 1) / 2.0, ptr(tp),
                                       fp['L'] if fp is not None else 1, fp['pl'] if fp is not None else 0, Dp, Po,
@@ -223,7 +224,9 @@ def tune_level(lv, Np, reps=3, max_parents=1024, seed=0):
             consider(dict(best, fir=k))
         for c in cand['copies']:
             consider(dict(best, copies=c))
-        for nt in cand['nt']:
+        for c in cand['consumers']:
+            consider(dict(best, consumers=c))
+        for nt in (cand['nt16'] if best.get('consumers') == 4 else cand['nt']):
             consider(dict(best, nt=nt))
         if cand['repeat_off']:
             for nt in cand['nt16']:

@@ -25,7 +25,7 @@ def test_library_loads_and_exports_every_symbol():
     L = _lib.load()
     for name in _declared():
         assert hasattr(L, name), name
-    assert L.ffbp_abi_version() == 3
+    assert L.ffbp_abi_version() == 4
 
 
 def test_argument_errors_without_a_gpu():

@@ -148,7 +148,7 @@ def _run_level_tc(lib, x, c0, sl, fk, fp, Ko, Po, Dk, Dp, window=None, bad=None,
     if opts is None:
         lib.check(L.ffbp_level_tc(*args, s), 'ffbp_level_tc')
     else:
-        o = lib.TcOpts(*(int(opts.get(k, 0)) for k in ('nt', 'sb', 'copies', 'repeat', 'fir')))
+        o = lib.TcOpts(*(int(opts.get(k, 0)) for k in ('nt', 'sb', 'copies', 'repeat', 'fir', 'consumers')))
         lib.check(L.ffbp_level_tc_ex(*args, ctypes.byref(o), s), 'ffbp_level_tc_ex')
     torch.cuda.synchronize()
     return out.cpu().numpy(), status.cpu().numpy()
@@ -213,7 +213,8 @@ def test_level_tensor_cores_launch_options_same_bits(lib, case):
     default_fir = 2 if (Po >= 512 or AP > 12) else 1            # the launcher's default for the pulse FIR's kernel
     sets = [dict(copies=4), dict(copies=2), dict(nt=32), dict(nt=64, copies=4), dict(nt=96), dict(nt=128, sb=2),
             dict(sb=3), dict(repeat=1, nt=16), dict(repeat=1, nt=48, copies=4), dict(repeat=1, nt=80), dict(nt=48),
-            dict(fir=1), dict(fir=2), dict(fir=1, copies=4)]
+            dict(fir=1), dict(fir=2), dict(fir=1, copies=4), dict(consumers=4), dict(consumers=4, nt=48, copies=4),
+            dict(consumers=4, repeat=1, nt=80), dict(consumers=8)]
     ran = 0
     for o in sets:
         try:
@@ -222,7 +223,7 @@ def test_level_tensor_cores_launch_options_same_bits(lib, case):
             assert 'columns per tile' in str(e) or 'B stages' in str(e), (o, str(e))
             continue
         assert st[0] == 0
-        if set(o) <= {'copies', 'sb'} or (o == dict(fir=default_fir)):
+        if set(o) <= {'copies', 'sb'} or o == dict(fir=default_fir) or o == dict(consumers=8):
             assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), o
         else:
             assert _rel(got, want) < 1e-4, (o, _rel(got, want))
