@@ -21,8 +21,8 @@ struct LevelLaunch {
     unsigned test_wait_ns = 0;   // tensor-core pass 1 only, for tests of the failure report: when nonzero the MMA
                                  // issuer first waits this long on a barrier nothing completes, as a stuck pipeline
     // tensor-core pass 1 launch options (0: the default): output columns per tile, B stages, plane copies (2 or 4),
-    // row repeat (1: off), consumer warps (8 or 4, the others copying Hankel rows); pass 2's kernel (1: CUDA cores,
-    // 2: tensor cores)
+    // row repeat (1: off), consumer warps (8, 4 or 12, 16 less them copying Hankel rows); pass 2's kernel (1: CUDA
+    // cores, 2: tensor cores)
     int tc_nt = 0, tc_sb = 0, tc_pc = 0, tc_rp = 0, tc_fir = 0, tc_cw = 0;
 };
 

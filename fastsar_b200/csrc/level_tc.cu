@@ -36,6 +36,8 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -216,8 +218,9 @@ __device__ __forceinline__ float y_scale(const int *amax)
 template <int NKC, int PC, int CW>
 __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
 {
-    // CW consumer warps (8, or 4 where the consumers idle and the Hankel copies bound the stage), the other warps'
-    // roles after them: 4 A', 4 planes, 16 - CW Hankel rows, the MMA issuer last (warp 24)
+    // CW consumer warps (8; 4 where the consumers idle and the Hankel copies bound the stage; 12 where the
+    // accumulator read-out does), the other warps' roles after them: 4 A', 4 planes, 16 - CW Hankel rows, the MMA
+    // issuer last (warp 24)
     constexpr int NCW_ = CW, NHW_ = NBW + NCW - CW - NLW, NHT_ = NHW_ * 32;
     static_assert(NCW_ + NAW + NLW + NHW_ == MMAW, "warp roles");
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -900,28 +903,37 @@ cudaError_t launch_level_tc_gemm(const LevelLaunch &L, const int *amax_in, void 
     const int pc = L.tc_pc == 4 ? 4 : 2;
     if (L.tc_pc != 0 && L.tc_pc != 2 && L.tc_pc != 4) { *why = "plane copies: 2 or 4"; return cudaErrorNotSupported; }
     a.rp = (a.Lkp > 32 && L.C <= 32 && L.tc_rp != 1) ? 2 : 1;
-    if (L.tc_cw != 0 && L.tc_cw != 4 && L.tc_cw != 8) { *why = "consumer warps: 4 or 8"; return cudaErrorNotSupported; }
-    const int cw = L.tc_cw == 4 ? 4 : 8;
-    const int unit = (cw == 8 && a.rp == 2) ? 32 : 16;       // the consumers' column split: 8-column chunks per warp
+    if (L.tc_cw != 0 && L.tc_cw != 4 && L.tc_cw != 8 && L.tc_cw != 12) { *why = "consumer warps: 4, 8 or 12"; return cudaErrorNotSupported; }
+    const int cw = L.tc_cw ? L.tc_cw : 8;
+    // the consumers split a tile's columns cw / 4 ways (cw / 2 with repeated rows) in 8-column chunks; the MMA's N
+    // (2 Nt) a multiple of 16
+    const int unit = std::max(16, 8 * (cw / 4) * a.rp);
     auto need = [&](int nt, int sb) { return gemm_smem(a.Lkp, a.Dk, nt, sb, pc); };
     int best = 0;
     if (L.tc_nt) {
         if (L.tc_nt % unit || L.tc_nt > 128 || need(L.tc_nt, 2) > avail) {
-            *why = "columns per tile: a multiple of 16 (32 with repeated rows and 8 consumer warps) up to 128 whose operands fit shared memory";
+            *why = "columns per tile: a multiple of 16 and of 8 x consumer warps / 4 (x 2 with repeated rows), up to 128, whose operands fit shared memory";
             return cudaErrorNotSupported;
         }
         best = L.tc_nt;
     } else {
-        // a multiple of 32 up to 128 whose operands fit shared memory with two B stages, the one that wastes the
-        // fewest columns on the last tile counting each tile as 32 columns of fixed cost
+        // a multiple of the unit (of 32 where the unit divides 32) up to 128 whose operands fit shared memory with two
+        // B stages, the one that wastes the fewest columns on the last tile counting each tile as 32 columns of fixed
+        // cost
+        const int step = 32 % unit == 0 ? 32 : unit;
         int bestw = 1 << 30;
-        for (int nt = 128; nt >= 32; nt -= 32) {
+        for (int nt = (128 / step) * step; nt >= step; nt -= step) {
             if (need(nt, 2) > avail) continue;
             const int nti = (L.Ko + nt - 1) / nt, waste = nti * nt - L.Ko + nti * 32;
             if (waste < bestw) { bestw = waste; best = nt; }
         }
     }
     if (!best) { *why = "the tensor-core level's operands do not fit shared memory"; return cudaErrorNotSupported; }
+    // every consumer warp's columns are whole 8-column chunks (the accumulator loads' column alignment)
+    if (best % unit != 0 || (best / (cw / 4) / a.rp) % 8 != 0) {
+        *why = "columns per tile do not split into the consumer warps' 8-column chunks";
+        return cudaErrorNotSupported;
+    }
     a.Nt = best;
     a.ntile = (L.Ko + a.Nt - 1) / a.Nt;
     a.W = a.Dk * (a.Nt - 1) + a.Lkp;
@@ -952,7 +964,8 @@ cudaError_t launch_level_tc_gemm(const LevelLaunch &L, const int *amax_in, void 
     cudaError_t e;
 #define FFBP_GEMM_RUN(N)                                                                                     \
     (cw == 4 ? (pc == 4 ? run(level_tc_gemm<N, 4, 4>) : run(level_tc_gemm<N, 2, 4>))                         \
-             : (pc == 4 ? run(level_tc_gemm<N, 4, 8>) : run(level_tc_gemm<N, 2, 8>)))
+     : cw == 12 ? (pc == 4 ? run(level_tc_gemm<N, 4, 12>) : run(level_tc_gemm<N, 2, 12>))                    \
+                : (pc == 4 ? run(level_tc_gemm<N, 4, 8>) : run(level_tc_gemm<N, 2, 8>)))
     switch (a.Lkp / 8) {
         case 2: e = FFBP_GEMM_RUN(2); break;
         case 4: e = FFBP_GEMM_RUN(4); break;

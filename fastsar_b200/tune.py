@@ -136,12 +136,13 @@ def level_signature(lv, Np):
 
 def _level_candidates(C, Lk):
     """Launch option sets of a tensor-core level in the order a coordinate search visits them: the pulse FIR's kernel
-    (CUDA or tensor cores), plane copies, consumer warps (8, or 4 with 12 Hankel-row warps), then columns per tile
-    (multiples of 32 with repeated A rows and 8 consumer warps, of 16 otherwise), then the row repeat off, then the B
+    (CUDA or tensor cores), plane copies, consumer warps (8, 4 or 12; 16 less them copy Hankel rows), then columns per
+    tile (the multiples of 8 x consumer warps / 4 that the launcher takes), then the row repeat off, then the B
     stages."""
     Lkp = ((max(Lk, 1) + 15) // 16) * 16
     rep_ok = Lkp > 32 and C <= 32
-    return dict(fir=[1, 2], copies=[2, 4], consumers=[8, 4], nt=list(range(32, 129, 32)),
+    return dict(fir=[1, 2], copies=[2, 4], consumers=[8, 4, 12],
+                nt={8: list(range(32, 129, 32)), 4: list(range(16, 129, 16)), 12: list(range(24, 129, 24))},
                 nt16=list(range(16, 129, 16)), repeat_off=rep_ok, sb=[2, 3, 4])
 
 
@@ -226,7 +227,7 @@ def tune_level(lv, Np, reps=3, max_parents=1024, seed=0):
             consider(dict(best, copies=c))
         for c in cand['consumers']:
             consider(dict(best, consumers=c))
-        for nt in (cand['nt16'] if best.get('consumers') == 4 else cand['nt']):
+        for nt in cand['nt'][best.get('consumers', 8)]:
             consider(dict(best, nt=nt))
         if cand['repeat_off']:
             for nt in cand['nt16']:

@@ -72,7 +72,7 @@ typedef struct {
     int repeat;             /* 1: no repeated A rows (default: repeated when more than 32 taps and at most 32 children) */
     int fir;                /* the second pass's pulse FIR: 1 on the CUDA cores, 2 on the tensor cores (a banded    */
                             /* product per row; default: the tensor cores for 512 or more output pulses)            */
-    int consumers;          /* warps reading the accumulator: 8, or 4 with 12 instead of 8 copying Hankel rows      */
+    int consumers;          /* warps reading the accumulator: 8, 4 or 12 (16 less them copy Hankel rows)            */
 } ffbp_tc_opts;
 
 /* One level of the plan (fastsar/ffbp2.py:192-250, make_plan's per-level record). All pointers are host memory. */

@@ -214,7 +214,8 @@ def test_level_tensor_cores_launch_options_same_bits(lib, case):
     sets = [dict(copies=4), dict(copies=2), dict(nt=32), dict(nt=64, copies=4), dict(nt=96), dict(nt=128, sb=2),
             dict(sb=3), dict(repeat=1, nt=16), dict(repeat=1, nt=48, copies=4), dict(repeat=1, nt=80), dict(nt=48),
             dict(fir=1), dict(fir=2), dict(fir=1, copies=4), dict(consumers=4), dict(consumers=4, nt=48, copies=4),
-            dict(consumers=4, repeat=1, nt=80), dict(consumers=8)]
+            dict(consumers=4, repeat=1, nt=80), dict(consumers=8), dict(consumers=12), dict(consumers=12, nt=48),
+            dict(consumers=12, nt=96, copies=4)]
     ran = 0
     for o in sets:
         try:

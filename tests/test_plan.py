@@ -179,7 +179,7 @@ def test_packaged_level_options_cache_is_well_formed(tmp_path, monkeypatch):
     for k, v in doc['levels'].items():
         assert len([int(x) for x in k.split(',')]) == 10
         assert set(v) <= {'nt', 'sb', 'copies', 'repeat', 'fir', 'consumers'}
-        assert v.get('consumers', 8) in (4, 8)
+        assert v.get('consumers', 8) in (4, 8, 12)
         assert v.get('copies', 2) in (2, 4) and v.get('fir', 1) in (1, 2) and v.get('repeat', 0) in (0, 1)
         assert v.get('nt', 16) % 16 == 0 and 2 <= v.get('sb', 2) <= 4
     monkeypatch.setattr(tune, '_LEVEL_CACHE', {})
