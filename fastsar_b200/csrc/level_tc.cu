@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
     float2 *s_x = reinterpret_cast<float2 *>(s_tk + a.Lkp);                        // [XS][Wp] staged windows
     uint64_t *bars = reinterpret_cast<uint64_t *>(s_x + (size_t)XS * Wp);
     uint64_t *afull = bars, *aempty = bars + 2, *bfull = bars + 4, *bempty = bfull + a.SB, *dfull = bempty + a.SB,
-             *dempty = dfull + 2, *pfull = dempty + 2, *pempty = pfull + 2;
+             *dempty = dfull + 2, *pfull = dempty + 2, *pempty = pfull + 2, *drain = pempty + 2;
     __shared__ uint32_t s_tmem;
     __shared__ volatile int s_abort;
     __shared__ float s_scale;
@@ -271,6 +271,7 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             mbar_init(&pempty[i], NHT_);
         }
         mbar_init(&s_never, 1);
+        mbar_init(drain, 1);                             // the issuer's commit at the end
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int i = t; i < a.Lkp; i += NTHR) s_tk[i] = i < a.Lk ? (a.tk ? a.tk[i] : 1.f) : 0.f;   // Dk = 1: one tap 1
@@ -700,13 +701,11 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
     __syncthreads();
     if (warp == MMAW) {
         if (lane == 0) {
-            // drain: a commit on a fresh barrier completes once every earlier MMA of this thread has
-            uint64_t *dr = &afull[0];
-            mbar_init(dr, 1);
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-            mma_commit(dr);
+            // drain: a commit on a barrier of its own, initialized with the others, completes once every earlier MMA
+            // of this thread has (a barrier initialized again here need not be visible to the tensor core's arrive)
+            mma_commit(drain);
             const uint64_t t0 = global_ns();
-            while (!mbar_test(dr, 0, 0) && global_ns() - t0 < WAIT_NS) {
+            while (!mbar_test(drain, 0, 0) && global_ns() - t0 < WAIT_NS) {
             }
         }
         __syncwarp();
@@ -865,9 +864,9 @@ static size_t gemm_smem(int Lkp, int Dk, int nt, int sb, int pc)
     const size_t apart = (size_t)128 * Lkp * 2, bpart = (size_t)2 * nt * Lkp * 2;
     const int W = Dk * (nt - 1) + Lkp, Wp = plane_len(W, pc);
     // two stages' planes (4 planes x pc copies); barriers: afull[2], aempty[2], bfull[sb], bempty[sb], dfull[2],
-    // dempty[2], pfull[2], pempty[2]
+    // dempty[2], pfull[2], pempty[2], drain
     return 4 * apart + (size_t)sb * 2 * bpart + (size_t)2 * 4 * pc * (Wp / 2) * 4 + (size_t)Lkp * 4 +
-           (size_t)XS * Wp * 8 + (size_t)(12 + 2 * sb) * 8;
+           (size_t)XS * Wp * 8 + (size_t)(13 + 2 * sb) * 8;
 }
 
 constexpr size_t GEMM_SMEM_MAX = 225 * 1024;                 // the opt-in limit less static shared memory and slack
