@@ -691,8 +691,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
         uint64_t *dr = &drain[warp - NEPI];
         mma_commit(dr);
         const uint64_t t0 = global_ns();
-        while (!mbar_test(dr, 0) && global_ns() - t0 < WAIT_NS) {
+        bool drained = false;
+        while (!(drained = mbar_test(dr, 0)) && global_ns() - t0 < WAIT_NS) {
         }
+        if (!drained && a.err) atomicAdd(a.err, 1);              // an MMA still running: reported
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();

@@ -322,8 +322,10 @@ __global__ void __launch_bounds__(R_NTHR, 1) level_fir_tc_kernel(const FirTcArgs
     if (warp == R_MMAW && lane == 0) {
         mma_commit(drain);
         const uint64_t t0 = global_ns();
-        while (!mbar_test(drain, 0, 0) && global_ns() - t0 < R_WAIT_NS) {
+        bool drained = false;
+        while (!(drained = mbar_test(drain, 0, 0)) && global_ns() - t0 < R_WAIT_NS) {
         }
+        if (!drained && a.err) atomicAdd(a.err, 1);              // an MMA still running: reported
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();

@@ -514,8 +514,10 @@ __global__ void __launch_bounds__(F_NTHR, 1) level_fused_kernel(const FusedArgs 
         uint64_t *dr = &drain[warp - F_IW0];
         mma_commit(dr);
         const uint64_t t0 = global_ns();
-        while (!mbar_test(dr, 0, 0) && global_ns() - t0 < F_WAIT_NS) {
+        bool drained = false;
+        while (!(drained = mbar_test(dr, 0, 0)) && global_ns() - t0 < F_WAIT_NS) {
         }
+        if (!drained && a.err) atomicAdd(a.err, 1);              // an MMA still running: reported
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();

@@ -705,8 +705,10 @@ __global__ void __launch_bounds__(NTHR, 1) level_tc_gemm(const GemmArgs a)
             // of this thread has (a barrier initialized again here need not be visible to the tensor core's arrive)
             mma_commit(drain);
             const uint64_t t0 = global_ns();
-            while (!mbar_test(drain, 0, 0) && global_ns() - t0 < WAIT_NS) {
+            bool drained = false;
+            while (!(drained = mbar_test(drain, 0, 0)) && global_ns() - t0 < WAIT_NS) {
             }
+            if (!drained && a.err) atomicAdd(a.err, 1);              // an MMA still running: reported
         }
         __syncwarp();
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
