@@ -40,7 +40,7 @@ def workload_plan(name='spotlight_12k', taps='learned', pmax=0.5):
                               e1=w['e1'], e2=w['e2'], taps=model)
 
 
-def level_case(level, parents, pulses=0, form='tc', taps='learned', reps=3, seed=1, pmax=0.5, fir=0):
+def level_case(level, parents, pulses=0, form='tc', taps='learned', reps=3, seed=1, pmax=0.5, fir=0, opts=None):
     import torch
     L = _lib.load()
     w, pl = workload_plan(taps=taps, pmax=pmax)
@@ -74,7 +74,8 @@ def level_case(level, parents, pulses=0, form='tc', taps='learned', reps=3, seed
                                           fk['pl'], Dk, Ko, (K - 1) / 2.0, tp.data_ptr(), fp['L'], fp['pl'], Dp, Po,
                                           None, None, out.data_ptr(), None, st.data_ptr(), s), 'ffbp_level_fused')
         elif form == 'tc':
-            o = _lib.TcOpts(0, 0, 0, 0, int(fir))
+            oo = dict(opts or {}, **({'fir': int(fir)} if fir else {}))
+            o = _lib.TcOpts(*(int(oo.get(k, 0)) for k in ('nt', 'sb', 'copies', 'repeat', 'fir', 'consumers')))
             _lib.check(L.ffbp_level_tc_ex(x.data_ptr(), parents, P, K, ph.data_ptr(), C, tk.data_ptr(), fk['L'],
                                           fk['pl'], Dk, Ko, (K - 1) / 2.0, tp.data_ptr(), fp['L'], fp['pl'], Dp, Po, None,
                                           None, out.data_ptr(), None, scr.data_ptr(), nb, st.data_ptr(),
@@ -165,6 +166,8 @@ def main(argv=None):
     ap.add_argument('--form', choices=('tc', 'fused', 'fp32'), default='tc')
     ap.add_argument('--fir', type=int, choices=(0, 1, 2), default=0,
                     help="tc: the pulse FIR's kernel (0 the launcher's default, 1 CUDA cores, 2 tensor cores)")
+    ap.add_argument('--opts', default=None,
+                    help='tc: launch options as JSON, e.g. \'{"consumers": 4, "copies": 4, "nt": 80}\'')
     ap.add_argument('--tiles', type=int, default=20000)
     ap.add_argument('--mode', choices=('f16', 'bf16x3', 'fp32'), default='f16')
     ap.add_argument('--taps', default='learned', help="'learned' or a Kaiser-sinc attenuation in dB (70, 80)")
@@ -176,7 +179,9 @@ def main(argv=None):
     if a.stage == 'exact':
         exact_case(a.workload, a.interp, a.pulses or 1024, a.reps)
     elif a.stage == 'level':
-        level_case(int(a.level[1]), a.parents, a.pulses, a.form, a.taps, a.reps, pmax=a.pmax, fir=a.fir)
+        import json
+        level_case(int(a.level[1]), a.parents, a.pulses, a.form, a.taps, a.reps, pmax=a.pmax, fir=a.fir,
+                   opts=json.loads(a.opts) if a.opts else None)
     else:
         final_case(a.tiles, a.mode, a.taps, a.reps, pmax=a.pmax)
 
