@@ -115,6 +115,7 @@ struct ffbp_plan {
     std::vector<DevLevel> lv;
     float *wp = nullptr, *wk = nullptr, *wf = nullptr;
     double *ux = nullptr, *uy = nullptr, *ucx = nullptr, *ucy = nullptr, *rc = nullptr;
+    float4 *seeds = nullptr;          // the float16 tensor-core final stage's ramp seeds [ntiles, Pf]
     int2 *first = nullptr;
     size_t bufA = 0, bufB = 0;
     std::vector<void *> owned;
@@ -338,6 +339,11 @@ int ffbp_plan_create(const ffbp_plan_desc *d, void *stream_, ffbp_plan **out)
     e = ffbp::launch_final_geom((const double *)dantf, d->Pf, (const double *)dcenf, B, d->e1, d->e2, p->ux, p->uy,
                                 p->ucx, p->ucy, p->rc, s);
     if (e != cudaSuccess) return cleanup(cuda_fail(e, "final geometry kernel"));
+    if ((d->final_mode & 0xff) == FFBP_FINAL_TC_F16) {
+        if ((e = p->alloc(&p->seeds, (size_t)B * d->Pf)) != cudaSuccess) return cleanup(cuda_fail(e, "allocate final seeds"));
+        e = ffbp::launch_final_seeds(p->ux, p->uy, (long)B * d->Pf, p->spx, p->spy, p->a0, p->a1, p->seeds, s);
+        if (e != cudaSuccess) return cleanup(cuda_fail(e, "final seeds kernel"));
+    }
     if ((e = p->alloc(&p->d_aborts, 1)) != cudaSuccess || (e = cudaMemsetAsync(p->d_aborts, 0, sizeof(int), s)) != cudaSuccess)
         return cleanup(cuda_fail(e, "allocate the abort count"));
     if ((e = cudaHostAlloc(reinterpret_cast<void **>(&p->h_aborts), sizeof(int), cudaHostAllocDefault)) != cudaSuccess)
@@ -471,7 +477,7 @@ static int form_impl(ffbp_plan *p, const void *d_S, void *d_img, void *d_ws, siz
         in = outp;
     }
     ffbp::FinalLaunch F;
-    F.d = in; F.B = p->ntiles; F.Pf = p->Pf; F.Qf = p->Qf; F.T = p->T; F.ux = p->ux; F.uy = p->uy;
+    F.d = in; F.B = p->ntiles; F.Pf = p->Pf; F.Qf = p->Qf; F.T = p->T; F.ux = p->ux; F.uy = p->uy; F.seeds = p->seeds;
     F.spx = p->spx; F.spy = p->spy; F.a0 = p->a0; F.a1 = p->a1; F.fc2 = p->fc2; F.ucx = p->ucx; F.ucy = p->ucy;
     F.rc = p->rc; F.w = p->wf; F.tiles = nullptr; F.img = static_cast<float2 *>(d_img); F.first = p->first;
     F.nx = p->nx; F.ny = p->ny; F.ox = p->ox; F.oy = p->oy; F.scale = 1.f; F.err = p->d_aborts;

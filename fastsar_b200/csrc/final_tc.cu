@@ -146,10 +146,13 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t *r)
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// bytes = 4 or 8; the copy of an invalid element reads nothing and zero-fills the destination
+// bytes = 4, 8 or 16 (dst and src aligned to it); the copy of an invalid element reads nothing and zero-fills the
+// destination
 __device__ __forceinline__ void cp_async(uint32_t dst, const void *src, int bytes, bool valid)
 {
-    if (bytes == 8)
+    if (bytes == 16)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" :: "r"(dst), "l"(src), "r"(valid ? 16 : 0) : "memory");
+    else if (bytes == 8)
         asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" :: "r"(dst), "l"(src), "r"(valid ? 8 : 0) : "memory");
     else
         asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" :: "r"(dst), "l"(src), "r"(valid ? 4 : 0) : "memory");
@@ -160,6 +163,7 @@ struct TcArgs {
     int B, Pf, Qf, Qfp, S, nunits, nis;
     const double *__restrict__ ux;
     const double *__restrict__ uy;
+    const float4 *__restrict__ seeds;      // float16 form: the ramp seeds per tile and subaperture (or null)
     double spx, spy, a0, a1, fc2;
     const double *__restrict__ ucx;
     const double *__restrict__ ucy;
@@ -366,6 +370,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
         const int nts = NTS;
         const int ntot = nul * a.Pf;
         const size_t nbp = (size_t)a.B * a.Pf;
+        const bool fs = !BF && a.seeds;                         // stage the float32 seeds in place of ux, uy
         auto prefetch_unit = [&](int ul) {
             if (ul >= nul) return;
             for (int ts = 0; ts < nts; ++ts) {
@@ -375,10 +380,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
                 const int dbytes = a.Pf * a.Qf * (int)sizeof(float2);
                 for (int o = lane * 128; o < dbytes; o += 32 * 128)
                     asm volatile("prefetch.global.L2 [%0];" :: "l"(dbeg + o));
-                const double *src = (lane < 16 ? a.ux : a.uy) + (size_t)tile * a.Pf;
-                const int ub = a.Pf * (int)sizeof(double);
+                const char *src = fs ? reinterpret_cast<const char *>(a.seeds + (size_t)tile * a.Pf)
+                                     : reinterpret_cast<const char *>((lane < 16 ? a.ux : a.uy) + (size_t)tile * a.Pf);
+                const int ub = a.Pf * (fs ? 16 : 8);
                 for (int o = (lane & 15) * 128; o < ub; o += 16 * 128)
-                    asm volatile("prefetch.global.L2 [%0];" :: "l"(reinterpret_cast<const char *>(src) + o));
+                    asm volatile("prefetch.global.L2 [%0];" :: "l"(src + o));
             }
         };
         int ul = 0, p = 0;
@@ -399,7 +405,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
                     cp_async(dst + 8u * q, v ? (const void *)(src + q) : (const void *)a.d, 8, v);
                 }
                 const uint32_t gd = dst + 8u * a.Qfp;
-                if (lane < 2) cp_async(gd + 8u * lane, (const void *)((lane ? a.uy : a.ux) + bp), 8, tv);
+                if (fs) {
+                    if (lane == 0) cp_async(gd, (const void *)(a.seeds + bp), 16, tv);
+                } else if (lane < 2) cp_async(gd + 8u * lane, (const void *)((lane ? a.uy : a.ux) + bp), 8, tv);
                 else if (WEIGHTED && lane < 5)
                     cp_async(gd + 16u + 4u * (lane - 2), (const void *)(a.w + (size_t)(lane - 2) * nbp + bp), 4, tv);
             }
@@ -473,13 +481,26 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
                 const unsigned char *tsp = slotb + (uint32_t)ts * tsb;
                 const float *gw = reinterpret_cast<const float *>(tsp + 8 * a.Qfp + 16);   // the weights
                 const bool isA = op == 0;
-                const double u = *reinterpret_cast<const double *>(tsp + 8 * a.Qfp + (isA ? 0 : 8));
                 const float dlf = ((float)r - 0.5f * (TT - 1)) * (isA ? sp32x : sp32y);      // r < TT / 2: dl < 0
-                const double dl = ((double)r - 0.5 * (TT - 1)) * (isA ? a.spx : a.spy);
-                const double ud = -(u * dl);
-                float2 wv = cis_cycles_d(ud * fma(a.a1, 8.0 * g, a.a0));
+                // the ramp of row offset dl = m sp / 2 (m = 2 r - (TT - 1)) at sample q: -u dl (a0 + a1 q) cycles,
+                // seeded at q = 8 g with step -u dl a1
+                float2 wv, st;
+                if (!BF && a.seeds) {
+                    // float32 from the plan's seeds (Y = frac(u sp a0 / 2), V = u sp a1 / 2): m Y carries the
+                    // phase modulo 1 exactly as m u sp a0 / 2 does, to float32's rounding of Y and V
+                    const float4 sd = *reinterpret_cast<const float4 *>(tsp + 8 * a.Qfp);
+                    const float Y = isA ? sd.x : sd.z, V = isA ? sd.y : sd.w;
+                    const float m = (float)(2 * r - (TT - 1)), mv = m * V;
+                    wv = cis_cycles(-fmaf(m, Y, mv * (8.f * (float)g)));
+                    st = cis_cycles(-mv);
+                } else {
+                    const double u = *reinterpret_cast<const double *>(tsp + 8 * a.Qfp + (isA ? 0 : 8));
+                    const double dl = ((double)r - 0.5 * (TT - 1)) * (isA ? a.spx : a.spy);
+                    const double ud = -(u * dl);
+                    wv = cis_cycles_d(ud * fma(a.a1, 8.0 * g, a.a0));
+                    st = cis_cycles_d(ud * a.a1);
+                }
                 if (isA) { wv.x *= dscale; wv.y *= dscale; }
-                const float2 st = cis_cycles_d(ud * a.a1);
                 float w1 = 1.f, w2 = 1.f;                       // the weights of rows r and 31 - r
                 if (WEIGHTED) {
                     if (isA) { w1 = gw[0] + gw[1] * dlf; w2 = gw[0] - gw[1] * dlf; }
@@ -702,7 +723,26 @@ __global__ void __launch_bounds__(NTHREADS, 1) final_tc_kernel(const TcArgs a)
     if (warp == NEPI) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TMEM_COLS));
 }
 
+__global__ void final_seeds_kernel(const double *__restrict__ ux, const double *__restrict__ uy, long n, double spx,
+                                   double spy, double a0, double a1, float4 *__restrict__ out)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const double yx = 0.5 * ux[i] * spx * a0, yy = 0.5 * uy[i] * spy * a0;
+        out[i] = make_float4((float)(yx - floor(yx)), (float)(0.5 * ux[i] * spx * a1), (float)(yy - floor(yy)),
+                             (float)(0.5 * uy[i] * spy * a1));
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_final_seeds(const double *ux, const double *uy, long n, double spx, double spy, double a0,
+                               double a1, float4 *out, cudaStream_t s)
+{
+    if (n <= 0) return cudaSuccess;
+    const long nb = (n + 255) / 256;
+    final_seeds_kernel<<<(int)(nb < 4096 ? nb : 4096), 256, 0, s>>>(ux, uy, n, spx, spy, a0, a1, out);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_final_tc(const FinalLaunch &F, int mode, cudaStream_t s, const char **why)
 {
@@ -719,7 +759,7 @@ cudaError_t launch_final_tc(const FinalLaunch &F, int mode, cudaStream_t s, cons
     a.d = F.d; a.B = F.B; a.Pf = F.Pf; a.Qf = F.Qf; a.Qfp = (F.Qf + 15) & ~15;
     a.nunits = (F.B + nts - 1) / nts;
     a.nis = F.Pf >= NISS ? NISS : 1;
-    a.ux = F.ux; a.uy = F.uy; a.spx = F.spx; a.spy = F.spy; a.a0 = F.a0; a.a1 = F.a1; a.fc2 = F.fc2;
+    a.ux = F.ux; a.uy = F.uy; a.seeds = F.seeds; a.spx = F.spx; a.spy = F.spy; a.a0 = F.a0; a.a1 = F.a1; a.fc2 = F.fc2;
     a.ucx = F.ucx; a.ucy = F.ucy; a.rc = F.rc; a.w = F.w; a.tiles = F.tiles; a.img = F.img; a.first = F.first;
     a.nx = F.nx; a.ny = F.ny; a.ox = F.ox; a.oy = F.oy; a.scale = F.scale; a.err = F.err; a.amax = F.amax;
     a.test_wait_ns = F.test_wait_ns;

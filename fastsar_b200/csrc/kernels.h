@@ -81,9 +81,15 @@ struct FinalLaunch {
     int *err = nullptr;   // raised (atomicAdd) by a kernel whose bounded wait ran out (tensor-core stage), or null
     const int *amax = nullptr;   // the largest |component| of d (float bits), for the float16 operands' scale
     unsigned test_wait_ns = 0;   // tensor-core stage only, for tests of the failure report (as in LevelLaunch)
+    const float4 *seeds = nullptr;   // [B, Pf] the float16 form's ramp seeds (launch_final_seeds), or null
 };
 cudaError_t launch_final_fp32(const FinalLaunch &F, cudaStream_t s, const char **why);
 cudaError_t launch_final_tc(const FinalLaunch &F, int mode, cudaStream_t s, const char **why);
+// The tensor-core final stage's ramp seeds per tile and final subaperture, reduced once in float64: (frac(ux spx a0 /
+// 2), ux spx a1 / 2, frac(uy spy a0 / 2), uy spy a1 / 2), from which the float16 form's producers seed each row's
+// ramp in float32 (row offset m = 2 r - (T - 1): phase -m (Y + 8 g V) at sample group g, step -m V).
+cudaError_t launch_final_seeds(const double *ux, const double *uy, long n, double spx, double spy, double a0,
+                               double a1, float4 *out, cudaStream_t s);
 
 // Exact backprojection at points in float64 and the phase-history synthesis (exact.cu).
 cudaError_t launch_bp_points_f64(const double2 *prof, int P, int nfft, const double *tx, const double *rcv,
