@@ -20,6 +20,9 @@ Fixtures:
   gate.npz            the range gate: _gate_plan on wide-band and spotlight geometries, the gated history of a seeded
                       random history (first pulses), and ImageFormer(backend='cpu', range_gate=True)'s image of a
                       simulated wide-band scene (python tests/golden/make_golden.py --only gate writes this file alone)
+  stack.npz           the stack products: registration (_detected, _peak, _estimate), translation (_translate),
+                      incoherent average (_Mean, _level) and products.multilook / interferogram / coherence of three
+                      seeded images (stack_scene below; --only stack writes this file alone)
   weights.npz         aperture weights: api.final_weights (plain and with gradients) of the test scene's 2-level plan
                       for a pixel- and pulse-dependent weight (WEIGHT below), and ImageFormer(backend='cpu',
                       aperture_weight=WEIGHT)'s image (--only weights writes this file alone)
@@ -218,14 +221,98 @@ def weights(fastsar):
     print('weights done', rec['w_grad'].shape)
 
 
+def stack_scene(n1=128, n2=160, seed=20261204):
+    """Three seeded complex images of one speckle scene on a common grid (band-limited to 0.35 of the sampling rate
+    along both axes, 12 bright points): a; b, the scene displaced by (3.3, -2.6) pixels (b(x) = a(x + d)) at 0.95
+    of a's amplitude plus an independent speckle at 0.3; c, an independent scene 1.7 times as bright with an
+    unprocessed (zero) corner of 8 x 10 pixels."""
+    rng = np.random.default_rng(seed)
+    k1, k2 = np.fft.fftfreq(n1)[:, None], np.fft.fftfreq(n2)[None, :]
+    band = (np.abs(k1) < 0.35) & (np.abs(k2) < 0.35)
+
+    def white():
+        w = (rng.standard_normal((n1, n2)) + 1j * rng.standard_normal((n1, n2))) / np.sqrt(2.0)
+        i, j = rng.integers(8, n1 - 8, 12), rng.integers(8, n2 - 8, 12)
+        w[i, j] += 8.0 * np.exp(2j * np.pi * rng.random(12))
+        return np.fft.fft2(w)
+
+    def image(F, d=(0.0, 0.0)):
+        return np.fft.ifft2(F * band * np.exp(2j * np.pi * (k1 * d[0] + k2 * d[1])))
+    F0, F1, F2 = white(), white(), white()
+    a = image(F0).astype(np.complex64)
+    b = (0.95 * image(F0, (3.3, -2.6)) + 0.3 * image(F1)).astype(np.complex64)
+    c = (1.7 * image(F2)).astype(np.complex64)
+    c[:8, :10] = 0
+    return a, b, c
+
+
+def stack(fastsar):
+    """stack.npz: the reference's registration, translation and incoherent average (fastsar/stack.py) and its
+    multilook, interferogram and coherence (fastsar/products.py) on stack_scene's images."""
+    from fastsar import stack as st, products as pr
+    a, b, c = stack_scene()
+    rec = dict(a=a, b=b, c=c)
+    rec['box5_a'] = st._box(st._power(a), 5)
+    rec['box4_c'] = st._box(st._power(c), 4)
+    da, db = st._detected(a, 5), st._detected(b, 5)
+    rec['det_a'], rec['det_b'] = da, db
+    rec['det3_c'] = st._detected(c, 3)
+    for tag, hp in (('hp', 32.0), ('nohp', None)):
+        e = st._estimate(da, db, 0.25, 0.3, 16, 2, hp)
+        for k in ('shift_px', 'shift', 'significance', 'correlation', 'found', 'tiles', 'tiles_used', 'tile_residuals',
+                  'tile_used', 'tile_significance', 'residual_rms', 'residual_median', 'residual_worst'):
+            rec[f'est_{tag}_{k}'] = np.asarray(e[k])
+        d, z, rho, clear = st._peak(da, db, 16, highpass=hp)
+        rec[f'peak_{tag}'] = np.array([d[0], d[1], z, rho, float(clear)])
+    # a peak searched about a given translation with a narrow window, as the tiles are
+    d, z, rho, clear = st._peak(da[:64, :80], db[:64, :80], 16, around=(-3, 3), narrow=8)
+    rec['peak_tile'] = np.array([d[0], d[1], z, rho, float(clear)])
+    pb = st._power(b)
+    rec['tr_real'] = st._translate(pb, (1.3, -0.4))
+    rec['tr_cplx'] = st._translate(c, (2.25, -1.5))
+    rec['tr_whole'] = st._translate(c, (-3.0, 2.0))
+    # the average: of the three small complex images (too small for the looks), and of a 256 x 256 scene given as
+    # one complex image and two amplitude (real) images
+    a2, b2, c2 = stack_scene(256, 256, seed=20261205)
+    b2, c2 = np.abs(b2).astype(np.float32), np.abs(c2).astype(np.float32)
+    rec.update(m_a=a2, m_b=b2, m_c=c2)
+    for tag, eq, w, imgs in (('small', None, (1.0, 2.0, 0.5), (a, b, c)), ('plain', None, (1.0, 2.0, 0.5), (a2, b2, c2)),
+                             ('mean', 'mean', (1.0, 1.0, 1.0), (a2, b2, c2)),
+                             ('median', 'median', (1.0, 0.5, 2.0), (a2, b2, c2))):
+        acc = st._Mean(eq, 32)
+        for img, wk in zip(imgs, w):
+            acc.add(dict(image=img), wk)
+        M = acc.image()
+        L = acc.looks(M)
+        rec[f'mean_{tag}_M'] = M
+        rec[f'mean_{tag}_gains'] = np.array(acc.gains)
+        rec[f'mean_{tag}_weights'] = np.array(w)
+        for k in ('looks', 'looks_single', 'looks_by_n', 'looks_ideal', 'looks_independent', 'brightness_spread_db',
+                  'tiles_selected', 'homogeneous'):
+            v = L.get(k)
+            rec[f'mean_{tag}_{k}'] = np.asarray(np.nan if v is None else v)
+    rec['level_mean'] = np.array(st._level(st._power(c), 'mean'))
+    rec['level_median'] = np.array(st._level(st._power(c), 'median'))
+    rec['ml_a_2_3'] = pr.multilook(a, 2, 3)
+    rec['ifg_ab_2_2'] = pr.interferogram(a, b, 2, 2)
+    rec['coh_ab_5_5'] = pr.coherence(a, b, 5, 5)
+    rec['coh_ac_7_3'] = pr.coherence(a, c, 7, 3)
+    rec['coh_ab_4_6'] = pr.coherence(a, b, 4, 6)
+    np.savez_compressed(os.path.join(HERE, 'stack.npz'), **rec)
+    print('stack done', rec['est_hp_shift_px'], rec['peak_hp'], rec['mean_plain_looks'], rec['mean_median_gains'])
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--ref', default=os.environ.get('FASTSAR_REFERENCE'))
-    ap.add_argument('--only', choices=('exact', 'gate', 'weights'), default=None)
+    ap.add_argument('--only', choices=('exact', 'gate', 'weights', 'stack'), default=None)
     args = ap.parse_args()
     if not args.ref:
         sys.exit('make_golden: name the reference checkout by --ref PATH or FASTSAR_REFERENCE')
     fs = import_reference(args.ref)
+    if args.only == 'stack':
+        stack(fs)
+        return
     if args.only == 'weights':
         weights(fs)
         return
