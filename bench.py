@@ -31,6 +31,10 @@ collections formed by one CUDA graph, against the same formers one after another
 --workload stack_8: a repeat-pass stack (run_stack): 8 passes of one scene formed to a common 8,192 x 8,192 grid by
 one CUDA graph, with per-pass errors and pairwise coherence against float64.
 
+--workload stack_products: the stack's products once its images exist (run_stack_products): registration, the
+incoherent average with its looks and coherence maps of 8 images on the 8,192 x 8,192 grid, against the oracle's
+NumPy restatement of the reference's functions on crops.
+
 --workload learned_4k: the learned decimation taps against the Kaiser-sinc decimators at oversamplings of the child
 data from 4x to about 1x (run_learned): error against float64 and time per image, the float32 former throughout.
 
@@ -230,6 +234,8 @@ def main():
         return run_reference(args, world, rank)
     if args.workload.startswith('patches'):
         return run_patches(args)
+    if args.workload == 'stack_products':
+        return run_stack_products(args)
     if args.workload.startswith('stack'):
         return run_stack(args)
     if args.workload.startswith('learned'):
@@ -669,8 +675,169 @@ def run_stack(args):
     print(json.dumps(line), flush=True)
 
 
+def run_stack_products(args):
+    """--workload stack_products: what the reference computes from a repeat-pass stack once its images exist
+    (fastsar/stack.py register and mean, fastsar/products.py coherence), on 8 seeded complex speckle images of the
+    stack's 8,192 x 8,192 grid held on the device: each image's detected form (box 5, dB, clipped), 7 translations
+    against the first (with 4 x 4 tiles after each), the 7 images translated onto the first, the incoherent average of
+    the 8 with its looks (equalized to the first's brightness), and 7 coherence maps against the first (7 x 7
+    windows). One step = all of it; the value is
+    the stack's pixels (8 x 8192^2) per second. The CPU baseline is the oracle (NumPy, scipy.fft on every core) on
+    2,048 x 2,048 crops of the same 8 images. One GPU; prints one JSON line."""
+    import torch
+    from fastsar_b200 import stack as st, products as pr, _lib
+    torch.cuda.set_device(0)
+    _lib.load()
+    n, nimg, sp = 8192, 8, 0.15
+    rng = np.random.default_rng(args.seed + 21)
+    shifts = [(0.0, 0.0)] + [tuple(rng.uniform(-6, 6, 2)) for _ in range(nimg - 1)]
+    g = torch.Generator(device='cuda').manual_seed(args.seed + 22)
+    f = torch.fft.fftfreq(n, device='cuda')
+    band = (f.abs() < 0.35)
+    base = torch.fft.fft2(torch.randn((n, n), dtype=torch.complex64, device='cuda', generator=g))
+    base *= band[:, None] & band[None, :]
+    imgs = []
+    for d in shifts:
+        ramp = torch.exp(2j * np.pi * (f[:, None] * d[0] + f[None, :] * d[1])).to(torch.complex64)
+        x = torch.fft.ifft2(base * ramp)
+        x = 0.95 * x + 0.3 * torch.fft.ifft2(torch.fft.fft2(torch.randn((n, n), dtype=torch.complex64, device='cuda',
+                                                                          generator=g)) * (band[:, None] & band[None, :]))
+        imgs.append(x.contiguous())
+        del ramp, x
+    del base
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+
+    def register():
+        dets = [st.detected(x, 5) for x in imgs]
+        return [st.estimate(dets[0], dets[k], sp, sp, 64, 4) for k in range(1, nimg)]
+
+    def align(regs):
+        # each image brought onto the first by its translation (whole pixels moved, the fraction a ramp on the
+        # spectrum: these images are at baseband, which is where the reference translates a complex image)
+        return [imgs[0]] + [st.translate(imgs[k], r['shift_px']) for k, r in zip(range(1, nimg), regs)]
+
+    def average(al):
+        acc = st.Mean('mean', 32)
+        for x in al:
+            acc.add(dict(image=x), 1.0)
+        M = acc.image()
+        return acc.looks(M)['looks'], M
+
+    def coherences(al):
+        return [pr.coherence(al[0], al[k], 7, 7) for k in range(1, nimg)]
+
+    def step():
+        regs = register()
+        al = align(regs)
+        return regs, average(al), coherences(al)
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    regs, (looks, M), cohs = step()
+    errs = [float(np.hypot(r['shift_px'][0] + d[0], r['shift_px'][1] + d[1])) for r, d in zip(regs, shifts[1:])]
+    coh_med = float(torch.stack([c[::16, ::16].median() for c in cohs]).median())
+    del cohs, M
+    clk = Clocks(0)
+    ms = timed(step, args.steps, args.warmup)
+    clocks = clk.stop()
+    regs = register()
+    al = align(regs)
+    ms_parts = dict(register=timed(register, 1, 1), align=timed(lambda: align(regs), 1, 1),
+                    average=timed(lambda: average(al), 1, 1), coherence=timed(lambda: coherences(al), 1, 1))
+    del al
+    # the pixel kernels alone (events on the current stream, the one they launch on): bytes they must move
+    hbm, _, peak_src = peaks()
+    out = torch.empty((n, n), dtype=torch.float32, device='cuda')
+    L = _lib.load()
+    sptr = pr.stream_ptr()
+
+    def kernel_ms(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+    k_coh = kernel_ms(lambda: L.ffbp_coherence(pr.ptr(imgs[0]), pr.ptr(imgs[1]), n, n, 7, 7, pr.ptr(out), sptr))
+    k_box = kernel_ms(lambda: L.ffbp_box_mean(pr.ptr(imgs[0]), _lib.PIX_POWER, n, n, 5, 1, pr.ptr(out), sptr))
+    acc_s = torch.empty_like(out)
+    acc_w = torch.empty_like(out)
+    k_add = kernel_ms(lambda: L.ffbp_mean_add(pr.ptr(imgs[1]), _lib.PIX_POWER, n * n, 1.0, 1.0, 0, pr.ptr(acc_s),
+                                              pr.ptr(acc_w), sptr))
+    px = n * n
+    kern = {'coherence_kernel': (k_coh, 20.0 * px), 'box_kernel': (k_box, 12.0 * px),
+            'mean_add_kernel': (k_add, 24.0 * px)}
+    top = max(('coherence_kernel', 'box_kernel', 'mean_add_kernel'), key=lambda k: kern[k][0] * (nimg - 1 if k ==
+                                                                                               'coherence_kernel' else nimg))
+    kms, kbytes = kern[top]
+    roof = dict(bound='hbm', achieved=kbytes / (kms * 1e-3) / 1e9, peak=hbm, unit='GB/s',
+                frac=kbytes / (kms * 1e-3) / 1e9 / hbm, traffic=None, kernel=top, peak_source=peak_src,
+                kernels={k: dict(ms=round(v[0], 4), algorithmic_bytes=v[1], gbs=round(v[1] / (v[0] * 1e-3) / 1e9, 1))
+                         for k, v in kern.items()})
+    del out, acc_s, acc_w
+    cpu = None
+    if not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+        import stack_oracle as so
+        c = 2048
+        crops = [x[:c, :c].cpu().numpy() for x in imgs]
+        t0 = time.perf_counter()
+        dets = [so.detected(x, 5) for x in crops]
+        ests = [so.estimate(dets[0], dets[k], sp, sp, 64, 4) for k in range(1, nimg)]
+        al = [crops[0]] + [so.translate(crops[k], e['shift_px']) for k, e in zip(range(1, nimg), ests)]
+        acc = so.Mean('mean', 32)
+        for x in al:
+            acc.add(x, 1.0)
+        acc.looks(acc.image())
+        for k in range(1, nimg):
+            so.coherence(al[0], al[k], 7, 7)
+        dt = time.perf_counter() - t0
+        cpu = dict(value=nimg * c * c / dt / 1e6, unit='Mpx/s', cores=os.cpu_count(), kind='port',
+                   sample=f'the same products of 2048 x 2048 crops of the 8 images (oracle/stack_oracle.py, NumPy and '
+                          f'scipy.fft on all cores): {dt:.1f} s')
+    # this package's kernels per step: a box mean per detected image; per registration a cross-spectrum of the whole
+    # images and one of the batch of 16 tiles; per translation a ramp and a crop; per image added to the average its
+    # intensity, the sums, its tile statistics, the running average and that average's statistics; the average, its
+    # statistics, its 9 x 9 means and theirs for the looks; a coherence map per pair (the transforms are cuFFT's, the
+    # sub-pixel products cuBLAS's)
+    launches = nimg + (nimg - 1) * 2 + (nimg - 1) * 2 + nimg * 5 + 4 + (nimg - 1)
+    line = dict(
+        metric='stack products (register 7, translate 7, mean of 8 with looks, 7 coherence maps) of an 8-image '
+               '8192 x 8192 stack',
+        value=nimg * px / (ms * 1e-3) / 1e6, unit='Mpx/s', n_gpus=1, steps=args.steps, warmup=args.warmup,
+        ms_per_step=ms, higher_is_better=True, scaling='weak', vs_baseline=None,
+        dtype='f32 pixels, f64 coherence sums, c64 transforms (cuFFT), c128 sub-pixel correlation (cuBLAS)',
+        data='synthetic: 8 seeded complex speckle images (band 0.35 of the sampling rate) of one scene, displaced by '
+             'seeded shifts up to 6 px, coherence about 0.95',
+        config=dict(workload='stack_products: 8 x 8192 x 8192 complex64 at 0.15 m (the repeat-pass stack grid)',
+                    register='detected box 5, max_shift 64, 4 x 4 tiles, high pass 32 px', mean="equalize='mean', tile 32",
+                    coherence='7 x 7 windows', l2='inputs larger than L2 (512 MB per image), no flush'),
+        ms_parts=ms_parts, registration_error_px=dict(max=max(errs), per_image=[round(e, 3) for e in errs]),
+        looks=looks, coherence_median=coh_med, roofline=roof, cpu_baseline=cpu,
+        gpu_launches=launches, clocks=clocks)
+    print(json.dumps(line), flush=True)
+
+
 def run_learned(args):
-    """--workload learned_4k: the learned decimation taps against the reference's Kaiser-sinc decimators on the
+    """--workload stack_products: the stack's products once its images exist (run_stack_products): registration, the
+incoherent average with its looks and coherence maps of 8 images on the 8,192 x 8,192 grid, against the oracle's
+NumPy restatement of the reference's functions on crops.
+
+--workload learned_4k: the learned decimation taps against the reference's Kaiser-sinc decimators on the
     4,096-pulse x 4,096-sample spotlight (the 512-pulse spotlight's geometry: 9.6 GHz, 300 MHz, 600 km, 45 deg,
     1.5 deg) formed to 2,048 x 2,048 pixels at 0.25 m, the float32 former (levels and final stage) throughout so that
     the filters alone differ. The oversampling of the child data is 1 / pmax: pmax 0.95, 0.5 and 0.25 are the "1x",

@@ -11,6 +11,7 @@ LIB_PATH = os.path.join(HERE, 'libffbp_b200.so')
 
 FFBP_OK, FFBP_E_ARG, FFBP_E_CUDA, FFBP_E_NOMEM, FFBP_E_WORKSPACE, FFBP_E_UNSUPPORTED = 0, -1, -2, -3, -4, -5
 FFBP_E_TRANSFER = -6
+PIX_AS_IS, PIX_POWER, PIX_SQUARE = 0, 1, 2          # ffbp_box_mean / ffbp_mean_add pixel kinds
 FFBP_FINAL_FP32, FFBP_FINAL_TC_F16, FFBP_FINAL_TC_BF16X3 = 0, 1, 2
 FFBP_LEVELS_TC = 0x100
 KIND_NAMES = {1: 'amax', 2: 'level_fp32', 3: 'level_tc_gemm', 4: 'level_tc_fir', 5: 'final_fp32', 6: 'final_tc',
@@ -25,7 +26,9 @@ EXPORTS = ('ffbp_last_error', 'ffbp_abi_version', 'ffbp_plan_create', 'ffbp_plan
            'ffbp_form_profile', 'ffbp_exact_pad', 'ffbp_exact_backproject', 'ffbp_mlp_param_count',
            'ffbp_mlp_max_decimation', 'ffbp_mlp_work_bytes', 'ffbp_plan_host_bytes', 'ffbp_form_host', 'ffbp_gate_pad',
            'ffbp_gate_fold', 'ffbp_gate_taper', 'ffbp_batch_create', 'ffbp_batch_form', 'ffbp_batch_destroy', 'ffbp_mlp_taps', 'ffbp_mlp_grad', 'ffbp_mlp_train_step',
-           'ffbp_plan_check', 'ffbp_plan_test_wait', 'ffbp_level_fused', 'ffbp_level_tc_ex', 'ffbp_plan_test_transfer')
+           'ffbp_plan_check', 'ffbp_plan_test_wait', 'ffbp_level_fused', 'ffbp_level_tc_ex', 'ffbp_plan_test_transfer',
+           'ffbp_box_mean', 'ffbp_coherence', 'ffbp_multilook', 'ffbp_mean_add', 'ffbp_mean_image', 'ffbp_tile_stats',
+           'ffbp_cross_spectrum', 'ffbp_ramp_multiply', 'ffbp_shift_crop')
 
 _c_int, _c_double, _vp = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
 
@@ -122,6 +125,16 @@ def load():
     L.ffbp_bp_points_f64.argtypes = [_vp, _c_int, _c_int, _vp, _vp, _vp, _vp, ctypes.c_long, _c_double, _c_double, _vp,
                                      _vp]
     L.ffbp_simulate.argtypes = [_vp, _c_int, _c_int, _c_double, _c_double, _vp, _vp, _c_int, _vp, _vp]
+    _f32, _long = ctypes.c_float, ctypes.c_long
+    L.ffbp_box_mean.argtypes = [_vp, _c_int, _c_int, _c_int, _c_int, _c_int, _vp, _vp]
+    L.ffbp_coherence.argtypes = [_vp, _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp]
+    L.ffbp_multilook.argtypes = [_vp, _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp]
+    L.ffbp_mean_add.argtypes = [_vp, _c_int, _long, _f32, _f32, _c_int, _vp, _vp, _vp]
+    L.ffbp_mean_image.argtypes = [_vp, _vp, _long, _vp, _vp]
+    L.ffbp_tile_stats.argtypes = [_vp, _c_int, _c_int, _c_int, _f32, _vp, _vp, _vp]
+    L.ffbp_cross_spectrum.argtypes = [_vp, _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp]
+    L.ffbp_ramp_multiply.argtypes = [_vp, _c_int, _c_int, _vp, _vp, _vp]
+    L.ffbp_shift_crop.argtypes = [_vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_int, _c_int, _vp, _vp]
     for name in EXPORTS:
         getattr(L, name).restype = _c_int
     L.ffbp_level_tc_scratch_bytes.restype = ctypes.c_size_t

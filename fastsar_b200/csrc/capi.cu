@@ -1056,6 +1056,107 @@ int ffbp_simulate(const double *d_ant, int P, int K, double fmin, double df, con
     return FFBP_OK;
 }
 
+// ------------------------------------------------------------------------------------------------ stack products
+static int image_args(const char *who, const void *p, int n1, int n2)
+{
+    if (!p) return fail(FFBP_E_ARG, "%s: null buffer", who);
+    if (n1 < 1 || n2 < 1) return fail(FFBP_E_ARG, "%s: image of %d x %d pixels", who, n1, n2);
+    if ((long long)n1 * n2 >= (1LL << 40)) return fail(FFBP_E_ARG, "%s: image of %d x %d pixels", who, n1, n2);
+    return FFBP_OK;
+}
+
+static int done(cudaError_t e, const char *who) { return e == cudaSuccess ? FFBP_OK : cuda_fail(e, who); }
+
+int ffbp_box_mean(const void *d_in, int kind, int n1, int n2, int w, int to_db, float *d_out, void *stream)
+{
+    if (int r = image_args("ffbp_box_mean", d_in, n1, n2)) return r;
+    if (!d_out) return fail(FFBP_E_ARG, "ffbp_box_mean: null output");
+    if (kind < FFBP_PIX_AS_IS || kind > FFBP_PIX_SQUARE) return fail(FFBP_E_ARG, "ffbp_box_mean: pixel kind %d", kind);
+    if (w < 1 || w > 33) return fail(FFBP_E_UNSUPPORTED, "ffbp_box_mean: window %d (1 to 33 pixels)", w);
+    return done(ffbp::launch_box_mean(d_in, kind, n1, n2, w, to_db, d_out, static_cast<cudaStream_t>(stream)),
+                "ffbp_box_mean");
+}
+
+int ffbp_coherence(const void *d_a, const void *d_b, int n1, int n2, int w1, int w2, float *d_out, void *stream)
+{
+    if (int r = image_args("ffbp_coherence", d_a, n1, n2)) return r;
+    if (!d_b || !d_out) return fail(FFBP_E_ARG, "ffbp_coherence: null buffer");
+    if (w1 < 1 || w1 > 1024 || w2 < 1 || w2 > 64)
+        return fail(FFBP_E_UNSUPPORTED, "ffbp_coherence: window %d x %d (1 to 1024 rows, 1 to 64 columns)", w1, w2);
+    return done(ffbp::launch_coherence(static_cast<const float2 *>(d_a), static_cast<const float2 *>(d_b), n1, n2, w1,
+                                       w2, d_out, static_cast<cudaStream_t>(stream)),
+                "ffbp_coherence");
+}
+
+int ffbp_multilook(const void *d_img, const void *d_b, int n1, int n2, int la, int lr, void *d_out, void *stream)
+{
+    if (int r = image_args("ffbp_multilook", d_img, n1, n2)) return r;
+    if (!d_out) return fail(FFBP_E_ARG, "ffbp_multilook: null output");
+    if (la < 1 || lr < 1) return fail(FFBP_E_ARG, "ffbp_multilook: looks %d x %d", la, lr);
+    return done(ffbp::launch_multilook(static_cast<const float2 *>(d_img), static_cast<const float2 *>(d_b), n1, n2,
+                                       la, lr, d_out, static_cast<cudaStream_t>(stream)),
+                "ffbp_multilook");
+}
+
+int ffbp_mean_add(const void *d_img, int kind, long n, float w, float weight, int first, float *d_sum, float *d_wsum,
+                  void *stream)
+{
+    if (!d_img || !d_sum || !d_wsum) return fail(FFBP_E_ARG, "ffbp_mean_add: null buffer");
+    if (n < 0) return fail(FFBP_E_ARG, "ffbp_mean_add: %ld pixels", n);
+    if (kind != FFBP_PIX_POWER && kind != FFBP_PIX_SQUARE) return fail(FFBP_E_ARG, "ffbp_mean_add: pixel kind %d", kind);
+    return done(ffbp::launch_mean_add(d_img, kind, n, w, weight, first, d_sum, d_wsum, static_cast<cudaStream_t>(stream)),
+                "ffbp_mean_add");
+}
+
+int ffbp_mean_image(const float *d_sum, const float *d_wsum, long n, float *d_out, void *stream)
+{
+    if (!d_sum || !d_wsum || !d_out) return fail(FFBP_E_ARG, "ffbp_mean_image: null buffer");
+    if (n < 0) return fail(FFBP_E_ARG, "ffbp_mean_image: %ld pixels", n);
+    return done(ffbp::launch_mean_image(d_sum, d_wsum, n, d_out, static_cast<cudaStream_t>(stream)), "ffbp_mean_image");
+}
+
+int ffbp_tile_stats(const float *d_x, int n1, int n2, int T, float gain, float *d_mean, float *d_var, void *stream)
+{
+    if (int r = image_args("ffbp_tile_stats", d_x, n1, n2)) return r;
+    if (!d_mean || !d_var) return fail(FFBP_E_ARG, "ffbp_tile_stats: null output");
+    if (T < 1) return fail(FFBP_E_ARG, "ffbp_tile_stats: tile %d", T);
+    if ((long long)(n1 / T) * (n2 / T) >= (1LL << 31)) return fail(FFBP_E_ARG, "ffbp_tile_stats: too many tiles");
+    return done(ffbp::launch_tile_stats(d_x, n1, n2, T, gain, d_mean, d_var, static_cast<cudaStream_t>(stream)),
+                "ffbp_tile_stats");
+}
+
+int ffbp_cross_spectrum(const void *d_A, const void *d_B, int batch, int m1, int m2h, int nyquist, const float *d_e1,
+                        const float *d_e2, void *d_X, double *d_energy, void *stream)
+{
+    if (int r = image_args("ffbp_cross_spectrum", d_A, m1, m2h)) return r;
+    if (!d_B || !d_X || !d_energy || (!d_e1 != !d_e2)) return fail(FFBP_E_ARG, "ffbp_cross_spectrum: null buffer");
+    if (batch < 1 || batch > 65535) return fail(FFBP_E_ARG, "ffbp_cross_spectrum: batch of %d", batch);
+    return done(ffbp::launch_cross_spectrum(static_cast<const float2 *>(d_A), static_cast<const float2 *>(d_B), batch,
+                                            m1, m2h, nyquist, d_e1, d_e2, static_cast<float2 *>(d_X), d_energy,
+                                            static_cast<cudaStream_t>(stream)),
+                "ffbp_cross_spectrum");
+}
+
+int ffbp_ramp_multiply(void *d_F, int m1, int m2, const void *d_r1, const void *d_r2, void *stream)
+{
+    if (int r = image_args("ffbp_ramp_multiply", d_F, m1, m2)) return r;
+    if (!d_r1 || !d_r2) return fail(FFBP_E_ARG, "ffbp_ramp_multiply: null ramp");
+    return done(ffbp::launch_ramp_multiply(static_cast<float2 *>(d_F), m1, m2, static_cast<const float2 *>(d_r1),
+                                           static_cast<const float2 *>(d_r2), static_cast<cudaStream_t>(stream)),
+                "ffbp_ramp_multiply");
+}
+
+int ffbp_shift_crop(const void *d_shifted, int ld, const void *d_src, int src_complex, int n1, int n2, int w0, int w1,
+                    void *d_out, void *stream)
+{
+    if (int r = image_args("ffbp_shift_crop", d_src, n1, n2)) return r;
+    if (!d_out) return fail(FFBP_E_ARG, "ffbp_shift_crop: null output");
+    if (d_shifted && ld < n2) return fail(FFBP_E_ARG, "ffbp_shift_crop: leading dimension %d below %d", ld, n2);
+    return done(ffbp::launch_shift_crop(static_cast<const float2 *>(d_shifted), ld, d_src, src_complex, n1, n2, w0, w1,
+                                        d_out, static_cast<cudaStream_t>(stream)),
+                "ffbp_shift_crop");
+}
+
 }  // extern "C"
 
 namespace ffbp {

@@ -128,4 +128,23 @@ cudaError_t mlp_train_step(float *params, float *adam, const float *x, int nq, c
                            const int *inst, const float *wt, int ninst, const double *f, const float2 *y, int S,
                            float lr, int t, float *loss, float *work, cudaStream_t s);
 
+// Stack products (products.cu): box means, coherence, multilook / interferogram, the running average, tile statistics,
+// the correlation's cross-spectrum, a spectrum's separable ramp and the translation's crop. kind: 0 the float as
+// is, 1 |z|^2 of complex64, 2 x^2 of float.
+cudaError_t launch_box_mean(const void *in, int kind, int n1, int n2, int w, int to_db, float *out, cudaStream_t s);
+cudaError_t launch_coherence(const float2 *a, const float2 *b, int n1, int n2, int w1, int w2, float *out,
+                             cudaStream_t s);
+cudaError_t launch_multilook(const float2 *a, const float2 *b, int n1, int n2, int la, int lr, void *out,
+                             cudaStream_t s);
+cudaError_t launch_mean_add(const void *img, int kind, long n, float w, float weight, int first, float *sum,
+                            float *wsum, cudaStream_t s);
+cudaError_t launch_mean_image(const float *sum, const float *wsum, long n, float *out, cudaStream_t s);
+cudaError_t launch_tile_stats(const float *x, int n1, int n2, int T, float gain, float *mean, float *var,
+                              cudaStream_t s);
+cudaError_t launch_cross_spectrum(const float2 *A, const float2 *B, int batch, int m1, int m2h, int nyquist,
+                                  const float *e1, const float *e2, float2 *X, double *energy, cudaStream_t s);
+cudaError_t launch_ramp_multiply(float2 *F, int m1, int m2, const float2 *r1, const float2 *r2, cudaStream_t s);
+cudaError_t launch_shift_crop(const float2 *shifted, int ld, const void *src, int src_complex, int n1, int n2, int w0,
+                              int w1, void *out, cudaStream_t s);
+
 }  // namespace ffbp

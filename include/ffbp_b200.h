@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define FFBP_B200_ABI_VERSION 4
+#define FFBP_B200_ABI_VERSION 5
 
 enum {
     FFBP_OK = 0,
@@ -363,6 +363,61 @@ int ffbp_bp_points_f64(const void *d_prof, int P, int nfft, const double *d_tx, 
  * float64, the sum in float64 per sample. d_ant [P, 3], d_pos [N, 3] float64; d_amp [N] complex128.               */
 int ffbp_simulate(const double *d_ant, int P, int K, double fmin, double df, const double *d_pos, const void *d_amp,
                   int N, void *d_S, void *stream);
+
+/* ---------------------------------------------------------------------------------------------------------------
+ * Stack products: what the reference computes from images formed on one grid (fastsar/stack.py:485-1124 register,
+ * shift_image, mean; fastsar/products.py:28-67 multilook, interferogram, coherence). Images are row-major [n1, n2]
+ * device buffers; complex images complex64. A pixel kind says what a buffer holds and which intensity is taken:  */
+enum {
+    FFBP_PIX_AS_IS = 0,     /* float32, taken as it is (an intensity already)                                  */
+    FFBP_PIX_POWER = 1,     /* complex64, intensity re*re + im*im (each product rounded to float32)            */
+    FFBP_PIX_SQUARE = 2     /* float32 amplitude, intensity x*x                                                */
+};
+
+/* The mean over w x w pixels about each pixel of the intensity, the edge pixels repeated (fastsar/stack.py:493-528
+ * _box of _power): the window spans (w - 1) / 2 before and w / 2 after; the w rows are summed in order and divided
+ * by w in float32, then the w columns likewise, so the result equals the reference's bit for bit. to_db: 10 log10
+ * of max(mean, 1e-30) instead (the registration's detected image before its clip). 1 <= w <= 33.              */
+int ffbp_box_mean(const void *d_in, int kind, int n1, int n2, int w, int to_db, float *d_out, void *stream);
+
+/* Sample coherence |<a b*>| / sqrt(<|a|^2> <|b|^2>) over w1 x w2 windows, float64 sums, the edge pixels repeated
+ * (fastsar/products.py:53-67 coherence, scipy.ndimage.uniform_filter's window placement: i - w/2 .. i - w/2 + w - 1).
+ * d_out [n1, n2] float32. 1 <= w1 <= 1024, 1 <= w2 <= 64.                                                        */
+int ffbp_coherence(const void *d_a, const void *d_b, int n1, int n2, int w1, int w2, float *d_out, void *stream);
+
+/* |img|^2 (d_b NULL; d_out float32) or img conj(b) (d_out complex64) averaged over la x lr boxes and decimated:
+ * d_out [n1 / la, n2 / lr] (fastsar/products.py:28-32 multilook, 42-50 interferogram).                         */
+int ffbp_multilook(const void *d_img, const void *d_b, int n1, int n2, int la, int lr, void *d_out, void *stream);
+
+/* One image into a running incoherent average (fastsar/stack.py:1060-1083): with p the pixel's intensity (kind
+ * FFBP_PIX_POWER or FFBP_PIX_SQUARE), d_sum = (first ? 0 : d_sum) + p w and d_wsum = (first ? 0 : d_wsum) + (p > 0 ?
+ * weight : 0), each product and sum rounded to float32 once. w: the weight times the equalizing gain.           */
+int ffbp_mean_add(const void *d_img, int kind, long n, float w, float weight, int first, float *d_sum, float *d_wsum,
+                  void *stream);
+
+/* The average: d_out = d_wsum > 0 ? d_sum / max(d_wsum, 1e-30) : 0, float32 (fastsar/stack.py:1092-1094).          */
+int ffbp_mean_image(const float *d_sum, const float *d_wsum, long n, float *d_out, void *stream);
+
+/* Mean and population variance of x gain over each whole T x T tile (fastsar/stack.py:1027-1034), float64 sums:
+ * d_mean, d_var [(n1 / T) (n2 / T)] float32, tiles row by row.                                                     */
+int ffbp_tile_stats(const float *d_x, int n1, int n2, int T, float gain, float *d_mean, float *d_var, void *stream);
+
+/* The correlation's cross-spectra of a batch of image pairs over a real transform's half plane, d_A, d_B, d_X
+ * [batch, m1, m2h] (fastsar/stack.py:570-592): X = conj(A) B hp with hp = 1 - e1[i] e2[j] (the separable factors of
+ * the Gaussian the high pass removes; d_e1 NULL: no high pass), and d_energy [batch, 2] float64 = the sums of
+ * |A|^2 wk hp and |B|^2 wk hp, wk 1 for the zero column and (nyquist != 0) the last, 2 for the others.           */
+int ffbp_cross_spectrum(const void *d_A, const void *d_B, int batch, int m1, int m2h, int nyquist, const float *d_e1,
+                        const float *d_e2, void *d_X, double *d_energy, void *stream);
+
+/* d_F [m1, m2] complex64 *= r1[i] r2[j]: a separable phase ramp on a spectrum (fastsar/stack.py:700-706).           */
+int ffbp_ramp_multiply(void *d_F, int m1, int m2, const void *d_r1, const void *d_r2, void *stream);
+
+/* The translation's crop (fastsar/stack.py:712-725): d_out[i, j] = shifted[i + w0, j + w1] where that source pixel
+ * lies in the image and d_src is not 0 there, else 0. d_shifted: the sub-pixel-shifted image (complex64, leading
+ * dimension ld), or NULL for a whole-pixel move of d_src itself. src_complex: d_src and d_out complex64; else
+ * float32, and the shifted image's real part clipped at 0.                                                       */
+int ffbp_shift_crop(const void *d_shifted, int ld, const void *d_src, int src_complex, int n1, int n2, int w0, int w1,
+                    void *d_out, void *stream);
 
 #ifdef __cplusplus
 }

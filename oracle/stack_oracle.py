@@ -14,7 +14,8 @@ common grid:
 Parity is pinned: tests/test_stack_oracle.py checks every function here against the reference's own outputs on
 seeded images (tests/golden/stack.npz, written by tests/golden/make_golden.py --only stack from saulpingerman/FastSAR
 0.3.1): the float32 box sums bit for bit (the same additions in the same order), the rest to the rounding of the
-transforms.
+transforms. Its transforms use every host core (scipy.fft workers=-1, as the reference's NumPy path does,
+fastsar/stack.py:464-466).
 """
 import numpy as np
 from scipy import fft as sfft
@@ -98,13 +99,13 @@ def peak(a, b, max_shift, around=(0, 0), narrow=None, up=16, highpass=32.0):
     win = hann(n1)[:, None] * hann(n2)[None, :]
     aw, bw = (a - a.mean()) * win, (b - b.mean()) * win
     fs = (sfft.next_fast_len(n1, real=True), sfft.next_fast_len(n2, real=True))
-    A, B = sfft.rfft2(aw, s=fs), sfft.rfft2(bw, s=fs)
+    A, B = sfft.rfft2(aw, s=fs, workers=-1), sfft.rfft2(bw, s=fs, workers=-1)
     X = np.conj(A) * B
     hp = None
     if highpass:
         hp = highpass_filter(fs, highpass)
         X = X * hp
-    cc = sfft.irfft2(X, s=fs)
+    cc = sfft.irfft2(X, s=fs, workers=-1)
     m1, m2 = min(int(max_shift), fs[0] // 2 - 1), min(int(max_shift), fs[1] // 2 - 1)
     r1 = (int(around[0]) + np.arange(-m1, m1 + 1)) % fs[0]
     r2 = (int(around[1]) + np.arange(-m2, m2 + 1)) % fs[1]
@@ -184,9 +185,9 @@ def translate(img, d):
     out = img
     if np.abs(frac).max() > 1e-6:
         fs = (sfft.next_fast_len(n1 + 16), sfft.next_fast_len(n2 + 16))
-        F = sfft.fft2(img if cplx else img.astype(np.complex64), s=fs)
+        F = sfft.fft2(img if cplx else img.astype(np.complex64), s=fs, workers=-1)
         F = F * (ramp(fs[0], frac[0])[:, None] * ramp(fs[1], frac[1])[None, :])
-        out = sfft.ifft2(F)[:n1, :n2]
+        out = sfft.ifft2(F, workers=-1)[:n1, :n2]
         if not cplx:
             out = np.maximum(out.real, 0).astype(img.dtype)
 
