@@ -4,6 +4,7 @@ at a time and for small profiler captures (the commands of profiles/*.md run it)
     python -m fastsar_b200.cases level L1 [--parents 8] [--pulses 2048] [--form tc|fused|fp32] [--fir 0|1|2] [--taps learned|80|70]
     python -m fastsar_b200.cases final [--tiles 20000] [--mode f16|bf16x3|fp32] [--taps learned|80|70]
     python -m fastsar_b200.cases exact [--workload spotlight_4k] [--interp cubic|linear] [--pulses 1024]
+    python -m fastsar_b200.cases products [--side 4096] [--window 7]
 
 `level`: one merge stage of the plan (its children, decimations and filters) on `--parents` parents of random
 samples and random child phases, through ffbp_level_tc (tensor cores in two passes: level_tc_gemm and level_fir),
@@ -157,9 +158,44 @@ def exact_case(workload='spotlight_4k', interp='cubic', pulses=1024, reps=5):
                   f'{f.nx * f.ny * n / (ms * 1e-3) / 1e9:.0f} GBP/s', flush=True)
 
 
+def products_case(side=4096, window=7, reps=3, seed=3):
+    """The stack products' pixel kernels alone on two seeded complex images side x side on the device: the coherence
+    map (window x window), the detected image's box mean in dB (box 5), a running-average step and the 32 x 32 tile
+    statistics, each event-timed with the bytes it must move (GB/s)."""
+    import torch
+    L = _lib.load()
+    g = torch.Generator(device='cuda').manual_seed(seed)
+    a = torch.randn((side, side), dtype=torch.complex64, device='cuda', generator=g)
+    b = torch.randn((side, side), dtype=torch.complex64, device='cuda', generator=g)
+    out = torch.empty((side, side), dtype=torch.float32, device='cuda')
+    acc, wacc = torch.empty_like(out), torch.empty_like(out)
+    tm, tv = torch.empty(max((side // 32) ** 2, 1), device='cuda'), torch.empty(max((side // 32) ** 2, 1), device='cuda')
+    st = torch.cuda.current_stream().cuda_stream
+    n = side * side
+    cases = [
+        ('coherence_kernel', 20 * n, lambda: L.ffbp_coherence(a.data_ptr(), b.data_ptr(), side, side, window, window,
+                                                              out.data_ptr(), st)),
+        ('box_kernel', 12 * n, lambda: L.ffbp_box_mean(a.data_ptr(), _lib.PIX_POWER, side, side, 5, 1, out.data_ptr(), st)),
+        ('mean_add_kernel', 24 * n, lambda: L.ffbp_mean_add(a.data_ptr(), _lib.PIX_POWER, n, 1.0, 1.0, 0, acc.data_ptr(),
+                                                            wacc.data_ptr(), st)),
+        ('tile_stats_kernel', 4 * n, lambda: L.ffbp_tile_stats(out.data_ptr(), side, side, 32, 1.0, tm.data_ptr(),
+                                                               tv.data_ptr(), st)),
+    ]
+    for name, nbytes, fn in cases:
+        for r in range(reps + 1):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            _lib.check(fn(), name)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            if r:
+                print(f'{name} {side} x {side}: {ms:.3f} ms, {nbytes / (ms * 1e-3) / 1e9:.0f} GB/s', flush=True)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description='time one stage of a workload plan')
-    ap.add_argument('stage', choices=('level', 'final', 'exact'))
+    ap.add_argument('stage', choices=('level', 'final', 'exact', 'products'))
     ap.add_argument('level', nargs='?', default='L1', choices=('L0', 'L1', 'L2'))
     ap.add_argument('--parents', type=int, default=8)
     ap.add_argument('--pulses', type=int, default=0)
@@ -175,8 +211,12 @@ def main(argv=None):
     ap.add_argument('--pmax', type=float, default=0.5)
     ap.add_argument('--workload', default='spotlight_4k', help='exact: the workload')
     ap.add_argument('--interp', choices=('cubic', 'linear'), default='cubic', help='exact: the interpolation')
+    ap.add_argument('--side', type=int, default=4096, help='products: the images\' side')
+    ap.add_argument('--window', type=int, default=7, help='products: the coherence window')
     a = ap.parse_args(argv)
-    if a.stage == 'exact':
+    if a.stage == 'products':
+        products_case(a.side, a.window, a.reps)
+    elif a.stage == 'exact':
         exact_case(a.workload, a.interp, a.pulses or 1024, a.reps)
     elif a.stage == 'level':
         import json

@@ -1120,7 +1120,7 @@ int ffbp_tile_stats(const float *d_x, int n1, int n2, int T, float gain, float *
     if (int r = image_args("ffbp_tile_stats", d_x, n1, n2)) return r;
     if (!d_mean || !d_var) return fail(FFBP_E_ARG, "ffbp_tile_stats: null output");
     if (T < 1) return fail(FFBP_E_ARG, "ffbp_tile_stats: tile %d", T);
-    if ((long long)(n1 / T) * (n2 / T) >= (1LL << 31)) return fail(FFBP_E_ARG, "ffbp_tile_stats: too many tiles");
+    if ((long long)(n1 / T) * (n2 / T) >= (1LL << 31) || n1 / T > 65535) return fail(FFBP_E_ARG, "ffbp_tile_stats: too many tiles");
     return done(ffbp::launch_tile_stats(d_x, n1, n2, T, gain, d_mean, d_var, static_cast<cudaStream_t>(stream)),
                 "ffbp_tile_stats");
 }

@@ -72,47 +72,66 @@ __global__ void __launch_bounds__(256) box_kernel(const void *__restrict__ in, i
 // Sample coherence over w1 x w2 windows, the edge pixels repeated, the window of pixel i spanning i - w / 2 to
 // i - w / 2 + w - 1 along each axis (scipy.ndimage.uniform_filter's placement, fastsar/products.py:35-39). A block
 // of 128 threads owns 128 - (w2 - 1) output columns and a run of rows: each thread keeps the float64 running sums
-// of (Re a b*, Im a b*, |a|^2, |b|^2) over the w1 rows of its column (one row in and one out per output row); the
-// row's 128 column sums go through shared memory to the w2-wide horizontal sums.
+// of (Re a b*, Im a b*, |a|^2, |b|^2) over the w1 rows of its column (one row in and one out per output row, fetched
+// an output row ahead of their use); the row's 128 column sums go through shared memory as float32 (16 bytes a
+// column: the shared-memory traffic of the w2-wide sums, which bounds the kernel, halved) to the horizontal sums,
+// and the coherence is formed from those in float64. Rounding the column sums to float32 moves a coherence by about
+// 1e-7.
 constexpr int COH_NT = 128;
 
 __global__ void __launch_bounds__(COH_NT) coherence_kernel(const float2 *__restrict__ a, const float2 *__restrict__ b,
                                                            int n1, int n2, int w1, int w2, int rows,
                                                            float *__restrict__ out)
 {
-    __shared__ double4 sv[COH_NT];
+    __shared__ float4 sv[COH_NT];
     const int t = threadIdx.x, oc = COH_NT - (w2 - 1);
     const int c0 = blockIdx.x * oc, lo1 = w1 / 2, lo2 = w2 / 2;
     const int c = clampi(c0 - lo2 + t, 0, n2 - 1);
     const int rbeg = blockIdx.y * rows, rend = min(rbeg + rows, n1);
     double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-    auto take = [&](int r, double sign) {
-        r = clampi(r, 0, n1 - 1);
-        const float2 za = a[(size_t)r * n2 + c], zb = b[(size_t)r * n2 + c];
+    auto fetch = [&](int r, float2 &za, float2 &zb) {
+        const size_t k = (size_t)clampi(r, 0, n1 - 1) * n2 + c;
+        za = a[k];
+        zb = b[k];
+    };
+    auto apply = [&](float2 za, float2 zb, double sign) {
         const double ar = za.x, ai = za.y, br = zb.x, bi = zb.y;
         s0 += sign * (ar * br + ai * bi);
         s1 += sign * (ai * br - ar * bi);
         s2 += sign * (ar * ar + ai * ai);
         s3 += sign * (br * br + bi * bi);
     };
-    for (int k = 0; k < w1; ++k) take(rbeg - lo1 + k, 1.0);
+    for (int k = 0; k < w1; ++k) {
+        float2 za, zb;
+        fetch(rbeg - lo1 + k, za, zb);
+        apply(za, zb, 1.0);
+    }
+    // the rows that enter and leave the window at the next slide, fetched an output row ahead of their use
+    float2 ia, ib, xa, xb;
+    fetch(rbeg + 1 - lo1 + w1 - 1, ia, ib);
+    fetch(rbeg - lo1, xa, xb);
     for (int r = rbeg; r < rend; ++r) {
-        sv[t] = make_double4(s0, s1, s2, s3);
+        sv[t] = make_float4((float)s0, (float)s1, (float)s2, (float)s3);
         __syncthreads();
         if (t < oc && c0 + t < n2) {
-            double h0 = 0.0, h1 = 0.0, h2 = 0.0, h3 = 0.0;
+            float h0 = 0.f, h1 = 0.f, h2 = 0.f, h3 = 0.f;
             for (int k = 0; k < w2; ++k) {
-                const double4 v = sv[t + k];
+                const float4 v = sv[t + k];
                 h0 += v.x; h1 += v.y; h2 += v.z; h3 += v.w;
             }
-            // the windows' 1 / (w1 w2) cancels between the numerator and the denominator
-            const double num = sqrt(h0 * h0 + h1 * h1), den = sqrt(fmax(h2, 0.0) * fmax(h3, 0.0));
-            out[(size_t)r * n2 + c0 + t] = (float)(num / fmax(den, 1e-300));
+            // |sum a b*|^2 / (sum |a|^2 sum |b|^2): the windows' 1 / (w1 w2) cancels; the ratio in float64 (the
+            // product of two intensity sums can pass float32's range), its square root to float32
+            const double num = (double)h0 * h0 + (double)h1 * h1, den = (double)fmaxf(h2, 0.f) * fmaxf(h3, 0.f);
+            out[(size_t)r * n2 + c0 + t] = sqrtf((float)(num / fmax(den, 1e-300)));
         }
         __syncthreads();
         if (r + 1 < rend) {
-            take(r + 1 - lo1 + w1 - 1, 1.0);
-            take(r - lo1, -1.0);
+            apply(ia, ib, 1.0);
+            apply(xa, xb, -1.0);
+            if (r + 2 < rend) {
+                fetch(r + 2 - lo1 + w1 - 1, ia, ib);
+                fetch(r + 1 - lo1, xa, xb);
+            }
         }
     }
 }
@@ -169,32 +188,35 @@ __global__ void mean_image_kernel(const float *__restrict__ sum, const float *__
     }
 }
 
-// One block per T x T tile: the mean and the (population) variance of x gain over the tile, from float64 sums.
-__global__ void __launch_bounds__(256) tile_stats_kernel(const float *__restrict__ x, int n2, int t2, int T,
-                                                         float gain, float *__restrict__ mean, float *__restrict__ var)
+// One warp per T x T tile, eight neighbouring tiles of a tile row per block (coalesced rows): the mean and the
+// (population) variance of x gain over the tile, from float64 sums.
+constexpr int TS_WARPS = 8;
+
+__global__ void __launch_bounds__(TS_WARPS * 32) tile_stats_kernel(const float *__restrict__ x, int n2, int t2, int T,
+                                                                   float gain, float *__restrict__ mean,
+                                                                   float *__restrict__ var)
 {
-    __shared__ double red[2][8];
-    const int ti = blockIdx.x / t2, tj = blockIdx.x - ti * t2;
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int ti = blockIdx.y, tj = blockIdx.x * TS_WARPS + warp;
+    if (tj >= t2) return;
+    const float *base = x + (size_t)ti * T * n2 + (size_t)tj * T;
     double s = 0.0, q = 0.0;
-    for (int e = threadIdx.x; e < T * T; e += blockDim.x) {
-        const int u = e / T, v = e - u * T;
-        const double val = __fmul_rn(x[(size_t)(ti * T + u) * n2 + tj * T + v], gain);
-        s += val;
-        q += val * val;
+#pragma unroll 8
+    for (int u = 0; u < T; ++u) {
+        for (int v = lane; v < T; v += 32) {
+            const double val = __fmul_rn(base[(size_t)u * n2 + v], gain);
+            s += val;
+            q += val * val;
+        }
     }
     for (int o = 16; o > 0; o >>= 1) {
         s += __shfl_xor_sync(0xffffffffu, s, o);
         q += __shfl_xor_sync(0xffffffffu, q, o);
     }
-    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    if (lane == 0) { red[0][warp] = s; red[1][warp] = q; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double S = 0.0, Q = 0.0;
-        for (int k = 0; k < (int)(blockDim.x / 32); ++k) { S += red[0][k]; Q += red[1][k]; }
-        const double nn = (double)T * T, m = S / nn;
-        mean[blockIdx.x] = (float)m;
-        var[blockIdx.x] = (float)fmax(Q / nn - m * m, 0.0);
+    if (lane == 0) {
+        const double nn = (double)T * T, m = s / nn;
+        mean[(size_t)ti * t2 + tj] = (float)m;
+        var[(size_t)ti * t2 + tj] = (float)fmax(q / nn - m * m, 0.0);
     }
 }
 
@@ -337,7 +359,8 @@ cudaError_t launch_tile_stats(const float *x, int n1, int n2, int T, float gain,
 {
     const int t1 = n1 / T, t2 = n2 / T;
     if (t1 * t2 == 0) return cudaSuccess;
-    tile_stats_kernel<<<t1 * t2, 256, 0, s>>>(x, n2, t2, T, gain, mean, var);
+    if (t1 > 65535) return cudaErrorInvalidValue;
+    tile_stats_kernel<<<dim3((t2 + TS_WARPS - 1) / TS_WARPS, t1), TS_WARPS * 32, 0, s>>>(x, n2, t2, T, gain, mean, var);
     return cudaGetLastError();
 }
 
