@@ -1146,6 +1146,39 @@ int ffbp_ramp_multiply(void *d_F, int m1, int m2, const void *d_r1, const void *
                 "ffbp_ramp_multiply");
 }
 
+int ffbp_mosaic_pad(const void *d_S, long ldS, int rows, int K, int K2, int npl, const double *d_shift, double f0,
+                    double df, void *d_out, void *stream)
+{
+    if (!d_S || !d_out) return fail(FFBP_E_ARG, "ffbp_mosaic_pad: null buffer");
+    if (rows < 0 || K < 1 || K2 < 1 || npl < 0 || npl + K > K2 || ldS < K)
+        return fail(FFBP_E_ARG, "ffbp_mosaic_pad: %d samples at %d of %d (leading dimension %ld)", K, npl, K2, ldS);
+    return done(ffbp::launch_mosaic_pad(static_cast<const float2 *>(d_S), ldS, rows, K, K2, npl, d_shift, f0, df,
+                                        static_cast<float2 *>(d_out), static_cast<cudaStream_t>(stream)),
+                "ffbp_mosaic_pad");
+}
+
+int ffbp_mosaic_gather(const void *d_Q, long ldQ, int rows, int K2, int N, const int *d_m, void *d_u, void *stream)
+{
+    if (!d_Q || !d_u) return fail(FFBP_E_ARG, "ffbp_mosaic_gather: null buffer");
+    if (rows < 0 || K2 < 1 || N < 1 || ldQ < K2)
+        return fail(FFBP_E_ARG, "ffbp_mosaic_gather: %d bins of %d (leading dimension %ld)", N, K2, ldQ);
+    return done(ffbp::launch_mosaic_gather(static_cast<const float2 *>(d_Q), ldQ, rows, K2, N, d_m,
+                                           static_cast<float2 *>(d_u), static_cast<cudaStream_t>(stream)),
+                "ffbp_mosaic_gather");
+}
+
+int ffbp_mosaic_gate(const void *d_U, long ldU, int rows, int k0, int nk, int N, const double *d_d, const void *d_cph,
+                     double scale, const float *d_taper, void *d_out, void *stream)
+{
+    if (!d_U || !d_taper || !d_out) return fail(FFBP_E_ARG, "ffbp_mosaic_gate: null buffer");
+    if (rows < 0 || k0 < 0 || nk < 0 || N < 1 || k0 + nk > ldU)
+        return fail(FFBP_E_ARG, "ffbp_mosaic_gate: samples %d .. %d of rows of %ld", k0, k0 + nk, ldU);
+    return done(ffbp::launch_mosaic_gate(static_cast<const float2 *>(d_U), ldU, rows, k0, nk, N, d_d,
+                                         static_cast<const double2 *>(d_cph), scale, d_taper,
+                                         static_cast<float2 *>(d_out), static_cast<cudaStream_t>(stream)),
+                "ffbp_mosaic_gate");
+}
+
 int ffbp_shift_crop(const void *d_shifted, int ld, const void *d_src, int src_complex, int n1, int n2, int w0, int w1,
                     void *d_out, void *stream)
 {

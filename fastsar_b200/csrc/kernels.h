@@ -147,4 +147,13 @@ cudaError_t launch_ramp_multiply(float2 *F, int m1, int m2, const float2 *r1, co
 cudaError_t launch_shift_crop(const float2 *shifted, int ld, const void *src, int src_complex, int n1, int n2, int w0,
                               int w1, void *out, cudaStream_t s);
 
+// A patch mosaic's per-patch history (mosaic.cu): padding with the re-referencing phase, the gate's gather, and the
+// gated spectrum's ramp, constant and taper.
+cudaError_t launch_mosaic_pad(const float2 *S, long ldS, int rows, int K, int K2, int npl, const double *shift,
+                              double f0, double df, float2 *out, cudaStream_t s);
+cudaError_t launch_mosaic_gather(const float2 *Q, long ldQ, int rows, int K2, int N, const int *m, float2 *u,
+                                 cudaStream_t s);
+cudaError_t launch_mosaic_gate(const float2 *U, long ldU, int rows, int k0, int nk, int N, const double *d,
+                               const double2 *cph, double scale, const float *taper, float2 *out, cudaStream_t s);
+
 }  // namespace ffbp

@@ -419,6 +419,25 @@ int ffbp_ramp_multiply(void *d_F, int m1, int m2, const void *d_r1, const void *
 int ffbp_shift_crop(const void *d_shifted, int ld, const void *d_src, int src_complex, int n1, int n2, int w0, int w1,
                     void *d_out, void *stream);
 
+/* ---------------------------------------------------------------------------------------------------------------
+ * Patch mosaic: one patch's phase history re-referenced to the patch centre and gated in range to the patch
+ * (fastsar/patches.py:315-500 range_profiles, patch_history), around the caller's transforms (cuFFT).            */
+
+/* d_out [rows, K2] complex64: row p's K samples of d_S (leading dimension ldS) at columns npl .. npl + K - 1, zeros
+ * elsewhere, times exp(-4 pi i f_k d_shift[p] / c) with f_k = f0 + k df (d_shift NULL: no phase; the shared range
+ * profiles' padding). Phases in float64.                                                                          */
+int ffbp_mosaic_pad(const void *d_S, long ldS, int rows, int K, int K2, int npl, const double *d_shift, double f0,
+                    double df, void *d_out, void *stream);
+
+/* d_u [rows, N] complex64: u[p, n] = Q[p, (j_n - m[p]) mod K2] with j_n = n for n < N / 2 and n - N otherwise (the
+ * gate's bins about the centre), Q with leading dimension ldQ; d_m [rows] int32 or NULL (no offset).                */
+int ffbp_mosaic_gather(const void *d_Q, long ldQ, int rows, int K2, int N, const int *d_m, void *d_u, void *stream);
+
+/* d_out [rows, nk] complex64: U[p, k0 + k] exp(-2 pi i d[p] (k0 + k) / N) cph[p] scale taper[k] (d_d, d_cph NULL:
+ * left out; d_cph complex128 [rows]; d_taper float32 [nk]); U with leading dimension ldU.                          */
+int ffbp_mosaic_gate(const void *d_U, long ldU, int rows, int k0, int nk, int N, const double *d_d, const void *d_cph,
+                     double scale, const float *d_taper, void *d_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -23,6 +23,10 @@ Fixtures:
   stack.npz           the stack products: registration (_detected, _peak, _estimate), translation (_translate),
                       incoherent average (_Mean, _level) and products.multilook / interferogram / coherence of three
                       seeded images (stack_scene below; --only stack writes this file alone)
+  mosaic.npz          the patch mosaic: form_mosaic (backend='cpu') on mosaic_scene's history in four cases (all
+                      pulses; a beam and a Hann azimuth window; one patch; uneven patches at T = 16 and 2 levels), the
+                      patch history of one patch with and without shared range profiles, and the helpers tile_plan,
+                      _levels, beam_span, fill_gaps, choose_buckets (--only mosaic writes this file alone)
   weights.npz         aperture weights: api.final_weights (plain and with gradients) of the test scene's 2-level plan
                       for a pixel- and pulse-dependent weight (WEIGHT below), and ImageFormer(backend='cpu',
                       aperture_weight=WEIGHT)'s image (--only weights writes this file alone)
@@ -302,16 +306,107 @@ def stack(fastsar):
     print('stack done', rec['est_hp_shift_px'], rec['peak_hp'], rec['mean_plain_looks'], rec['mean_median_gains'])
 
 
+def mosaic_scene(seed=20261206):
+    """A small collection for the mosaic fixtures: the reference's make_collect (0.5 m, 80 m scene, 5 km, 30 deg
+    grazing), 24 unit points of seeded phases in a 60 m square, simulated by direct sum; the FX history with its
+    reference ranges |a_p| and band. -> (collect, fx, beam): beam(idx, points) the normalized along-track offset of
+    the points seen from pulses idx, 1 at 20 m (a stripmap-like footprint of 40 m)."""
+    from fastsar import sim
+    rng = np.random.default_rng(seed)
+    col = sim.make_collect(res=0.5, scene=80.0, r0=5e3, graze_deg=30.0)
+    pos = np.c_[rng.uniform(-30.0, 30.0, (24, 2)), np.zeros(24)]
+    amp = np.exp(2j * np.pi * rng.random(24))
+    S = sim.simulate_brute(col, pos, amp).astype(np.complex64)
+    fx = dict(S=S, fmin=float(col.fmin), df=float(col.df), ref=np.linalg.norm(col.ant, axis=1),
+              band=(float(col.fmin), float(col.fmin + (col.K - 1) * col.df)))
+    ant = np.asarray(col.ant, np.float64)
+
+    def beam(idx, pts):
+        d = np.asarray(pts, np.float64)[None, :, :] - ant[np.asarray(idx)][:, None, :]
+        return d[..., 1] / 20.0
+    return col, fx, beam
+
+
+def mosaic(fastsar):
+    """mosaic.npz: the reference's patch mosaic (fastsar/patches.py form_mosaic with backend='cpu') on mosaic_scene,
+    its patch histories (patch_history with and without shared range profiles) and its host helpers."""
+    from fastsar import patches
+    col, fx, beam = mosaic_scene()
+    ant = np.asarray(col.ant, np.float64)
+    e1, e2 = (1.0, 0.0, 0.0), (0.0, 1.0, 0.0)
+    origin = np.array([-32.0, -32.0, 0.0])
+    rec = dict(S=fx['S'], fmin=fx['fmin'], df=fx['df'], ref=fx['ref'], band=np.array(fx['band']), ant=ant,
+               origin=origin)
+    cases = dict(
+        a=dict(nx=128, ny=128, patch=(64, 64), crop=8),
+        b=dict(nx=128, ny=128, patch=(64, 64), crop=8, beam=beam, umax=1.0, awin='hann'),
+        c=dict(nx=64, ny=64, patch=(64, 64), crop=0),
+        d=dict(nx=96, ny=128, patch=(48, 64), crop=4, beam=beam, umax=1.0, T=16, levels=2),
+    )
+    for tag, kw in cases.items():
+        info = []
+        kw = dict(kw)
+        nx, ny = kw.pop('nx'), kw.pop('ny')
+        img = patches.form_mosaic(fx, ant, origin, nx, ny, 0.5, 0.5, e1, e2, backend='cpu', info=info, **kw)
+        rec[f'img_{tag}'] = img
+        rec[f'info_{tag}'] = np.array([[i['pulses'][0], i['pulses'][1], i['K'], i['T'], i['sub'][0], i['sub'][1],
+                                        i['levels'], i['df']] for i in info], np.float64)
+        print('mosaic', tag, img.shape, len(info), float(np.abs(img).max()))
+    # patch histories of one patch: with the shared range profiles and without
+    c = origin + (32.0 + 8.0) * 0.5 * np.array(e1) + (32.0 + 8.0) * 0.5 * np.array(e2)
+    g = np.linspace(-40.0, 39.0, 9) * 0.5
+    pts = c + g[:, None, None] * np.array(e1) + g[None, :, None] * np.array(e2)
+    pts = pts.reshape(-1, 3)
+    lo, hi = 10, len(ant) - 12
+    prof = patches.range_profiles(fx)
+    for tag, pr in (('prof', prof), ('direct', None)):
+        Sp, a, f0, df2 = patches.patch_history(fx, ant, c, pts, lo, hi, prof=pr)
+        rec[f'ph_{tag}_S'] = Sp.astype(np.complex128)
+        rec[f'ph_{tag}_geo'] = np.array([f0, df2])
+        rec[f'ph_{tag}_a'] = a
+    rec['ph_center'], rec['ph_pts'], rec['ph_span'] = c, pts, np.array([lo, hi])
+    rec['ph_gate'] = np.array(patches.gate_bins(fx, ant, c, pts, lo, hi))
+    pad = patches._padding(fx)
+    rec['padding'] = np.array([pad[0], pad[2], pad[3], pad[4]])
+    # host helpers
+    rec['tile_plan'] = np.array([v for t in [patches.tile_plan(ant - c, col.fmin + col.K * col.df, 80, 80, 0.5, 0.5,
+                                                               e1, e2, -40.0)] for v in (t[0], t[1][0], t[1][1], t[2])])
+    rec['tile_plan_hard'] = np.array([v for t in [patches.tile_plan(ant - c, col.fmin + col.K * col.df, 400, 80, 0.25,
+                                                                    0.5, e1, e2, -70.0)]
+                                      for v in (t[0], t[1][0], t[1][1], t[2])])
+    rec['levels'] = np.array([patches._levels(n, T, longest=l) for n, T, l in
+                              ((80, 32, None), (80, 16, None), (300, 16, 900), (64, 32, 832), (5, 32, None))])
+    rec['beam_span'] = np.array(patches.beam_span(beam, len(ant), pts, 1.0))
+    gap = np.delete(ant, [5, 6, 40], axis=0)
+    fa, fi = patches.fill_gaps(gap)
+    rec['gaps_in'], rec['gaps_out'], rec['gaps_idx'] = gap, fa, fi
+    counts = [300, 310, 512, 700, 701, 1200, 1210, 1300, 257, 4000]
+    rec['buckets_counts'] = np.array(counts)
+    rec['buckets_3'] = np.array(patches.choose_buckets(counts, 3.0))
+    rec['buckets_0'] = np.array(patches.choose_buckets(counts, 0.0))
+    rec['buckets_50'] = np.array(patches.choose_buckets(counts, 50.0, step=64))
+    from fastsar import stripmap as sm
+    t = np.linspace(-1.2, 1.2, 25)
+    for tag, spec in (('taylor', 'taylor'), ('taylor30', ('taylor', 30.0, 5)), ('hann', 'hann'), ('kaiser', 'kaiser'),
+                      ('kaiser4', ('kaiser', 4.0)), ('none', None)):
+        rec[f'win_{tag}'] = sm.window(spec)(t)
+    np.savez_compressed(os.path.join(HERE, 'mosaic.npz'), **rec)
+    print('mosaic done', rec['ph_gate'], rec['tile_plan'], rec['beam_span'], rec['buckets_3'])
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--ref', default=os.environ.get('FASTSAR_REFERENCE'))
-    ap.add_argument('--only', choices=('exact', 'gate', 'weights', 'stack'), default=None)
+    ap.add_argument('--only', choices=('exact', 'gate', 'weights', 'stack', 'mosaic'), default=None)
     args = ap.parse_args()
     if not args.ref:
         sys.exit('make_golden: name the reference checkout by --ref PATH or FASTSAR_REFERENCE')
     fs = import_reference(args.ref)
     if args.only == 'stack':
         stack(fs)
+        return
+    if args.only == 'mosaic':
+        mosaic(fs)
         return
     if args.only == 'weights':
         weights(fs)
