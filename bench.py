@@ -35,6 +35,9 @@ one CUDA graph, with per-pass errors and pairwise coherence against float64.
 incoherent average with its looks and coherence maps of 8 images on the 8,192 x 8,192 grid, against the oracle's
 NumPy restatement of the reference's functions on crops.
 
+--workload mosaic_strip: a patch mosaic of a strip (run_mosaic): per-patch re-referenced, gated histories and
+formers with a beam and an azimuth window, error against float64 per patch.
+
 --workload learned_4k: the learned decimation taps against the Kaiser-sinc decimators at oversamplings of the child
 data from 4x to about 1x (run_learned): error against float64 and time per image, the float32 former throughout.
 
@@ -236,6 +239,8 @@ def main():
         return run_patches(args)
     if args.workload == 'stack_products':
         return run_stack_products(args)
+    if args.workload == 'mosaic_strip':
+        return run_mosaic(args)
     if args.workload.startswith('stack'):
         return run_stack(args)
     if args.workload.startswith('learned'):
@@ -832,10 +837,105 @@ def run_stack_products(args):
     print(json.dumps(line), flush=True)
 
 
+def run_mosaic(args):
+    """--workload mosaic_strip: a patch mosaic (fastsar_b200.mosaic.form_mosaic) of a straight-track strip: X band
+    (9.6 GHz, 600 MHz), 5 km slant range, 30 deg grazing, pulses every 0.25 m along 824 m of track, a 512 x 2,048 grid
+    at 0.25 m (128 m across, 512 m along the track) cut into 256 x 256 patches with 16 pixels of crop, each formed
+    from the pulses whose beam (a 312 m footprint along the track, the synthetic aperture of 0.25 m) reaches it, with
+    a Hann azimuth window in the final stage. One step = one whole mosaic (range profiles, per-patch histories, plans
+    and formers, as the reference's form_mosaic does them per call). The error: the same mosaic without the window
+    against the float64 exact backprojection of each patch's own pulses at random pixels of the patch (no gain)."""
+    import torch
+    from fastsar_b200 import mosaic as mo, sim
+    from fastsar_b200.exact import backproject_device
+    torch.cuda.set_device(0)
+    fc, bw, r0, psi, res, dy = 9.6e9, 600e6, 5e3, np.deg2rad(30.0), 0.25, 0.25
+    lap = r0 * (C / fc) / (2 * res)                              # the synthetic aperture of the resolution, m
+    P = int((512.0 + lap) / dy) // 2 * 2
+    ant = np.stack([np.full(P, -r0 * np.cos(psi)), (np.arange(P) - (P - 1) / 2.0) * dy, np.full(P, r0 * np.sin(psi))], 1)
+    df = C / (2 * 300.0)
+    K = int(bw / df) // 2 * 2
+    fmin = fc - (K // 2) * df
+    col = sim.Collect(fmin=fmin, df=df, K=K, ant=ant, res=res)
+    nx, ny, sp = 512, 2048, 0.25
+    e1, e2 = (1.0, 0.0, 0.0), (0.0, 1.0, 0.0)
+    origin = np.array([-nx * sp / 2, -ny * sp / 2, 0.0])
+    rng = np.random.default_rng(args.seed + 31)
+    n_pt = 400
+    pos = np.c_[rng.uniform(origin[0], -origin[0], n_pt), rng.uniform(origin[1], -origin[1], n_pt), np.zeros(n_pt)]
+    amp = np.exp(2j * np.pi * rng.random(n_pt))
+    S = sim.simulate(col, pos, amp)
+    fx = dict(S=S, fmin=fmin, df=df, ref=np.linalg.norm(ant, axis=1), band=(fmin, fmin + (K - 1) * df))
+
+    def beam(idx, pts):
+        d = np.asarray(pts, np.float64)[None, :, :] - ant[np.asarray(idx)][:, None, :]
+        return d[..., 1] / (lap / 2)
+    kw = dict(patch=(256, 256), crop=16, beam=beam, umax=1.0)
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1_.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1_) / steps
+    info = []
+    mo.form_mosaic(fx, ant, origin, nx, ny, sp, sp, e1, e2, awin='hann', info=info, device=True, **kw)
+    steps = max(1, min(args.steps, 3))
+    clk = Clocks(0)
+    ms = timed(lambda: mo.form_mosaic(fx, ant, origin, nx, ny, sp, sp, e1, e2, awin='hann', device=True, **kw), steps,
+               1)
+    clocks = clk.stop()
+    px = 256 + 32
+    bp = sum(px * px * (i['pulses'][1] - i['pulses'][0]) for i in info)
+    # accuracy: without the window, each patch against the exact sum over its own pulses
+    plain = mo.form_mosaic(fx, ant, origin, nx, ny, sp, sp, e1, e2, device=True, **kw)
+    num = den = 0.0
+    for i in info:
+        c = np.asarray(i['center'])
+        i0 = int(round((c[0] - origin[0]) / sp - px / 2)) + 16
+        j0 = int(round((c[1] - origin[1]) / sp - px / 2)) + 16
+        ii = rng.integers(i0, min(i0 + 256, nx), 200)
+        jj = rng.integers(j0, min(j0 + 256, ny), 200)
+        pts = origin + (ii[:, None] * sp) * np.array(e1) + (jj[:, None] * sp) * np.array(e2)
+        lo, hi = i['pulses']
+        ref = backproject_device(S[lo:hi], ant[lo:hi], fmin, df, pts, ref=fx['ref'][lo:hi], upsample=64,
+                                 window=False).cpu().numpy()
+        got = plain[torch.as_tensor(ii, device='cuda'), torch.as_tensor(jj, device='cuda')].cpu().numpy()
+        num += float(np.sum(np.abs(got - ref) ** 2))
+        den += float(np.sum(np.abs(ref) ** 2))
+    line = dict(
+        metric='patch mosaic of a strip (form_mosaic): giga-backprojections/s of the patches formed',
+        value=bp / (ms * 1e-3) / 1e9, unit='GBP/s', n_gpus=1, steps=steps, warmup=1, ms_per_step=ms,
+        higher_is_better=True, scaling='weak', vs_baseline=None,
+        dtype='f32 former (plain FFBP per patch), c64 transforms (cuFFT), f64 phases',
+        data=f'synthetic: {n_pt} seeded unit points, the history simulated on the GPU in float64',
+        config=dict(workload=f'mosaic_strip: {P} pulses x {K} samples, X band 600 MHz, 5 km, 30 deg, 0.25 m pulse '
+                             f'spacing -> {nx} x {ny} px at 0.25 m in 256 x 256 patches (crop 16), beam footprint '
+                             f'{lap:.0f} m, Hann azimuth window',
+                    patches=len(info), backprojections=bp,
+                    plans=sorted({(i['T'], i['sub'], i['levels']) for i in info}),
+                    pulses_per_patch=[int(i['pulses'][1] - i['pulses'][0]) for i in info][:4]),
+        err_db=dict(no_window=10 * np.log10(num / den),
+                    reference='float64 exact backprojection of each patch\'s pulses, 64x, 200 random pixels a patch, '
+                              'no gain fitted'),
+        cpu_baseline=None, cpu_baseline_note='the reference\'s mosaic runs its CPU former per patch from its own '
+                                             'package, which the GPU box does not hold',
+        gpu_launches=None, clocks=clocks)
+    print(json.dumps(line), flush=True)
+
+
 def run_learned(args):
     """--workload stack_products: the stack's products once its images exist (run_stack_products): registration, the
 incoherent average with its looks and coherence maps of 8 images on the 8,192 x 8,192 grid, against the oracle's
 NumPy restatement of the reference's functions on crops.
+
+--workload mosaic_strip: a patch mosaic of a strip (run_mosaic): per-patch re-referenced, gated histories and
+formers with a beam and an azimuth window, error against float64 per patch.
 
 --workload learned_4k: the learned decimation taps against the reference's Kaiser-sinc decimators on the
     4,096-pulse x 4,096-sample spotlight (the 512-pulse spotlight's geometry: 9.6 GHz, 300 MHz, 600 km, 45 deg,
