@@ -495,9 +495,11 @@ def test_image_tensor_cores_repeatable_bitwise(golden, monkeypatch, precision, f
 
 def test_image_tuned_levels_match_default(golden):
     """ImageFormer(tune_levels=True) times the tensor-core levels' launch options per level shape when it is built
-    and plans with the fastest: every tuned level records its choice, and the image is the default's to within 1e-4
-    (the options move only the seeding of the output ramp's recurrence, and with it a float16 rounding here and
-    there)."""
+    and plans with the fastest: every tuned level records its choice, and the image is the default's to within 3e-4
+    relative (-70 dB; the chosen form itself is about -64 dB from float64): the options move the seeding of the
+    output ramp's recurrence, and with it a float16 rounding here and there, and the pulse FIR's kernel (on the tensor
+    cores its operands are split into float16 halves) rounds differently from the CUDA-core one (1.0e-4 measured with
+    the tensor-core FIR on all three levels)."""
     from fastsar_b200 import ImageFormer, sim, tune
     g = golden('image_spot512')
     w = sim.workload('spotlight_512')
@@ -510,7 +512,7 @@ def test_image_tuned_levels_match_default(golden):
     a = f(g['S'])
     b = ImageFormer(*args, precision='float16')(g['S'])
     print(f'tuned against default: {_rel(a, b):.1e}')
-    assert _rel(a, b) < 1e-4, _rel(a, b)
+    assert _rel(a, b) < 3e-4, _rel(a, b)
     # a second former of the same shapes takes the options from the cache
     n = len(tune._LEVEL_CACHE)
     ImageFormer(*args, precision='float16', tune_levels=True).release()
