@@ -327,6 +327,13 @@ def mosaic_scene(seed=20261206):
     return col, fx, beam
 
 
+def mosaic_pulses(center):
+    """The mosaic fixtures' pulse span as a function of a patch centre: 150 pulses about the track point abeam of it
+    (the collection's 284 pulses are 0.55 m apart along y)."""
+    mid = int(round(142 + float(center[1]) / 0.55))
+    return max(0, mid - 75), min(284, mid + 75)
+
+
 def mosaic(fastsar):
     """mosaic.npz: the reference's patch mosaic (fastsar/patches.py form_mosaic with backend='cpu') on mosaic_scene,
     its patch histories (patch_history with and without shared range profiles) and its host helpers."""
@@ -343,11 +350,18 @@ def mosaic(fastsar):
         c=dict(nx=64, ny=64, patch=(64, 64), crop=0),
         d=dict(nx=96, ny=128, patch=(48, 64), crop=4, beam=beam, umax=1.0, T=16, levels=2),
     )
+    # dropped pulses (filled by zero pulses at their positions), and pulses chosen by a function of the patch centre
+    keep = np.setdiff1d(np.arange(len(ant)), [100, 101, 102, 170])
+    fx_gap = dict(fx, S=fx['S'][keep], ref=fx['ref'][keep])
+    rec['gap_keep'] = keep
+    cases['e'] = dict(nx=128, ny=128, patch=(64, 64), crop=8, fx=fx_gap, ant=ant[keep])
+    cases['f'] = dict(nx=128, ny=128, patch=(64, 64), crop=8, pulses=mosaic_pulses)
     for tag, kw in cases.items():
         info = []
         kw = dict(kw)
         nx, ny = kw.pop('nx'), kw.pop('ny')
-        img = patches.form_mosaic(fx, ant, origin, nx, ny, 0.5, 0.5, e1, e2, backend='cpu', info=info, **kw)
+        fxc, antc = kw.pop('fx', fx), kw.pop('ant', ant)
+        img = patches.form_mosaic(fxc, antc, origin, nx, ny, 0.5, 0.5, e1, e2, backend='cpu', info=info, **kw)
         rec[f'img_{tag}'] = img
         rec[f'info_{tag}'] = np.array([[i['pulses'][0], i['pulses'][1], i['K'], i['T'], i['sub'][0], i['sub'][1],
                                         i['levels'], i['df']] for i in info], np.float64)

@@ -49,7 +49,15 @@ CASES = dict(
     b=dict(nx=128, ny=128, patch=(64, 64), crop=8, beam=True, umax=1.0, awin='hann'),
     c=dict(nx=64, ny=64, patch=(64, 64), crop=0),
     d=dict(nx=96, ny=128, patch=(48, 64), crop=4, beam=True, umax=1.0, T=16, levels=2),
+    e=dict(nx=128, ny=128, patch=(64, 64), crop=8, gap=True),
+    f=dict(nx=128, ny=128, patch=(64, 64), crop=8, pulses=True),
 )
+
+
+def _pulses(center):
+    # 150 pulses about the track point abeam of the patch centre (the fixtures' 284 pulses are 0.55 m apart along y)
+    mid = int(round(142 + float(center[1]) / 0.55))
+    return max(0, mid - 75), min(284, mid + 75)
 
 
 @pytest.mark.parametrize('tag', sorted(CASES))
@@ -59,8 +67,14 @@ def test_mosaic_matches_reference(g, tag):
     nx, ny = kw.pop('nx'), kw.pop('ny')
     if kw.pop('beam', False):
         kw['beam'] = _beam(g['ant'])
+    if kw.pop('pulses', False):
+        kw['pulses'] = _pulses
+    fx, ant = _fx(g), g['ant']
+    if kw.pop('gap', False):        # pulses dropped from the collection: the mosaic fills them with zero pulses
+        keep = g['gap_keep']
+        fx, ant = dict(fx, S=fx['S'][keep], ref=fx['ref'][keep]), ant[keep]
     info = []
-    img = mo.form_mosaic(_fx(g), g['ant'], g['origin'], nx, ny, 0.5, 0.5, E1, E2, info=info, **kw)
+    img = mo.form_mosaic(fx, ant, g['origin'], nx, ny, 0.5, 0.5, E1, E2, info=info, **kw)
     ref = g[f'img_{tag}']
     assert img.shape == ref.shape and img.dtype == np.complex64
     err = _rel_db(img, ref)
