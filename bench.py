@@ -814,12 +814,12 @@ def run_stack_products(args):
         cpu = dict(value=nimg * c * c / dt / 1e6, unit='Mpx/s', cores=os.cpu_count(), kind='port',
                    sample=f'the same products of 2048 x 2048 crops of the 8 images (oracle/stack_oracle.py, NumPy and '
                           f'scipy.fft on all cores): {dt:.1f} s')
-    # this package's kernels per step: a box mean per detected image; per registration a cross-spectrum of the whole
-    # images and one of the batch of 16 tiles; per translation a ramp and a crop; per image added to the average its
+    # this package's kernels per step: a box mean per detected image; per registration the two images' windowing and
+    # a cross-spectrum, for the whole images and for the batch of 16 tiles; per translation a ramp and a crop; per image added to the average its
     # intensity, the sums, its tile statistics, the running average and that average's statistics; the average, its
     # statistics, its 9 x 9 means and theirs for the looks; a coherence map per pair (the transforms are cuFFT's, the
     # sub-pixel products cuBLAS's)
-    launches = nimg + (nimg - 1) * 2 + (nimg - 1) * 2 + nimg * 5 + 4 + (nimg - 1)
+    launches = nimg + (nimg - 1) * 6 + (nimg - 1) * 2 + nimg * 5 + 4 + (nimg - 1)
     line = dict(
         metric='stack products (register 7, translate 7, mean of 8 with looks, 7 coherence maps) of an 8-image '
                '8192 x 8192 stack',

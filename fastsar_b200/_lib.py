@@ -28,7 +28,7 @@ EXPORTS = ('ffbp_last_error', 'ffbp_abi_version', 'ffbp_plan_create', 'ffbp_plan
            'ffbp_gate_fold', 'ffbp_gate_taper', 'ffbp_batch_create', 'ffbp_batch_form', 'ffbp_batch_destroy', 'ffbp_mlp_taps', 'ffbp_mlp_grad', 'ffbp_mlp_train_step',
            'ffbp_plan_check', 'ffbp_plan_test_wait', 'ffbp_level_fused', 'ffbp_level_tc_ex', 'ffbp_plan_test_transfer',
            'ffbp_box_mean', 'ffbp_coherence', 'ffbp_multilook', 'ffbp_mean_add', 'ffbp_mean_image', 'ffbp_tile_stats',
-           'ffbp_cross_spectrum', 'ffbp_ramp_multiply', 'ffbp_shift_crop', 'ffbp_mosaic_pad', 'ffbp_mosaic_gather',
+           'ffbp_cross_spectrum', 'ffbp_ramp_multiply', 'ffbp_shift_crop', 'ffbp_window', 'ffbp_mosaic_pad', 'ffbp_mosaic_gather',
            'ffbp_mosaic_gate')
 
 _c_int, _c_double, _vp = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
@@ -135,6 +135,7 @@ def load():
     L.ffbp_tile_stats.argtypes = [_vp, _c_int, _c_int, _c_int, _f32, _vp, _vp, _vp]
     L.ffbp_cross_spectrum.argtypes = [_vp, _vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp]
     L.ffbp_ramp_multiply.argtypes = [_vp, _c_int, _c_int, _vp, _vp, _vp]
+    L.ffbp_window.argtypes = [_vp, _c_int, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp]
     L.ffbp_shift_crop.argtypes = [_vp, _c_int, _vp, _c_int, _c_int, _c_int, _c_int, _c_int, _vp, _vp]
     L.ffbp_mosaic_pad.argtypes = [_vp, _long, _c_int, _c_int, _c_int, _c_int, _vp, _c_double, _c_double, _vp, _vp]
     L.ffbp_mosaic_gather.argtypes = [_vp, _long, _c_int, _c_int, _c_int, _vp, _vp, _vp]

@@ -1137,6 +1137,16 @@ int ffbp_cross_spectrum(const void *d_A, const void *d_B, int batch, int m1, int
                 "ffbp_cross_spectrum");
 }
 
+int ffbp_window(const float *d_x, int batch, int n1, int n2, const float *d_mean, const float *d_w1, const float *d_w2,
+                float *d_out, void *stream)
+{
+    if (int r = image_args("ffbp_window", d_x, n1, n2)) return r;
+    if (!d_mean || !d_w1 || !d_w2 || !d_out) return fail(FFBP_E_ARG, "ffbp_window: null buffer");
+    if (batch < 1 || batch > 65535) return fail(FFBP_E_ARG, "ffbp_window: batch of %d", batch);
+    return done(ffbp::launch_window(d_x, batch, n1, n2, d_mean, d_w1, d_w2, d_out, static_cast<cudaStream_t>(stream)),
+                "ffbp_window");
+}
+
 int ffbp_ramp_multiply(void *d_F, int m1, int m2, const void *d_r1, const void *d_r2, void *stream)
 {
     if (int r = image_args("ffbp_ramp_multiply", d_F, m1, m2)) return r;

@@ -144,6 +144,8 @@ cudaError_t launch_tile_stats(const float *x, int n1, int n2, int T, float gain,
 cudaError_t launch_cross_spectrum(const float2 *A, const float2 *B, int batch, int m1, int m2h, int nyquist,
                                   const float *e1, const float *e2, float2 *X, double *energy, cudaStream_t s);
 cudaError_t launch_ramp_multiply(float2 *F, int m1, int m2, const float2 *r1, const float2 *r2, cudaStream_t s);
+cudaError_t launch_window(const float *x, int batch, int n1, int n2, const float *mean, const float *w1, const float *w2,
+                          float *out, cudaStream_t s);
 cudaError_t launch_shift_crop(const float2 *shifted, int ld, const void *src, int src_complex, int n1, int n2, int w0,
                               int w1, void *out, cudaStream_t s);
 

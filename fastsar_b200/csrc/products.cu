@@ -263,6 +263,21 @@ __global__ void __launch_bounds__(256) cross_spectrum_kernel(const float2 *__res
     }
 }
 
+// out[b, i, j] = ((x[b, i, j] - mean[b]) w1[i]) w2[j], each step rounded to float32 as the reference's separate
+// array operations round them (fastsar/stack.py:567-568): the correlation's mean removal and Hann windows, one pass
+// over a batch of images [nb, n1, n2] (blockIdx.y: the image).
+__global__ void window_kernel(const float *__restrict__ x, int n1, int n2, const float *__restrict__ mean,
+                              const float *__restrict__ w1, const float *__restrict__ w2, float *__restrict__ out)
+{
+    const long n = (long)n1 * n2;
+    const size_t img = (size_t)blockIdx.y * n;
+    const float m = mean[blockIdx.y];
+    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(k / n2), j = (int)(k - (long)i * n2);
+        out[img + k] = __fmul_rn(__fmul_rn(__fsub_rn(x[img + k], m), w1[i]), w2[j]);
+    }
+}
+
 // F[i, j] *= r1[i] r2[j] (complex64): a separable phase ramp on a spectrum [m1, m2]
 __global__ void ramp_multiply_kernel(float2 *__restrict__ F, int m1, int m2, const float2 *__restrict__ r1,
                                      const float2 *__restrict__ r2)
@@ -371,6 +386,14 @@ cudaError_t launch_cross_spectrum(const float2 *A, const float2 *B, int batch, i
     if (e != cudaSuccess) return e;
     const int gx = (grid_for((long)m1 * m2h, 256) + batch - 1) / batch;
     cross_spectrum_kernel<<<dim3(gx < 1 ? 1 : gx, batch), 256, 0, s>>>(A, B, m1, m2h, nyquist, e1, e2, X, energy);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_window(const float *x, int batch, int n1, int n2, const float *mean, const float *w1, const float *w2,
+                          float *out, cudaStream_t s)
+{
+    const int gx = (grid_for((long)n1 * n2, 256) + batch - 1) / batch;
+    window_kernel<<<dim3(gx < 1 ? 1 : gx, batch), 256, 0, s>>>(x, n1, n2, mean, w1, w2, out);
     return cudaGetLastError();
 }
 

@@ -95,9 +95,16 @@ def peaks(a, b, max_shift, around=(0, 0), narrow=None, up=16, highpass=32.0):
     call. -> a list of (d, z, rho, clear), one per pair."""
     nb, n1, n2 = a.shape
     dev = a.device
-    w1, w2 = _hann(n1, dev)[:, None], _hann(n2, dev)[None, :]
-    aw = (a - a.mean(dim=(1, 2), keepdim=True)) * w1 * w2
-    bw = (b - b.mean(dim=(1, 2), keepdim=True)) * w1 * w2
+    h1, h2 = _hann(n1, dev), _hann(n2, dev)
+    L = _lib.load()
+
+    def windowed(x):      # ((x - its mean) w1) w2 per image, one pass (ffbp_window)
+        x = x.contiguous()
+        m = x.mean(dim=(1, 2)).contiguous()
+        out = torch.empty_like(x)
+        _lib.check(L.ffbp_window(ptr(x), nb, n1, n2, ptr(m), ptr(h1), ptr(h2), ptr(out), stream_ptr()), 'ffbp_window')
+        return out
+    aw, bw = windowed(a), windowed(b)
     fs = (sfft.next_fast_len(n1, real=True), sfft.next_fast_len(n2, real=True))
     A = torch.fft.rfft2(aw, s=fs).contiguous()
     B = torch.fft.rfft2(bw, s=fs).contiguous()

@@ -409,6 +409,12 @@ int ffbp_tile_stats(const float *d_x, int n1, int n2, int T, float gain, float *
 int ffbp_cross_spectrum(const void *d_A, const void *d_B, int batch, int m1, int m2h, int nyquist, const float *d_e1,
                         const float *d_e2, void *d_X, double *d_energy, void *stream);
 
+/* The correlation's windowing of a batch of float32 images [batch, n1, n2] (fastsar/stack.py:565-568): d_out =
+ * ((x - mean[b]) w1[i]) w2[j], each operation rounded to float32 as the reference's array operations are; d_mean
+ * [batch] (each image's mean), d_w1 [n1], d_w2 [n2] float32.                                                       */
+int ffbp_window(const float *d_x, int batch, int n1, int n2, const float *d_mean, const float *d_w1, const float *d_w2,
+                float *d_out, void *stream);
+
 /* d_F [m1, m2] complex64 *= r1[i] r2[j]: a separable phase ramp on a spectrum (fastsar/stack.py:700-706).           */
 int ffbp_ramp_multiply(void *d_F, int m1, int m2, const void *d_r1, const void *d_r2, void *stream);
 

@@ -60,3 +60,5 @@ def test_stack_product_argument_errors_without_a_gpu():
     assert L.ffbp_cross_spectrum(p, p, 1, 4, 3, 1, p, None, p, p, None) == E
     assert L.ffbp_cross_spectrum(p, p, 0, 4, 3, 1, None, None, p, p, None) == E
     assert L.ffbp_shift_crop(p, 2, p, 1, 4, 4, 0, 0, p, None) == E and 'leading' in _lib.last_error()
+    assert L.ffbp_window(p, 0, 4, 4, p, p, p, p, None) == E
+    assert L.ffbp_window(p, 1, 4, 4, None, p, p, p, None) == E
