@@ -261,9 +261,10 @@ def tune_levels(plan, reps=3):
 
 
 def main():
-    """python -m fastsar_b200.tune --workload spotlight_12k [--out path] [--reps 5]: time the launch options of the
-    chosen form's tensor-core levels (precision float16, learned taps, pmax 0.5) for a named workload's plan and
-    write them, with whatever the cache already held, to `out` (default: the packaged file)."""
+    """python -m fastsar_b200.tune --workload spotlight_12k [--pmax 0.52] [--out path] [--reps 5]: time the launch
+    options of the chosen form's tensor-core levels (precision float16, learned taps, 80 dB fallback filters, the
+    given pmax) for a named workload's plan and write them, with whatever the cache already held, to `out` (default:
+    the packaged file)."""
     import argparse
     from . import sim, learned
     ap = argparse.ArgumentParser()
@@ -271,6 +272,7 @@ def main():
     ap.add_argument('--out', default=PACKAGED_CACHE)
     ap.add_argument('--reps', type=int, default=5)
     ap.add_argument('--max-parents', type=int, default=4096)
+    ap.add_argument('--pmax', type=float, default=0.52)
     a = ap.parse_args()
     _load_cache()
     taps = learned.LearnedTaps.load()
@@ -279,7 +281,7 @@ def main():
         col = w['col']
         T, _ = _plan.choose_T(col.ant, col.fmin + col.K * col.df, w['nx'], w['ny'], w['spx'], w['spy'], w['e1'],
                               w['e2'], -40.0)
-        pl = _plan.make_plan(col, w['nx'], w['ny'], w['spx'], w['spy'], T=T, nlev=3, pmax=0.5, atten=80.0,
+        pl = _plan.make_plan(col, w['nx'], w['ny'], w['spx'], w['spy'], T=T, nlev=3, pmax=a.pmax, atten=80.0,
                              e1=w['e1'], e2=w['e2'], taps=taps)
         Np = 1
         for i, lv in enumerate(pl['levels']):
