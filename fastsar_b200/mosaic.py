@@ -353,7 +353,14 @@ def form_mosaic(fx, ant, origin, nx, ny, spx, spy, e1=(1.0, 0.0, 0.0), e2=(0.0, 
     fx['_dev'] = _device_history(fx)
     out = torch.zeros((nx, ny), dtype=torch.complex64, device=fx['_dev'].device)
     npatch = -(-nx // mx) * -(-ny // my)
-    prof = range_profiles(fx, guard) if npatch > 1 else None
+    # the shared range profiles [P, K2] where they take under 40 % of the free device memory (as the reference keeps
+    # them on the device); else each patch transforms its own pulses (the direct form of patch_history)
+    prof = None
+    if npatch > 1:
+        K2 = _padding(fx, guard)[3]
+        free, _ = torch.cuda.mem_get_info(fx['_dev'].device)
+        if 2 * len(ant) * K2 * 8 < 0.4 * free:          # the padded history and its transform
+            prof = range_profiles(fx, guard)
     for i0 in range(0, nx, mx):
         for j0 in range(0, ny, my):
             c = o + (i0 - crop + px / 2) * spx * e1v + (j0 - crop + py / 2) * spy * e2v
