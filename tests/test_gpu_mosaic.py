@@ -94,3 +94,18 @@ def test_mosaic_arguments(g):
         mo.form_mosaic(dict(S=g['S']), g['ant'], g['origin'], 64, 64, 0.5, 0.5, E1, E2)
     with pytest.raises(ValueError, match='patch'):
         mo.form_mosaic(fx, g['ant'], g['origin'], 64, 64, 0.5, 0.5, E1, E2, patch=(0, 64))
+
+
+def test_mosaic_without_shared_profiles(g, monkeypatch):
+    """Where the shared range profiles would not fit the device, each patch takes the direct form: the same image
+    as with them (the gate's edge samples aside), and the reference's within the same bar."""
+    import torch
+    from fastsar_b200 import mosaic as mo
+    fx = _fx(g)
+    with_prof = mo.form_mosaic(fx, g['ant'], g['origin'], 128, 128, 0.5, 0.5, E1, E2, patch=(64, 64), crop=8)
+    monkeypatch.setattr(torch.cuda, 'mem_get_info', lambda *a, **k: (1 << 20, 1 << 30))
+    direct = mo.form_mosaic(fx, g['ant'], g['origin'], 128, 128, 0.5, 0.5, E1, E2, patch=(64, 64), crop=8)
+    print(f'mosaic without shared profiles: {_rel_db(direct, with_prof.astype(np.complex128)):.1f} dB from the shared '
+          f'form, {_rel_db(direct, g["img_a"]):.1f} dB from the reference')
+    assert _rel_db(direct, with_prof.astype(np.complex128)) < -70
+    assert _rel_db(direct, g['img_a']) < -75
